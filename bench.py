@@ -1,0 +1,322 @@
+"""Benchmark: Boussinesq steps/s on one B200 (or N independent replicas).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--config etd_192x128x256] [--precision fp64|split]
+
+Workload: the ETD2AB-CN timestep at NR x NTH x NX = 192 x 128 x 256 (Re 5000,
+hyperviscosity P=2 nu_p=kappa_p=1e-10, Omega 1, N 2, dt 5e-4) from a Gaussian
+q-vortex plus a seeded spectral perturbation (mlegs_b200/inputs.py), one CUDA
+graph replay per step.  Per-GPU work is fixed (replicas only, "weak").
+Every step touches several GB (100 MB physical fields), far above the 126 MB
+L2, so no explicit L2 flush is needed between steps.
+
+--impl reference times the reference's path as restated on the CPU (the
+numpy/scipy FP64 oracle under oracle/, all host cores): the reference itself
+is Fortran 90 + MPI + FFTW + MKL and cannot be built in this image.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Boussinesq steps/s 192x128x256: mixed-prec vs FP64 GPU at same error bound"
+UNIT = "steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="etd_192x128x256")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl"
+        try:
+            import torch
+            if not torch.cuda.is_available():
+                backend = "gloo"
+            else:
+                torch.cuda.set_device(local)
+        except Exception:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampler running while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.5)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+        except Exception:
+            return None
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def traffic_table():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return {}
+
+
+def oracle_steps(cfg, nsteps, warm=0):
+    """Time steady-state oracle steps (zeroed AB/ETD history: same arithmetic)."""
+    import numpy as np
+
+    from mlegs_b200.inputs import perturbation_coefficients
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import Grid
+    g = Grid(cfg.nr, cfg.nth, cfg.nx, cfg.nrchop, cfg.ntchop, cfg.nxchop, cfg.ell, cfg.zlen)
+    ph = BQ.Physics(dt=cfg.dt, omega=cfg.omega, bv0=cfg.bv0, kappa=cfg.kappa, kappap=cfg.kappap,
+                    adams=cfg.adams, visc_sw=cfg.visc_sw, nu=cfg.nu, nup=cfg.nup, p=cfg.p)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, ph, P, C, B)
+    z = lambda: g.alloc(1)  # noqa: E731
+    if cfg.adams:
+        s.n_psi, s.n_chi, s.n_b = z(), z(), z()
+    else:
+        s.etd_e, s.etd_nl = BQ.calc_boussi_etd_op(cfg.bv0, cfg.omega, cfg.dt)
+        s.n_b, s.r_n_r, s.r_n_p, s.n_z, s.r_pi_r, s.r_pi_p, s.pi_z = (z() for _ in range(7))
+    for _ in range(warm):
+        s.step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        s.step()
+    dt = time.perf_counter() - t0
+    assert np.isfinite(s.psi.E).all()
+    return nsteps / dt
+
+
+def run_reference(args, cfg, ws, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count()
+    v = oracle_steps(cfg, args.steps, warm=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded q-vortex + spectral perturbation)",
+            "config": {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx],
+                       "chops": [cfg.nrchop, cfg.ntchop, cfg.nxchop], "scheme": "ETD2AB-CN" if not cfg.adams else "AB2-CN",
+                       "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d steady steps after %d warm-up, FP64 numpy/scipy restatement of the "
+                                       "reference path (reference Fortran not buildable here)" % (args.steps, args.warmup)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, ws, rank, local):
+    import numpy as np
+    import torch
+
+    import mlegs_b200 as M
+    prec = M.PREC_FP64 if args.precision == "fp64" else M.PREC_SPLIT
+    ctx = M.Context(cfg, precision=prec, device=local)
+    psi, chi, b = M.initial_state(ctx)
+    ctx.initialize(psi, chi, b)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+    ctx.step(max(args.warmup, 1), graph=True)  # first call captures the graph
+    ctx.sync()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    smi_index = int(vis.split(",")[local]) if vis else local
+    barrier(ws)
+    ctx.reset_launches()
+    with Clocks(smi_index) as clk:
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step(args.steps, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+    launches = ctx.launches()
+    ms_total = e0.elapsed_time(e1)
+    barrier(ws)
+    ms_total = max_over_ranks(ws, ms_total)
+    ms_step = ms_total / args.steps
+    value = ws * args.steps / (ms_total / 1000.0)
+    ctx.check_finite()
+
+    # ---- e2e: per step, upload state from pinned host, one graph step, download
+    shape = ctx.shape(M.FFF)
+    nbytes = int(np.prod(shape)) * 16
+    hosts = []
+    for f in (psi, chi, b):
+        buf = torch.empty(int(np.prod(shape)), dtype=torch.complex128, pin_memory=True).numpy()
+        arr = np.ndarray(shape, dtype=np.complex128, buffer=buf, order="F")
+        hosts.append(arr)
+    lns = [0.0, 0.0, 0.0]
+    for i, f in enumerate((psi, chi, b)):
+        _, lns[i] = f.download(out=hosts[i])
+    barrier(ws)
+    ctx.sync()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e2.record(stream)
+    for _ in range(args.steps):
+        for i, f in enumerate((psi, chi, b)):
+            f.upload(hosts[i], lns[i], M.FFF)
+        ctx.step(1, graph=True)
+        for i, f in enumerate((psi, chi, b)):
+            _, lns[i] = f.download(out=hosts[i])
+    e3.record(stream)
+    e3.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(e2.elapsed_time(e3), wall * 1000.0)
+    barrier(ws)
+    e2e_ms = max_over_ranks(ws, e2e_ms)
+    e2e_value = ws * args.steps / (e2e_ms / 1000.0)
+
+    # ---- roofline of the dominant kernel (live CUDA-event timing on the library stream)
+    pk, pk_kind = peaks()
+    kernels = {}
+    for name in ctx.KERNELS:
+        ms, by = ctx.kernel_time(name, reps=20)
+        kernels[name] = {"ms": ms, "bytes": by, "gbs": by / (ms * 1e-3) / 1e9}
+    dom = DOMINANT
+    tr = traffic_table().get(cfg.name, {}).get(dom)
+    ach = kernels[dom]["gbs"]
+    roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": ach / pk["hbm_gbs"], "traffic": tr, "peak_source": pk_kind,
+            "algorithmic_bytes_per_launch": kernels[dom]["bytes"], "ms_per_launch": kernels[dom]["ms"]}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v = oracle_steps(cfg, args.cpu_steps)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": "%d steady-state steps of the FP64 numpy/scipy oracle at %s (zeroed AB/ETD "
+                         "history, same arithmetic as a steady step)" % (args.cpu_steps, cfg.name)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16-split/f32/f64",
+                "data": "synthetic (seeded q-vortex + spectral perturbation)",
+                "config": {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx],
+                           "chops": [cfg.nrchop, cfg.ntchop, cfg.nxchop],
+                           "scheme": "ETD2AB-CN" if not cfg.adams else "AB2-CN", "dt": cfg.dt,
+                           "precision": args.precision, "graph": True,
+                           "parallelism": "replicas x%d" % ws,
+                           "l2": "inputs larger than L2 (several GB touched per step)"},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * nbytes,
+                        "d2h_bytes_per_step": 3 * nbytes},
+                "gpu_launches": int(launches),
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+DOMINANT = "horfft_b"
+
+
+def main():
+    args = parse()
+    from mlegs_b200.inputs import CONFIGS
+    cfg = CONFIGS[args.config]
+    ws, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, cfg, ws, rank)
+        else:
+            run_ours(args, cfg, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * mlegs_b200.h -- C ABI of the B200-native MLegS transform-and-step library.
+ *
+ * Each entry point replaces one Fortran module procedure of the reference
+ * (paths relative to the MLegS project root).  Fields live on the device,
+ * owned by the context; hosts move data with upload/download in the
+ * reference's own array layout (Fortran column-major COMPLEX(P8) E(:,:,:)
+ * with the per-space shapes of SALLOC, mod_fft.f90:603-670):
+ *   FFF  E(NRCHOPDIM, NTCHOPDIM, NXCHOPDIM)
+ *   PFF  E(NDIMR,     NTCHOPDIM, NXCHOPDIM)
+ *   PFP  E(NDIMR,     NDIMTH,    NX)
+ *   PPP  E(NDIMR,     NDIMTH,    NX)
+ * with NDIMR = NR+3, NDIMTH = NTH+1, NRCHOPDIM = min(NRCHOP+6, NR),
+ * NTCHOPDIM = min(NTCHOP, NTH), NXCHOPDIM = 2*NXCHOP-1 (mod_fft.f90:225-235).
+ *
+ * Truncation: the reference's global CHOPSET(+p)/CHOPSET(-p) state
+ * (mod_scalar3.f90:165-211) becomes the explicit `pad` argument: every
+ * operator uses NRCHOPS(m) = max(NRCHOP + pad - m, 0).
+ *
+ * Errors: every function returns 0 on success, otherwise one of the
+ * reference's ERR_FLAGS codes (mod_scalar3.f90:88-106) or an MLEGS_ERR_*
+ * code below; nothing aborts the process.  Calls on one context are
+ * stream-ordered on that context's CUDA stream and must not be issued
+ * concurrently from several host threads; distinct contexts are independent.
+ */
+#ifndef MLEGS_B200_H
+#define MLEGS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ERR_FLAGS values of the reference (mod_scalar3.f90:88-106). */
+#define MLEGS_OK                 0
+#define MLEGS_ERR_SCALAR3        1
+#define MLEGS_ERR_SCALAR3_ISNAN 10
+#define MLEGS_ERR_DEALIASING    11
+#define MLEGS_ERR_DIVERGENCE    12
+#define MLEGS_ERR_LOGTERM       13
+#define MLEGS_ERR_TRANSFORM      2
+#define MLEGS_ERR_LEGOPERATOR    3
+#define MLEGS_ERR_CALCULATION   31
+#define MLEGS_ERR_DIMMISMATCH   32
+#define MLEGS_ERR_SOLVER         5
+/* Codes with no counterpart in the reference. */
+#define MLEGS_ERR_CUDA         100
+#define MLEGS_ERR_ARG          101
+#define MLEGS_ERR_NOMEM        102
+#define MLEGS_ERR_NONFINITE    103
+#define MLEGS_ERR_STATE        104
+
+/* Space tags, mod_scalar3.f90:82-85. */
+#define MLEGS_PPP 0
+#define MLEGS_FFF 1
+#define MLEGS_PFP 2
+#define MLEGS_PFF 3
+
+/* Arithmetic of the mapped-Legendre GEMMs (RTRAN, PROJECT). */
+#define MLEGS_PREC_FP64   0   /* FP64 FMA                                          */
+#define MLEGS_PREC_SPLIT  1   /* split-BF16 (Ozaki) slices on tcgen05, FP64 combine */
+
+/* Run parameters: the read.input keys the hot path reads (mod_init.f90:401-705,
+ * with VISCOSITY NU/NUP >= 1 already inverted as READIN0 does, 539-551). */
+typedef struct mlegs_params {
+    int32_t nr, nth, nx;              /* DIMENSION                                 */
+    int32_t nrchop, ntchop, nxchop;   /* CHOPS                                     */
+    double  ell, zlen;                /* ELL, ZLEN (MINC = 1, MKLINK = 0)          */
+    double  dt;                       /* DT                                        */
+    int32_t adams;                    /* BOUSSINESQ ABSW: 1 AB2-CN, 0 ETD2AB-CN    */
+    double  omega, bv0, kappa, kappap;/* BOUSSINESQ OMEGA, BV0, KAPPA, KAPPAP      */
+    int32_t visc_sw, visc_p;          /* VISCOSITY SW, P                           */
+    double  nu, nup;                  /* VISCOSITY NU, NUP                         */
+    int32_t precision;                /* MLEGS_PREC_*                              */
+    int32_t split_slices;             /* slices per operand for MLEGS_PREC_SPLIT   */
+    int32_t device;                   /* CUDA device ordinal                        */
+} mlegs_params;
+
+typedef struct mlegs_ctx mlegs_ctx;
+typedef struct mlegs_field mlegs_field;
+
+/* Context: LEGINIT + SETUP_GRID (mod_fft.f90:165-367) for one grid; builds the
+ * Gauss-Legendre nodes and the orthonormal P^m_n table in FP64 on the device. */
+int mlegs_create(const mlegs_params* p, mlegs_ctx** out);
+int mlegs_destroy(mlegs_ctx* ctx);
+const char* mlegs_last_error(const mlegs_ctx* ctx);
+int mlegs_sync(mlegs_ctx* ctx);
+/* Sizes (NDIMR, NDIMTH, NX, NRCHOPDIM, NTCHOPDIM, NXCHOPDIM, NRH, NR, NTH). */
+int mlegs_dims(const mlegs_ctx* ctx, int32_t out[9]);
+
+/* Fields: TYPE(SCALAR) (mod_scalar3.f90:41-47) with device storage;
+ * SALLOC/SFREE (mod_fft.f90:603-703). */
+int mlegs_field_alloc(mlegs_ctx* ctx, int space, mlegs_field** out);
+int mlegs_field_free(mlegs_ctx* ctx, mlegs_field* f);
+int mlegs_field_space(const mlegs_field* f);
+/* host: interleaved (re, im) doubles in the reference layout of `space`. */
+int mlegs_field_upload(mlegs_ctx* ctx, mlegs_field* f, int space, const double* host, double ln);
+int mlegs_field_download(mlegs_ctx* ctx, const mlegs_field* f, double* host, double* ln);
+/* Collocation grid built by mlegs_create: x (Gauss-Legendre nodes, ascending),
+ * w (weights), r = ELL sqrt((1+x)/(1-x)); arrays of NR doubles (TFM%X/W/R,
+ * mod_scalar3.f90:53-56).  Any pointer may be NULL. */
+int mlegs_grid(const mlegs_ctx* ctx, double* x, double* w, double* r);
+/* y = c*y + a*x1 + b*x2 on FFF fields, applied to E and LN alike (x2 may be
+ * NULL); the array arithmetic the steppers write inline (mod_march.f90:639-643). */
+int mlegs_field_axpby(mlegs_ctx* ctx, mlegs_field* y, double a, const mlegs_field* x1, double b,
+                      const mlegs_field* x2, double c);
+int mlegs_field_set_ln(mlegs_ctx* ctx, mlegs_field* f, double ln);
+/* COPY0 (mod_fft.f90:705-769): dst = src (with CHOPDO at pad for FFF). */
+int mlegs_field_copy(mlegs_ctx* ctx, mlegs_field* dst, const mlegs_field* src, int pad);
+/* CHOPDO (mod_scalar3.f90:213-257). */
+int mlegs_chopdo(mlegs_ctx* ctx, mlegs_field* f, int pad);
+
+/* Space transitions, mod_fft.f90:771-1398. is = +1: towards physical, -1: towards spectral. */
+int mlegs_rtran(mlegs_ctx* ctx, mlegs_field* f, int is, int pad);   /* RTRAN  1150 */
+int mlegs_horfft(mlegs_ctx* ctx, mlegs_field* f, int is);           /* HORFFT  771 */
+int mlegs_verfft(mlegs_ctx* ctx, mlegs_field* f, int is);           /* VERFFT  928 */
+int mlegs_plnfft(mlegs_ctx* ctx, mlegs_field* f, int is);           /* PLNFFT 1115 */
+int mlegs_toff(mlegs_ctx* ctx, mlegs_field* f, int pad);            /* TOFF   1342 */
+int mlegs_tofp(mlegs_ctx* ctx, mlegs_field* f, int pad);            /* TOFP   1371 */
+
+/* Spectral operators, mod_legops.f90 (b = op(a) unless noted). */
+int mlegs_delsqh(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad);   /* DELSQH   76 */
+int mlegs_idelsqh(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad);  /* IDELSQH 136 */
+int mlegs_mulxm(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad);    /* MULXM   371 */
+int mlegs_xxdx(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad);     /* XXDX    680 */
+int mlegs_del2(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad);     /* DEL2    751 */
+/* IDEL2 (823): has_ln = 0 means the LN argument is absent. */
+int mlegs_idel2(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int has_ln, double ln, int pad);
+int mlegs_idel2ln(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad);  /* IDEL2LN 1013 */
+int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad); /* IHELM 1204 */
+int mlegs_grad(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* rgr, mlegs_field* rgp,
+               mlegs_field* gz, int pad);                                            /* GRAD   1727 */
+int mlegs_pc2vel(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
+                 mlegs_field* rur, mlegs_field* rup, mlegs_field* uz, int pad);      /* PC2VEL 1789 */
+int mlegs_pc2vor(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
+                 mlegs_field* ror, mlegs_field* rop, mlegs_field* oz, int pad);      /* PC2VOR 1856 */
+/* PROJECT (2397): ln_mode 0 = LN absent, 1 = LN given (ln), 2 = PSI%LN passed
+ * by reference (the steppers' call form). rur/rup/uz are consumed. */
+int mlegs_project(mlegs_ctx* ctx, mlegs_field* rur, mlegs_field* rup, mlegs_field* uz,
+                  mlegs_field* psi, mlegs_field* chi, int ln_mode, double ln);
+
+/* Boussinesq right-hand side, mod_boussinesq.f90:317-410 (CALC_BOUSSI_FORCE). */
+int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
+                       const mlegs_field* b, mlegs_field* psin, mlegs_field* chin,
+                       mlegs_field* bn);
+
+/* Solver: SOLVER_T%INITIALIZE (mod_march.f90:171-240, Richardson start-up) and
+ * TIME_STEPPING's state update (243-307: STEP_BOUSSI_AB_CN 609 or
+ * STEP_BOUSSI_ETDAB_CN 811).  The state fields stay owned by the caller. */
+int mlegs_solver_init(mlegs_ctx* ctx, mlegs_field* psi, mlegs_field* chi, mlegs_field* b);
+int mlegs_step(mlegs_ctx* ctx, int nsteps);
+/* Capture one steady-state step as a CUDA graph and replay it nsteps times. */
+int mlegs_step_graph(mlegs_ctx* ctx, int nsteps);
+/* Simulation time and step counter (TIM%T, TIM%N). */
+int mlegs_time(const mlegs_ctx* ctx, double* t, int32_t* n);
+/* Non-finite check of the state (ANYNAN, mod_scalar3.f90:998-1045):
+ * returns MLEGS_ERR_NONFINITE if any state coefficient is NaN/Inf. */
+int mlegs_check_finite(mlegs_ctx* ctx);
+
+/* Kernel timing for profiling and roofline reports: launches one internal
+ * kernel `reps` times on scratch fields of this context, bracketed by CUDA
+ * events on the context's stream, and returns the mean device time per launch
+ * (ms) and the kernel's algorithmic HBM bytes per launch.  No counterpart in
+ * the reference.  kernel ids: MLEGS_K_* below. */
+#define MLEGS_K_RTRAN_B2P   0   /* RTRAN(+1)  FFF -> PFF               */
+#define MLEGS_K_RTRAN_P2B   1   /* RTRAN(-1)  PFF -> FFF               */
+#define MLEGS_K_VERFFT_B    2   /* VERFFT(+1) PFF -> PFP               */
+#define MLEGS_K_VERFFT_F    3   /* VERFFT(-1) PFP -> PFF               */
+#define MLEGS_K_HORFFT_B    4   /* HORFFT(+1) PFP -> PPP               */
+#define MLEGS_K_HORFFT_F    5   /* HORFFT(-1) PPP -> PFP               */
+#define MLEGS_K_POINTWISE   6   /* VPRODSUB+VDOTPSUB+linear terms, PPP */
+#define MLEGS_K_SOLVE       7   /* IDEL2LN banded solves               */
+int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
+
+/* Number of this library's kernel launches issued since the counter was reset. */
+int64_t mlegs_launch_count(const mlegs_ctx* ctx);
+void    mlegs_reset_launch_count(mlegs_ctx* ctx);
+/* CUDA stream of the context (cudaStream_t), for event timing by hosts. */
+void*   mlegs_stream(mlegs_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MLEGS_B200_H */

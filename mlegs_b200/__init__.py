@@ -1,0 +1,318 @@
+"""B200-native MLegS transform-and-step library: Python host binding.
+
+The compute path is the CUDA library ``libmlegs_b200.so`` (C ABI in
+include/mlegs_b200.h).  This module mirrors the reference's Fortran module
+interface for the hot path -- TYPE(SCALAR) fields with space tags and log
+terms, RTRAN/HORFFT/VERFFT/TOFF/TOFP, the mod_legops operators,
+CALC_BOUSSI_FORCE and the SOLVER_T stepping -- over ctypes.  Arrays cross
+the boundary in the reference's own layouts (Fortran index order (n|r, m|j,
+k|z), complex128).  There is no CPU fallback: if the library cannot be
+loaded, construction fails.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .inputs import CONFIGS, Config, buoyancy_perturbation, perturbation_coefficients  # noqa: F401
+
+PPP, FFF, PFP, PFF = 0, 1, 2, 3
+PREC_FP64, PREC_SPLIT = 0, 1
+
+
+class MlegsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("mlegs error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Field:
+    """TYPE(SCALAR) (mod_scalar3.f90:41-47) living on the device."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+
+    @property
+    def space(self):
+        return self.ctx.lib.mlegs_field_space(self.h)
+
+    def upload(self, E, ln=0.0, space=None):
+        """Copy a reference-layout complex array (shape of ``space``) to the device."""
+        space = self.ctx.space_of(E.shape) if space is None else space
+        want = self.ctx.shape(space)
+        if tuple(E.shape) != want:
+            raise ValueError("shape %s does not match space %d %s" % (E.shape, space, want))
+        buf = np.asfortranarray(E, dtype=np.complex128)
+        self.ctx._ck(self.ctx.lib.mlegs_field_upload(self.ctx.c, self.h, space,
+                                                     buf.ctypes.data_as(ctypes.c_void_p), float(ln)))
+        return self
+
+    def download(self, out=None):
+        """Return (E, LN) in the reference layout of the field's current space.
+
+        ``out``: optional preallocated Fortran-ordered complex128 array of that
+        shape (e.g. in pinned host memory); it is filled and returned as is."""
+        shape = self.ctx.shape(self.space)
+        if out is None:
+            E = np.empty(shape, dtype=np.complex128, order="F")
+        else:
+            if tuple(out.shape) != shape or out.dtype != np.complex128 or not out.flags.f_contiguous:
+                raise ValueError("out must be a Fortran-ordered complex128 array of shape %s" % (shape,))
+            E = out
+        ln = ctypes.c_double(0.0)
+        self.ctx._ck(self.ctx.lib.mlegs_field_download(self.ctx.c, self.h,
+                                                       E.ctypes.data_as(ctypes.c_void_p),
+                                                       ctypes.byref(ln)))
+        return (np.ascontiguousarray(E) if out is None else E), ln.value
+
+
+class Context:
+    """One grid + solver on one GPU (LEGINIT, mod_fft.f90:180-367)."""
+
+    def __init__(self, cfg, precision=PREC_FP64, split_slices=0, device=0):
+        self.lib = _lib.load()
+        self.cfg = cfg
+        p = _lib.Params()
+        p.nr, p.nth, p.nx = cfg.nr, cfg.nth, cfg.nx
+        p.nrchop, p.ntchop, p.nxchop = cfg.nrchop, cfg.ntchop, cfg.nxchop
+        p.ell, p.zlen, p.dt = cfg.ell, cfg.zlen, cfg.dt
+        p.adams = 1 if cfg.adams else 0
+        p.omega, p.bv0, p.kappa, p.kappap = cfg.omega, cfg.bv0, cfg.kappa, cfg.kappap
+        p.visc_sw, p.visc_p = cfg.visc_sw, cfg.p
+        p.nu, p.nup = cfg.nu, cfg.nup
+        p.precision, p.split_slices, p.device = precision, split_slices, device
+        h = ctypes.c_void_p()
+        rc = self.lib.mlegs_create(ctypes.byref(p), ctypes.byref(h))
+        if rc != 0:
+            raise MlegsError(rc, "mlegs_create failed")
+        self.c = h
+        d = (ctypes.c_int32 * 9)()
+        self.lib.mlegs_dims(self.c, d)
+        (self.NDIMR, self.NDIMTH, self.NX, self.NRCHOPDIM, self.NTCHOPDIM, self.NXCHOPDIM,
+         self.NRH, self.NR, self.NTH) = list(d)
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "c", None):
+            self.lib.mlegs_destroy(self.c)
+            self.c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        if rc != 0:
+            msg = self.lib.mlegs_last_error(self.c)
+            raise MlegsError(rc, msg.decode() if msg else "")
+        return rc
+
+    def shape(self, space):
+        if space == FFF:
+            return (self.NRCHOPDIM, self.NTCHOPDIM, self.NXCHOPDIM)
+        if space == PFF:
+            return (self.NDIMR, self.NTCHOPDIM, self.NXCHOPDIM)
+        return (self.NDIMR, self.NDIMTH, self.NX)
+
+    def space_of(self, shape):
+        for sp in (FFF, PFF):
+            if tuple(shape) == self.shape(sp):
+                return sp
+        raise ValueError("ambiguous space for shape %s; pass space=" % (shape,))
+
+    def field(self, space=FFF, E=None, ln=0.0):
+        h = ctypes.c_void_p()
+        self._ck(self.lib.mlegs_field_alloc(self.c, space, ctypes.byref(h)))
+        f = Field(self, h)
+        if E is not None:
+            f.upload(E, ln, space)
+        return f
+
+    def grid(self):
+        n = self.NR
+        x, w, r = (np.empty(n) for _ in range(3))
+        dp = ctypes.POINTER(ctypes.c_double)
+        self.lib.mlegs_grid(self.c, x.ctypes.data_as(dp), w.ctypes.data_as(dp), r.ctypes.data_as(dp))
+        return x, w, r
+
+    def sync(self):
+        self._ck(self.lib.mlegs_sync(self.c))
+
+    def launches(self):
+        return self.lib.mlegs_launch_count(self.c)
+
+    def reset_launches(self):
+        self.lib.mlegs_reset_launch_count(self.c)
+
+    # ------------------------------------------------------- transforms
+    def RTRAN(self, f, IS, pad=0):
+        self._ck(self.lib.mlegs_rtran(self.c, f.h, IS, pad))
+
+    def HORFFT(self, f, IS):
+        self._ck(self.lib.mlegs_horfft(self.c, f.h, IS))
+
+    def VERFFT(self, f, IS):
+        self._ck(self.lib.mlegs_verfft(self.c, f.h, IS))
+
+    def PLNFFT(self, f, IS):
+        self._ck(self.lib.mlegs_plnfft(self.c, f.h, IS))
+
+    def TOFF(self, f, pad=0):
+        self._ck(self.lib.mlegs_toff(self.c, f.h, pad))
+
+    def TOFP(self, f, pad=0):
+        self._ck(self.lib.mlegs_tofp(self.c, f.h, pad))
+
+    def CHOPDO(self, f, pad=0):
+        self._ck(self.lib.mlegs_chopdo(self.c, f.h, pad))
+
+    def COPY(self, dst, src, pad=0):
+        self._ck(self.lib.mlegs_field_copy(self.c, dst.h, src.h, pad))
+
+    def AXPBY(self, y, a, x1, b=0.0, x2=None, c=0.0):
+        self._ck(self.lib.mlegs_field_axpby(self.c, y.h, a, x1.h if x1 else None, b,
+                                            x2.h if x2 else None, c))
+
+    def SET_LN(self, f, ln):
+        self._ck(self.lib.mlegs_field_set_ln(self.c, f.h, ln))
+
+    # -------------------------------------------------------- operators
+    def _unary(self, name, a, b, pad):
+        self._ck(getattr(self.lib, name)(self.c, a.h, b.h, pad))
+        return b
+
+    def DELSQH(self, a, b, pad=0):
+        return self._unary("mlegs_delsqh", a, b, pad)
+
+    def IDELSQH(self, b, a, pad=0):
+        return self._unary("mlegs_idelsqh", b, a, pad)
+
+    def MULXM(self, a, b, pad=0):
+        return self._unary("mlegs_mulxm", a, b, pad)
+
+    def XXDX(self, a, b, pad=0):
+        return self._unary("mlegs_xxdx", a, b, pad)
+
+    def DEL2(self, a, b, pad=0):
+        return self._unary("mlegs_del2", a, b, pad)
+
+    def IDEL2LN(self, b, a, pad=0):
+        return self._unary("mlegs_idel2ln", b, a, pad)
+
+    def IDEL2(self, b, a, LN=None, pad=0):
+        self._ck(self.lib.mlegs_idel2(self.c, b.h, a.h, 0 if LN is None else 1,
+                                      0.0 if LN is None else float(LN), pad))
+        return a
+
+    def IHELM(self, b, a, alp, pad=0):
+        self._ck(self.lib.mlegs_ihelm(self.c, b.h, a.h, float(alp), pad))
+        return a
+
+    def GRAD(self, a, rr, rp, gz, pad=0):
+        self._ck(self.lib.mlegs_grad(self.c, a.h, rr.h, rp.h, gz.h, pad))
+
+    def PC2VEL(self, psi, chi, rur, rup, uz, pad=0):
+        self._ck(self.lib.mlegs_pc2vel(self.c, psi.h, chi.h, rur.h, rup.h, uz.h, pad))
+
+    def PC2VOR(self, psi, chi, ror, rop, oz, pad=0):
+        self._ck(self.lib.mlegs_pc2vor(self.c, psi.h, chi.h, ror.h, rop.h, oz.h, pad))
+
+    def PROJECT(self, rur, rup, uz, psi, chi, LN=None):
+        """LN: None, a number, or "psi" (the steppers' PSI%LN-by-reference form)."""
+        if LN is None:
+            mode, v = 0, 0.0
+        elif isinstance(LN, str):
+            mode, v = 2, 0.0
+        else:
+            mode, v = 1, float(LN)
+        self._ck(self.lib.mlegs_project(self.c, rur.h, rup.h, uz.h, psi.h, chi.h, mode, v))
+
+    def CALC_BOUSSI_FORCE(self, psi, chi, b, psin, chin, bn):
+        self._ck(self.lib.mlegs_boussi_force(self.c, psi.h, chi.h, b.h, psin.h, chin.h, bn.h))
+
+    # ------------------------------------------------------------ solver
+    def initialize(self, psi, chi, b):
+        """SOLVER_T%INITIALIZE: Richardson start-up step (mod_march.f90:171-240)."""
+        self.state = (psi, chi, b)
+        self._ck(self.lib.mlegs_solver_init(self.c, psi.h, chi.h, b.h))
+
+    def step(self, n=1, graph=False):
+        """n steady-state steps (STEP_BOUSSI_AB_CN / STEP_BOUSSI_ETDAB_CN)."""
+        fn = self.lib.mlegs_step_graph if graph else self.lib.mlegs_step
+        self._ck(fn(self.c, int(n)))
+
+    def time(self):
+        t = ctypes.c_double()
+        n = ctypes.c_int32()
+        self.lib.mlegs_time(self.c, ctypes.byref(t), ctypes.byref(n))
+        return t.value, n.value
+
+    def check_finite(self):
+        self._ck(self.lib.mlegs_check_finite(self.c))
+
+    def stream(self):
+        return self.lib.mlegs_stream(self.c)
+
+    KERNELS = {"rtran_b2p": 0, "rtran_p2b": 1, "verfft_b": 2, "verfft_f": 3, "horfft_b": 4,
+               "horfft_f": 5, "pointwise": 6, "solve": 7}
+
+    def kernel_time(self, name, reps=20):
+        """Mean device ms per launch of one internal kernel (CUDA events on the
+        library's stream) and its algorithmic HBM bytes per launch."""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.lib.mlegs_kernel_time(self.c, self.KERNELS[name], reps, ctypes.byref(ms),
+                                            ctypes.byref(by)))
+        return ms.value, by.value
+
+
+def qvortex(ctx, q=1.0, r0=1.0, xc=0.0, yc=0.0):
+    """QVORTEX (mod_layout.f90:449-609) for one vortex with H = 0, on the device.
+
+    omega_z = 2Q exp(-((x-xc)^2 + (y-yc)^2)/R0^2)/R0^2 is laid out at the
+    collocation points divided by (1-x)^2 (LAY with IPIN = 2, 64-117), taken
+    to FFF by TOFF, negated with its log term muted, and inverted by IDELSQH.
+    Returns (psi, chi) Fields; chi = 0.
+    """
+    x, _, r = ctx.grid()
+    nth = ctx.NTH
+    th = np.pi / nth * np.arange(2 * nth)
+    X = r[:, None] * np.cos(th)[None, :]
+    Y = r[:, None] * np.sin(th)[None, :]
+    val = 2.0 * q / r0 ** 2 * np.exp(-1.0 * ((X - xc) ** 2 + (Y - yc) ** 2) / r0 ** 2)
+    val = val / ((1 - x[:, None]) ** 2)
+    E = np.zeros(ctx.shape(PPP), dtype=np.complex128)
+    E[:ctx.NR, :nth, :] = (val[:, 0::2] + 1j * val[:, 1::2])[:, :, None]
+    A = ctx.field(PPP, E, 0.0)
+    ctx.TOFF(A)
+    ctx.AXPBY(A, -1.0, A)
+    ctx.SET_LN(A, 0.0)
+    psi = ctx.field(FFF)
+    ctx.IDELSQH(A, psi)
+    chi = ctx.field(FFF)
+    return psi, chi
+
+
+def initial_state(ctx, cfg=None):
+    """Vortex + seeded perturbation (construction in mlegs_b200.inputs), on the device."""
+    cfg = ctx.cfg if cfg is None else cfg
+    psi, chi = qvortex(ctx)
+    b = ctx.field(FFF)
+    tmp = ctx.field(FFF)
+    out = ctx.field(FFF)
+    for F, fid in ((psi, 0), (chi, 1)):
+        c = perturbation_coefficients(cfg, fid)
+        tmp.upload(-c, 0.0, FFF)
+        ctx.CHOPDO(tmp)
+        ctx.IDELSQH(tmp, out)
+        ctx.AXPBY(F, 1.0, out, 0.0, None, 1.0)
+        ctx.CHOPDO(F)
+    b.upload(buoyancy_perturbation(cfg), 0.0, FFF)
+    return psi, chi, b
+
+
+__all__ = ["Context", "Field", "MlegsError", "qvortex", "initial_state", "CONFIGS", "Config",
+           "PPP", "FFF", "PFP", "PFF", "PREC_FP64", "PREC_SPLIT"]

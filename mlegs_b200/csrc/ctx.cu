@@ -1,0 +1,1487 @@
+// Context, fields, operator composition, Boussinesq steppers and the C ABI.
+//
+// Host-side composition follows the reference routine by routine (file:line
+// in each method's comment); the arithmetic runs in the kernels of
+// tables.cu / kernels.cu / fft.cu / gemm.cu / solve.cu on one CUDA stream.
+// Nothing here computes on the CPU except the FP64 set-up tables that the
+// reference also builds once (LOGNORM, band-operator coefficients, ETD 4x4
+// matrices, hyperviscosity masks).
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mlegs_internal.h"
+
+using namespace mlegs;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& s) : std::runtime_error(s), code(c) {}
+};
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+// Every device allocation of a context is recorded here and released in one
+// place, whatever field or scratch slot currently points at it.
+thread_local std::vector<void*>* g_allocs = nullptr;
+
+template <class T>
+T* dalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) throw ApiError(MLEGS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (g_allocs) g_allocs->push_back(p);
+    return (T*)p;
+}
+
+}  // namespace
+
+struct mlegs_field {
+    Field f;
+    mlegs_ctx* owner;
+};
+
+struct mlegs_ctx {
+    mlegs_params p{};
+    Dims d{};
+    DevGrid g{};
+    cudaStream_t s = nullptr;
+    int dev = 0;
+    std::string err;
+    int64_t launches = 0;
+    int64_t graph_launches = 0;   // kernels in one captured step
+    std::vector<void*> allocs;
+
+    // device tables
+    double *x = nullptr, *w = nullptr, *r = nullptr, *lnx = nullptr, *pf = nullptr, *ak = nullptr;
+    double *norm0 = nullptr, *explog0 = nullptr, *at1 = nullptr, *tb_xxdx = nullptr, *tb_xm = nullptr,
+           *tb_del2h = nullptr;
+    double *V = nullptr, *D = nullptr, *T = nullptr;
+    double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
+    double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
+    FFTPlan fft;
+    std::vector<double> h_x, h_w, h_lognorm;
+
+    // memory
+    double* lnslots = nullptr;
+    int nslots = 0, used_slots = 0;
+    double2* scratch = nullptr;
+    double* solve_scr = nullptr;
+    double2* staging = nullptr;
+    int* dflag = nullptr;
+    std::vector<std::unique_ptr<mlegs_field>> owned;  // every field, incl. user ones
+    std::vector<Field*> pool;                         // free temporaries (stack)
+    std::vector<Field*> temps;                        // all temporaries
+    Field* hist[7] = {};
+
+    // solver state
+    Field *psi = nullptr, *chi = nullptr, *b = nullptr;
+    bool solver_ready = false;
+    double t = 0.0;
+    int n = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+
+    // ------------------------------------------------------------------
+    mlegs_field* new_field_h(int space, bool persistent) {
+        auto mf = std::make_unique<mlegs_field>();
+        mf->owner = this;
+        Field& f = mf->f;
+        f.data = dalloc<double2>(d.cap());
+        f.home = f.data;
+        if (used_slots >= nslots) throw ApiError(MLEGS_ERR_NOMEM, "out of LN slots");
+        f.slot = used_slots++;
+        f.ln = lnslots + f.slot;
+        f.space = space;
+        f.persistent = persistent;
+        CK(cudaMemsetAsync(f.data, 0, d.cap() * sizeof(double2), s));
+        mlegs_field* out = mf.get();
+        owned.push_back(std::move(mf));
+        return out;
+    }
+    Field* new_field(int space, bool persistent) { return &new_field_h(space, persistent)->f; }
+    Field* tmp(int space = MLEGS_FFF) {
+        if (pool.empty()) throw ApiError(MLEGS_ERR_NOMEM, "temporary field pool exhausted");
+        Field* f = pool.back();
+        pool.pop_back();
+        f->space = space;
+        return f;
+    }
+    void rel(Field* f) { pool.push_back(f); }
+
+    void set_error(const std::string& e) { err = e; }
+
+    // ------------------------------------------------------------------ set-up
+    void init(const mlegs_params& prm);
+    void destroy();
+
+    // ------------------------------------------------------------------ basic
+    size_t fff() const { return d.fff(); }
+    void zero_fff(Field* f) { k_fill(f->data, fff(), s); }
+    void ln_zero(Field* f) { CK(cudaMemsetAsync(f->ln, 0, sizeof(double), s)); }
+    void chopdo(Field* f, int pad) {
+        if (f->space == MLEGS_FFF) k_chopdo_fff(g, f->data, pad, s);
+        // PFF/PFP/PPP: the device layouts do not store the padded rows/columns.
+    }
+    void require(const Field* f, int space, const char* who) {
+        if (f->space != space)
+            throw ApiError(MLEGS_ERR_TRANSFORM, std::string(who) + ": input not in the expected space");
+    }
+    // COPY0 (mod_fft.f90:705-769): dst = src, CHOPDO for FFF, LN copied.
+    void copy0(Field* dst, const Field* src, int pad) {
+        if (dst == src) return;
+        k_copy(dst->data, src->data, d.elems(src->space), s);
+        dst->space = src->space;
+        CK(cudaMemcpyAsync(dst->ln, src->ln, sizeof(double), cudaMemcpyDeviceToDevice, s));
+        chopdo(dst, pad);
+    }
+    void swap_scratch(Field* f) {
+        if (f->persistent) throw ApiError(MLEGS_ERR_STATE, "in-place transform of a persistent field");
+        std::swap(f->data, scratch);
+    }
+    void swap_scratch_any(Field* f) { std::swap(f->data, scratch); }
+
+    // ------------------------------------------------------------------ transforms
+    // RTRAN(A, IS), mod_fft.f90:1150-1340.  Both directions zero A%LN.
+    void rtran(Field* f, int is, int pad) {
+        if (is == -1) {
+            require(f, MLEGS_PFF, "RTRAN");
+            k_fold_gemm(g, pf, d.NRCHOPDIM + 1, f->data, scratch, 0 | 2, 0, 0, pad, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_FFF;
+        } else {
+            require(f, MLEGS_FFF, "RTRAN");
+            k_rtran_b2p(g, f->data, scratch, f->ln, pad, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_PFF;
+        }
+        ln_zero(f);
+    }
+    // VERFFT(A, IS), mod_fft.f90:928-1113 (LN preserved).
+    void verfft(Field* f, int is) {
+        if (is == -1) {
+            require(f, MLEGS_PFP, "VERFFT");
+            k_verfft_f(g, fft, f->data, scratch, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_PFF;
+        } else {
+            require(f, MLEGS_PFF, "VERFFT");
+            k_verfft_b(g, fft, f->data, scratch, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_PFP;
+        }
+    }
+    // HORFFT(A, IS), mod_fft.f90:771-926.
+    void horfft(Field* f, int is) {
+        if (is == -1) {
+            require(f, MLEGS_PPP, "HORFFT");
+            k_horfft_f(g, fft, f->data, scratch, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_PFP;
+        } else {
+            require(f, MLEGS_PFP, "HORFFT");
+            k_horfft_b(g, fft, f->data, scratch, s);
+            swap_scratch_any(f);
+            f->space = MLEGS_PPP;
+        }
+    }
+    void plnfft(Field* f, int is) {
+        if (is == -1) {
+            horfft(f, -1);
+            verfft(f, -1);
+        } else {
+            verfft(f, 1);
+            horfft(f, 1);
+        }
+    }
+    void toff(Field* f, int pad) {
+        if (f->space == MLEGS_PPP) horfft(f, -1);
+        if (f->space == MLEGS_PFP) verfft(f, -1);
+        if (f->space == MLEGS_PFF) rtran(f, -1, pad);
+    }
+    void tofp(Field* f, int pad) {
+        if (f->space == MLEGS_FFF) rtran(f, 1, pad);
+        if (f->space == MLEGS_PFF) verfft(f, 1);
+        if (f->space == MLEGS_PFP) horfft(f, 1);
+    }
+
+    // ------------------------------------------------------------------ operators
+    void delsqh(const Field* a, Field* b, int pad) {  // mod_legops.f90:76-133
+        require(a, MLEGS_FFF, "DELSQH");
+        k_delsqh(g, a->data, a->ln, b->data, pad, s);
+        b->space = MLEGS_FFF;
+        ln_zero(b);
+    }
+    void idelsqh(const Field* bb, Field* a, int pad) {  // mod_legops.f90:136-241
+        require(bb, MLEGS_FFF, "IDELSQH");
+        // A%LN = B(1,1,1) NORM(1,1) ELL2
+        k_idelsqh(g, bb->data, a->data, pad, s);
+        a->space = MLEGS_FFF;
+        ln_from_coef(a->ln, bb->data, d.ELL2);
+        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
+    }
+    void ln_from_coef(double* ln, const double2* data, double scale);
+    void mulxm(const Field* a, Field* b, int pad) {  // 371-428
+        require(a, MLEGS_FFF, "MULXM");
+        k_band3(g, a->data, b->data, 1, pad, s);
+        b->space = MLEGS_FFF;
+        ln_zero(b);
+    }
+    void xxdx(const Field* a, Field* b, int pad) {  // 680-748
+        require(a, MLEGS_FFF, "XXDX");
+        k_band3(g, a->data, b->data, 0, pad, s);
+        k_logterm_rows(g, b->data, a->ln, 0, 1.0, s);
+        b->space = MLEGS_FFF;
+        ln_zero(b);
+    }
+    void del2(const Field* a, Field* b, int pad) {  // 751-820
+        require(a, MLEGS_FFF, "DEL2");
+        k_del2(g, a->data, b->data, pad, s);
+        k_logterm_rows(g, b->data, a->ln, 1, 1.0, s);
+        b->space = MLEGS_FFF;
+        ln_zero(b);
+    }
+    // IDEL2 (823-1010): has_ln = 0 -> LN absent.
+    void idel2(const Field* bb, Field* a, int has_ln, double ln, int pad) {
+        require(bb, MLEGS_FFF, "IDEL2");
+        copy0(a, bb, pad);
+        ln_zero(a);
+        k_solve_del2(g, a->data, a->ln, 1, 0.0, has_ln, ln, nullptr, solve_scr, pad, s);
+        chopdo(a, pad);
+        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
+    }
+    void idel2ln(const Field* bb, Field* a, int pad) {  // 1013-1176
+        require(bb, MLEGS_FFF, "IDEL2LN");
+        copy0(a, bb, pad);
+        ln_zero(a);
+        k_solve_del2(g, a->data, a->ln, 0, 0.0, 0, 0.0, nullptr, solve_scr, pad, s);
+        chopdo(a, pad);
+        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
+    }
+    void ihelm(const Field* bb, Field* a, double alp, int pad) {  // 1204-1354
+        require(bb, MLEGS_FFF, "IHELM");
+        if (alp == 0.0) throw ApiError(MLEGS_ERR_LEGOPERATOR, "IHELM: ALP CAN'T BE ZERO");
+        copy0(a, bb, pad);
+        k_ln_copy(a->ln, bb->ln, -1.0 / alp, s);      // A%LN = -B%LN/ALP
+        k_logterm_rows(g, a->data, a->ln, 2, 1.0, s);  // rhs -= LN * DEL2(log)
+        k_solve_del2(g, a->data, nullptr, 2, alp, 0, 0.0, nullptr, solve_scr, pad, s);
+        chopdo(a, pad);
+    }
+    void grad(const Field* a, Field* rr, Field* rp, Field* gz, int pad) {  // 1727-1786
+        xxdx(a, rr, pad);
+        k_mk_combine(g, 4, a->data, nullptr, rp->data, pad, s);
+        k_mk_combine(g, 5, a->data, nullptr, gz->data, pad, s);
+        rp->space = gz->space = MLEGS_FFF;
+        ln_zero(rp);
+        ln_zero(gz);
+    }
+    void pc2vel(const Field* psi_, const Field* chi_, Field* rur, Field* rup, Field* uz, int pad) {  // 1789-1853
+        xxdx(chi_, rur, pad);
+        xxdx(psi_, rup, pad);
+        k_mk_combine(g, 0, psi_->data, rur->data, rur->data, pad, s);
+        k_mk_combine(g, 1, chi_->data, rup->data, rup->data, pad, s);
+        delsqh(chi_, uz, pad);
+        Field* W = tmp();
+        mulxm(uz, W, pad);
+        mulxm(W, uz, pad);
+        rel(W);
+        k_mk_combine(g, 6, uz->data, nullptr, uz->data, pad, s);
+    }
+    void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad) {  // 1856-1919
+        del2(chi_, oz, pad);
+        xxdx(psi_, ror, pad);
+        xxdx(oz, rop, pad);
+        k_mk_combine(g, 2, oz->data, ror->data, ror->data, pad, s);
+        k_mk_combine(g, 3, psi_->data, rop->data, rop->data, pad, s);
+        delsqh(psi_, oz, pad);
+        Field* W = tmp();
+        mulxm(oz, W, pad);
+        mulxm(W, oz, pad);
+        rel(W);
+        k_mk_combine(g, 6, oz->data, nullptr, oz->data, pad, s);
+    }
+    // PROJECT (mod_legops.f90:2397-2545).  ln_mode: 0 none, 1 value, 2 PSI%LN by reference.
+    void project(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_, int ln_mode, double ln) {
+        if (!(rur->space == rup->space && rup->space == uz->space))
+            throw ApiError(MLEGS_ERR_TRANSFORM, "PROJECT: RUR, RUP, UZ MUST BE IN THE SAME SPACE.");
+        if (rur->space == MLEGS_PPP) {
+            plnfft(rur, -1);
+            plnfft(rup, -1);
+            plnfft(uz, -1);
+        } else if (rur->space == MLEGS_FFF) {
+            rtran(rur, 1, 0);
+            rtran(rup, 1, 0);
+            rtran(uz, 1, 0);
+        } else if (rur->space != MLEGS_PFF) {
+            throw ApiError(MLEGS_ERR_TRANSFORM, "PROJECT: bad input space");
+        }
+        psi_->space = chi_->space = MLEGS_FFF;
+        ln_zero(psi_);
+        ln_zero(chi_);
+        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, explog0, d.NRCHOP, s);
+        if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, explog0, d.NRCHOP, s);
+        const int wr = d.NRCHOPDIM;
+        // PSI = -(i m) EO(V, RUR) - OE(D, RUP)
+        k_fold_gemm(g, V, wr, rur->data, psi_->data, 0, 2, 0, 0, s);
+        k_fold_gemm(g, D, wr, rup->data, psi_->data, 1, 1, 1, 0, s);
+        // CHI = (i k) OE(D, RUR) + m k EO(V, RUP) - EO(T, UZ)
+        k_fold_gemm(g, D, wr, rur->data, chi_->data, 1, 3, 0, 0, s);
+        k_fold_gemm(g, V, wr, rup->data, chi_->data, 0, 4, 1, 0, s);
+        k_fold_gemm(g, T, wr, uz->data, chi_->data, 0, 1, 1, 0, s);
+        k_farfield_fix(g, psi_->data, d.NRCHOP, s);
+    }
+
+    // ------------------------------------------------------------------ physics
+    void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
+    void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
+                Field* BN);
+    void visc1(Field* A, double nu, double dt);
+    void visc2(Field* A, const Field* AO, double nu, double dt);
+    void visc_be(Field* P, Field* C, Field* B, double dt);
+    void visc_cn(Field* P, Field* C, Field* B, const Field* PO, const Field* CO, const Field* BO);
+    void hyperv3(Field* P, Field* C, Field* B, double tf);
+    void etd_hyperv(Field* R, Field* Pp, Field* Z, Field* B, double tf);
+    void rich_fe_be();
+    void step_ab_cn();
+    void etdfe_be(Field* P, Field* C, Field* B, const double* E, const double* NL, double dt, bool store);
+    void rich_etdfe_be();
+    void step_etdab_cn();
+    void step_once() { p.adams ? step_ab_cn() : step_etdab_cn(); }
+
+    // snapshot of the temporaries' buffers so every step reuses the same pointers
+    std::vector<double2*> snap;
+    double2* snap_scratch = nullptr;
+    void mark() {
+        snap.clear();
+        for (Field* f : temps) snap.push_back(f->data);
+        snap_scratch = scratch;
+    }
+    void restore() {
+        for (size_t i = 0; i < temps.size(); ++i) temps[i]->data = snap[i];
+        scratch = snap_scratch;
+    }
+};
+
+// ====================================================================== set-up
+namespace {
+
+// LEG_LOG_NORMT (mod_lin_legendre.f90:306-377) for MS = (0..ntchopdim-1).
+std::vector<double> leg_log_norm(int ndim, int ntchopdim) {
+    int me = ntchopdim - 1;
+    std::vector<double> wk(me + 1);
+    wk[0] = std::log(0.5);
+    for (int m = 1; m <= me; ++m) wk[m] = wk[m - 1] + std::log(2 * m + 1.0) - std::log(2 * m * std::pow(2 * m - 1.0, 2));
+    std::vector<double> out((size_t)ntchopdim * ndim);
+    for (int m = 0; m < ntchopdim; ++m) {
+        double* o = &out[(size_t)m * ndim];
+        o[0] = wk[m];
+        for (int nn = 2; nn <= ndim; ++nn) {
+            int n = m + (nn - 1);
+            o[nn - 1] = o[nn - 2] + std::log(2 * n + 1.0) - std::log(2 * n - 1.0) + std::log(1.0 * (n - m)) -
+                        std::log(1.0 * (n + m));
+        }
+        for (int nn = 0; nn < ndim; ++nn) o[nn] = 0.5 * o[nn];
+    }
+    return out;
+}
+
+}  // namespace
+
+void mlegs_ctx::init(const mlegs_params& prm) {
+    p = prm;
+    if (p.nr < 4 || p.nth < 2 || p.nx < 2 || p.nrchop < 1 || p.ntchop < 1 || p.nxchop < 1)
+        throw ApiError(MLEGS_ERR_ARG, "bad dimensions");
+    auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+    if (!pow2(p.nth) || !pow2(p.nx)) throw ApiError(MLEGS_ERR_ARG, "NTH and NX must be powers of two");
+    if (p.nr % 2) throw ApiError(MLEGS_ERR_ARG, "NR must be even");
+    if (2 * p.nxchop > p.nx) throw ApiError(MLEGS_ERR_ARG, "NXCHOP MUST BE < NX/2");  // mod_fft.f90:237-243
+    dev = p.device;
+    CK(cudaSetDevice(dev));
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    g_launch_counter = &launches;
+    fft_set_attributes();
+
+    d.NR = p.nr;
+    d.NRH = p.nr / 2;
+    d.NTH = p.nth;
+    d.NX = p.nx;
+    d.NRCHOP = p.nrchop;
+    d.NTCHOP = p.ntchop;
+    d.NXCHOP = p.nxchop;
+    d.NDIMR = p.nr + 3;
+    d.NDIMTH = p.nth + 1;
+    d.NRCHOPDIM = std::min(p.nrchop + 6, p.nr);
+    d.NTCHOPDIM = std::min(p.ntchop, p.nth);
+    d.NXCHOPDIM = 2 * p.nxchop - 1;
+    d.NXCHOPH = p.nx - p.nxchop + 2;
+    d.NLN = d.NRCHOPDIM + 14;
+    d.ELL = p.ell;
+    d.ELL2 = std::pow(p.ell, 2.0);
+    d.ZLEN = p.zlen;
+    if (d.NRCHOP > d.NRCHOPDIM) throw ApiError(MLEGS_ERR_ARG, "NRCHOP > NRCHOPDIM");
+    const int NB = d.NRCHOPDIM + 2;
+
+    // --- Gauss-Legendre nodes and weights on the device (FP64 Newton)
+    x = dalloc<double>(d.NR);
+    w = dalloc<double>(d.NR);
+    k_tables_gauss(x, w, d.NR, s);
+    h_x.resize(d.NR);
+    h_w.resize(d.NR);
+    CK(cudaMemcpyAsync(h_x.data(), x, d.NR * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_w.data(), w, d.NR * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<double> h_r(d.NR), h_lnx(d.NR);
+    for (int i = 0; i < d.NR; ++i) {
+        h_r[i] = d.ELL * std::sqrt((1 + h_x[i]) / (1 - h_x[i]));  // LEG_ZERO, mod_lin_legendre.f90:172
+        h_lnx[i] = -std::log(1 - h_x[i]);                          // TFM%LN, mod_fft.f90:287
+    }
+    r = dalloc<double>(d.NR);
+    lnx = dalloc<double>(d.NR);
+    CK(cudaMemcpyAsync(r, h_r.data(), d.NR * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(lnx, h_lnx.data(), d.NR * sizeof(double), cudaMemcpyHostToDevice, s));
+
+    // --- orthonormal P^m_n table on the device
+    const int ne = d.NRCHOPDIM + 1;
+    pf = dalloc<double>((size_t)d.NTCHOPDIM * ne * d.NRH);
+    k_tables_pf(x, pf, d.NRH, ne, d.NTCHOPDIM, s);
+
+    // --- LOGNORM, NORM(:,m=0), AT1, AK, band coefficients (host FP64)
+    h_lognorm = leg_log_norm(d.NLN, d.NTCHOPDIM);
+    std::vector<double> h_norm0(d.NLN), h_explog0(d.NLN), h_at1(d.NRCHOPDIM), h_ak(d.NXCHOPDIM);
+    {
+        double v = 0.5;  // LEG_NORMT, m = 0 (mod_lin_legendre.f90:246-270)
+        h_norm0[0] = std::sqrt(v);
+        for (int nn = 2; nn <= d.NLN; ++nn) {
+            int nv = nn - 1;
+            v = v * (2 * nv + 1.0) / (2 * nv - 1.0) * nv / nv;
+            h_norm0[nn - 1] = std::sqrt(v);
+        }
+    }
+    for (int nn = 0; nn < d.NLN; ++nn) h_explog0[nn] = std::exp(h_lognorm[nn]);
+    for (int nn = 0; nn < d.NRCHOPDIM; ++nn) h_at1[nn] = std::sqrt((2 * nn + 1) / 2.0);
+    for (int kk = 0; kk < d.NXCHOPDIM; ++kk) {
+        int kv = kk;
+        if (kk + 1 > d.NXCHOP) kv = -(d.NXCHOPDIM - (kk + 1) + 1);
+        h_ak[kk] = 2 * M_PI / d.ZLEN * kv;  // mod_fft.f90:255-263
+    }
+    std::vector<double> h_xxdx((size_t)d.NTCHOPDIM * NB * 2, 0.0), h_xm((size_t)d.NTCHOPDIM * NB * 2, 0.0),
+        h_del2h((size_t)d.NTCHOPDIM * NB * 5, 0.0);
+    for (int m = 0; m < d.NTCHOPDIM; ++m) {
+        const double* ln = &h_lognorm[(size_t)m * d.NLN];
+        const double am = m;
+        for (int nn = 0; nn < NB; ++nn) {
+            const double N = am + nn;
+            auto ex = [&](int a, int b2) { return std::exp(ln[a] - ln[b2]); };
+            double* xb = &h_xxdx[((size_t)m * NB + nn) * 2];
+            double* mb = &h_xm[((size_t)m * NB + nn) * 2];
+            double* db = &h_del2h[((size_t)m * NB + nn) * 5];
+            // BAND_LOGLEG_XXDX (1683-1757) and BAND_LOGLEG_XM (910-981)
+            if (nn >= 1) {
+                xb[0] = -(N - 1.0) * (N - am) / (2 * N - 1.0) * ex(nn - 1, nn);
+                mb[0] = -(N - am) / (2 * N - 1.0) * ex(nn - 1, nn);
+            }
+            xb[1] = (N + 2.0) * (N + am + 1.0) / (2 * N + 3.0) * ex(nn + 1, nn);
+            mb[1] = -(N + am + 1.0) / (2 * N + 3.0) * ex(nn + 1, nn);
+            // BAND_LOGLEG_RAT_DEL2H with S = 0 (1986-2092)
+            const double e2 = d.ELL2;
+            if (nn >= 2)
+                db[0] = -(N - am - 1.0) * (N - am) * (N - 2) * (N - 1) / (2 * N - 3.) / (2 * N - 1.0) / e2 *
+                        ex(nn - 2, nn);
+            if (nn >= 1) db[1] = 2.0 * N * (N - am) * (N - 1) / (2 * N - 1.0) / e2 * ex(nn - 1, nn);
+            db[2] = (-2.0 * N * (N + 1.0) * (3.0 * N * N + 3 * N - am * am - 2)) / (2 * N - 1.0) / (2 * N + 3.0) / e2;
+            db[3] = 2.0 * (N + 1) * (N + am + 1.0) * (N + 2) / (2 * N + 3.0) / e2 * ex(nn + 1, nn);
+            db[4] = -(N + am + 1.0) * (N + am + 2.0) * (N + 3) * (N + 2) / (2 * N + 3.0) / (2 * N + 5.0) / e2 *
+                    ex(nn + 2, nn);
+        }
+    }
+    auto up = [&](const std::vector<double>& h) {
+        double* dp = dalloc<double>(h.size());
+        CK(cudaMemcpyAsync(dp, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        return dp;
+    };
+    norm0 = up(h_norm0);
+    explog0 = up(h_explog0);
+    at1 = up(h_at1);
+    ak = up(h_ak);
+    tb_xxdx = up(h_xxdx);
+    tb_xm = up(h_xm);
+    tb_del2h = up(h_del2h);
+
+    g.NR = d.NR;
+    g.NRH = d.NRH;
+    g.NTH = d.NTH;
+    g.NX = d.NX;
+    g.NRCHOP = d.NRCHOP;
+    g.NTCHOP = d.NTCHOP;
+    g.NXCHOP = d.NXCHOP;
+    g.NRCHOPDIM = d.NRCHOPDIM;
+    g.NTCHOPDIM = d.NTCHOPDIM;
+    g.NXCHOPDIM = d.NXCHOPDIM;
+    g.NLN = d.NLN;
+    g.ELL2 = d.ELL2;
+    g.x = x;
+    g.w = w;
+    g.r = r;
+    g.lnx = lnx;
+    g.pf = pf;
+    g.ak = ak;
+    g.norm0 = norm0;
+    g.at1 = at1;
+    g.xxdx = tb_xxdx;
+    g.xm = tb_xm;
+    g.del2h = tb_del2h;
+    g.NB = NB;
+
+    // --- PROJECT weights (device, from PF)
+    size_t vsz = (size_t)d.NTCHOPDIM * d.NRCHOPDIM * d.NRH;
+    V = dalloc<double>(vsz);
+    D = dalloc<double>(vsz);
+    T = dalloc<double>(vsz);
+    k_tables_project(g, V, D, T, 0, s);
+
+    // --- FFT twiddles (host long double, rounded once)
+    auto lg2 = [](int v) { int l = 0; while ((1 << l) < v) ++l; return l; };
+    fft.lx = lg2(d.NX);
+    fft.lt = lg2(d.NTH);
+    auto twid = [&](int N, double scale) {
+        std::vector<double2> h(N + 1);
+        for (int q = 0; q <= N; ++q) {
+            long double a = -(long double)scale * 3.141592653589793238462643383279502884L * q / N;
+            h[q] = make_double2((double)std::cos(a), (double)std::sin(a));
+        }
+        double2* dp = dalloc<double2>(N + 1);
+        CK(cudaMemcpyAsync(dp, h.data(), (N + 1) * sizeof(double2), cudaMemcpyHostToDevice, s));
+        return dp;
+    };
+    fft.tw_x = twid(d.NX, 2.0);
+    fft.tw_t = twid(d.NTH, 2.0);
+    fft.tw_h = twid(d.NTH, 1.0);
+
+    // --- hyperviscosity (HYP3SET, mod_march.f90:3320-3408)
+    if (p.visc_sw == 3) {
+        auto mask = [](const std::vector<double>& kv, size_t size, double ratio, double steep) {
+            std::vector<double> out(size, 1.0);
+            double kmax = -1e300;
+            for (double v : kv) kmax = std::max(kmax, v);
+            if (kv.empty() || kmax < 1e-12) kmax = 1.0;
+            double ta = std::tanh(steep);
+            for (size_t i = 0; i < kv.size(); ++i) {
+                double kn = kv[i] / kmax;
+                if (kn < ratio) out[i] = 0.0;
+                else {
+                    double xr = (kn - ratio) / (1.0 - ratio), yr = steep * (2.0 * xr - 1.0);
+                    out[i] = (std::tanh(yr) + ta) / (2.0 * ta);
+                }
+            }
+            return out;
+        };
+        const int nrc = d.NRCHOP;
+        std::vector<double> mr((size_t)nrc * d.NTCHOPDIM), mt, mx;
+        for (int m = 0; m < d.NTCHOPDIM; ++m) {
+            int nrs = std::max(d.NRCHOP - m, 0);
+            std::vector<double> kv(nrs);
+            for (int q = 0; q < nrs; ++q) kv[q] = q;
+            auto mm = mask(kv, nrc, 0.5, 2.0);
+            for (int q = 0; q < nrc; ++q) mr[(size_t)m * nrc + q] = mm[q];
+        }
+        {
+            std::vector<double> kv(d.NTCHOPDIM);
+            for (int m = 0; m < d.NTCHOPDIM; ++m) kv[m] = m;
+            mt = mask(kv, d.NTCHOPDIM, 2.0 / 3.0, 2.0);
+            std::vector<double> kx(d.NXCHOPDIM);
+            for (int q = 0; q < d.NXCHOPDIM; ++q) kx[q] = std::fabs(h_ak[q]);
+            mx = mask(kx, d.NXCHOPDIM, 2.0 / 3.0, 2.0);
+        }
+        const int ph2 = p.visc_p / 2;
+        auto ipow = [](double v, int e) { double r2 = 1.0; for (int q = 0; q < e; ++q) r2 *= v; return r2; };
+        double k2r = 1.5 * 1.5 * (double)((nrc - 1) * nrc) / d.ELL2;
+        double k2t = (double)((d.NTCHOPDIM - 1) * (d.NTCHOPDIM - 1));
+        double k2x = 0.0;
+        for (double v : h_ak) k2x = std::max(k2x, v * v);
+        auto set = [&](double nu, double** outp) {
+            std::vector<double> hr((size_t)nrc * d.NTCHOPDIM), ht(d.NTCHOPDIM), hx(d.NXCHOPDIM);
+            for (int m = 0; m < d.NTCHOPDIM; ++m) {
+                ht[m] = std::exp(-nu * mt[m] * ipow((double)(m * m) / k2t, ph2));
+                for (int nn = 1; nn <= nrc; ++nn)
+                    hr[(size_t)m * nrc + nn - 1] =
+                        std::exp(-nu * mr[(size_t)m * nrc + nn - 1] *
+                                 ipow(1.5 * 1.5 * (double)((nn - 1) * nn) / d.ELL2 / k2r, ph2));
+            }
+            for (int q = 0; q < d.NXCHOPDIM; ++q) hx[q] = std::exp(-nu * mx[q] * ipow(h_ak[q] * h_ak[q] / k2x, ph2));
+            outp[0] = up(hr);
+            outp[1] = up(ht);
+            outp[2] = up(hx);
+        };
+        set(p.nup, hv);
+        set(p.kappap, hd);
+    }
+
+    // --- ETD operators (CALC_BOUSSI_ETD_OP, mod_march.f90:906-945; host FP64)
+    if (!p.adams) {
+        if (p.bv0 == 0.0) throw ApiError(MLEGS_ERR_SOLVER, "CALC_BOUSSI_DIAG: N_FREQ = 0, CANNOT DIAGONALIZE");
+        typedef std::complex<double> C;
+        const C I(0.0, 1.0);
+        auto etd = [&](double dt, double** Eo, double** No) {
+            C J[4] = {-I * p.bv0, I * p.bv0, -2.0 * I * p.omega, 2.0 * I * p.omega};
+            C S[4][4] = {}, Si[4][4] = {};
+            S[0][2] = I; S[0][3] = -I; S[1][2] = 1.0; S[1][3] = 1.0;
+            S[2][0] = -I / p.bv0; S[2][1] = I / p.bv0; S[3][0] = 1.0; S[3][1] = 1.0;
+            Si[0][2] = I * p.bv0 / 2.0; Si[0][3] = 0.5; Si[1][2] = -I * p.bv0 / 2.0; Si[1][3] = 0.5;
+            Si[2][0] = -I / 2.0; Si[2][1] = 0.5; Si[3][0] = I / 2.0; Si[3][1] = 0.5;
+            C je[4], jp[4];
+            for (int q = 0; q < 4; ++q) {
+                je[q] = std::exp(J[q] * dt);
+                jp[q] = (std::abs(J[q]) > 1e-14) ? (je[q] - 1.0) / J[q] : C(dt);
+            }
+            std::vector<double> e(16), nl(16);
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j) {
+                    C a = 0.0, b2 = 0.0;
+                    for (int q = 0; q < 4; ++q) {
+                        a += S[i][q] * je[q] * Si[q][j];
+                        b2 += S[i][q] * jp[q] * Si[q][j];
+                    }
+                    e[i * 4 + j] = a.real();
+                    nl[i * 4 + j] = b2.real();
+                }
+            *Eo = up(e);
+            *No = up(nl);
+        };
+        etd(p.dt, &etdE, &etdN);
+        etd(p.dt * 0.5, &hetdE, &hetdN);
+    }
+
+    // --- memory: LN slots, scratch buffers, temporaries, history
+    nslots = 256;
+    lnslots = dalloc<double>(nslots);
+    CK(cudaMemsetAsync(lnslots, 0, nslots * sizeof(double), s));
+    scratch = dalloc<double2>(d.cap());
+    size_t nsys = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
+    solve_scr = dalloc<double>((size_t)d.NRCHOPDIM * 4 * nsys);
+    size_t ref_max = (size_t)d.NDIMR * d.NDIMTH * d.NX;
+    size_t ref_fff = (size_t)d.NRCHOPDIM * d.NTCHOPDIM * d.NXCHOPDIM;
+    size_t ref_pff = (size_t)d.NDIMR * d.NTCHOPDIM * d.NXCHOPDIM;
+    staging = dalloc<double2>(std::max(ref_max, std::max(ref_fff, ref_pff)));
+    dflag = dalloc<int>(1);
+    for (int q = 0; q < 24; ++q) {
+        Field* f = new_field(MLEGS_FFF, false);
+        temps.push_back(f);
+        pool.push_back(f);
+    }
+    for (int q = 0; q < 7; ++q) hist[q] = new_field(MLEGS_FFF, true);
+    CK(cudaStreamSynchronize(s));
+}
+
+void mlegs_ctx::destroy() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* q : allocs) cudaFree(q);
+    allocs.clear();
+    if (s) cudaStreamDestroy(s);
+    s = nullptr;
+}
+
+__global__ void ln_from_coef_kernel(double* ln, const double2* data, double n0, double scale) {
+    *ln = data[0].x * n0 * scale;
+}
+void mlegs_ctx::ln_from_coef(double* ln, const double2* data, double scale) {
+    // IDELSQH: A%LN = B%E(1,1,1) * NORM(1,1) * ELL2  (mod_legops.f90:207)
+    double v0 = std::sqrt(0.5);
+    ln_from_coef_kernel<<<1, 1, 0, s>>>(ln, data, v0, scale);
+    count_launch();
+}
+
+// ====================================================================== physics
+// CALC_BOUSSI_FORCE(PSI, CHI, B, PSIN, CHIN, BN), mod_boussinesq.f90:317-410.
+void mlegs_ctx::force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BNout) {
+    Field *RUR = tmp(), *RUP = tmp(), *UZ = tmp(), *ROR = tmp(), *ROP = tmp(), *OZ = tmp(), *RBR = tmp(),
+          *RBP = tmp(), *BZ = tmp(), *W = tmp(), *BN = tmp();
+    const int P3 = 3;  // CHOPSET(3) ... CHOPSET(-3)
+    grad(B, RBR, RBP, BZ, P3);
+    pc2vel(PSI, CHI, RUR, RUP, UZ, P3);
+    pc2vor(PSI, CHI, ROR, ROP, OZ, P3);
+    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) tofp(f, P3);
+    copy0(W, B, 0);  // W = B; TOFP(W) after CHOPSET(-3)
+    tofp(W, 0);
+    // VPRODSUB + VDOTPSUB + the linear terms (385-391) in one pointwise pass
+    BN->space = MLEGS_PPP;
+    ln_zero(BN);
+    k_force_pointwise(g, RUR->data, RUP->data, UZ->data, ROR->data, ROP->data, OZ->data, RBR->data,
+                      RBP->data, BZ->data, BN->data, W->data, p.omega, p.bv0, 1, s);
+    rel(UZ);
+    rel(RBR);
+    rel(RBP);
+    rel(BZ);
+    rel(W);
+    Field* Wf = RUP;  // W = DEL2(CHIN) in FFF
+    project(ROR, ROP, OZ, PSIN, Wf, 1, 0.0);
+    idel2ln(Wf, CHIN, 0);
+    toff(BN, 0);
+    copy0(BNout, BN, 0);
+    rel(BN);
+    rel(RUR);
+    rel(RUP);
+    rel(ROR);
+    rel(ROP);
+    rel(OZ);
+}
+
+// CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
+// On exit ROR, ROP, OZ hold the projected u x omega in velocity form (FFF).
+void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
+                       Field* BN) {
+    Field *RBR = tmp(), *RBP = tmp(), *BZ = tmp();
+    grad(B, RBR, RBP, BZ, 1);
+    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) tofp(f, 0);
+    BN->space = MLEGS_PPP;
+    ln_zero(BN);
+    k_force_pointwise(g, RUR->data, RUP->data, UZ->data, ROR->data, ROP->data, OZ->data, RBR->data,
+                      RBP->data, BZ->data, BN->data, nullptr, 0.0, 0.0, 0, s);
+    rel(RBR);
+    rel(RBP);
+    rel(BZ);
+    Field *PSI = tmp(), *W = tmp(), *CHI = tmp();
+    project(ROR, ROP, OZ, PSI, W, 1, 0.0);
+    idel2(W, CHI, 0, 0.0, 0);
+    pc2vel(PSI, CHI, ROR, ROP, OZ, 3);
+    rel(PSI);
+    rel(W);
+    rel(CHI);
+    toff(BN, 0);
+}
+
+// VISC1 (mod_march.f90:1529-1576): A <- IHELM(-ALP A, ALP), ALP = 1/(NU DT).
+void mlegs_ctx::visc1(Field* A, double nu, double dt) {
+    if (nu == 0.0) throw ApiError(MLEGS_ERR_SOLVER, "VISC1: NU CAN'T BE ZERO");
+    double alp = 1 / (nu * dt);
+    Field* WK = tmp();
+    k_axpby(WK->data, -alp, A->data, 0.0, nullptr, 0.0, fff(), s);
+    k_ln_copy(WK->ln, A->ln, -alp, s);
+    WK->space = MLEGS_FFF;
+    ihelm(WK, A, alp, 0);
+    rel(WK);
+}
+// VISC2 (mod_march.f90:1579-1636): A <- IHELM(-DEL2(AO) - ALP A, ALP), ALP = 2/(NU DT).
+void mlegs_ctx::visc2(Field* A, const Field* AO, double nu, double dt) {
+    if (nu == 0.0) throw ApiError(MLEGS_ERR_SOLVER, "VISC2: NU CAN'T BE ZERO");
+    double alp = 2 / nu / dt;
+    Field* WK = tmp();
+    del2(AO, WK, 2);
+    chopdo(WK, 0);
+    k_axpby(WK->data, -alp, A->data, 0.0, nullptr, -1.0, fff(), s);
+    k_ln_copy(WK->ln, A->ln, -alp, s);
+    ihelm(WK, A, alp, 0);
+    rel(WK);
+}
+void mlegs_ctx::visc_be(Field* P, Field* C, Field* B, double dt) {  // 1200-1230
+    if (p.visc_sw != 1) return;
+    visc1(P, p.nu, dt);
+    visc1(C, p.nu, dt);
+    if (p.kappa != 0.0) visc1(B, p.kappa, dt);
+}
+void mlegs_ctx::visc_cn(Field* P, Field* C, Field* B, const Field* PO, const Field* CO, const Field* BO) {
+    if (p.visc_sw != 1) return;  // 1233-1265
+    visc2(P, PO, p.nu, p.dt);
+    visc2(C, CO, p.nu, p.dt);
+    if (p.kappa != 0.0) visc2(B, BO, p.kappa, p.dt);
+}
+void mlegs_ctx::hyperv3(Field* P, Field* C, Field* B, double tf) {  // CALC_BOUSSI_HYPERV 1305-1349
+    if (p.visc_sw == 2) throw ApiError(MLEGS_ERR_SOLVER, "VISC%SW = 2 is not on the configured path");
+    if (p.visc_sw != 3) return;
+    k_hyperv(g, P->data, hv[0], hv[1], hv[2], tf, 0, s);
+    k_hyperv(g, C->data, hv[0], hv[1], hv[2], tf, 0, s);
+    k_hyperv(g, B->data, hd[0], hd[1], hd[2], tf, 0, s);
+}
+void mlegs_ctx::etd_hyperv(Field* R, Field* Pp, Field* Z, Field* B, double tf) {  // 1352-1416
+    if (p.visc_sw != 3) return;
+    k_hyperv(g, R->data, hv[0], hv[1], hv[2], tf, 0, s);
+    k_hyperv(g, Pp->data, hv[0], hv[1], hv[2], tf, 0, s);
+    k_hyperv(g, Z->data, hv[0], hv[1], hv[2], tf, 0, s);
+    k_hyperv(g, B->data, hd[0], hd[1], hd[2], tf, 0, s);
+}
+
+// RICH_BOUSSI_FE_BE (mod_march.f90:535-606).  hist: 0 N_PSI, 1 N_CHI, 2 N_B.
+void mlegs_ctx::rich_fe_be() {
+    const double dt = p.dt, hdt = dt * 0.5;
+    t += dt;
+    n += 1;
+    Field *NP = hist[0], *NC = hist[1], *NB = hist[2];
+    force(psi, chi, b, NP, NC, NB);
+    Field *P2 = tmp(), *C2 = tmp(), *B2 = tmp();
+    const size_t N = fff();
+    k_axpby(P2->data, 1.0, psi->data, hdt, NP->data, 0.0, N, s);
+    k_ln_axpby(P2->ln, 1.0, psi->ln, hdt, NP->ln, 0.0, s);
+    k_axpby(C2->data, 1.0, chi->data, hdt, NC->data, 0.0, N, s);
+    k_ln_axpby(C2->ln, 1.0, chi->ln, hdt, NC->ln, 0.0, s);
+    k_axpby(B2->data, 1.0, b->data, hdt, NB->data, 0.0, N, s);
+    k_ln_set(B2->ln, 0.0, s);
+    P2->space = C2->space = B2->space = MLEGS_FFF;
+    visc_be(P2, C2, B2, hdt);
+    hyperv3(P2, C2, B2, hdt / p.dt);
+    Field *PN = tmp(), *CN = tmp(), *BN = tmp();
+    force(P2, C2, B2, PN, CN, BN);
+    k_axpby(P2->data, hdt, PN->data, 0.0, nullptr, 1.0, N, s);
+    k_ln_axpby(P2->ln, hdt, PN->ln, 0.0, nullptr, 1.0, s);
+    k_axpby(C2->data, hdt, CN->data, 0.0, nullptr, 1.0, N, s);
+    k_ln_axpby(C2->ln, hdt, CN->ln, 0.0, nullptr, 1.0, s);
+    k_axpby(B2->data, hdt, BN->data, 0.0, nullptr, 1.0, N, s);
+    rel(PN);
+    rel(CN);
+    rel(BN);
+    visc_be(P2, C2, B2, hdt);
+    hyperv3(P2, C2, B2, hdt / p.dt);
+    k_axpby(psi->data, dt, NP->data, 0.0, nullptr, 1.0, N, s);
+    k_ln_axpby(psi->ln, dt, NP->ln, 0.0, nullptr, 1.0, s);
+    k_axpby(chi->data, dt, NC->data, 0.0, nullptr, 1.0, N, s);
+    k_ln_axpby(chi->ln, dt, NC->ln, 0.0, nullptr, 1.0, s);
+    k_axpby(b->data, dt, NB->data, 0.0, nullptr, 1.0, N, s);
+    visc_be(psi, chi, b, dt);
+    hyperv3(psi, chi, b, 1.0);
+    k_axpby(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, s);
+    k_ln_axpby(psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, s);
+    k_ln_axpby(chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby(b->data, 2.0, B2->data, 0.0, nullptr, -1.0, N, s);
+    rel(P2);
+    rel(C2);
+    rel(B2);
+}
+
+// STEP_BOUSSI_AB_CN (mod_march.f90:609-661).
+void mlegs_ctx::step_ab_cn() {
+    const double dt = p.dt;
+    t += dt;
+    n += 1;
+    Field *NP = hist[0], *NC = hist[1], *NB = hist[2];
+    Field *PN = tmp(), *CN = tmp(), *BN = tmp();
+    force(psi, chi, b, PN, CN, BN);
+    Field *P0 = tmp(), *C0 = tmp(), *B0 = tmp();
+    copy0(P0, psi, 0);
+    copy0(C0, chi, 0);
+    copy0(B0, b, 0);
+    const size_t N = fff();
+    k_axpby(psi->data, 1.5 * dt, PN->data, -0.5 * dt, NP->data, 1.0, N, s);
+    k_ln_axpby(psi->ln, 1.5 * dt, PN->ln, -0.5 * dt, NP->ln, 1.0, s);
+    k_axpby(chi->data, 1.5 * dt, CN->data, -0.5 * dt, NC->data, 1.0, N, s);
+    k_ln_axpby(chi->ln, 1.5 * dt, CN->ln, -0.5 * dt, NC->ln, 1.0, s);
+    k_axpby(b->data, 1.5 * dt, BN->data, -0.5 * dt, NB->data, 1.0, N, s);
+    copy0(NP, PN, 0);
+    copy0(NC, CN, 0);
+    copy0(NB, BN, 0);
+    rel(PN);
+    rel(CN);
+    rel(BN);
+    visc_cn(psi, chi, b, P0, C0, B0);
+    rel(P0);
+    rel(C0);
+    rel(B0);
+    hyperv3(psi, chi, b, 1.0);
+}
+
+// STEP_BOUSSI_ETDFE_BE (mod_march.f90:664-753), in place on (P, C, B).
+// hist (store = true): 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z.
+void mlegs_ctx::etdfe_be(Field* P, Field* C, Field* B, const double* E, const double* NL, double dt, bool store) {
+    Field *RURN = tmp(), *RUPN = tmp(), *UZN = tmp(), *RORN = tmp(), *ROPN = tmp(), *OZN = tmp(), *BN = tmp();
+    pc2vel(P, C, RURN, RUPN, UZN, 3);
+    pc2vor(P, C, RORN, ROPN, OZN, 3);
+    nonlin(B, RURN, RUPN, UZN, RORN, ROPN, OZN, BN);
+    etd_hyperv(RORN, ROPN, OZN, BN, dt / p.dt);
+    pc2vel(P, C, RURN, RUPN, UZN, 3);
+    k_etd(g, E, NL, dt, 0, RURN->data, RUPN->data, UZN->data, B->data, RORN->data, ROPN->data, OZN->data,
+          BN->data, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, s);
+    etd_hyperv(RURN, RUPN, UZN, B, dt / p.dt);
+    if (store) {
+        const size_t N = fff();
+        k_copy(hist[0]->data, BN->data, N, s);
+        k_copy(hist[1]->data, RORN->data, N, s);
+        k_copy(hist[2]->data, ROPN->data, N, s);
+        k_copy(hist[3]->data, OZN->data, N, s);
+        k_copy(hist[4]->data, RURN->data, N, s);
+        k_copy(hist[5]->data, RUPN->data, N, s);
+        k_copy(hist[6]->data, UZN->data, N, s);
+    }
+    rel(BN);
+    rel(RORN);
+    rel(ROPN);
+    rel(OZN);
+    Field* W = tmp();
+    Field* Pn = tmp();
+    project(RURN, RUPN, UZN, Pn, W, 2, 0.0);
+    copy0(P, Pn, 0);
+    idel2ln(W, C, 0);
+    rel(W);
+    rel(Pn);
+    if (store) {
+        pc2vel(P, C, RURN, RUPN, UZN, 3);
+        const size_t N = fff();
+        k_axpby(hist[4]->data, 0.5, hist[4]->data, -0.5, RURN->data, 0.0, N, s);
+        k_axpby(hist[5]->data, 0.5, hist[5]->data, -0.5, RUPN->data, 0.0, N, s);
+        k_axpby(hist[6]->data, 0.5, hist[6]->data, -0.5, UZN->data, 0.0, N, s);
+    }
+    rel(RURN);
+    rel(RUPN);
+    rel(UZN);
+}
+
+// RICH_BOUSSI_ETDFE_BE (mod_march.f90:756-808).
+void mlegs_ctx::rich_etdfe_be() {
+    const double dt = p.dt, hdt = dt * 0.5;
+    t += dt;
+    n += 1;
+    Field *P2 = tmp(), *C2 = tmp(), *B2 = tmp();
+    copy0(P2, psi, 0);
+    copy0(C2, chi, 0);
+    copy0(B2, b, 0);
+    etdfe_be(P2, C2, B2, hetdE, hetdN, hdt, false);
+    visc_be(P2, C2, B2, hdt);
+    etdfe_be(P2, C2, B2, hetdE, hetdN, hdt, false);
+    visc_be(P2, C2, B2, hdt);
+    etdfe_be(psi, chi, b, etdE, etdN, dt, true);
+    visc_be(psi, chi, b, dt);
+    const size_t N = fff();
+    k_axpby(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, s);
+    k_ln_axpby(psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, s);
+    k_ln_axpby(chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby(b->data, 2.0, B2->data, 0.0, nullptr, -1.0, N, s);
+    rel(P2);
+    rel(C2);
+    rel(B2);
+}
+
+// STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901).
+void mlegs_ctx::step_etdab_cn() {
+    const double dt = p.dt;
+    t += dt;
+    n += 1;
+    Field *RURN = tmp(), *RUPN = tmp(), *UZN = tmp(), *RORN = tmp(), *ROPN = tmp(), *OZN = tmp(), *BN = tmp();
+    pc2vel(psi, chi, RURN, RUPN, UZN, 3);
+    pc2vor(psi, chi, RORN, ROPN, OZN, 3);
+    nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN);
+    etd_hyperv(RORN, ROPN, OZN, BN, 1.0);
+    Field* B0 = tmp();
+    copy0(B0, b, 0);
+    pc2vel(psi, chi, RURN, RUPN, UZN, 3);
+    k_etd(g, etdE, etdN, dt, 1, RURN->data, RUPN->data, UZN->data, b->data, RORN->data, ROPN->data, OZN->data,
+          BN->data, hist[4]->data, hist[5]->data, hist[6]->data, hist[1]->data, hist[2]->data, hist[3]->data,
+          hist[0]->data, s);
+    const size_t N = fff();
+    k_copy(hist[0]->data, BN->data, N, s);
+    k_copy(hist[1]->data, RORN->data, N, s);
+    k_copy(hist[2]->data, ROPN->data, N, s);
+    k_copy(hist[3]->data, OZN->data, N, s);
+    rel(BN);
+    rel(RORN);
+    rel(ROPN);
+    rel(OZN);
+    etd_hyperv(RURN, RUPN, UZN, b, 1.0);
+    k_copy(hist[4]->data, RURN->data, N, s);
+    k_copy(hist[5]->data, RUPN->data, N, s);
+    k_copy(hist[6]->data, UZN->data, N, s);
+    Field *P0 = tmp(), *C0 = tmp();
+    copy0(P0, psi, 0);
+    copy0(C0, chi, 0);
+    Field *W = tmp(), *Pn = tmp();
+    project(RURN, RUPN, UZN, Pn, W, 2, 0.0);
+    copy0(psi, Pn, 0);
+    idel2ln(W, chi, 0);
+    rel(W);
+    rel(Pn);
+    pc2vel(psi, chi, RURN, RUPN, UZN, 3);
+    k_axpby(hist[4]->data, -1.0, RURN->data, 0.0, nullptr, 1.0, N, s);
+    k_axpby(hist[5]->data, -1.0, RUPN->data, 0.0, nullptr, 1.0, N, s);
+    k_axpby(hist[6]->data, -1.0, UZN->data, 0.0, nullptr, 1.0, N, s);
+    rel(RURN);
+    rel(RUPN);
+    rel(UZN);
+    visc_cn(psi, chi, b, P0, C0, B0);
+    rel(P0);
+    rel(C0);
+    rel(B0);
+}
+
+// ====================================================================== C ABI
+namespace {
+template <class F>
+int guard(mlegs_ctx* ctx, F&& fn) {
+    if (!ctx) return MLEGS_ERR_ARG;
+    int64_t* prev = g_launch_counter;
+    std::vector<void*>* prev_allocs = g_allocs;
+    g_launch_counter = &ctx->launches;
+    g_allocs = &ctx->allocs;
+    int rc = MLEGS_OK;
+    try {
+        cudaSetDevice(ctx->dev);
+        fn();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e));
+    } catch (const ApiError& e) {
+        ctx->set_error(e.what());
+        rc = e.code;
+    } catch (const CudaError& e) {
+        ctx->set_error(e.what());
+        rc = MLEGS_ERR_CUDA;
+    } catch (const std::exception& e) {
+        ctx->set_error(e.what());
+        rc = MLEGS_ERR_STATE;
+    }
+    g_launch_counter = prev;
+    g_allocs = prev_allocs;
+    return rc;
+}
+Field* F(mlegs_field* f) {
+    if (!f) throw ApiError(MLEGS_ERR_ARG, "null field");
+    return &f->f;
+}
+const Field* F(const mlegs_field* f) {
+    if (!f) throw ApiError(MLEGS_ERR_ARG, "null field");
+    return &f->f;
+}
+void check_pad(const mlegs_ctx* c, int pad) {
+    if (c->d.NRCHOP + pad > c->d.NRCHOPDIM || c->d.NRCHOP + pad < 0)
+        throw ApiError(MLEGS_ERR_SCALAR3, "CHOPSET: NRCHOP TOO LARGE");
+}
+}  // namespace
+
+extern "C" {
+
+int mlegs_create(const mlegs_params* p, mlegs_ctx** out) {
+    if (!p || !out) return MLEGS_ERR_ARG;
+    *out = nullptr;
+    mlegs_ctx* c = new (std::nothrow) mlegs_ctx();
+    if (!c) return MLEGS_ERR_NOMEM;
+    int64_t* prev = g_launch_counter;
+    std::vector<void*>* prev_allocs = g_allocs;
+    g_allocs = &c->allocs;
+    try {
+        c->init(*p);
+    } catch (const ApiError& e) {
+        fprintf(stderr, "mlegs_create: %s\n", e.what());
+        g_launch_counter = prev;
+        g_allocs = prev_allocs;
+        c->destroy();
+        delete c;
+        return e.code;
+    } catch (const std::exception& e) {
+        fprintf(stderr, "mlegs_create: %s\n", e.what());
+        g_launch_counter = prev;
+        g_allocs = prev_allocs;
+        c->destroy();
+        delete c;
+        return MLEGS_ERR_CUDA;
+    }
+    g_launch_counter = prev;
+    g_allocs = prev_allocs;
+    *out = c;
+    return MLEGS_OK;
+}
+
+int mlegs_destroy(mlegs_ctx* ctx) {
+    if (!ctx) return MLEGS_ERR_ARG;
+    cudaSetDevice(ctx->dev);
+    if (ctx->s) cudaStreamSynchronize(ctx->s);
+    ctx->destroy();
+    delete ctx;
+    return MLEGS_OK;
+}
+
+const char* mlegs_last_error(const mlegs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int mlegs_sync(mlegs_ctx* ctx) {
+    return guard(ctx, [&] { CK(cudaStreamSynchronize(ctx->s)); });
+}
+
+int mlegs_dims(const mlegs_ctx* c, int32_t out[9]) {
+    if (!c || !out) return MLEGS_ERR_ARG;
+    const Dims& d = c->d;
+    int32_t v[9] = {d.NDIMR, d.NDIMTH, d.NX, d.NRCHOPDIM, d.NTCHOPDIM, d.NXCHOPDIM, d.NRH, d.NR, d.NTH};
+    memcpy(out, v, sizeof(v));
+    return MLEGS_OK;
+}
+
+int mlegs_field_alloc(mlegs_ctx* ctx, int space, mlegs_field** out) {
+    if (!out) return MLEGS_ERR_ARG;
+    if (space < 0 || space > 3) return MLEGS_ERR_TRANSFORM;  // SALLOC: INVALID SPACE TAG
+    return guard(ctx, [&] { *out = ctx->new_field_h(space, true); });
+}
+
+int mlegs_field_free(mlegs_ctx* ctx, mlegs_field* f) {
+    // Memory is released with the context; the handle just stops being used.
+    if (!ctx || !f) return MLEGS_ERR_ARG;
+    return MLEGS_OK;
+}
+
+int mlegs_field_space(const mlegs_field* f) { return f ? f->f.space : -1; }
+
+int mlegs_grid(const mlegs_ctx* c, double* x, double* w, double* r) {
+    if (!c) return MLEGS_ERR_ARG;
+    for (int i = 0; i < c->d.NR; ++i) {
+        if (x) x[i] = c->h_x[i];
+        if (w) w[i] = c->h_w[i];
+        if (r) r[i] = c->d.ELL * std::sqrt((1 + c->h_x[i]) / (1 - c->h_x[i]));
+    }
+    return MLEGS_OK;
+}
+
+int mlegs_field_axpby(mlegs_ctx* ctx, mlegs_field* y, double a, const mlegs_field* x1, double b,
+                      const mlegs_field* x2, double c) {
+    return guard(ctx, [&] {
+        Field* fy = F(y);
+        const Field* f1 = x1 ? F(x1) : nullptr;
+        const Field* f2 = x2 ? F(x2) : nullptr;
+        for (const Field* q : {(const Field*)fy, f1, f2})
+            if (q && q->space != MLEGS_FFF) throw ApiError(MLEGS_ERR_TRANSFORM, "axpby: FFF fields only");
+        k_axpby(fy->data, a, f1 ? f1->data : nullptr, b, f2 ? f2->data : nullptr, c, ctx->fff(), ctx->s);
+        k_ln_axpby(fy->ln, a, f1 ? f1->ln : nullptr, b, f2 ? f2->ln : nullptr, c, ctx->s);
+    });
+}
+
+int mlegs_field_set_ln(mlegs_ctx* ctx, mlegs_field* f, double ln) {
+    return guard(ctx, [&] { k_ln_set(F(f)->ln, ln, ctx->s); });
+}
+
+int mlegs_field_upload(mlegs_ctx* ctx, mlegs_field* f, int space, const double* host, double ln) {
+    if (!host) return MLEGS_ERR_ARG;
+    if (space < 0 || space > 3) return MLEGS_ERR_TRANSFORM;
+    return guard(ctx, [&] {
+        Field* fd = F(f);
+        const Dims& d = ctx->d;
+        size_t ref = (space == MLEGS_FFF) ? (size_t)d.NRCHOPDIM * d.NTCHOPDIM * d.NXCHOPDIM
+                     : (space == MLEGS_PFF) ? (size_t)d.NDIMR * d.NTCHOPDIM * d.NXCHOPDIM
+                                            : (size_t)d.NDIMR * d.NDIMTH * d.NX;
+        CK(cudaMemcpyAsync(ctx->staging, host, ref * sizeof(double2), cudaMemcpyHostToDevice, ctx->s));
+        k_from_ref(ctx->g, space, ctx->staging, fd->data, ctx->s);
+        fd->space = space;
+        CK(cudaMemcpyAsync(fd->ln, &ln, sizeof(double), cudaMemcpyHostToDevice, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+    });
+}
+
+int mlegs_field_download(mlegs_ctx* ctx, const mlegs_field* f, double* host, double* ln) {
+    if (!host) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        const Field* fd = F(f);
+        const Dims& d = ctx->d;
+        int space = fd->space;
+        size_t ref = (space == MLEGS_FFF) ? (size_t)d.NRCHOPDIM * d.NTCHOPDIM * d.NXCHOPDIM
+                     : (space == MLEGS_PFF) ? (size_t)d.NDIMR * d.NTCHOPDIM * d.NXCHOPDIM
+                                            : (size_t)d.NDIMR * d.NDIMTH * d.NX;
+        k_to_ref(ctx->g, space, fd->data, ctx->staging, ctx->s);
+        CK(cudaMemcpyAsync(host, ctx->staging, ref * sizeof(double2), cudaMemcpyDeviceToHost, ctx->s));
+        double lv = 0.0;
+        CK(cudaMemcpyAsync(&lv, fd->ln, sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        if (ln) *ln = lv;
+    });
+}
+
+int mlegs_field_copy(mlegs_ctx* ctx, mlegs_field* dst, const mlegs_field* src, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        ctx->copy0(F(dst), F(src), pad);
+    });
+}
+
+int mlegs_chopdo(mlegs_ctx* ctx, mlegs_field* f, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        ctx->chopdo(F(f), pad);
+    });
+}
+
+// In-place transforms on user fields swap with the context's scratch buffer
+// and then copy back so that the handle keeps its own buffer.
+static void user_inplace(mlegs_ctx* ctx, Field* f, const std::function<void(Field*)>& fn);
+
+int mlegs_rtran(mlegs_ctx* ctx, mlegs_field* f, int is, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        if (is != 1 && is != -1) throw ApiError(MLEGS_ERR_ARG, "RTRAN: IS must be +1 or -1");
+        user_inplace(ctx, F(f), [&](Field* x) { ctx->rtran(x, is, pad); });
+    });
+}
+int mlegs_horfft(mlegs_ctx* ctx, mlegs_field* f, int is) {
+    return guard(ctx, [&] { user_inplace(ctx, F(f), [&](Field* x) { ctx->horfft(x, is); }); });
+}
+int mlegs_verfft(mlegs_ctx* ctx, mlegs_field* f, int is) {
+    return guard(ctx, [&] { user_inplace(ctx, F(f), [&](Field* x) { ctx->verfft(x, is); }); });
+}
+int mlegs_plnfft(mlegs_ctx* ctx, mlegs_field* f, int is) {
+    return guard(ctx, [&] { user_inplace(ctx, F(f), [&](Field* x) { ctx->plnfft(x, is); }); });
+}
+int mlegs_toff(mlegs_ctx* ctx, mlegs_field* f, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        user_inplace(ctx, F(f), [&](Field* x) { ctx->toff(x, pad); });
+    });
+}
+int mlegs_tofp(mlegs_ctx* ctx, mlegs_field* f, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        user_inplace(ctx, F(f), [&](Field* x) { ctx->tofp(x, pad); });
+    });
+}
+
+int mlegs_delsqh(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->delsqh(F(a), F(b), pad); });
+}
+int mlegs_idelsqh(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->idelsqh(F(b), F(a), pad); });
+}
+int mlegs_mulxm(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->mulxm(F(a), F(b), pad); });
+}
+int mlegs_xxdx(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->xxdx(F(a), F(b), pad); });
+}
+int mlegs_del2(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->del2(F(a), F(b), pad); });
+}
+int mlegs_idel2(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int has_ln, double ln, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->idel2(F(b), F(a), has_ln, ln, pad); });
+}
+int mlegs_idel2ln(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->idel2ln(F(b), F(a), pad); });
+}
+int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->ihelm(F(b), F(a), alp, pad); });
+}
+int mlegs_grad(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* rgr, mlegs_field* rgp, mlegs_field* gz,
+               int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->grad(F(a), F(rgr), F(rgp), F(gz), pad); });
+}
+int mlegs_pc2vel(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, mlegs_field* rur,
+                 mlegs_field* rup, mlegs_field* uz, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->pc2vel(F(psi), F(chi), F(rur), F(rup), F(uz), pad); });
+}
+int mlegs_pc2vor(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, mlegs_field* ror,
+                 mlegs_field* rop, mlegs_field* oz, int pad) {
+    return guard(ctx, [&] { check_pad(ctx, pad); ctx->pc2vor(F(psi), F(chi), F(ror), F(rop), F(oz), pad); });
+}
+int mlegs_project(mlegs_ctx* ctx, mlegs_field* rur, mlegs_field* rup, mlegs_field* uz, mlegs_field* psi,
+                  mlegs_field* chi, int ln_mode, double ln) {
+    return guard(ctx, [&] {
+        if (ln_mode < 0 || ln_mode > 2) throw ApiError(MLEGS_ERR_ARG, "PROJECT: bad ln_mode");
+        Field *a = F(rur), *b2 = F(rup), *c = F(uz);
+        // work on temporaries so the user fields keep their buffers
+        Field *ta = ctx->tmp(), *tb = ctx->tmp(), *tc = ctx->tmp();
+        ctx->copy0(ta, a, 0);
+        ctx->copy0(tb, b2, 0);
+        ctx->copy0(tc, c, 0);
+        ctx->project(ta, tb, tc, F(psi), F(chi), ln_mode, ln);
+        ctx->copy0(a, ta, 0);
+        ctx->copy0(b2, tb, 0);
+        ctx->copy0(c, tc, 0);
+        ctx->rel(ta);
+        ctx->rel(tb);
+        ctx->rel(tc);
+    });
+}
+int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
+                       mlegs_field* psin, mlegs_field* chin, mlegs_field* bn) {
+    return guard(ctx, [&] {
+        ctx->mark();
+        ctx->force(F(psi), F(chi), F(b), F(psin), F(chin), F(bn));
+        ctx->restore();
+    });
+}
+
+int mlegs_solver_init(mlegs_ctx* ctx, mlegs_field* psi, mlegs_field* chi, mlegs_field* b) {
+    return guard(ctx, [&] {
+        Field *P = F(psi), *C = F(chi), *B = F(b);
+        if (P->space != MLEGS_FFF || C->space != MLEGS_FFF || B->space != MLEGS_FFF)
+            throw ApiError(MLEGS_ERR_TRANSFORM, "solver state must be in FFF space");
+        ctx->psi = P;
+        ctx->chi = C;
+        ctx->b = B;
+        ctx->t = 0.0;
+        ctx->n = 0;
+        for (Field* h : ctx->hist) {
+            ctx->zero_fff(h);
+            ctx->ln_zero(h);
+            h->space = MLEGS_FFF;
+        }
+        ctx->mark();
+        if (ctx->p.adams) ctx->rich_fe_be();
+        else ctx->rich_etdfe_be();
+        ctx->restore();
+        ctx->solver_ready = true;
+        if (ctx->gexec) {
+            cudaGraphExecDestroy(ctx->gexec);
+            ctx->gexec = nullptr;
+        }
+        if (ctx->graph) {
+            cudaGraphDestroy(ctx->graph);
+            ctx->graph = nullptr;
+        }
+    });
+}
+
+int mlegs_step(mlegs_ctx* ctx, int nsteps) {
+    return guard(ctx, [&] {
+        if (!ctx->solver_ready) throw ApiError(MLEGS_ERR_STATE, "mlegs_solver_init has not run");
+        for (int q = 0; q < nsteps; ++q) {
+            ctx->mark();
+            ctx->step_once();
+            ctx->restore();
+        }
+    });
+}
+
+int mlegs_step_graph(mlegs_ctx* ctx, int nsteps) {
+    return guard(ctx, [&] {
+        if (!ctx->solver_ready) throw ApiError(MLEGS_ERR_STATE, "mlegs_solver_init has not run");
+        if (!ctx->gexec) {
+            ctx->mark();
+            double t0 = ctx->t;
+            int n0 = ctx->n;
+            int64_t before = ctx->launches;
+            CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+            try {
+                ctx->step_once();
+            } catch (...) {
+                cudaGraph_t gtmp = nullptr;
+                cudaStreamEndCapture(ctx->s, &gtmp);
+                if (gtmp) cudaGraphDestroy(gtmp);
+                ctx->restore();
+                throw;
+            }
+            CK(cudaStreamEndCapture(ctx->s, &ctx->graph));
+            ctx->graph_launches = ctx->launches - before;
+            ctx->launches = before;
+            ctx->restore();
+            ctx->t = t0;
+            ctx->n = n0;
+            CK(cudaGraphInstantiate(&ctx->gexec, ctx->graph, 0));
+        }
+        for (int q = 0; q < nsteps; ++q) {
+            CK(cudaGraphLaunch(ctx->gexec, ctx->s));
+            ctx->launches += ctx->graph_launches;
+            ctx->t += ctx->p.dt;
+            ctx->n += 1;
+        }
+    });
+}
+
+int mlegs_time(const mlegs_ctx* ctx, double* t, int32_t* n) {
+    if (!ctx) return MLEGS_ERR_ARG;
+    if (t) *t = ctx->t;
+    if (n) *n = ctx->n;
+    return MLEGS_OK;
+}
+
+int mlegs_check_finite(mlegs_ctx* ctx) {
+    int flag = 0;
+    int rc = guard(ctx, [&] {
+        if (!ctx->psi) throw ApiError(MLEGS_ERR_STATE, "no solver state");
+        CK(cudaMemsetAsync(ctx->dflag, 0, sizeof(int), ctx->s));
+        for (Field* f : {ctx->psi, ctx->chi, ctx->b}) k_finite(f->data, ctx->fff(), ctx->dflag, ctx->s);
+        CK(cudaMemcpyAsync(&flag, ctx->dflag, sizeof(int), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+    });
+    if (rc) return rc;
+    if (flag) {
+        ctx->set_error("ANYNAN: non-finite value in the solver state");
+        return MLEGS_ERR_NONFINITE;
+    }
+    return MLEGS_OK;
+}
+
+int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
+    if (reps < 1 || kernel < 0 || kernel > 7) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        const Dims& d = ctx->d;
+        const DevGrid& g = ctx->g;
+        cudaStream_t s = ctx->s;
+        Field *a = ctx->tmp(), *b = ctx->tmp(), *c = ctx->tmp();
+        Field* f9[9];
+        for (auto& q : f9) q = ctx->tmp();
+        // deterministic non-trivial contents: fill FFF/PPP-sized buffers via axpby of zeros
+        // is pointless for timing, so keep whatever the scratch buffers hold (finite zeros
+        // after allocation) -- arithmetic cost does not depend on the values.
+        auto launch = [&]() {
+            switch (kernel) {
+                case 0: k_rtran_b2p(g, a->data, b->data, nullptr, 0, s); break;
+                case 1: k_fold_gemm(g, ctx->pf, d.NRCHOPDIM + 1, a->data, b->data, 2, 0, 0, 0, s); break;
+                case 2: k_verfft_b(g, ctx->fft, a->data, b->data, s); break;
+                case 3: k_verfft_f(g, ctx->fft, a->data, b->data, s); break;
+                case 4: k_horfft_b(g, ctx->fft, a->data, b->data, s); break;
+                case 5: k_horfft_f(g, ctx->fft, a->data, b->data, s); break;
+                case 6:
+                    k_force_pointwise(g, f9[0]->data, f9[1]->data, f9[2]->data, f9[3]->data, f9[4]->data,
+                                      f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data, b->data,
+                                      1.0, 1.0, 1, s);
+                    break;
+                default:
+                    k_solve_del2(g, a->data, c->ln, 0, 0.0, 0, 0.0, nullptr, ctx->solve_scr, 0, s);
+                    break;
+            }
+        };
+        const double B16 = 16.0;
+        double bytes = 0.0;
+        switch (kernel) {
+            case 0: case 1: bytes = B16 * ((double)d.fff() + (double)d.pff()); break;
+            case 2: case 3: bytes = B16 * ((double)d.pff() + (double)d.pfp()); break;
+            case 4: case 5: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
+            case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written
+            default: bytes = B16 * 2.0 * (double)d.fff(); break;
+        }
+        for (int q = 0; q < 3; ++q) launch();  // warm-up
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, s));
+        for (int q = 0; q < reps; ++q) launch();
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        for (auto& q : f9) ctx->rel(q);
+        ctx->rel(c);
+        ctx->rel(b);
+        ctx->rel(a);
+        if (ms_per_launch) *ms_per_launch = ms / reps;
+        if (bytes_per_launch) *bytes_per_launch = bytes;
+    });
+}
+
+int64_t mlegs_launch_count(const mlegs_ctx* ctx) { return ctx ? ctx->launches : 0; }
+void mlegs_reset_launch_count(mlegs_ctx* ctx) {
+    if (ctx) ctx->launches = 0;
+}
+void* mlegs_stream(mlegs_ctx* ctx) { return ctx ? (void*)ctx->s : nullptr; }
+
+}  // extern "C"
+
+static void user_inplace(mlegs_ctx* ctx, Field* f, const std::function<void(Field*)>& fn) {
+    Field* t = ctx->tmp(f->space);
+    ctx->mark();
+    k_copy(t->data, f->data, ctx->d.elems(f->space), ctx->s);
+    cudaMemcpyAsync(t->ln, f->ln, sizeof(double), cudaMemcpyDeviceToDevice, ctx->s);
+    t->space = f->space;
+    fn(t);
+    k_copy(f->data, t->data, ctx->d.elems(t->space), ctx->s);
+    cudaMemcpyAsync(f->ln, t->ln, sizeof(double), cudaMemcpyDeviceToDevice, ctx->s);
+    f->space = t->space;
+    ctx->rel(t);
+    ctx->restore();
+}

@@ -1,0 +1,564 @@
+// Elementwise, banded-stencil and pointwise kernels of the hot path.
+//
+// Band operators restate mod_legops.f90 (DELSQH 76-133, MULXM 371-428,
+// XXDX 680-748, DEL2 751-820, GRAD 1727-1786, PC2VEL 1789-1853,
+// PC2VOR 1856-1919) on the FFF layout [m][n][k]; the truncation BANMUL
+// applies (rows/columns beyond NN = NRCHOPS(m) dropped, mod_bandmat.f90:
+// 1111-1153) is a mask on the column index.  Pointwise products restate
+// VPRODSUB/VDOTPSUB (mod_legops.f90:2105-2130, 2207-2225) and the linear
+// terms of CALC_BOUSSI_FORCE (mod_boussinesq.f90:385-391).
+#include "mlegs_internal.h"
+
+namespace mlegs {
+
+thread_local int64_t* g_launch_counter = nullptr;
+
+static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cmuli(double2 a, double s) { return make_double2(-a.y * s, a.x * s); }  // i s a
+
+__device__ __forceinline__ int nrchops(const DevGrid& g, int m, int pad) {
+    int nn = g.NRCHOP + pad - m;
+    return nn < 0 ? 0 : nn;
+}
+
+// ---------------------------------------------------------------- fill/copy
+__global__ void fill_kernel(double2* p, size_t n) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = make_double2(0.0, 0.0);
+}
+void k_fill(double2* p, size_t n, cudaStream_t s) {
+    if (!n) return;
+    fill_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n);
+    count_launch();
+}
+__global__ void copy_kernel(double2* d, const double2* a, size_t n) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) d[t] = a[t];
+}
+void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s) {
+    if (!n || dst == src) return;
+    copy_kernel<<<nblk(n, 256), 256, 0, s>>>(dst, src, n);
+    count_launch();
+}
+
+// CHOPDO on FFF (mod_scalar3.f90:227-234): rows n >= NRCHOPS(m) -> 0.
+__global__ void chopdo_fff_kernel(DevGrid g, double2* a, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    if (n >= nrchops(g, m, pad) || m >= g.NTCHOP) a[t] = make_double2(0.0, 0.0);
+}
+void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s) {
+    size_t n = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    chopdo_fff_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, pad);
+    count_launch();
+}
+
+// ------------------------------------------------------------ band operators
+// DELSQH: b = -n(n+1)/L^2 a for n < NN; b(0,0,0) = LN/L^2/NORM(1,1).
+__global__ void delsqh_kernel(DevGrid g, const double2* a, const double* ln, double2* b, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    double2 v = make_double2(0.0, 0.0);
+    if (n < nrchops(g, m, pad)) {
+        int N = m + n;
+        v = cscale(a[t], -(double)(N * (N + 1)) / g.ELL2);
+    }
+    if (m == 0 && n == 0 && k == 0) v = make_double2((ln ? *ln : 0.0) / g.ELL2 / g.norm0[0], 0.0);
+    b[t] = v;
+}
+void k_delsqh(const DevGrid& g, const double2* a, const double* ln_a, double2* b, int pad, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    delsqh_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, ln_a, b, pad);
+    count_launch();
+}
+
+// IDELSQH (mod_legops.f90:136-241) without the log-term/far-field steps
+// (done by k_ln / k_farfield_fix): a = -b L^2/(n(n+1)), a(n=0,m=0) = 0.
+__global__ void idelsqh_kernel(DevGrid g, const double2* b, double2* a, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    double2 v = make_double2(0.0, 0.0);
+    int N = m + n;
+    if (n < nrchops(g, m, pad) && N != 0) v = cscale(b[t], -(g.ELL2 / (double)(N * (N + 1))));
+    a[t] = v;
+}
+void k_idelsqh(const DevGrid& g, const double2* b, double2* a, int pad, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    idelsqh_kernel<<<nblk(n, 256), 256, 0, s>>>(g, b, a, pad);
+    count_launch();
+}
+
+// Tri-band apply: which 0 = XXDX (diag 0), 1 = MULXM (diag 1).
+__global__ void band3_kernel(DevGrid g, const double2* a, double2* b, int which, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    int nn = nrchops(g, m, pad);
+    double2 v = make_double2(0.0, 0.0);
+    if (n < nn) {
+        const double* tb = (which == 0 ? g.xxdx : g.xm) + ((size_t)m * g.NB + n) * 2;
+        const double2* col = a + ((size_t)m * g.NRCHOPDIM) * g.NXCHOPDIM + k;
+        if (which == 1) v = col[(size_t)n * g.NXCHOPDIM];
+        if (n >= 1) {
+            double2 am = col[(size_t)(n - 1) * g.NXCHOPDIM];
+            v.x += tb[0] * am.x;
+            v.y += tb[0] * am.y;
+        }
+        if (n + 1 < nn) {
+            double2 ap = col[(size_t)(n + 1) * g.NXCHOPDIM];
+            v.x += tb[1] * ap.x;
+            v.y += tb[1] * ap.y;
+        }
+    }
+    b[t] = v;
+}
+void k_band3(const DevGrid& g, const double2* a, double2* b, int which, int pad, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    band3_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, b, which, pad);
+    count_launch();
+}
+
+// DEL2 without the log-term rows: b = DEL2H_m a - k^2 a (penta band).
+__global__ void del2_kernel(DevGrid g, const double2* a, double2* b, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    int nn = nrchops(g, m, pad);
+    double2 v = make_double2(0.0, 0.0);
+    if (n < nn) {
+        const double* tb = g.del2h + ((size_t)m * g.NB + n) * 5;
+        const double2* col = a + ((size_t)m * g.NRCHOPDIM) * g.NXCHOPDIM + k;
+        for (int d = 0; d < 5; ++d) {
+            int j = n + d - 2;
+            if (j < 0 || j >= nn) continue;
+            double2 aj = col[(size_t)j * g.NXCHOPDIM];
+            v.x += tb[d] * aj.x;
+            v.y += tb[d] * aj.y;
+        }
+        double k2 = g.ak[k] * g.ak[k];
+        double2 an = col[(size_t)n * g.NXCHOPDIM];
+        v.x -= k2 * an.x;
+        v.y -= k2 * an.y;
+    }
+    b[t] = v;
+}
+void k_del2(const DevGrid& g, const double2* a, double2* b, int pad, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    del2_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, b, pad);
+    count_launch();
+}
+
+// Log-term rows of the (m,k) = (0,0) line:
+//  which 0 (XXDX, 742-745):  b0 += LN/N0, b1 += LN/N1
+//  which 1 (DEL2, 813-817):  b0 += 4/3 LN/L2/N0, b1 -= 2 LN/L2/N1, b2 += 2/3 LN/L2/N2
+//  which 2 (IHELM, 1249-1255): b0 -= LN 4/3/L2/N0, b1 -= LN (-2/N1/L2), b2 -= LN (2/3/N2/L2)
+// coef multiplies LN first (used for the IHELM LN = -B%LN/ALP form).
+__global__ void logterm_kernel(DevGrid g, double2* b, const double* lnp, int which, double coef) {
+    double ln = (*lnp) * coef;
+    const double* n0 = g.norm0;
+    size_t st = g.NXCHOPDIM;  // row stride of the (m=0) column
+    if (which == 0) {
+        b[0].x += ln / n0[0];
+        b[st].x += ln / n0[1];
+    } else if (which == 1) {
+        b[0].x += 4.0 / 3 * ln / g.ELL2 / n0[0];
+        b[st].x -= 2.0 * ln / g.ELL2 / n0[1];
+        b[2 * st].x += 2.0 / 3 * ln / g.ELL2 / n0[2];
+    } else {
+        b[0].x -= ln * (4.0 / 3 / g.ELL2) / n0[0];
+        b[st].x -= ln * (-2 / n0[1] / g.ELL2);
+        b[2 * st].x -= ln * (+2.0 / 3 / n0[2] / g.ELL2);
+    }
+}
+void k_logterm_rows(const DevGrid& g, double2* b, const double* ln, int which, double coef, cudaStream_t s) {
+    logterm_kernel<<<1, 1, 0, s>>>(g, b, ln, which, coef);
+    count_launch();
+}
+
+// m/k combinations of PC2VEL, PC2VOR and GRAD (rows n < NN, zero beyond):
+//  op 0: i m x + i k y    op 1: -y - m k x    op 2: -i m x + i k y
+//  op 3:  y - k m x       op 4: i m x         op 5: i k x          op 6: -x
+__global__ void mk_kernel(DevGrid g, int op, const double2* x, const double2* y, double2* out, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    double2 v = make_double2(0.0, 0.0);
+    if (n < nrchops(g, m, pad)) {
+        double mv = (double)m, kv = g.ak[k];
+        double2 xv = x ? x[t] : make_double2(0.0, 0.0);
+        double2 yv = y ? y[t] : make_double2(0.0, 0.0);
+        switch (op) {
+            case 0: v = cadd(cmuli(xv, mv), cmuli(yv, kv)); break;
+            case 1: v = make_double2(-yv.x - (mv * kv) * xv.x, -yv.y - (mv * kv) * xv.y); break;
+            case 2: v = cadd(cmuli(xv, -mv), cmuli(yv, kv)); break;
+            case 3: v = make_double2(yv.x - (kv * mv) * xv.x, yv.y - (kv * mv) * xv.y); break;
+            case 4: v = cmuli(xv, mv); break;
+            case 5: v = cmuli(xv, kv); break;
+            default: v = make_double2(-xv.x, -xv.y); break;
+        }
+    }
+    out[t] = v;
+}
+void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, double2* out, int pad,
+                  cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    mk_kernel<<<nblk(n, 256), 256, 0, s>>>(g, op, x, y, out, pad);
+    count_launch();
+}
+
+// a(n=0, m=0, k) -= sum_{n < nr_sum} AT1(n) a(n, 0, k) / AT1(0)   (CALCAT1 fix)
+__global__ void farfield_kernel(DevGrid g, double2* a, int nr_sum) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.NXCHOPDIM) return;
+    double sx = 0.0, sy = 0.0;
+    for (int n = 0; n < nr_sum; ++n) {
+        double2 v = a[(size_t)n * g.NXCHOPDIM + k];
+        sx += g.at1[n] * v.x;
+        sy += g.at1[n] * v.y;
+    }
+    a[k].x -= sx / g.at1[0];
+    a[k].y -= sy / g.at1[0];
+}
+void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s) {
+    farfield_kernel<<<nblk(g.NXCHOPDIM, 128), 128, 0, s>>>(g, a, nr_sum);
+    count_launch();
+}
+
+// VEL2PLN (mod_legops.f90:2277-2339) on the (m,k) = (0,0) radial line of a PFF
+// field.  mode 0: PSI%LN <- extracted value; mode 1: PSI%LN <- ln.
+// explog0 (= exp(LOGNORM(:,1))) is passed as g.norm0's sibling table.
+__global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in,
+                               const double* explog0, int nn) {
+    extern __shared__ double sh[];
+    double* be = sh;             // [NRH]
+    double* bo = sh + g.NRH;     // [NRH]
+    double* part = bo + g.NRH;   // [blockDim]
+    const size_t st = g.NXCHOPDIM;  // PFF row stride for m = 0 ([0][r][k])
+    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
+        double lo = rup[(size_t)i * st].x, hi = rup[(size_t)(g.NR - 1 - i) * st].x;
+        be[i] = (lo + hi) * g.w[i];
+        bo[i] = (lo - hi) * g.w[i];
+    }
+    __syncthreads();
+    const double* pf = g.pf;  // m = 0 slice: [n][i]
+    double acc = 0.0;
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
+        const double* src = (n % 2 == 0) ? be : bo;
+        double s = 0.0;
+        for (int i = 0; i < g.NRH; ++i) s += src[i] * pf[(size_t)n * g.NRH + i];
+        acc += s * explog0[n];
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    double pln = -part[0] / 2.0;
+    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
+        double e2 = -pf[i] * pln / g.norm0[0];
+        double o2 = -pf[(size_t)g.NRH + i] * pln / g.norm0[1];
+        rup[(size_t)i * st].x -= (e2 + o2);
+        rup[(size_t)(g.NR - 1 - i) * st].x -= (e2 - o2);
+    }
+    if (threadIdx.x == 0) *psi_ln = (mode == 1) ? ln_in : pln;
+}
+void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
+                    const double* explog0, int nn, cudaStream_t s) {
+    size_t sm = (2 * g.NRH + 128) * sizeof(double);
+    vel2pln_kernel<<<1, 128, sm, s>>>(g, rup_pff, psi_ln, mode, ln, explog0, nn);
+    count_launch();
+}
+
+// ------------------------------------------------------------ pointwise PPP
+// VPRODSUB + VDOTPSUB (+ linear terms of CALC_BOUSSI_FORCE when linear = 1).
+__global__ void force_pointwise_kernel(int nr, int plane, const double* rad, double2* rur, double2* rup,
+                                       double2* uz, double2* ror, double2* rop, double2* oz,
+                                       const double2* rbr, const double2* rbp, const double2* bz,
+                                       double2* bn, const double2* bphys, double omega, double bv0,
+                                       int linear) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)nr * plane;
+    if (t >= total) return;
+    int r = (int)(t / plane);
+    double rr = rad[r];
+    double r2 = rr * rr;
+    double2 a1 = rur[t], a2 = rup[t], a3 = uz[t];
+    double2 b1 = ror[t], b2 = rop[t], b3 = oz[t];
+    double2 c1 = rbr[t], c2 = rbp[t], c3 = bz[t];
+    double2 nr_ = make_double2(a2.x * b3.x - a3.x * b2.x, a2.y * b3.y - a3.y * b2.y);
+    double2 np_ = make_double2(a3.x * b1.x - a1.x * b3.x, a3.y * b1.y - a1.y * b3.y);
+    double2 nz_ = make_double2((a1.x * b2.x - a2.x * b1.x) / r2, (a1.y * b2.y - a2.y * b1.y) / r2);
+    double2 d = make_double2((a1.x * c1.x + a2.x * c2.x) / r2 + a3.x * c3.x,
+                             (a1.y * c1.y + a2.y * c2.y) / r2 + a3.y * c3.y);
+    double2 bnv = make_double2(-d.x, -d.y);
+    if (linear) {
+        double2 bp = bphys[t];
+        nr_.x += 2 * omega * a2.x;
+        nr_.y += 2 * omega * a2.y;
+        np_.x -= 2 * omega * a1.x;
+        np_.y -= 2 * omega * a1.y;
+        nz_.x -= bp.x;
+        nz_.y -= bp.y;
+        double n2 = bv0 * bv0;
+        bnv.x += n2 * a3.x;
+        bnv.y += n2 * a3.y;
+    }
+    ror[t] = nr_;
+    rop[t] = np_;
+    oz[t] = nz_;
+    bn[t] = bnv;
+}
+void k_force_pointwise(const DevGrid& g, double2* rur, double2* rup, double2* uz, double2* ror,
+                       double2* rop, double2* oz, const double2* rbr, const double2* rbp,
+                       const double2* bz, double2* bn, const double2* bphys, double omega,
+                       double bv0, int linear, cudaStream_t s) {
+    size_t n = (size_t)g.NR * g.NX * g.NTH;
+    force_pointwise_kernel<<<nblk(n, 256), 256, 0, s>>>(g.NR, g.NX * g.NTH, g.r, rur, rup, uz, ror,
+                                                        rop, oz, rbr, rbp, bz, bn, bphys, omega, bv0,
+                                                        linear);
+    count_launch();
+}
+
+// ------------------------------------------------------------ FFF updates
+// y = c*y + a*x1 + b*x2  (x2 may be null)
+__global__ void axpby_kernel(double2* y, double a, const double2* x1, double b, const double2* x2,
+                             double c, size_t n) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double2 v = make_double2(0.0, 0.0);
+    if (c != 0.0) v = cscale(y[t], c);
+    if (x1) {
+        double2 u = x1[t];
+        v.x += a * u.x;
+        v.y += a * u.y;
+    }
+    if (x2) {
+        double2 u = x2[t];
+        v.x += b * u.x;
+        v.y += b * u.y;
+    }
+    y[t] = v;
+}
+void k_axpby(double2* y, double a, const double2* x1, double b, const double2* x2, double c, size_t n,
+             cudaStream_t s) {
+    axpby_kernel<<<nblk(n, 256), 256, 0, s>>>(y, a, x1, b, x2, c, n);
+    count_launch();
+}
+__global__ void ln_axpby_kernel(double* y, double a, const double* x1, double b, const double* x2, double c) {
+    double v = (c != 0.0) ? c * (*y) : 0.0;
+    if (x1) v += a * (*x1);
+    if (x2) v += b * (*x2);
+    *y = v;
+}
+void k_ln_axpby(double* y, double a, const double* x1, double b, const double* x2, double c, cudaStream_t s) {
+    ln_axpby_kernel<<<1, 1, 0, s>>>(y, a, x1, b, x2, c);
+    count_launch();
+}
+__global__ void ln_set_kernel(double* y, double v) { *y = v; }
+void k_ln_set(double* y, double v, cudaStream_t s) {
+    ln_set_kernel<<<1, 1, 0, s>>>(y, v);
+    count_launch();
+}
+__global__ void ln_copy_kernel(double* y, const double* x, double sc) { *y = (*x) * sc; }
+void k_ln_copy(double* y, const double* x, double scale, cudaStream_t s) {
+    ln_copy_kernel<<<1, 1, 0, s>>>(y, x, scale);
+    count_launch();
+}
+
+// ETD update per FFF coefficient (CALC_BOUSSI_ETDFE_SUB 948-1047 with ab2 = 0,
+// CALC_BOUSSI_ETDAB_SUB 1050-1139 with ab2 = 1).  E, NL: real parts, row-major 4x4.
+__global__ void etd_kernel(DevGrid g, const double* Em, const double* Nm, double dt, int ab2,
+                           double2* rur, double2* rup, double2* uz, double2* b, const double2* rnr,
+                           const double2* rnp, const double2* nz, const double2* nb, const double2* hr,
+                           const double2* hp, const double2* hz, const double2* onr,
+                           const double2* onp, const double2* onz, const double2* onb) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    double E[16], N[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        E[q] = Em[q];
+        N[q] = Nm[q];
+    }
+    if (k == 0) {
+        for (int q = 0; q < 4; ++q) {
+            E[q] = 0.0;
+            E[4 + q] = 0.0;
+            N[q] = 0.0;
+            N[4 + q] = 0.0;
+        }
+        E[0] = 1.0;
+        E[5] = 1.0;
+        N[0] = dt;
+        N[5] = dt;
+    }
+    double2 ev[4], av[4];
+    if (ab2) {
+        double notm0 = (m == 0) ? 0.0 : 1.0, notk0 = (k == 0) ? 0.0 : 1.0;
+        ev[0] = csub(rur[t], hr[t]);
+        ev[1] = csub(rup[t], cscale(hp[t], notm0));
+        ev[2] = csub(uz[t], cscale(hz[t], notk0));
+        ev[3] = b[t];
+        av[0] = csub(cscale(rnr[t], 1.5), cscale(onr[t], 0.5));
+        av[1] = csub(cscale(rnp[t], 1.5), cscale(onp[t], 0.5));
+        av[2] = csub(cscale(nz[t], 1.5), cscale(onz[t], 0.5));
+        av[3] = csub(cscale(nb[t], 1.5), cscale(onb[t], 0.5));
+    } else {
+        ev[0] = rur[t];
+        ev[1] = rup[t];
+        ev[2] = uz[t];
+        ev[3] = b[t];
+        av[0] = rnr[t];
+        av[1] = rnp[t];
+        av[2] = nz[t];
+        av[3] = nb[t];
+    }
+    double2 cv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double2 a = make_double2(0.0, 0.0), c = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a.x += E[i * 4 + j] * ev[j].x;
+            a.y += E[i * 4 + j] * ev[j].y;
+            c.x += N[i * 4 + j] * av[j].x;
+            c.y += N[i * 4 + j] * av[j].y;
+        }
+        cv[i] = cadd(a, c);
+    }
+    rur[t] = cv[0];
+    rup[t] = cv[1];
+    uz[t] = cv[2];
+    b[t] = cv[3];
+}
+void k_etd(const DevGrid& g, const double* E, const double* NL, double dt, int ab2, double2* rur,
+           double2* rup, double2* uz, double2* b, const double2* rnr, const double2* rnp,
+           const double2* nz, const double2* nb, const double2* hr, const double2* hp, const double2* hz,
+           const double2* onr, const double2* onp, const double2* onz, const double2* onb, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    etd_kernel<<<nblk(n, 256), 256, 0, s>>>(g, E, NL, dt, ab2, rur, rup, uz, b, rnr, rnp, nz, nb, hr, hp,
+                                            hz, onr, onp, onz, onb);
+    count_launch();
+}
+
+// HYPERV3 / CALC_BOUSSI_ETD_HYPERV filter (mod_march.f90:3521-3560, 1388-1408)
+// followed by CHOPDO at pad.  hr: [NRCHOP][NTCHOPDIM] (column-major as HYPER_R).
+__global__ void hyperv_kernel(DevGrid g, double2* a, const double* hr, const double* ht, const double* hx,
+                              double tf, int pad) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return;
+    int k = (int)(t % g.NXCHOPDIM);
+    int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    if (n < nrchops(g, m, pad)) {
+        double f = hr[(size_t)m * g.NRCHOP + n] * ht[m] * hx[k];
+        if (tf != 1.0) f = pow(f, tf);
+        a[t] = cscale(a[t], f);
+    } else {
+        a[t] = make_double2(0.0, 0.0);
+    }
+}
+void k_hyperv(const DevGrid& g, double2* a, const double* hr, const double* ht, const double* hx, double tf,
+              int pad, cudaStream_t s) {
+    size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    hyperv_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, hr, ht, hx, tf, pad);
+    count_launch();
+}
+
+__global__ void finite_kernel(const double2* a, size_t n, int* flag) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double2 v = a[t];
+    if (!isfinite(v.x) || !isfinite(v.y)) atomicOr(flag, 1);
+}
+void k_finite(const double2* a, size_t n, int* flag, cudaStream_t s) {
+    finite_kernel<<<nblk(n, 256), 256, 0, s>>>(a, n, flag);
+    count_launch();
+}
+
+// ------------------------------------------------------ layout conversions
+// ref index (Fortran column-major) -> device index, or -1 for padding.
+__device__ __forceinline__ long long ref_to_dev(const DevGrid& g, int space, size_t t) {
+    int ndimr = g.NR + 3, ndimth = g.NTH + 1;
+    if (space == MLEGS_FFF) {
+        int n = (int)(t % g.NRCHOPDIM);
+        int m = (int)((t / g.NRCHOPDIM) % g.NTCHOPDIM);
+        int k = (int)(t / ((size_t)g.NRCHOPDIM * g.NTCHOPDIM));
+        return ((long long)m * g.NRCHOPDIM + n) * g.NXCHOPDIM + k;
+    }
+    if (space == MLEGS_PFF) {
+        int r = (int)(t % ndimr);
+        int m = (int)((t / ndimr) % g.NTCHOPDIM);
+        int k = (int)(t / ((size_t)ndimr * g.NTCHOPDIM));
+        if (r >= g.NR) return -1;
+        return ((long long)m * g.NR + r) * g.NXCHOPDIM + k;
+    }
+    int r = (int)(t % ndimr);
+    int j = (int)((t / ndimr) % ndimth);
+    int z = (int)(t / ((size_t)ndimr * ndimth));
+    if (r >= g.NR) return -1;
+    if (space == MLEGS_PFP) {
+        if (j >= g.NTCHOPDIM) return -1;
+        return ((long long)r * g.NX + z) * g.NTCHOPDIM + j;
+    }
+    if (j >= g.NTH) return -1;
+    return ((long long)r * g.NX + z) * g.NTH + j;
+}
+__global__ void from_ref_kernel(DevGrid g, int space, const double2* ref, double2* dev, size_t n) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    long long d = ref_to_dev(g, space, t);
+    if (d >= 0) dev[d] = ref[t];
+}
+__global__ void to_ref_kernel(DevGrid g, int space, const double2* dev, double2* ref, size_t n) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    long long d = ref_to_dev(g, space, t);
+    ref[t] = (d >= 0) ? dev[d] : make_double2(0.0, 0.0);
+}
+static size_t ref_elems(const DevGrid& g, int space) {
+    size_t ndimr = g.NR + 3, ndimth = g.NTH + 1;
+    if (space == MLEGS_FFF) return (size_t)g.NRCHOPDIM * g.NTCHOPDIM * g.NXCHOPDIM;
+    if (space == MLEGS_PFF) return ndimr * g.NTCHOPDIM * g.NXCHOPDIM;
+    return ndimr * ndimth * g.NX;
+}
+void k_from_ref(const DevGrid& g, int space, const double2* ref, double2* dev, cudaStream_t s) {
+    size_t n = ref_elems(g, space);
+    from_ref_kernel<<<nblk(n, 256), 256, 0, s>>>(g, space, ref, dev, n);
+    count_launch();
+}
+void k_to_ref(const DevGrid& g, int space, const double2* dev, double2* ref, cudaStream_t s) {
+    size_t n = ref_elems(g, space);
+    to_ref_kernel<<<nblk(n, 256), 256, 0, s>>>(g, space, dev, ref, n);
+    count_launch();
+}
+
+}  // namespace mlegs

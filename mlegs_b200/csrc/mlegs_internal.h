@@ -1,0 +1,154 @@
+// Internal declarations of the B200 MLegS library (not part of the C ABI).
+//
+// Device layouts (0-based, all complex values are double2 = (re, im)):
+//   FFF  [m][n][k]  (NTCHOPDIM, NRCHOPDIM, NXCHOPDIM)   k fastest
+//   PFF  [m][r][k]  (NTCHOPDIM, NR,        NXCHOPDIM)
+//   PFP  [r][z][m]  (NR,        NX,        NTCHOPDIM)
+//   PPP  [r][z][j]  (NR,        NX,        NTH)  packed samples: re -> theta_{2j},
+//                                                 im -> theta_{2j+1} (mod_fft.f90:844-848)
+// The reference's zero padding (rows NR+1..NR+3, theta column NTH+1, chopped
+// m/k) is not stored; upload/download map to and from the Fortran layout.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mlegs_b200.h"
+
+namespace mlegs {
+
+struct Dims {
+    int NR, NRH, NTH, NX, NRCHOP, NTCHOP, NXCHOP;
+    int NDIMR, NDIMTH, NRCHOPDIM, NTCHOPDIM, NXCHOPDIM, NXCHOPH, NLN;
+    double ELL, ELL2, ZLEN;
+    size_t fff() const { return (size_t)NTCHOPDIM * NRCHOPDIM * NXCHOPDIM; }
+    size_t pff() const { return (size_t)NTCHOPDIM * NR * NXCHOPDIM; }
+    size_t pfp() const { return (size_t)NR * NX * NTCHOPDIM; }
+    size_t ppp() const { return (size_t)NR * NX * NTH; }
+    size_t elems(int space) const {
+        switch (space) {
+            case MLEGS_FFF: return fff();
+            case MLEGS_PFF: return pff();
+            case MLEGS_PFP: return pfp();
+            default: return ppp();
+        }
+    }
+    size_t cap() const {
+        size_t c = fff();
+        if (pff() > c) c = pff();
+        if (pfp() > c) c = pfp();
+        if (ppp() > c) c = ppp();
+        return c;
+    }
+};
+
+// Device-side copy of the grid constants passed to kernels by value.
+struct DevGrid {
+    int NR, NRH, NTH, NX, NRCHOP, NTCHOP, NXCHOP;
+    int NRCHOPDIM, NTCHOPDIM, NXCHOPDIM, NLN;
+    double ELL2;
+    const double* x;        // [NR] Gauss-Legendre nodes (ascending)
+    const double* w;        // [NR] weights
+    const double* r;        // [NR] mapped radii
+    const double* lnx;      // [NR] -log(1-x)
+    const double* pf;       // [NTCHOPDIM][NRCHOPDIM+1][NRH]
+    const double* ak;       // [NXCHOPDIM] axial wavenumbers (AK(m,k) is m-independent)
+    const double* norm0;    // [NLN] NORM(:, m=0)
+    const double* at1;      // [NRCHOPDIM] Pbar_n(+1)
+    // band tables per (m, n), n < NRCHOPDIM+1 (row index of the band):
+    const double* xxdx;     // [NTCHOPDIM][NB][2]  (sub, super)
+    const double* xm;       // [NTCHOPDIM][NB][2]  (sub, super)     diag = 1
+    const double* del2h;    // [NTCHOPDIM][NB][5]
+    int NB;                 // NRCHOPDIM + 2
+};
+
+struct Field {
+    double2* data = nullptr;   // current buffer (capacity Dims::cap())
+    double2* home = nullptr;   // buffer owned at allocation time
+    double* ln = nullptr;      // device scalar LN (mod_scalar3.f90:43)
+    int space = MLEGS_FFF;
+    int slot = -1;
+    bool persistent = false;
+};
+
+// Kernel launch helpers (kernels.cu, fft.cu, gemm.cu, solve.cu, tables.cu).
+void k_tables_gauss(double* x, double* w, int n, cudaStream_t s);
+void k_tables_pf(const double* x, double* pf, int nrh, int ne, int ntchopdim, cudaStream_t s);
+void k_tables_project(const DevGrid& g, double* V, double* D, double* T, int pad, cudaStream_t s);
+
+void fft_set_attributes();
+void k_fill(double2* p, size_t n, cudaStream_t s);
+void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s);
+void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s);
+
+// Legendre transforms (FP64 and split-BF16 tensor-core forms).
+void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
+// out[m][n][k] (+)= scale(m,k) * sum_i Wt[m][n][i] * fold(in)(i,k); fold parity per row given by mode
+//   mode 0 (EO): row n even -> even fold, odd -> odd fold;  mode 1 (OE): swapped
+//   scale: 0 -> 1, 1 -> -1, 2 -> -i m, 3 -> i k, 4 -> m k
+void k_fold_gemm(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out,
+                 int mode, int scale, int accumulate, int pad, cudaStream_t s);
+
+// FFTs.
+struct FFTPlan {
+    double2* tw_x = nullptr;     // exp(-2 pi i q / NX), q < NX
+    double2* tw_t = nullptr;     // exp(-2 pi i q / NTH), q < NTH
+    double2* tw_h = nullptr;     // exp(-i pi q / NTH),  q <= NTH (real-FFT post-processing)
+    int lx = 0, lt = 0;          // log2 NX, log2 NTH
+};
+void k_verfft_b(const DevGrid& g, const FFTPlan& p, const double2* pff, double2* pfp, cudaStream_t s);
+void k_verfft_f(const DevGrid& g, const FFTPlan& p, const double2* pfp, double2* pff, cudaStream_t s);
+void k_horfft_b(const DevGrid& g, const FFTPlan& p, const double2* pfp, double2* ppp, cudaStream_t s);
+void k_horfft_f(const DevGrid& g, const FFTPlan& p, const double2* ppp, double2* pfp, cudaStream_t s);
+
+// Spectral operators on FFF.
+void k_delsqh(const DevGrid& g, const double2* a, const double* ln_a, double2* b, int pad, cudaStream_t s);
+void k_idelsqh(const DevGrid& g, const double2* b, double2* a, int pad, cudaStream_t s);
+void k_band3(const DevGrid& g, const double2* a, double2* b, int which /*0 xxdx, 1 xm*/, int pad, cudaStream_t s);
+void k_del2(const DevGrid& g, const double2* a, double2* b, int pad, cudaStream_t s);
+void k_logterm_rows(const DevGrid& g, double2* b, const double* ln, int which, double coef, cudaStream_t s);
+void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, double2* out, int pad, cudaStream_t s);
+void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
+void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
+                    const double* explog0, int nn, cudaStream_t s);
+
+// Banded solves (IDEL2LN, IDEL2, IHELM) with per-system elimination scratch.
+void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln,
+                  double ln_in, const double* b_ln, double* scratch, int pad, cudaStream_t s);
+
+// Pointwise physics in PPP.
+void k_force_pointwise(const DevGrid& g, double2* rur, double2* rup, double2* uz, double2* ror,
+                       double2* rop, double2* oz, const double2* rbr, const double2* rbp,
+                       const double2* bz, double2* bn, const double2* bphys, double omega,
+                       double bv0, int linear, cudaStream_t s);
+
+// FFF-space updates.
+void k_axpby(double2* y, double a, const double2* x1, double b, const double2* x2, double c,
+             size_t n, cudaStream_t s);
+void k_ln_axpby(double* y, double a, const double* x1, double b, const double* x2, double c, cudaStream_t s);
+void k_ln_set(double* y, double v, cudaStream_t s);
+void k_ln_copy(double* y, const double* x, double scale, cudaStream_t s);
+void k_etd(const DevGrid& g, const double* E, const double* NL, double dt, int ab2,
+           double2* rur, double2* rup, double2* uz, double2* b,
+           const double2* rnr, const double2* rnp, const double2* nz, const double2* nb,
+           const double2* hr, const double2* hp, const double2* hz,
+           const double2* onr, const double2* onp, const double2* onz, const double2* onb,
+           cudaStream_t s);
+void k_hyperv(const DevGrid& g, double2* a, const double* hr, const double* ht, const double* hx,
+              double tf, int pad, cudaStream_t s);
+void k_finite(const double2* a, size_t n, int* flag, cudaStream_t s);
+
+// Layout conversion between the reference's Fortran arrays and device layouts.
+void k_from_ref(const DevGrid& g, int space, const double2* ref, double2* dev, cudaStream_t s);
+void k_to_ref(const DevGrid& g, int space, const double2* dev, double2* ref, cudaStream_t s);
+
+extern thread_local int64_t* g_launch_counter;
+inline void count_launch() {
+    if (g_launch_counter) ++(*g_launch_counter);
+}
+
+}  // namespace mlegs

@@ -1,0 +1,198 @@
+// Batched banded solves of the Laplacian / Helmholtz operators, FP64.
+//
+// Restates the per-(m,k) systems of mod_legops.f90 IDEL2LN (1013-1176),
+// IDEL2 (823-1010) and IHELM (1204-1354), factored without pivoting as
+// LUDCMPB/LUBKSBB do (mod_bandmat.f90:65-155, 320-401).  One thread owns one
+// (m, k) system: it builds each band row on the fly from the DEL2H/XM
+// coefficient tables, eliminates its sub-diagonal entries against the
+// previous pivot rows (kept in registers), writes the resulting U row to a
+// scratch array laid out [row][entry][system] (coalesced across threads),
+// and back-substitutes in place.  Band entries that reach past the system's
+// size are dropped, which is BANDAUX's truncation of each leading block.
+//
+//  kind 0  IDEL2LN: m = 0 systems carry the log-term column (k = 0), 5-band
+//  kind 1  IDEL2:   m = 0 uses the 7-band row-shifted system (k = 0: row 0 is
+//                   the log-term boundary condition)
+//  kind 2  IHELM:   m = 0 solves (H XM) y = rhs on NN-1 rows, A = XM y
+#include "mlegs_internal.h"
+
+namespace mlegs {
+
+namespace {
+constexpr int MAXW = 7;  // band width bound (7-band m = 0 systems)
+}
+
+struct BandRowCtx {
+    const double* del2h;  // [NB][5] for this m
+    const double* xm;     // [NB][2] for this m (m = 0 only)
+    double shift;         // k^2 + alpha
+    int kind, m, k;
+    double l0, l1, l2;    // log-term column entries (IDEL2LN / IDEL2 at m = k = 0)
+};
+
+// Entry (row, col) of the original DEL2H - shift operator (with the log column).
+__device__ __forceinline__ double del2_entry(const BandRowCtx& c, int row, int col) {
+    int d = col - row;
+    if (d < -2 || d > 2 || row < 0 || col < 0) return 0.0;
+    double v = c.del2h[(size_t)row * 5 + (d + 2)];
+    if (d == 0) v -= c.shift;
+    if (col == 0 && (c.kind == 0 || c.kind == 1) && c.m == 0 && c.k == 0) {
+        if (row == 0) v += c.l0;
+        else if (row == 1) v += c.l1;
+        else if (row == 2) v += c.l2;
+    }
+    return v;
+}
+
+// Row `row` of the system matrix, as entries at columns row-3..row+3 (w[0..6]).
+__device__ __forceinline__ void build_row(const BandRowCtx& c, int row, double* w) {
+#pragma unroll
+    for (int q = 0; q < MAXW; ++q) w[q] = 0.0;
+    if (c.m != 0 || c.kind == 0) {
+        for (int d = -2; d <= 2; ++d) w[d + 3] = del2_entry(c, row, row + d);
+        return;
+    }
+    if (c.kind == 1) {
+        if (c.k != 0) {
+            for (int d = -2; d <= 2; ++d) w[d + 3] = del2_entry(c, row, row + d);
+        } else if (row == 0) {
+            w[3] = 1.0;
+        } else {
+            // new row r = original row r-1 over the same columns
+            for (int col = row - 3; col <= row + 1; ++col)
+                if (col >= 0) w[col - row + 3] = del2_entry(c, row - 1, col);
+        }
+        return;
+    }
+    // kind 2, m = 0: (H XM)(row, col) = sum_l H(row, l) XM(l, col)
+    for (int l = row - 2; l <= row + 2; ++l) {
+        if (l < 0) continue;
+        double h = del2_entry(c, row, l);
+        if (h == 0.0) continue;
+        const double* x = c.xm + (size_t)l * 2;
+        // XM(l, l-1) = sub(l), XM(l, l) = 1, XM(l, l+1) = super(l)
+        if (l - 1 >= 0) w[(l - 1) - row + 3] += h * x[0];
+        w[l - row + 3] += h;
+        w[(l + 1) - row + 3] += h * x[1];
+    }
+}
+
+__global__ void solve_kernel(DevGrid g, double2* A, double* ln_out, int kind, double alp, int has_ln,
+                             double ln_in, const double* b_ln, double* scratch, int pad) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nsys) return;
+    const int k = t % g.NXCHOPDIM;
+    const int m = t / g.NXCHOPDIM;
+    int nn = g.NRCHOP + pad - m;
+    if (nn < 0) nn = 0;
+    BandRowCtx c;
+    c.del2h = g.del2h + (size_t)m * g.NB * 5;
+    c.xm = g.xm + (size_t)m * g.NB * 2;
+    c.shift = g.ak[k] * g.ak[k] + ((kind == 2) ? alp : 0.0);
+    c.kind = kind;
+    c.m = m;
+    c.k = k;
+    c.l0 = 4.0 / 3 / g.ELL2;
+    c.l1 = -2 * g.norm0[0] / g.norm0[1] / g.ELL2;
+    c.l2 = 2.0 / 3 * g.norm0[0] / g.norm0[2] / g.ELL2;
+    int lo = 2, up = 2;
+    if (m == 0 && kind != 0) {
+        lo = 3;
+        up = 3;
+    }
+    int size = (m == 0 && kind == 2) ? nn - 1 : nn;
+    double2* col = A + (size_t)m * g.NRCHOPDIM * g.NXCHOPDIM + k;
+    const size_t st = g.NXCHOPDIM;
+    if (size <= 0) return;
+    // IDEL2 (m = 0, k = 0): shift the rhs down one row, row 0 <- LN BC (929-936)
+    if (kind == 1 && m == 0 && k == 0) {
+        for (int r = size - 1; r >= 1; --r) col[(size_t)r * st] = col[(size_t)(r - 1) * st];
+        col[0] = make_double2(has_ln ? ln_in / g.norm0[0] : 0.0, 0.0);
+    }
+    // forward elimination; window of the last 3 pivot rows (U entries d = 0..up)
+    double U[3][4];
+    double2 R[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        R[a] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) U[a][b] = 0.0;
+    }
+    for (int r = 0; r < size; ++r) {
+        double w[MAXW];
+        build_row(c, r, w);
+        double2 rhs = col[(size_t)r * st];
+        // eliminate columns r-lo .. r-1 (left to right)
+        for (int d = lo; d >= 1; --d) {
+            int cidx = r - d;
+            if (cidx < 0) continue;
+            const double* u = U[(cidx) % 3];
+            double f = w[3 - d] / u[0];
+            w[3 - d] = 0.0;
+            for (int j = 1; j <= up; ++j) {
+                int q = 3 - d + j;
+                if (q < MAXW) w[q] -= f * u[j];
+            }
+            double2 pr = R[cidx % 3];
+            rhs.x -= f * pr.x;
+            rhs.y -= f * pr.y;
+        }
+        double* u = U[r % 3];
+        u[0] = w[3];
+        for (int j = 1; j <= 3; ++j) u[j] = (j <= up) ? w[3 + j] : 0.0;
+        R[r % 3] = rhs;
+        for (int j = 0; j <= 3; ++j) scratch[((size_t)r * 4 + j) * nsys + t] = u[j];
+        col[(size_t)r * st] = rhs;
+    }
+    // back substitution
+    double2 x1 = make_double2(0.0, 0.0), x2 = x1, x3 = x1;  // x[r+1], x[r+2], x[r+3]
+    for (int r = size - 1; r >= 0; --r) {
+        double2 v = col[(size_t)r * st];
+        double u1 = scratch[((size_t)r * 4 + 1) * nsys + t];
+        double u2 = scratch[((size_t)r * 4 + 2) * nsys + t];
+        double u3 = scratch[((size_t)r * 4 + 3) * nsys + t];
+        double u0 = scratch[((size_t)r * 4 + 0) * nsys + t];
+        if (r + 1 < size) { v.x -= u1 * x1.x; v.y -= u1 * x1.y; }
+        if (r + 2 < size) { v.x -= u2 * x2.x; v.y -= u2 * x2.y; }
+        if (r + 3 < size) { v.x -= u3 * x3.x; v.y -= u3 * x3.y; }
+        v.x /= u0;
+        v.y /= u0;
+        col[(size_t)r * st] = v;
+        x3 = x2;
+        x2 = x1;
+        x1 = v;
+    }
+    if (m == 0 && kind == 2) {
+        // A(NN) = 0; A(:NN) = XM(:NN) y  (1310-1316)
+        col[(size_t)(nn - 1) * st] = make_double2(0.0, 0.0);
+        double2 prev = make_double2(0.0, 0.0);
+        for (int r = 0; r < nn; ++r) {
+            double2 cur = col[(size_t)r * st];
+            double2 nxt = (r + 1 < nn) ? col[(size_t)(r + 1) * st] : make_double2(0.0, 0.0);
+            const double* x = c.xm + (size_t)r * 2;
+            double2 v = cur;
+            if (r >= 1) { v.x += x[0] * prev.x; v.y += x[0] * prev.y; }
+            if (r + 1 < nn) { v.x += x[1] * nxt.x; v.y += x[1] * nxt.y; }
+            col[(size_t)r * st] = v;
+            prev = cur;
+        }
+    }
+    if (m == 0 && k == 0) {
+        if (kind == 0) {
+            *ln_out = col[0].x * g.norm0[0];
+            col[0] = make_double2(0.0, 0.0);
+        } else if (kind == 1 && has_ln) {
+            *ln_out = col[0].x * g.norm0[0];
+        }
+    }
+}
+
+void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln, double ln_in,
+                  const double* b_ln, double* scratch, int pad, cudaStream_t s) {
+    int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    solve_kernel<<<(nsys + 127) / 128, 128, 0, s>>>(g, a, ln_out, kind, alp, has_ln, ln_in, b_ln, scratch, pad);
+    count_launch();
+}
+
+}  // namespace mlegs

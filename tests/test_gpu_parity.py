@@ -1,0 +1,326 @@
+"""GPU parity of every hot-path operator against the oracle, through the C ABI.
+
+FP64 GPU path vs FP64 oracle: per-operator relative error (max|d|/max|ref|)
+below 1e-12 (transforms, band operators, projection) and 1e-10 for the
+banded solves; whole steps below 1e-9 per field after the stated number of
+steps (the north_star tolerance).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import oracle_grid, oracle_physics, random_fff, rel, small_cfg
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module", params=[(32, 16, 16), (64, 32, 32)], ids=["32x16x16", "64x32x32"])
+def env(request, lib_built):
+    import mlegs_b200 as M
+    cfg = small_cfg(*request.param)
+    ctx = M.Context(cfg)
+    g = oracle_grid(cfg)
+    yield M, ctx, g, cfg
+    ctx.close()
+
+
+def up(ctx, F, space=None):
+    import mlegs_b200 as M
+    f = ctx.field(M.FFF if space is None else space)
+    f.upload(F.E, F.LN, F.space)
+    return f
+
+
+def test_grid_tables(env):
+    M, ctx, g, cfg = env
+    x, w, r = ctx.grid()
+    assert np.abs(x - g.X).max() < 5e-15
+    assert rel(w, g.W) < 5e-14
+    assert rel(r, g.R) < 1e-13
+
+
+@pytest.mark.parametrize("pad", [0, 3])
+def test_rtran_forward(env, pad):
+    from oracle import transforms as T
+    M, ctx, g, cfg = env
+    A = random_fff(g, 1, pad=pad)
+    A.LN = 0.37
+    f = up(ctx, A)
+    ctx.RTRAN(f, 1, pad)
+    g.chopset(pad)
+    T.rtran(g, A, 1)
+    g.chopset(-pad)
+    E, ln = f.download()
+    assert f.space == M.PFF and ln == 0.0
+    assert rel(E, A.E) < TOL
+
+
+def test_rtran_backward(env):
+    from oracle import transforms as T
+    from oracle.grid import PFF
+    M, ctx, g, cfg = env
+    rng = np.random.default_rng(2)
+    A = g.alloc(PFF)
+    A.E[: g.NR] = rng.standard_normal(A.E[: g.NR].shape) + 1j * rng.standard_normal(A.E[: g.NR].shape)
+    f = up(ctx, A, M.PFF)
+    ctx.RTRAN(f, -1)
+    T.rtran(g, A, -1)
+    E, _ = f.download()
+    assert rel(E, A.E) < TOL
+
+
+def test_verfft_both_ways(env):
+    from oracle import transforms as T
+    from oracle.grid import PFF, PFP
+    M, ctx, g, cfg = env
+    rng = np.random.default_rng(3)
+    A = g.alloc(PFF)
+    A.E[: g.NR] = rng.standard_normal(A.E[: g.NR].shape) + 1j * rng.standard_normal(A.E[: g.NR].shape)
+    f = up(ctx, A, M.PFF)
+    ctx.VERFFT(f, 1)
+    T.verfft(g, A, 1)
+    E, _ = f.download()
+    assert f.space == M.PFP and rel(E, A.E) < TOL
+    ctx.VERFFT(f, -1)
+    T.verfft(g, A, -1)
+    E, _ = f.download()
+    assert rel(E, A.E) < TOL
+
+
+def test_horfft_both_ways(env):
+    from oracle import transforms as T
+    from oracle.grid import PFP
+    M, ctx, g, cfg = env
+    rng = np.random.default_rng(4)
+    A = g.alloc(PFP)
+    sh = (g.NR, g.NTCHOPDIM, g.NX)
+    A.E[: g.NR, : g.NTCHOPDIM, :] = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    f = up(ctx, A, M.PFP)
+    ctx.HORFFT(f, 1)
+    T.horfft(g, A, 1)
+    E, _ = f.download()
+    assert f.space == M.PPP and rel(E, A.E) < TOL
+    ctx.HORFFT(f, -1)
+    T.horfft(g, A, -1)
+    E, _ = f.download()
+    assert rel(E, A.E) < TOL
+
+
+def test_tofp_toff_roundtrip(env):
+    from oracle import transforms as T
+    M, ctx, g, cfg = env
+    A = random_fff(g, 5)
+    f = up(ctx, A)
+    ctx.TOFP(f)
+    B = A.copy()
+    T.tofp(g, B)
+    E, _ = f.download()
+    assert rel(E, B.E) < TOL
+    ctx.TOFF(f)
+    E, _ = f.download()
+    assert rel(E, A.E) < 1e-12
+
+
+@pytest.mark.parametrize("op", ["DELSQH", "XXDX", "MULXM", "DEL2"])
+@pytest.mark.parametrize("pad", [0, 3])
+def test_band_operators(env, op, pad):
+    from oracle import legops as L
+    M, ctx, g, cfg = env
+    A = random_fff(g, 6, pad=0)
+    A.LN = 0.0 if op == "MULXM" else -0.41
+    f = up(ctx, A)
+    out = ctx.field(M.FFF)
+    getattr(ctx, op)(f, out, pad)
+    g.chopset(pad)
+    B = getattr(L, op.lower())(g, A)
+    g.chopset(-pad)
+    E, ln = out.download()
+    assert ln == 0.0
+    assert rel(E, B.E) < TOL
+
+
+def test_idelsqh(env):
+    from oracle import legops as L
+    M, ctx, g, cfg = env
+    A = random_fff(g, 7)
+    f = up(ctx, A)
+    out = ctx.field(M.FFF)
+    ctx.IDELSQH(f, out)
+    B = L.idelsqh(g, A)
+    E, ln = out.download()
+    assert rel(E, B.E) < TOL and abs(ln - B.LN) < 1e-13 * max(1, abs(B.LN))
+
+
+@pytest.mark.parametrize("kind", ["IDEL2LN", "IDEL2", "IDEL2_LN", "IHELM"])
+def test_banded_solves(env, kind):
+    from oracle import legops as L
+    M, ctx, g, cfg = env
+    A = random_fff(g, 8)
+    A.LN = 0.0 if kind != "IHELM" else -0.3
+    f = up(ctx, A)
+    out = ctx.field(M.FFF)
+    if kind == "IDEL2LN":
+        ctx.IDEL2LN(f, out)
+        B = L.idel2ln(g, A)
+    elif kind == "IDEL2":
+        ctx.IDEL2(f, out)
+        B = L.idel2(g, A)
+    elif kind == "IDEL2_LN":
+        ctx.IDEL2(f, out, LN=0.25)
+        B = L.idel2(g, A, LN=0.25)
+    else:
+        ctx.IHELM(f, out, 2000.0)
+        B = L.ihelm(g, A, 2000.0)
+    E, ln = out.download()
+    assert rel(E, B.E) < 1e-10
+    assert abs(ln - B.LN) <= 1e-10 * max(1.0, abs(B.LN))
+
+
+def test_pc2vel_pc2vor_grad(env):
+    from oracle import legops as L
+    M, ctx, g, cfg = env
+    P = random_fff(g, 9)
+    P.LN = -0.5
+    C = random_fff(g, 10)
+    C.LN = 0.2
+    fp, fc = up(ctx, P), up(ctx, C)
+    outs = [ctx.field(M.FFF) for _ in range(3)]
+    g.chopset(3)
+    for name in ("pc2vel", "pc2vor"):
+        getattr(ctx, name.upper())(fp, fc, *outs, 3)
+        ref = getattr(L, name)(g, P, C)
+        for o, r_ in zip(outs, ref):
+            assert rel(o.download()[0], r_.E) < TOL, name
+    ctx.GRAD(fc, *outs, 3)
+    ref = L.grad(g, C)
+    g.chopset(-3)
+    for o, r_ in zip(outs, ref):
+        assert rel(o.download()[0], r_.E) < TOL
+
+
+@pytest.mark.parametrize("mode", ["ppp_ln0", "fff_psi", "pff_none"])
+def test_project(env, mode):
+    from oracle import legops as L
+    from oracle import transforms as T
+    M, ctx, g, cfg = env
+    U = [random_fff(g, 20 + i, decay=4.0) for i in range(3)]
+    if mode == "ppp_ln0":
+        for u in U:
+            T.tofp(g, u)
+        ln = 0.0
+    elif mode == "pff_none":
+        for u in U:
+            T.rtran(g, u, 1)
+        ln = None
+    else:
+        ln = "psi"
+    fs = [up(ctx, u, u.space) for u in U]
+    psi, chi = ctx.field(M.FFF), ctx.field(M.FFF)
+    ctx.PROJECT(*fs, psi, chi, ln)
+    P, W = L.project(g, *U, ln)
+    Ep, lnp = psi.download()
+    Ec, _ = chi.download()
+    assert rel(Ep, P.E) < 1e-11
+    assert rel(Ec, W.E) < 1e-11
+    assert abs(lnp - P.LN) < 1e-12 * max(1.0, abs(P.LN))
+
+
+def test_qvortex_on_device(env):
+    M, ctx, g, cfg = env
+    from oracle import layout
+    psi, chi = M.qvortex(ctx)
+    P, C = layout.qvortex(g)
+    E, ln = psi.download()
+    assert abs(ln + 0.5) < 1e-12
+    assert rel(E, P.E) < 1e-12
+
+
+def test_boussi_force(env):
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    M, ctx, g, cfg = env
+    from mlegs_b200.inputs import buoyancy_perturbation, perturbation_coefficients
+    cs = [perturbation_coefficients(cfg, i) for i in range(3)]
+    P, C, B = layout.initial_state(g, *cs)
+    fp, fc, fb = up(ctx, P), up(ctx, C), up(ctx, B)
+    outs = [ctx.field(M.FFF) for _ in range(3)]
+    ctx.CALC_BOUSSI_FORCE(fp, fc, fb, *outs)
+    ref = BQ.calc_boussi_force(g, oracle_physics(cfg), P, C, B)
+    for o, r_ in zip(outs, ref):
+        E, ln = o.download()
+        assert rel(E, r_.E) < 1e-11
+        assert abs(ln - r_.LN) < 1e-10 * max(1.0, abs(r_.LN))
+
+
+def test_initial_state_matches_oracle(env):
+    from oracle import layout
+    M, ctx, g, cfg = env
+    from mlegs_b200.inputs import perturbation_coefficients
+    cs = [perturbation_coefficients(cfg, i) for i in range(3)]
+    P, C, B = layout.initial_state(g, *cs)
+    fp, fc, fb = M.initial_state(ctx)
+    for f, R in ((fp, P), (fc, C), (fb, B)):
+        E, ln = f.download()
+        assert rel(E, R.E) < 1e-12
+        assert abs(ln - R.LN) < 1e-12
+
+
+def _run_pair(cfg, nsteps, graph=False):
+    import mlegs_b200 as M
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from mlegs_b200.inputs import perturbation_coefficients
+    g = oracle_grid(cfg)
+    cs = [perturbation_coefficients(cfg, i) for i in range(3)]
+    P, C, B = layout.initial_state(g, *cs)
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    for _ in range(nsteps):
+        s.step()
+    ctx = M.Context(cfg)
+    fp, fc, fb = M.initial_state(ctx)
+    ctx.initialize(fp, fc, fb)
+    ctx.step(nsteps, graph=graph)
+    out = [f.download() for f in (fp, fc, fb)]
+    ctx.check_finite()
+    t, n = ctx.time()
+    ctx.close()
+    assert n == nsteps + 1 and abs(t - s.t) < 1e-12
+    return out, (s.psi, s.chi, s.b)
+
+
+@pytest.mark.parametrize("adams", [True, False], ids=["ab2cn", "etd2ab"])
+def test_steps_small(lib_built, adams):
+    cfg = small_cfg(32, 16, 16, adams=adams)
+    out, ref = _run_pair(cfg, 5)
+    for (E, ln), R in zip(out, ref):
+        assert rel(E, R.E) < 1e-10
+        assert abs(ln - R.LN) < 1e-10 * max(1.0, abs(R.LN))
+
+
+def test_ab2_config_100_steps(lib_built):
+    """The AB2-CN IVP configuration, 1 Richardson + 99 AB2 steps, <= 1e-9 per field."""
+    from mlegs_b200.inputs import CONFIGS
+    cfg = CONFIGS["ab2_64x32x32"]
+    out, ref = _run_pair(cfg, 99)
+    for (E, ln), R in zip(out, ref):
+        assert rel(E, R.E) < 1e-9
+        assert abs(ln - R.LN) < 1e-9 * max(1.0, abs(R.LN))
+
+
+@pytest.mark.parametrize("adams", [True, False], ids=["ab2cn", "etd2ab"])
+def test_graph_replay_matches_eager(lib_built, adams):
+    import mlegs_b200 as M
+    cfg = small_cfg(32, 16, 16, adams=adams)
+    res = []
+    for graph in (False, True):
+        ctx = M.Context(cfg)
+        fs = M.initial_state(ctx)
+        ctx.initialize(*fs)
+        ctx.step(4, graph=graph)
+        res.append([f.download() for f in fs])
+        ctx.close()
+    for (E0, l0), (E1, l1) in zip(*res):
+        assert np.array_equal(E0, E1) and l0 == l1

@@ -1,0 +1,177 @@
+"""CPU tests of the oracle against the reference's known answers and golden vectors.
+
+Known answers restated from the reference's own tests and notes:
+  * divxm analytic case (tests/mlegs/divxm_test.f90:79-86): (1-x) Pbar_2 has
+    normalised coefficients (-2/5 N3/N2, 1, -3/5 N3/N4) -> MULXM KAT;
+  * one Gaussian q-vortex has psi log term -0.5 wherever it sits (notes:3-8);
+  * PF is orthonormal under the Gauss weights (RTRAN +-1 symmetry,
+    mod_fft.f90:1230-1243 vs 1284-1292; tests/mlegs/test_prodct.f90:41-45);
+  * FFF -> PPP -> FFF is the identity for band-limited fields;
+  * ETD_E / ETD_NL against a dense matrix exponential (the reference echoes
+    S S^-1 and S J S^-1 for this check, mod_boussinesq.f90:92-105);
+  * the golden 50-digit tables of tests/golden/legendre_golden.npz.
+"""
+
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from conftest import oracle_grid, random_fff, rel, small_cfg
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "legendre_golden.npz")
+
+
+def test_gauss_legendre_golden():
+    from oracle.grid import gauss_legendre
+    z = np.load(GOLDEN)
+    for ci in range(4):
+        nr = int(z["c%d_nr" % ci])
+        x, w = gauss_legendre(nr)
+        assert np.abs(x - z["c%d_x" % ci]).max() < 5e-15
+        assert rel(w, z["c%d_w" % ci]) < 5e-14
+
+
+def test_legendre_table_golden():
+    from oracle.grid import gauss_legendre, leg_log_norm, leg_table
+    z = np.load(GOLDEN)
+    for ci in range(4):
+        nr = int(z["c%d_nr" % ci])
+        ms = list(z["c%d_ms" % ci])
+        gold = z["c%d_pf" % ci]
+        ne = gold.shape[1]
+        x = z["c%d_x" % ci][: nr // 2]
+        pf = leg_table(x, ne, ms)
+        # relative to each (m) slice's scale; entries that underflow stay zero
+        for j in range(len(ms)):
+            assert rel(pf[:, :, j], gold[:, :, j]) < 1e-12, (ci, ms[j])
+            assert np.array_equal(pf[:, :, j] == 0.0, gold[:, :, j] == 0.0)
+        ln = leg_log_norm(ne + 14, ms)
+        assert rel(ln, z["c%d_lognorm" % ci]) < 1e-14
+        # the nodes the oracle itself produces give the same table to roundoff
+        xo, _ = gauss_legendre(nr)
+        assert rel(leg_table(xo[: nr // 2], ne, ms), gold) < 1e-11
+
+
+def test_pf_orthonormal():
+    g = oracle_grid(small_cfg(64, 32, 32))
+    for mm in (0, 3, 15):
+        pf = g.PF[:, :30, mm]
+        G = 2 * (pf.T * g.W[: g.NRH]) @ pf
+        par = (np.arange(30)[:, None] + np.arange(30)[None, :]) % 2
+        G[par == 1] = 0
+        assert np.abs(G - np.eye(30)).max() < 1e-13
+
+
+def test_roundtrip_identity():
+    from oracle import transforms as T
+    g = oracle_grid(small_cfg(64, 32, 32))
+    A = random_fff(g, 0)
+    B = A.copy()
+    T.tofp(g, B)
+    T.toff(g, B)
+    assert rel(B.E, A.E) < 1e-13
+
+
+def test_mulxm_divxm_kat():
+    from oracle import legops as L
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(64, 32, 32))
+    A = g.alloc(FFF)
+    A.E[2, 0, :] = 1.0
+    B = L.mulxm(g, A)
+    n0 = g.NORM0
+    assert abs(B.E[1, 0, 0] - (-2.0 / 5.0 * n0[2] / n0[1])) < 1e-15
+    assert abs(B.E[2, 0, 0] - 1.0) < 1e-15
+    assert abs(B.E[3, 0, 0] - (-3.0 / 5.0 * n0[2] / n0[3])) < 1e-15
+
+
+@pytest.mark.parametrize("xc", [0.0, 0.7])
+def test_qvortex_logterm(xc):
+    from oracle import layout
+    g = oracle_grid(small_cfg(64, 32, 32))
+    psi, chi = layout.qvortex(g, xc=xc)
+    assert abs(psi.LN + 0.5) < 1e-12
+    assert chi.LN == 0.0
+
+
+def test_etd_matches_expm():
+    from oracle.boussinesq import calc_boussi_diag, calc_boussi_etd_op
+    J, S, Si = calc_boussi_diag(2.0, 1.0)
+    L = S @ J @ Si
+    E, NL = calc_boussi_etd_op(2.0, 1.0, 5e-4)
+    assert np.abs(E - sl.expm(L * 5e-4)).max() < 1e-14
+    # phi_1(L dt) dt = L^-1 (e^{L dt} - I)
+    assert np.abs(NL - np.linalg.solve(L, sl.expm(L * 5e-4) - np.eye(4))).max() < 1e-14
+
+
+def test_band_lu_matches_dense():
+    from oracle.bandmat import band_del2h, band_lu_solve, band_to_full
+    g = oracle_grid(small_cfg(32, 16, 16))
+    b = band_del2h(20, 3, 1.0, g.LOGNORM[:, 3])
+    b[:, 2] -= 2.5
+    rhs = np.random.default_rng(1).standard_normal(20) + 0j
+    x = band_lu_solve(b[None], 2, rhs[None])[0]
+    full = band_to_full(b, 2)
+    assert rel(full @ x, rhs) < 1e-12
+
+
+def test_projection_identity_physical():
+    """PC2VEL -> TOFP (CHOPSET(3)) -> PROJECT -> IDEL2LN recovers (psi, chi)."""
+    from oracle import legops as L
+    from oracle import transforms as T
+    g = oracle_grid(small_cfg(64, 32, 32))
+    psi = random_fff(g, 1, decay=4.0)
+    chi = random_fff(g, 2, decay=4.0)
+    for F in (psi, chi):
+        F.E[0, 0, :] -= g.calcat1(F) / g.AT1[0]
+    g.chopset(3)
+    U = L.pc2vel(g, psi, chi)
+    for u in U:
+        T.tofp(g, u)
+    g.chopset(-3)
+    P2, W2 = L.project(g, *U, None)
+    C2 = L.idel2ln(g, W2)
+    assert rel(P2.E, psi.E) < 1e-11
+    assert rel(C2.E, chi.E) < 1e-9
+
+
+def test_buoyancy_column_accelerates():
+    """z-uniform axisymmetric b accelerates u_z = -b t (no pressure gradient at k = 0)."""
+    from oracle import boussinesq as BQ
+    from oracle import legops as L
+    from oracle import transforms as T
+    from oracle.grid import FFF
+    from conftest import oracle_physics
+    cfg = small_cfg(64, 32, 32)
+    g = oracle_grid(cfg)
+    b = random_fff(g, 3, decay=4.0)
+    b.E[:, 1:, :] = 0
+    b.E[:, :, 1:] = 0
+    b.E *= 1e-3
+    b.E[0, 0, 0] -= g.calcat1(b)[0] / g.AT1[0]
+    b0 = b.copy()
+    s = BQ.Solver(g, oracle_physics(cfg), g.alloc(FFF), g.alloc(FFF), b)
+    s.initialize()
+    for _ in range(9):
+        s.step()
+    g.chopset(3)
+    uz = L.pc2vel(g, s.psi, s.chi)[2]
+    g.chopset(-3)
+    T.tofp(g, uz)
+    T.tofp(g, b0)
+    want = -b0.E[: g.NR, 0, 0].real * s.t
+    assert rel(uz.E[: g.NR, 0, 0].real, want) < 5e-3
+
+
+def test_inputs_deterministic():
+    from mlegs_b200.inputs import CONFIGS, perturbation_coefficients
+    cfg = CONFIGS["ab2_64x32x32"]
+    a = perturbation_coefficients(cfg, 0)
+    b = perturbation_coefficients(cfg, 0)
+    assert np.array_equal(a, b)
+    neg = np.r_[0, np.arange(a.shape[2] - 1, 0, -1)]
+    assert np.allclose(a[:, 0, :], np.conj(a[:, 0, neg]))
+    assert a[0, 0, 0] == 0

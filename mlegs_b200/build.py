@@ -16,13 +16,23 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=s
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
 
+def _digest():
+    import hashlib
+    h = hashlib.sha256()
+    for f in sorted(os.listdir(CSRC)):
+        h.update(f.encode())
+        h.update(open(os.path.join(CSRC, f), "rb").read())
+    h.update(open(os.path.join(HERE, "..", "include", "mlegs_b200.h"), "rb").read())
+    h.update(" ".join(FLAGS).encode())
+    return h.hexdigest()
+
+
 def _stale():
-    if not os.path.exists(OUT):
+    """Rebuild only when the sources or flags changed (content hash, not mtimes,
+    so a copied tree with a prebuilt library does not recompile)."""
+    if not os.path.exists(OUT) or not os.path.exists(OUT + ".sha256"):
         return True
-    t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    deps.append(os.path.join(HERE, "..", "include", "mlegs_b200.h"))
-    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+    return open(OUT + ".sha256").read().strip() != _digest()
 
 
 def build(force=False, verbose=False):
@@ -48,6 +58,8 @@ def build(force=False, verbose=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s" % r.stderr)
+    with open(OUT + ".sha256", "w") as fh:
+        fh.write(_digest())
     return OUT
 
 

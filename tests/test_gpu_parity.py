@@ -233,7 +233,9 @@ def test_qvortex_on_device(env):
     psi, chi = M.qvortex(ctx)
     P, C = layout.qvortex(g)
     E, ln = psi.download()
-    assert abs(ln + 0.5) < 1e-12
+    assert abs(ln - P.LN) < 1e-13
+    # the -0.5 known answer (notes:3-8) once the grid resolves the vortex
+    assert abs(ln + 0.5) < (1e-12 if cfg.nr >= 64 else 1e-9)
     assert rel(E, P.E) < 1e-12
 
 

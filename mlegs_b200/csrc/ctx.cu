@@ -192,12 +192,12 @@ struct mlegs_ctx {
     void horfft(Field* f, int is) {
         if (is == -1) {
             require(f, MLEGS_PPP, "HORFFT");
-            k_horfft_f(g, fft, f->data, scratch, s);
+            k_horfft_warp(g, fft, f->data, scratch, -1, s);
             swap_scratch_any(f);
             f->space = MLEGS_PFP;
         } else {
             require(f, MLEGS_PFP, "HORFFT");
-            k_horfft_b(g, fft, f->data, scratch, s);
+            k_horfft_warp(g, fft, f->data, scratch, +1, s);
             swap_scratch_any(f);
             f->space = MLEGS_PPP;
         }
@@ -325,6 +325,10 @@ struct mlegs_ctx {
             plnfft(rur, -1);
             plnfft(rup, -1);
             plnfft(uz, -1);
+        } else if (rur->space == MLEGS_PFP) {  // PPP already taken through HORFFT(-1)
+            verfft(rur, -1);
+            verfft(rup, -1);
+            verfft(uz, -1);
         } else if (rur->space == MLEGS_FFF) {
             rtran(rur, 1, 0);
             rtran(rup, 1, 0);
@@ -417,6 +421,7 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     g_launch_counter = &launches;
     fft_set_attributes();
+    phys_set_attributes();
 
     d.NR = p.nr;
     d.NRH = p.nr / 2;
@@ -712,35 +717,36 @@ void mlegs_ctx::ln_from_coef(double* ln, const double2* data, double scale) {
 // CALC_BOUSSI_FORCE(PSI, CHI, B, PSIN, CHIN, BN), mod_boussinesq.f90:317-410.
 void mlegs_ctx::force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BNout) {
     Field *RUR = tmp(), *RUP = tmp(), *UZ = tmp(), *ROR = tmp(), *ROP = tmp(), *OZ = tmp(), *RBR = tmp(),
-          *RBP = tmp(), *BZ = tmp(), *W = tmp(), *BN = tmp();
+          *RBP = tmp(), *BZ = tmp(), *W = tmp();
     const int P3 = 3;  // CHOPSET(3) ... CHOPSET(-3)
     grad(B, RBR, RBP, BZ, P3);
     pc2vel(PSI, CHI, RUR, RUP, UZ, P3);
     pc2vor(PSI, CHI, ROR, ROP, OZ, P3);
-    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) tofp(f, P3);
+    // TOFP up to PFP; the HORFFT(+1) of each field happens inside the fused kernel
+    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) {
+        rtran(f, 1, P3);
+        verfft(f, 1);
+    }
     copy0(W, B, 0);  // W = B; TOFP(W) after CHOPSET(-3)
-    tofp(W, 0);
-    // VPRODSUB + VDOTPSUB + the linear terms (385-391) in one pointwise pass
-    BN->space = MLEGS_PPP;
-    ln_zero(BN);
-    k_force_pointwise(g, RUR->data, RUP->data, UZ->data, ROR->data, ROP->data, OZ->data, RBR->data,
-                      RBP->data, BZ->data, BN->data, W->data, p.omega, p.bv0, 1, s);
-    rel(UZ);
-    rel(RBR);
-    rel(RBP);
-    rel(BZ);
-    rel(W);
-    Field* Wf = RUP;  // W = DEL2(CHIN) in FFF
-    project(ROR, ROP, OZ, PSIN, Wf, 1, 0.0);
+    rtran(W, 1, 0);
+    verfft(W, 1);
+    // VPRODSUB + VDOTPSUB + the linear terms (385-391), then HORFFT(-1) of the results
+    Field *NR = tmp(), *NP = tmp(), *NZ = tmp(), *BN = tmp();
+    const double2* in[10] = {RUR->data, RUP->data, UZ->data, ROR->data, ROP->data,
+                             OZ->data,  RBR->data, RBP->data, BZ->data,  W->data};
+    double2* out[4] = {NR->data, NP->data, NZ->data, BN->data};
+    k_theta_fused(g, fft, in, out, p.omega, p.bv0, 1, s);
+    for (Field* f : {NR, NP, NZ, BN}) {
+        f->space = MLEGS_PFP;
+        ln_zero(f);
+    }
+    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ, W}) rel(f);
+    Field* Wf = tmp();  // W = DEL2(CHIN) in FFF
+    project(NR, NP, NZ, PSIN, Wf, 1, 0.0);
     idel2ln(Wf, CHIN, 0);
     toff(BN, 0);
     copy0(BNout, BN, 0);
-    rel(BN);
-    rel(RUR);
-    rel(RUP);
-    rel(ROR);
-    rel(ROP);
-    rel(OZ);
+    for (Field* f : {Wf, NR, NP, NZ, BN}) rel(f);
 }
 
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
@@ -749,21 +755,27 @@ void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field*
                        Field* BN) {
     Field *RBR = tmp(), *RBP = tmp(), *BZ = tmp();
     grad(B, RBR, RBP, BZ, 1);
-    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) tofp(f, 0);
-    BN->space = MLEGS_PPP;
-    ln_zero(BN);
-    k_force_pointwise(g, RUR->data, RUP->data, UZ->data, ROR->data, ROP->data, OZ->data, RBR->data,
-                      RBP->data, BZ->data, BN->data, nullptr, 0.0, 0.0, 0, s);
+    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) {
+        rtran(f, 1, 0);
+        verfft(f, 1);
+    }
+    Field *NR = tmp(), *NP = tmp(), *NZ = tmp();
+    const double2* in[10] = {RUR->data, RUP->data, UZ->data, ROR->data, ROP->data,
+                             OZ->data,  RBR->data, RBP->data, BZ->data,  nullptr};
+    double2* out[4] = {NR->data, NP->data, NZ->data, BN->data};
+    k_theta_fused(g, fft, in, out, 0.0, 0.0, 0, s);
+    for (Field* f : {NR, NP, NZ, BN}) {
+        f->space = MLEGS_PFP;
+        ln_zero(f);
+    }
     rel(RBR);
     rel(RBP);
     rel(BZ);
     Field *PSI = tmp(), *W = tmp(), *CHI = tmp();
-    project(ROR, ROP, OZ, PSI, W, 1, 0.0);
+    project(NR, NP, NZ, PSI, W, 1, 0.0);
     idel2(W, CHI, 0, 0.0, 0);
     pc2vel(PSI, CHI, ROR, ROP, OZ, 3);
-    rel(PSI);
-    rel(W);
-    rel(CHI);
+    for (Field* f : {PSI, W, CHI, NR, NP, NZ}) rel(f);
     toff(BN, 0);
 }
 

@@ -230,20 +230,28 @@ void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, 
 }
 
 // a(n=0, m=0, k) -= sum_{n < nr_sum} AT1(n) a(n, 0, k) / AT1(0)   (CALCAT1 fix)
+// One warp per k: lanes stride over n, shuffle reduction.
 __global__ void farfield_kernel(DevGrid g, double2* a, int nr_sum) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
     if (k >= g.NXCHOPDIM) return;
     double sx = 0.0, sy = 0.0;
-    for (int n = 0; n < nr_sum; ++n) {
+    for (int n = lane; n < nr_sum; n += 32) {
         double2 v = a[(size_t)n * g.NXCHOPDIM + k];
         sx += g.at1[n] * v.x;
         sy += g.at1[n] * v.y;
     }
-    a[k].x -= sx / g.at1[0];
-    a[k].y -= sy / g.at1[0];
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (lane == 0) {
+        a[k].x -= sx / g.at1[0];
+        a[k].y -= sy / g.at1[0];
+    }
 }
 void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s) {
-    farfield_kernel<<<nblk(g.NXCHOPDIM, 128), 128, 0, s>>>(g, a, nr_sum);
+    farfield_kernel<<<nblk(g.NXCHOPDIM, 8), 256, 0, s>>>(g, a, nr_sum);
     count_launch();
 }
 

@@ -105,6 +105,12 @@ void k_verfft_f(const DevGrid& g, const FFTPlan& p, const double2* pfp, double2*
 void k_horfft_b(const DevGrid& g, const FFTPlan& p, const double2* pfp, double2* ppp, cudaStream_t s);
 void k_horfft_f(const DevGrid& g, const FFTPlan& p, const double2* ppp, double2* pfp, cudaStream_t s);
 
+// Fused physical stage (phys.cu): 9 (10 with linear terms) PFP inputs -> 4 PFP outputs.
+void phys_set_attributes();
+void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[10], double2* const out[4],
+                   double omega, double bv0, int linear, cudaStream_t s);
+void k_horfft_warp(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s);
+
 // Spectral operators on FFF.
 void k_delsqh(const DevGrid& g, const double2* a, const double* ln_a, double2* b, int pad, cudaStream_t s);
 void k_idelsqh(const DevGrid& g, const double2* b, double2* a, int pad, cudaStream_t s);

@@ -1,0 +1,334 @@
+// Fused physical-space stage of CALC_BOUSSI_FORCE / CALC_BOUSSI_NONLIN:
+//   HORFFT(+1) of the 9 (10) input fields  ->  VPRODSUB + VDOTPSUB (+ the
+//   linear Coriolis/buoyancy terms)  ->  HORFFT(-1) of the 4 results,
+// one (r, z) line per warp, so the NR x 2NTH x NX physical fields never reach
+// HBM.  Inputs and outputs are PFP lines [r][z][m] (m < NTCHOPDIM).
+//
+// Restates mod_fft.f90:771-926 (HORFFT, packed real FFT of length 2*NTH),
+// mod_legops.f90:2105-2130 (VPRODSUB cross product, z component / r^2),
+// 2207-2225 (VDOTPSUB), mod_boussinesq.f90:385-391 (2 Omega z x u - b z,
+// + N^2 u_z).  Each warp runs its line's FFT as a warp-synchronous Stockham
+// (radix 4, radix 2 for an odd log2 NTH) in its own shared-memory slice;
+// after the inverse transform every lane keeps its PP = NTH/32 packed
+// samples of the running products in registers.
+#include "mlegs_internal.h"
+
+namespace mlegs {
+
+namespace {
+
+__device__ __forceinline__ double2 cm(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y); }
+
+// Warp-synchronous Stockham FFT of length N on buffer a (scratch b); returns result buffer.
+template <int SIGN>
+__device__ __forceinline__ double2* warp_fft(double2* a, double2* b, int N, int L, const double2* tw, int lane) {
+    int Ns = 1, bits = L;
+    while (bits > 0) {
+        if (bits >= 2) {
+            const int nb = N >> 2, step = N / (Ns * 4);
+            for (int j = lane; j < nb; j += 32) {
+                int k = j % Ns;
+                double2 v0 = a[j], v1 = a[j + nb], v2 = a[j + 2 * nb], v3 = a[j + 3 * nb];
+                if (k) {
+                    double2 w1 = tw[k * step], w2 = tw[2 * k * step], w3 = tw[3 * k * step];
+                    if (SIGN > 0) { w1 = cj(w1); w2 = cj(w2); w3 = cj(w3); }
+                    v1 = cm(v1, w1);
+                    v2 = cm(v2, w2);
+                    v3 = cm(v3, w3);
+                }
+                double2 s02 = make_double2(v0.x + v2.x, v0.y + v2.y), d02 = make_double2(v0.x - v2.x, v0.y - v2.y);
+                double2 s13 = make_double2(v1.x + v3.x, v1.y + v3.y), d13 = make_double2(v1.x - v3.x, v1.y - v3.y);
+                double2 id = (SIGN > 0) ? make_double2(-d13.y, d13.x) : make_double2(d13.y, -d13.x);
+                int base = (j / Ns) * Ns * 4 + k;
+                b[base] = make_double2(s02.x + s13.x, s02.y + s13.y);
+                b[base + Ns] = make_double2(d02.x + id.x, d02.y + id.y);
+                b[base + 2 * Ns] = make_double2(s02.x - s13.x, s02.y - s13.y);
+                b[base + 3 * Ns] = make_double2(d02.x - id.x, d02.y - id.y);
+            }
+            Ns *= 4;
+            bits -= 2;
+        } else {
+            const int nb = N >> 1, step = N / (Ns * 2);
+            for (int j = lane; j < nb; j += 32) {
+                int k = j % Ns;
+                double2 v0 = a[j], v1 = a[j + nb];
+                if (k) {
+                    double2 w = tw[k * step];
+                    if (SIGN > 0) w = cj(w);
+                    v1 = cm(v1, w);
+                }
+                int base = (j / Ns) * Ns * 2 + k;
+                b[base] = make_double2(v0.x + v1.x, v0.y + v1.y);
+                b[base + Ns] = make_double2(v0.x - v1.x, v0.y - v1.y);
+            }
+            Ns *= 2;
+            bits -= 1;
+        }
+        __syncwarp();
+        double2* t = a;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Inverse HORFFT of one PFP line into packed samples held in registers v[q] = z_{lane + 32 q}.
+template <int PP>
+__device__ __forceinline__ void line_inverse(const double2* __restrict__ src, int md, int ntchop, int N, int L,
+                                             const double2* tw, const double2* twh, double2* X, double2* a,
+                                             double2* b, int lane, double2 (&v)[PP]) {
+    for (int m = lane; m <= N; m += 32) {
+        double2 x = make_double2(0.0, 0.0);
+        if (m < md && m < ntchop) x = src[m];
+        if (m == 0) x.y = 0.0;
+        X[m] = x;
+    }
+    __syncwarp();
+    for (int m = lane; m < N; m += 32) {
+        double2 xm = X[m], xc = cj(X[N - m]);
+        double2 s = make_double2(xm.x + xc.x, xm.y + xc.y), d = make_double2(xm.x - xc.x, xm.y - xc.y);
+        double2 ed = cm(cj(twh[m]), d);
+        a[m] = make_double2(s.x - ed.y, s.y + ed.x);
+    }
+    __syncwarp();
+    double2* r = warp_fft<+1>(a, b, N, L, tw, lane);
+#pragma unroll
+    for (int q = 0; q < PP; ++q) {
+        int j = lane + 32 * q;
+        v[q] = (j < N) ? r[j] : make_double2(0.0, 0.0);
+    }
+    __syncwarp();
+}
+
+// Forward HORFFT of packed samples in registers to a PFP line (m < md).
+template <int PP>
+__device__ __forceinline__ void line_forward(double2* __restrict__ dst, int md, int ntchop, int N, int L,
+                                             const double2* tw, const double2* twh, double2* a, double2* b,
+                                             int lane, const double2 (&v)[PP]) {
+#pragma unroll
+    for (int q = 0; q < PP; ++q) {
+        int j = lane + 32 * q;
+        if (j < N) a[j] = v[q];
+    }
+    __syncwarp();
+    double2* Z = warp_fft<-1>(a, b, N, L, tw, lane);
+    const double sc = 1.0 / (2.0 * N);
+    for (int m = lane; m < md; m += 32) {
+        double2 zm = Z[m % N], zc = cj(Z[(N - m) % N]);
+        double2 s = make_double2(zm.x + zc.x, zm.y + zc.y), d = make_double2(zm.x - zc.x, zm.y - zc.y);
+        double2 ed = cm(twh[m], d);
+        double2 x = make_double2(0.5 * (s.x + ed.y) * sc, 0.5 * (s.y - ed.x) * sc);
+        if (m >= ntchop) x = make_double2(0.0, 0.0);
+        if (m == 0) x.y = 0.0;
+        dst[m] = x;
+    }
+    __syncwarp();
+}
+
+}  // namespace
+
+// in[0..8]: RUR RUP UZ ROR ROP OZ RBR RBP BZ (PFP); in[9]: B (PFP, linear only)
+// out[0..3]: N_r N_theta N_z N_b (PFP)
+struct PhysArgs {
+    const double2* in[10];
+    double2* out[4];
+    double omega, bv0;
+    int linear;
+};
+
+template <int PP>
+__global__ void __launch_bounds__(256, 1) theta_fused_kernel(DevGrid g, PhysArgs A, const double2* tw,
+                                                          const double2* twh, int L) {
+    extern __shared__ double2 sm[];
+    const int N = g.NTH, md = g.NTCHOPDIM;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    double2* X = sm + (size_t)warp * (3 * N + 1);
+    double2* a = X + (N + 1);
+    double2* b = a + N;
+    const int nlines = g.NR * g.NX;
+    for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
+        const int r = line / g.NX;
+        const double rr = g.r[r];
+        const double r2 = rr * rr;
+        const size_t off = (size_t)line * md;
+        double2 a1[PP], a2[PP], a3[PP], t[PP];
+        double2 nr_[PP], np_[PP], nz_[PP], bn_[PP];
+        line_inverse<PP>(A.in[0] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, a1);
+        line_inverse<PP>(A.in[1] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, a2);
+        line_inverse<PP>(A.in[2] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, a3);
+        // b1 = r omega_r:  N_theta = a3 b1,  N_z = -a2 b1
+        line_inverse<PP>(A.in[3] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) {
+            np_[q] = make_double2(a3[q].x * t[q].x, a3[q].y * t[q].y);
+            nz_[q] = make_double2(-a2[q].x * t[q].x, -a2[q].y * t[q].y);
+        }
+        // b2 = r omega_theta: N_r = -a3 b2, N_z += a1 b2
+        line_inverse<PP>(A.in[4] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) {
+            nr_[q] = make_double2(-a3[q].x * t[q].x, -a3[q].y * t[q].y);
+            nz_[q].x += a1[q].x * t[q].x;
+            nz_[q].y += a1[q].y * t[q].y;
+        }
+        // b3 = omega_z: N_r += a2 b3, N_theta -= a1 b3
+        line_inverse<PP>(A.in[5] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) {
+            nr_[q].x += a2[q].x * t[q].x;
+            nr_[q].y += a2[q].y * t[q].y;
+            np_[q].x -= a1[q].x * t[q].x;
+            np_[q].y -= a1[q].y * t[q].y;
+            nz_[q].x /= r2;
+            nz_[q].y /= r2;
+        }
+        // -(u . grad b): (a1 c1 + a2 c2)/r^2 + a3 c3
+        line_inverse<PP>(A.in[6] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) bn_[q] = make_double2(a1[q].x * t[q].x, a1[q].y * t[q].y);
+        line_inverse<PP>(A.in[7] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) {
+            bn_[q].x += a2[q].x * t[q].x;
+            bn_[q].y += a2[q].y * t[q].y;
+            bn_[q].x /= r2;
+            bn_[q].y /= r2;
+        }
+        line_inverse<PP>(A.in[8] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+#pragma unroll
+        for (int q = 0; q < PP; ++q) {
+            bn_[q].x = -(bn_[q].x + a3[q].x * t[q].x);
+            bn_[q].y = -(bn_[q].y + a3[q].y * t[q].y);
+        }
+        if (A.linear) {
+            line_inverse<PP>(A.in[9] + off, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, t);
+            const double o2 = 2 * A.omega, n2 = A.bv0 * A.bv0;
+#pragma unroll
+            for (int q = 0; q < PP; ++q) {
+                nr_[q].x += o2 * a2[q].x;
+                nr_[q].y += o2 * a2[q].y;
+                np_[q].x -= o2 * a1[q].x;
+                np_[q].y -= o2 * a1[q].y;
+                nz_[q].x -= t[q].x;
+                nz_[q].y -= t[q].y;
+                bn_[q].x += n2 * a3[q].x;
+                bn_[q].y += n2 * a3[q].y;
+            }
+        }
+        line_forward<PP>(A.out[0] + off, md, g.NTCHOP, N, L, tw, twh, a, b, lane, nr_);
+        line_forward<PP>(A.out[1] + off, md, g.NTCHOP, N, L, tw, twh, a, b, lane, np_);
+        line_forward<PP>(A.out[2] + off, md, g.NTCHOP, N, L, tw, twh, a, b, lane, nz_);
+        line_forward<PP>(A.out[3] + off, md, g.NTCHOP, N, L, tw, twh, a, b, lane, bn_);
+    }
+}
+
+// Single-field warp-per-line HORFFT (same arithmetic as the fused kernel):
+//  dir +1: PFP -> PPP,  dir -1: PPP -> PFP.
+template <int PP>
+__global__ void __launch_bounds__(256) horfft_warp_kernel(DevGrid g, const double2* src, double2* dst,
+                                                          const double2* tw, const double2* twh, int L,
+                                                          int dir) {
+    extern __shared__ double2 sm[];
+    const int N = g.NTH, md = g.NTCHOPDIM;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    double2* X = sm + (size_t)warp * (3 * N + 1);
+    double2* a = X + (N + 1);
+    double2* b = a + N;
+    const int nlines = g.NR * g.NX;
+    for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
+        double2 v[PP];
+        if (dir > 0) {
+            line_inverse<PP>(src + (size_t)line * md, md, g.NTCHOP, N, L, tw, twh, X, a, b, lane, v);
+#pragma unroll
+            for (int q = 0; q < PP; ++q) {
+                int j = lane + 32 * q;
+                if (j < N) dst[(size_t)line * N + j] = v[q];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < PP; ++q) {
+                int j = lane + 32 * q;
+                v[q] = (j < N) ? src[(size_t)line * N + j] : make_double2(0.0, 0.0);
+            }
+            line_forward<PP>(dst + (size_t)line * md, md, g.NTCHOP, N, L, tw, twh, a, b, lane, v);
+        }
+    }
+}
+
+static int pp_of(int nth) {
+    int pp = (nth + 31) / 32;
+    if (pp <= 1) return 1;
+    if (pp <= 2) return 2;
+    if (pp <= 4) return 4;
+    if (pp <= 8) return 8;
+    return 16;
+}
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+void phys_set_attributes() {
+    const int lim = 200 * 1024;
+    cudaFuncSetAttribute(theta_fused_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(theta_fused_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(theta_fused_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(theta_fused_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(theta_fused_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(horfft_warp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(horfft_warp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(horfft_warp_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(horfft_warp_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(horfft_warp_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
+void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[10], double2* const out[4],
+                   double omega, double bv0, int linear, cudaStream_t s) {
+    PhysArgs A;
+    for (int q = 0; q < 10; ++q) A.in[q] = in[q];
+    for (int q = 0; q < 4; ++q) A.out[q] = out[q];
+    A.omega = omega;
+    A.bv0 = bv0;
+    A.linear = linear;
+    const int warps = 8;
+    size_t sm = (size_t)warps * (3 * g.NTH + 1) * sizeof(double2);
+    int nlines = g.NR * g.NX;
+    int blocks = std::min((nlines + warps - 1) / warps, sm_count() * 8);
+    switch (pp_of(g.NTH)) {
+        case 1: theta_fused_kernel<1><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h, p.lt); break;
+        case 2: theta_fused_kernel<2><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h, p.lt); break;
+        case 4: theta_fused_kernel<4><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h, p.lt); break;
+        case 8: theta_fused_kernel<8><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h, p.lt); break;
+        default: theta_fused_kernel<16><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h, p.lt); break;
+    }
+    count_launch();
+}
+
+void k_horfft_warp(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s) {
+    const int warps = 8;
+    size_t sm = (size_t)warps * (3 * g.NTH + 1) * sizeof(double2);
+    int nlines = g.NR * g.NX;
+    int blocks = std::min((nlines + warps - 1) / warps, sm_count() * 8);
+    switch (pp_of(g.NTH)) {
+        case 1: horfft_warp_kernel<1><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, p.lt, dir); break;
+        case 2: horfft_warp_kernel<2><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, p.lt, dir); break;
+        case 4: horfft_warp_kernel<4><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, p.lt, dir); break;
+        case 8: horfft_warp_kernel<8><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, p.lt, dir); break;
+        default: horfft_warp_kernel<16><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, p.lt, dir); break;
+    }
+    count_launch();
+}
+
+}  // namespace mlegs

@@ -171,6 +171,9 @@ int mlegs_check_finite(mlegs_ctx* ctx);
 #define MLEGS_K_HORFFT_F    5   /* HORFFT(-1) PPP -> PFP               */
 #define MLEGS_K_POINTWISE   6   /* VPRODSUB+VDOTPSUB+linear terms, PPP */
 #define MLEGS_K_SOLVE       7   /* IDEL2LN banded solves               */
+#define MLEGS_K_PHYS        8   /* fused HORFFT+VPRODSUB+VDOTPSUB+linear+HORFFT, PFP -> PFP */
+#define MLEGS_K_HORFFT_WB   9   /* warp-per-line HORFFT(+1) PFP -> PPP */
+#define MLEGS_K_HORFFT_WF  10   /* warp-per-line HORFFT(-1) PPP -> PFP */
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
 /* Number of this library's kernel launches issued since the counter was reset. */

@@ -178,12 +178,12 @@ struct mlegs_ctx {
     void verfft(Field* f, int is) {
         if (is == -1) {
             require(f, MLEGS_PFP, "VERFFT");
-            k_verfft_f(g, fft, f->data, scratch, s);
+            if (!k_verfft4(g, fft, f->data, scratch, -1, s)) k_verfft_f(g, fft, f->data, scratch, s);
             swap_scratch_any(f);
             f->space = MLEGS_PFF;
         } else {
             require(f, MLEGS_PFF, "VERFFT");
-            k_verfft_b(g, fft, f->data, scratch, s);
+            if (!k_verfft4(g, fft, f->data, scratch, +1, s)) k_verfft_b(g, fft, f->data, scratch, s);
             swap_scratch_any(f);
             f->space = MLEGS_PFP;
         }
@@ -1417,7 +1417,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 7) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 10) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1432,8 +1432,12 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             switch (kernel) {
                 case 0: k_rtran_b2p(g, a->data, b->data, nullptr, 0, s); break;
                 case 1: k_fold_gemm(g, ctx->pf, d.NRCHOPDIM + 1, a->data, b->data, 2, 0, 0, 0, s); break;
-                case 2: k_verfft_b(g, ctx->fft, a->data, b->data, s); break;
-                case 3: k_verfft_f(g, ctx->fft, a->data, b->data, s); break;
+                case 2:
+                    if (!k_verfft4(g, ctx->fft, a->data, b->data, +1, s)) k_verfft_b(g, ctx->fft, a->data, b->data, s);
+                    break;
+                case 3:
+                    if (!k_verfft4(g, ctx->fft, a->data, b->data, -1, s)) k_verfft_f(g, ctx->fft, a->data, b->data, s);
+                    break;
                 case 4: k_horfft_b(g, ctx->fft, a->data, b->data, s); break;
                 case 5: k_horfft_f(g, ctx->fft, a->data, b->data, s); break;
                 case 6:
@@ -1441,9 +1445,17 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                                       f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data, b->data,
                                       1.0, 1.0, 1, s);
                     break;
-                default:
+                case 7:
                     k_solve_del2(g, a->data, c->ln, 0, 0.0, 0, 0.0, nullptr, ctx->solve_scr, 0, s);
                     break;
+                case 8: {
+                    const double2* in[10] = {f9[0]->data, f9[1]->data, f9[2]->data, f9[3]->data, f9[4]->data,
+                                             f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data};
+                    double2* out[4] = {b->data, c->data, f9[0]->data, f9[1]->data};
+                    k_theta_fused(g, ctx->fft, in, out, 1.0, 1.0, 1, s);
+                } break;
+                case 9: k_horfft_warp(g, ctx->fft, a->data, b->data, +1, s); break;
+                default: k_horfft_warp(g, ctx->fft, a->data, b->data, -1, s); break;
             }
         };
         const double B16 = 16.0;
@@ -1453,7 +1465,9 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 2: case 3: bytes = B16 * ((double)d.pff() + (double)d.pfp()); break;
             case 4: case 5: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
             case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written
-            default: bytes = B16 * 2.0 * (double)d.fff(); break;
+            case 7: bytes = B16 * 2.0 * (double)d.fff(); break;
+            case 8: bytes = B16 * 14.0 * (double)d.pfp(); break;  // 10 PFP lines read, 4 written
+            default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
         }
         for (int q = 0; q < 3; ++q) launch();  // warm-up
         cudaEvent_t e0, e1;

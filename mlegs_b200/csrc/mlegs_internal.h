@@ -110,6 +110,8 @@ void phys_set_attributes();
 void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[10], double2* const out[4],
                    double omega, double bv0, int linear, cudaStream_t s);
 void k_horfft_warp(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s);
+// Four-step VERFFT (dir +1: PFF -> PFP, -1: PFP -> PFF); false if NX has no specialisation.
+bool k_verfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s);
 
 // Spectral operators on FFF.
 void k_delsqh(const DevGrid& g, const double2* a, const double* ln_a, double2* b, int pad, cudaStream_t s);

@@ -12,6 +12,9 @@
 // after the inverse transform every lane keeps its PP = NTH/32 packed
 // samples of the running products in registers.
 #include "mlegs_internal.h"
+#include "fft4.cuh"
+
+#include <algorithm>
 
 namespace mlegs {
 
@@ -260,6 +263,168 @@ __global__ void __launch_bounds__(256) horfft_warp_kernel(DevGrid g, const doubl
     }
 }
 
+// ------------------------------------------------------------------------
+// Four-step versions (fft4.cuh): NTH = N1 * N2, G = 32 / N2 fields or lines
+// per warp in parallel, packed samples staged in per-warp shared-memory lines.
+namespace {
+
+// Inverse HORFFT of one PFP line by one lane group; packed samples -> P[0..N).
+template <int N1, int N2>
+__device__ __forceinline__ void grp_inverse(const double2* __restrict__ src, bool valid, int md, int ntchop,
+                                            const double2* tw, const double2* twh, double2* S, double2* P, int t) {
+    constexpr int N = N1 * N2;
+    double2 v[N1], o[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        const int m = t + N2 * n1, mc = N - m;
+        double2 xm = make_double2(0.0, 0.0), xc = make_double2(0.0, 0.0);
+        if (valid) {
+            if (m < md && m < ntchop) xm = src[m];
+            if (mc < md && mc < ntchop) xc = src[mc];
+        }
+        if (m == 0) xm.y = 0.0;
+        if (mc == 0) xc.y = 0.0;
+        xc = fft4::conj(xc);
+        double2 sm = make_double2(xm.x + xc.x, xm.y + xc.y), d = make_double2(xm.x - xc.x, xm.y - xc.y);
+        double2 ed = fft4::cmul(fft4::conj(twh[m]), d);  // e^{+i pi m/N} d
+        v[n1] = make_double2(sm.x - ed.y, sm.y + ed.x);
+    }
+    fft4::line_fft<N1, N2, +1>(v, S, tw, t, o);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) P[fft4::out_index<N1, N2>(t, q)] = o[q];
+}
+
+// Forward HORFFT of packed samples P[0..N) by one lane group -> PFP line dst (m < md).
+template <int N1, int N2>
+__device__ __forceinline__ void grp_forward(const double2* P, bool valid, double2* __restrict__ dst, int md,
+                                            int ntchop, const double2* tw, const double2* twh, double2* S, int t) {
+    constexpr int N = N1 * N2;
+    double2 v[N1], o[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = P[t + N2 * n1];
+    fft4::line_fft<N1, N2, -1>(v, S, tw, t, o);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) S[fft4::out_index<N1, N2>(t, q)] = o[q];  // Z_k, natural order
+    __syncwarp();
+    const double sc = 1.0 / (2.0 * N);
+    for (int m = t; m < md; m += N2) {
+        double2 zm = S[m % N], zc = fft4::conj(S[(N - m) % N]);
+        double2 sm = make_double2(zm.x + zc.x, zm.y + zc.y), d = make_double2(zm.x - zc.x, zm.y - zc.y);
+        double2 ed = fft4::cmul(twh[m], d);  // e^{-i pi m/N} d
+        double2 x = make_double2(0.5 * (sm.x + ed.y) * sc, 0.5 * (sm.y - ed.x) * sc);
+        if (m >= ntchop) x = make_double2(0.0, 0.0);
+        if (m == 0) x.y = 0.0;
+        if (valid) dst[m] = x;
+    }
+    __syncwarp();
+}
+
+}  // namespace
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) theta4_kernel(DevGrid g, PhysArgs A, const double2* tw_g,
+                                                     const double2* twh_g) {
+    constexpr int N = N1 * N2, G = 32 / N2;
+    constexpr int TILE = N1 * (N2 + 1);
+    extern __shared__ double2 sm[];
+    double2* tw = sm;
+    double2* twh = tw + (N + 1);
+    for (int q = threadIdx.x; q <= N; q += blockDim.x) {
+        tw[q] = tw_g[q];
+        twh[q] = twh_g[q];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int gid = lane / N2, t = lane % N2;
+    double2* P = twh + (N + 1) + (size_t)warp * (11 * N + G * TILE);  // 10 packed lines + 1 spare
+    double2* S = P + 11 * N + gid * TILE;
+    const int md = g.NTCHOPDIM, nin = A.linear ? 10 : 9;
+    const int nlines = g.NR * g.NX;
+    for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
+        const size_t off = (size_t)line * md;
+        for (int f0 = 0; f0 < nin; f0 += G) {
+            const int f = f0 + gid;
+            const bool ok = f < nin;
+            grp_inverse<N1, N2>(ok ? A.in[f] + off : nullptr, ok, md, g.NTCHOP, tw, twh, S, P + (ok ? f : 10) * N, t);
+        }
+        __syncwarp();
+        const double rr = g.r[line / g.NX];
+        const double r2 = rr * rr;
+        const double o2 = 2 * A.omega, n2 = A.bv0 * A.bv0;
+        for (int j = lane; j < N; j += 32) {
+            double2 a1 = P[j], a2 = P[N + j], a3 = P[2 * N + j];
+            double2 b1 = P[3 * N + j], b2 = P[4 * N + j], b3 = P[5 * N + j];
+            double2 c1 = P[6 * N + j], c2 = P[7 * N + j], c3 = P[8 * N + j];
+            double2 nr_ = make_double2(a2.x * b3.x - a3.x * b2.x, a2.y * b3.y - a3.y * b2.y);
+            double2 np_ = make_double2(a3.x * b1.x - a1.x * b3.x, a3.y * b1.y - a1.y * b3.y);
+            double2 nz_ = make_double2((a1.x * b2.x - a2.x * b1.x) / r2, (a1.y * b2.y - a2.y * b1.y) / r2);
+            double2 bn_ = make_double2(-((a1.x * c1.x + a2.x * c2.x) / r2 + a3.x * c3.x),
+                                       -((a1.y * c1.y + a2.y * c2.y) / r2 + a3.y * c3.y));
+            if (A.linear) {
+                double2 bp = P[9 * N + j];
+                nr_.x += o2 * a2.x;
+                nr_.y += o2 * a2.y;
+                np_.x -= o2 * a1.x;
+                np_.y -= o2 * a1.y;
+                nz_.x -= bp.x;
+                nz_.y -= bp.y;
+                bn_.x += n2 * a3.x;
+                bn_.y += n2 * a3.y;
+            }
+            P[3 * N + j] = nr_;
+            P[4 * N + j] = np_;
+            P[5 * N + j] = nz_;
+            P[6 * N + j] = bn_;
+        }
+        __syncwarp();
+        for (int f0 = 0; f0 < 4; f0 += G) {
+            const int f = f0 + gid;
+            const bool ok = f < 4;
+            grp_forward<N1, N2>(P + (3 + (ok ? f : 0)) * N, ok, ok ? A.out[f] + off : nullptr, md, g.NTCHOP, tw,
+                                twh, S, t);
+        }
+        __syncwarp();
+    }
+}
+
+// Single-field HORFFT with the four-step blocks, G lines per warp.  dir +1: PFP -> PPP, -1: PPP -> PFP.
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) horfft4_kernel(DevGrid g, const double2* src, double2* dst,
+                                                      const double2* tw_g, const double2* twh_g, int dir) {
+    constexpr int N = N1 * N2, G = 32 / N2;
+    constexpr int TILE = N1 * (N2 + 1);
+    extern __shared__ double2 sm[];
+    double2* tw = sm;
+    double2* twh = tw + (N + 1);
+    for (int q = threadIdx.x; q <= N; q += blockDim.x) {
+        tw[q] = tw_g[q];
+        twh[q] = twh_g[q];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int gid = lane / N2, t = lane % N2;
+    double2* P = twh + (N + 1) + (size_t)warp * G * (N + TILE) + gid * (N + TILE);
+    double2* S = P + N;
+    const int md = g.NTCHOPDIM;
+    const int nlines = g.NR * g.NX;
+    const int stride = gridDim.x * nw * G;
+    for (int l0 = (blockIdx.x * nw + warp) * G; l0 < nlines; l0 += stride) {
+        const int line = l0 + gid;
+        const bool ok = line < nlines;
+        if (dir > 0) {
+            grp_inverse<N1, N2>(ok ? src + (size_t)line * md : nullptr, ok, md, g.NTCHOP, tw, twh, S, P, t);
+            __syncwarp();
+            if (ok)
+                for (int j = t; j < N; j += N2) dst[(size_t)line * N + j] = P[j];
+        } else {
+            for (int j = t; j < N; j += N2) P[j] = ok ? src[(size_t)line * N + j] : make_double2(0.0, 0.0);
+            __syncwarp();
+            grp_forward<N1, N2>(P, ok, ok ? dst + (size_t)line * md : nullptr, md, g.NTCHOP, tw, twh, S, t);
+        }
+        __syncwarp();
+    }
+}
+
 static int pp_of(int nth) {
     int pp = (nth + 31) / 32;
     if (pp <= 1) return 1;
@@ -294,6 +459,145 @@ void phys_set_attributes() {
     cudaFuncSetAttribute(horfft_warp_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
+// ------------------------------------------------------------------------
+// VERFFT with the four-step blocks.  CTA = (r, block of MB = W*G consecutive m);
+// group (warp w, gid) owns line m0 + w*G + gid.  PFP rows [r][z][m0..m0+MB)
+// move through a shared tile T[z][mloc] so global accesses stay contiguous.
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* src, double2* dst,
+                                                      const double2* tw_g, int dir) {
+    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int gid = lane / N2, t = lane % N2;
+    const int MB = nw * G;
+    double2* tw = sm;
+    double2* T = tw + (N + 1);                  // [N][MB + 1]
+    double2* S = T + (size_t)N * (MB + 1) + (size_t)(warp * G + gid) * TILE;
+    for (int q = threadIdx.x; q <= N; q += blockDim.x) tw[q] = tw_g[q];
+    const int r = blockIdx.x, m0 = blockIdx.y * MB;
+    const int mloc = warp * G + gid, m = m0 + mloc;
+    const bool ok = m < g.NTCHOPDIM;
+    const int kd = g.NXCHOPDIM, kc = g.NXCHOP, md = g.NTCHOPDIM;
+    const int nmb = min(MB, md - m0);
+    double2 v[N1], o[N1];
+    if (dir > 0) {  // PFF [m][r][k] -> PFP [r][z][m]
+        __syncthreads();
+        const double2* line = src + ((size_t)m * g.NR + r) * kd;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int q = t + N2 * n1;
+            int kk = -1;
+            if (q < kc) kk = q;
+            else if (q >= N - kd + kc) kk = q - (N - kd);
+            v[n1] = (ok && kk >= 0) ? line[kk] : make_double2(0.0, 0.0);
+        }
+        fft4::line_fft<N1, N2, +1>(v, S, tw, t, o);
+#pragma unroll
+        for (int q = 0; q < N1; ++q) T[(size_t)fft4::out_index<N1, N2>(t, q) * (MB + 1) + mloc] = o[q];
+        __syncthreads();
+        for (int e = threadIdx.x; e < N * nmb; e += blockDim.x) {
+            const int z = e / nmb, ml = e - z * nmb;
+            dst[((size_t)r * N + z) * md + m0 + ml] = T[(size_t)z * (MB + 1) + ml];
+        }
+    } else {  // PFP [r][z][m] -> PFF [m][r][k], scaled 1/NX, chopped
+        __syncthreads();
+        for (int e = threadIdx.x; e < N * nmb; e += blockDim.x) {
+            const int z = e / nmb, ml = e - z * nmb;
+            T[(size_t)z * (MB + 1) + ml] = src[((size_t)r * N + z) * md + m0 + ml];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? T[(size_t)(t + N2 * n1) * (MB + 1) + mloc] : make_double2(0.0, 0.0);
+        fft4::line_fft<N1, N2, -1>(v, S, tw, t, o);
+#pragma unroll
+        for (int q = 0; q < N1; ++q) S[fft4::out_index<N1, N2>(t, q)] = o[q];
+        __syncwarp();
+        const double sc = 1.0 / N;
+        double2* line = dst + ((size_t)m * g.NR + r) * kd;
+        for (int kk = t; kk < kd; kk += N2) {
+            const int q = (kk < kc) ? kk : (N - kd + kk);
+            double2 y = S[q];
+            if (ok) line[kk] = make_double2(y.x * sc, y.y * sc);
+        }
+    }
+}
+
+template <int N1, int N2>
+static void launch_verfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
+                           cudaStream_t s) {
+    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    int warps = 8;
+    auto need = [&](int w) {
+        int MB = w * G;
+        return (size_t)((N + 1) + N * (MB + 1) + MB * TILE) * sizeof(double2);
+    };
+    while (warps > 1 && need(warps) > 200 * 1024) --warps;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(verfft4_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    const int MB = warps * G;
+    dim3 grid(g.NR, (g.NTCHOPDIM + MB - 1) / MB);
+    verfft4_kernel<N1, N2><<<grid, warps * 32, need(warps), s>>>(g, src, dst, p.tw_x, dir);
+    count_launch();
+}
+
+bool k_verfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s) {
+    switch (g.NX) {
+        case 16: launch_verfft4<4, 4>(g, p, src, dst, dir, s); return true;
+        case 32: launch_verfft4<8, 4>(g, p, src, dst, dir, s); return true;
+        case 64: launch_verfft4<8, 8>(g, p, src, dst, dir, s); return true;
+        case 128: launch_verfft4<16, 8>(g, p, src, dst, dir, s); return true;
+        case 256: launch_verfft4<16, 16>(g, p, src, dst, dir, s); return true;
+        case 512: launch_verfft4<32, 16>(g, p, src, dst, dir, s); return true;
+        default: return false;
+    }
+}
+
+template <int N1, int N2>
+static void launch_theta4(const DevGrid& g, const FFTPlan& p, const PhysArgs& A, cudaStream_t s) {
+    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    const size_t per_warp = (size_t)(11 * N + G * TILE) * sizeof(double2);
+    const size_t fixed = 2 * (size_t)(N + 1) * sizeof(double2);
+    int warps = (int)((227 * 1024 - fixed) / per_warp);
+    if (warps > 8) warps = 8;
+    if (warps < 1) warps = 1;
+    size_t sm = fixed + warps * per_warp;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(theta4_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    int nlines = g.NR * g.NX;
+    int blocks = std::min((nlines + warps - 1) / warps, sm_count() * 2);
+    theta4_kernel<N1, N2><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h);
+    count_launch();
+}
+
+template <int N1, int N2>
+static void launch_horfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
+                           cudaStream_t s) {
+    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    const size_t per_warp = (size_t)G * (N + TILE) * sizeof(double2);
+    const size_t fixed = 2 * (size_t)(N + 1) * sizeof(double2);
+    int warps = (int)((110 * 1024 - fixed) / per_warp);
+    if (warps > 8) warps = 8;
+    if (warps < 1) warps = 1;
+    size_t sm = fixed + warps * per_warp;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(horfft4_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    int nlines = g.NR * g.NX;
+    int per_cta = warps * G;
+    int blocks = std::min((nlines + per_cta - 1) / per_cta, sm_count() * 4);
+    horfft4_kernel<N1, N2><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, dir);
+    count_launch();
+}
+
 void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[10], double2* const out[4],
                    double omega, double bv0, int linear, cudaStream_t s) {
     PhysArgs A;
@@ -302,6 +606,15 @@ void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[1
     A.omega = omega;
     A.bv0 = bv0;
     A.linear = linear;
+    switch (g.NTH) {
+        case 16: launch_theta4<4, 4>(g, p, A, s); return;
+        case 32: launch_theta4<8, 4>(g, p, A, s); return;
+        case 64: launch_theta4<8, 8>(g, p, A, s); return;
+        case 128: launch_theta4<16, 8>(g, p, A, s); return;
+        case 256: launch_theta4<16, 16>(g, p, A, s); return;
+        case 512: launch_theta4<32, 16>(g, p, A, s); return;
+        default: break;
+    }
     const int warps = 8;
     size_t sm = (size_t)warps * (3 * g.NTH + 1) * sizeof(double2);
     int nlines = g.NR * g.NX;
@@ -317,6 +630,15 @@ void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[1
 }
 
 void k_horfft_warp(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s) {
+    switch (g.NTH) {
+        case 16: launch_horfft4<4, 4>(g, p, src, dst, dir, s); return;
+        case 32: launch_horfft4<8, 4>(g, p, src, dst, dir, s); return;
+        case 64: launch_horfft4<8, 8>(g, p, src, dst, dir, s); return;
+        case 128: launch_horfft4<16, 8>(g, p, src, dst, dir, s); return;
+        case 256: launch_horfft4<16, 16>(g, p, src, dst, dir, s); return;
+        case 512: launch_horfft4<32, 16>(g, p, src, dst, dir, s); return;
+        default: break;
+    }
     const int warps = 8;
     size_t sm = (size_t)warps * (3 * g.NTH + 1) * sizeof(double2);
     int nlines = g.NR * g.NX;

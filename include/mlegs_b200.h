@@ -128,6 +128,18 @@ int mlegs_del2(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* b, int pad);  
 /* IDEL2 (823): has_ln = 0 means the LN argument is absent. */
 int mlegs_idel2(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int has_ln, double ln, int pad);
 int mlegs_idel2ln(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad);  /* IDEL2LN 1013 */
+/* IDEL2LN that allocates nothing; no counterpart in the reference.  For
+ * callers that cannot call cudaMalloc where they solve (their own pool
+ * allocator holds the memory they may use, or the implicit device-wide
+ * synchronisation of cudaMalloc is unaffordable in their time loop).  The
+ * elimination scratch is a fixed 64 MiB __device__ array inside this library,
+ * held by every GPU that loads it until the process exits; grids needing more
+ * (NRCHOPDIM*4*NTCHOPDIM*NXCHOPDIM doubles > 8,388,608) get MLEGS_ERR_ARG.
+ * The first call on a device looks the array up (cudaGetSymbolAddress), so
+ * make it before any stream capture.  All calls on a device share the array:
+ * calls whose kernels overlap on the GPU race and must be ordered by the
+ * caller.  Results equal mlegs_idel2ln's. */
+int mlegs_idel2ln_static(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad);
 int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad); /* IHELM 1204 */
 int mlegs_grad(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* rgr, mlegs_field* rgp,
                mlegs_field* gz, int pad);                                            /* GRAD   1727 */
@@ -136,7 +148,8 @@ int mlegs_pc2vel(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
 int mlegs_pc2vor(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
                  mlegs_field* ror, mlegs_field* rop, mlegs_field* oz, int pad);      /* PC2VOR 1856 */
 /* PROJECT (2397): ln_mode 0 = LN absent, 1 = LN given (ln), 2 = PSI%LN passed
- * by reference (the steppers' call form). rur/rup/uz are consumed. */
+ * by reference (the steppers' call form: PSI%LN then ends as the far-field
+ * value VEL2PLN extracts). rur/rup/uz are consumed. */
 int mlegs_project(mlegs_ctx* ctx, mlegs_field* rur, mlegs_field* rup, mlegs_field* uz,
                   mlegs_field* psi, mlegs_field* chi, int ln_mode, double ln);
 

@@ -66,6 +66,7 @@ SIGNATURES = {
     "mlegs_del2": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_idel2": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_int]),
     "mlegs_idel2ln": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "mlegs_idel2ln_static": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_ihelm": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int]),
     "mlegs_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_pc2vel": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),

@@ -1272,6 +1272,28 @@ int mlegs_idel2(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int has_ln
 int mlegs_idel2ln(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad) {
     return guard(ctx, [&] { check_pad(ctx, pad); ctx->idel2ln(F(b), F(a), pad); });
 }
+// IDEL2LN with the elimination scratch in the library's fixed __device__
+// array instead of the context's allocation: the same kernels in the same
+// order as mlegs_idel2ln, and no device allocation of any kind.
+int mlegs_idel2ln_static(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        const Field* fb = F(b);
+        Field* fa = F(a);
+        ctx->require(fb, MLEGS_FFF, "IDEL2LN");
+        const size_t need = (size_t)ctx->d.NRCHOPDIM * 4 * ctx->d.NTCHOPDIM * ctx->d.NXCHOPDIM;
+        double* scr = nullptr;
+        char msg[256];
+        int rc = static_solve_scratch(ctx->dev, need, &scr, msg, sizeof msg);
+        if (rc == 1) throw ApiError(MLEGS_ERR_ARG, msg);
+        if (rc != 0) throw CudaError(msg);
+        ctx->copy0(fa, fb, pad);
+        ctx->ln_zero(fa);
+        k_solve_del2(ctx->g, fa->data, fa->ln, 0, 0.0, 0, 0.0, nullptr, scr, pad, ctx->s);
+        ctx->chopdo(fa, pad);
+        k_farfield_fix(ctx->g, fa->data, ctx->d.NRCHOP + pad, ctx->s);
+    });
+}
 int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad) {
     return guard(ctx, [&] { check_pad(ctx, pad); ctx->ihelm(F(b), F(a), alp, pad); });
 }

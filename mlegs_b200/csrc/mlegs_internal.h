@@ -127,6 +127,12 @@ void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode
 // Banded solves (IDEL2LN, IDEL2, IHELM) with per-system elimination scratch.
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln,
                   double ln_in, const double* b_ln, double* scratch, int pad, cudaStream_t s);
+// Fixed __device__ solve scratch (solve_static.cu) for the allocation-free
+// IDEL2LN entry point: returns 0 and its address on `device` (the current
+// device), 1 if need_doubles exceeds kStaticSolveBytes, 2 on a CUDA error;
+// `msg` receives the reason.
+extern const size_t kStaticSolveBytes;
+int static_solve_scratch(int device, size_t need_doubles, double** out, char* msg, size_t msg_len);
 
 // Pointwise physics in PPP.
 void k_force_pointwise(const DevGrid& g, double2* rur, double2* rup, double2* uz, double2* ror,

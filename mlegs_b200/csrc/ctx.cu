@@ -84,6 +84,22 @@ struct mlegs_ctx {
     int nslots = 0, used_slots = 0;
     double2* scratch = nullptr;
     double* solve_scr = nullptr;
+    // split-BF16 tensor-core GEMMs (MLEGS_PREC_SPLIT)
+    int split_S = 0;                 // slices per operand; 0 = FP64 GEMMs
+    uint8_t* split_img = nullptr;    // PF slice images for RTRAN(+1)
+    int* split_eA = nullptr;         // PF row scale exponents
+    int* split_err = nullptr;        // raised by a timed-out wait in a tensor-core kernel
+    uint8_t* fimg[4] = {};           // weight slice images: 0 PF (RTRAN -1), 1 V, 2 D, 3 T (PROJECT)
+    int* feA[4] = {};
+    // out (+)= s Wt . fold(in): FP64 kernel, or the split tensor-core kernel when enabled
+    void fold(int w, const double* Wt, int wt_rows, const double2* in, double2* out, int mode, int scale,
+              int accumulate, int pad) {
+        if (split_S)
+            k_split_fold(g, split_S, fimg[w], feA[w], wt_rows, in, out, mode & 1, scale, accumulate, pad,
+                         (mode & 2) ? 1 : 0, split_err, s);
+        else
+            k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, s);
+    }
     double2* staging = nullptr;
     int* dflag = nullptr;
     std::vector<std::unique_ptr<mlegs_field>> owned;  // every field, incl. user ones
@@ -163,12 +179,15 @@ struct mlegs_ctx {
     void rtran(Field* f, int is, int pad) {
         if (is == -1) {
             require(f, MLEGS_PFF, "RTRAN");
-            k_fold_gemm(g, pf, d.NRCHOPDIM + 1, f->data, scratch, 0 | 2, 0, 0, pad, s);
+            fold(0, pf, d.NRCHOPDIM + 1, f->data, scratch, 0 | 2, 0, 0, pad);
             swap_scratch_any(f);
             f->space = MLEGS_FFF;
         } else {
             require(f, MLEGS_FFF, "RTRAN");
-            k_rtran_b2p(g, f->data, scratch, f->ln, pad, s);
+            if (split_S)
+                k_split_b2p(g, split_S, split_img, split_eA, f->data, scratch, f->ln, pad, split_err, s);
+            else
+                k_rtran_b2p(g, f->data, scratch, f->ln, pad, s);
             swap_scratch_any(f);
             f->space = MLEGS_PFF;
         }
@@ -343,12 +362,12 @@ struct mlegs_ctx {
         if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, explog0, d.NRCHOP, s);
         const int wr = d.NRCHOPDIM;
         // PSI = -(i m) EO(V, RUR) - OE(D, RUP)
-        k_fold_gemm(g, V, wr, rur->data, psi_->data, 0, 2, 0, 0, s);
-        k_fold_gemm(g, D, wr, rup->data, psi_->data, 1, 1, 1, 0, s);
+        fold(1, V, wr, rur->data, psi_->data, 0, 2, 0, 0);
+        fold(2, D, wr, rup->data, psi_->data, 1, 1, 1, 0);
         // CHI = (i k) OE(D, RUR) + m k EO(V, RUP) - EO(T, UZ)
-        k_fold_gemm(g, D, wr, rur->data, chi_->data, 1, 3, 0, 0, s);
-        k_fold_gemm(g, V, wr, rup->data, chi_->data, 0, 4, 1, 0, s);
-        k_fold_gemm(g, T, wr, uz->data, chi_->data, 0, 1, 1, 0, s);
+        fold(2, D, wr, rur->data, chi_->data, 1, 3, 0, 0);
+        fold(1, V, wr, rup->data, chi_->data, 0, 4, 1, 0);
+        fold(3, T, wr, uz->data, chi_->data, 0, 1, 1, 0);
         k_farfield_fix(g, psi_->data, d.NRCHOP, s);
     }
 
@@ -685,6 +704,27 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     size_t ref_pff = (size_t)d.NDIMR * d.NTCHOPDIM * d.NXCHOPDIM;
     staging = dalloc<double2>(std::max(ref_max, std::max(ref_fff, ref_pff)));
     dflag = dalloc<int>(1);
+    split_err = dalloc<int>(1);
+    CK(cudaMemsetAsync(split_err, 0, sizeof(int), s));
+    if (p.precision == MLEGS_PREC_SPLIT) {
+        const int S = p.split_slices > 0 ? p.split_slices : 5;
+        if (!split_supported(g, S) || !split_fold_supported(g, S, d.NRCHOPDIM + 1))
+            throw ApiError(MLEGS_ERR_ARG, "MLEGS_PREC_SPLIT: needs 3 <= split_slices <= 6, NR <= 256 and the "
+                                          "slice tiles within 227 KB of shared memory");
+        split_S = S;
+        split_img = dalloc<uint8_t>(split_b2p_image_bytes(g, S));
+        split_eA = dalloc<int>((size_t)d.NTCHOPDIM * 2 * 128);
+        k_split_prepare(g, S, split_img, split_eA, s);
+        const double* W[4] = {pf, V, D, T};
+        const int rows[4] = {d.NRCHOPDIM + 1, d.NRCHOPDIM, d.NRCHOPDIM, d.NRCHOPDIM};
+        for (int q = 0; q < 4; ++q) {
+            fimg[q] = dalloc<uint8_t>(split_fold_image_bytes(g, S, rows[q]));
+            feA[q] = dalloc<int>((size_t)d.NTCHOPDIM * 2 * 128);
+            k_split_prepare_wt(g, S, W[q], rows[q], fimg[q], feA[q], s);
+        }
+    } else if (p.precision != MLEGS_PREC_FP64) {
+        throw ApiError(MLEGS_ERR_ARG, "unknown precision");
+    }
     for (int q = 0; q < 24; ++q) {
         Field* f = new_field(MLEGS_FFF, false);
         temps.push_back(f);
@@ -1117,7 +1157,12 @@ int mlegs_destroy(mlegs_ctx* ctx) {
 const char* mlegs_last_error(const mlegs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int mlegs_sync(mlegs_ctx* ctx) {
-    return guard(ctx, [&] { CK(cudaStreamSynchronize(ctx->s)); });
+    return guard(ctx, [&] {
+        CK(cudaStreamSynchronize(ctx->s));
+        int e = 0;
+        CK(cudaMemcpy(&e, ctx->split_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) throw CudaError("tensor-core GEMM: a bounded wait timed out (results invalid)");
+    });
 }
 
 int mlegs_dims(const mlegs_ctx* c, int32_t out[9]) {
@@ -1439,7 +1484,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 10) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 12) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1477,13 +1522,23 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     k_theta_fused(g, ctx->fft, in, out, 1.0, 1.0, 1, s);
                 } break;
                 case 9: k_horfft_warp(g, ctx->fft, a->data, b->data, +1, s); break;
-                default: k_horfft_warp(g, ctx->fft, a->data, b->data, -1, s); break;
+                case 11:
+                    if (!ctx->split_S) throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
+                    k_split_b2p(g, ctx->split_S, ctx->split_img, ctx->split_eA, a->data, b->data, nullptr, 0,
+                                ctx->split_err, s);
+                    break;
+                case 10: k_horfft_warp(g, ctx->fft, a->data, b->data, -1, s); break;
+                case 12:
+                    if (!ctx->split_S) throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
+                    k_split_fold(g, ctx->split_S, ctx->fimg[0], ctx->feA[0], d.NRCHOPDIM + 1, a->data, b->data, 0,
+                                 0, 0, 0, 1, ctx->split_err, s);
+                    break;
             }
         };
         const double B16 = 16.0;
         double bytes = 0.0;
         switch (kernel) {
-            case 0: case 1: bytes = B16 * ((double)d.fff() + (double)d.pff()); break;
+            case 0: case 1: case 11: case 12: bytes = B16 * ((double)d.fff() + (double)d.pff()); break;
             case 2: case 3: bytes = B16 * ((double)d.pff() + (double)d.pfp()); break;
             case 4: case 5: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
             case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written

@@ -269,7 +269,7 @@ def test_initial_state_matches_oracle(env):
         assert abs(ln - R.LN) < 1e-12
 
 
-def _run_pair(cfg, nsteps, graph=False):
+def _run_pair(cfg, nsteps, graph=False, **ctx_kw):
     import mlegs_b200 as M
     from oracle import boussinesq as BQ
     from oracle import layout
@@ -281,7 +281,7 @@ def _run_pair(cfg, nsteps, graph=False):
     s.initialize()
     for _ in range(nsteps):
         s.step()
-    ctx = M.Context(cfg)
+    ctx = M.Context(cfg, **ctx_kw)
     fp, fc, fb = M.initial_state(ctx)
     ctx.initialize(fp, fc, fb)
     ctx.step(nsteps, graph=graph)

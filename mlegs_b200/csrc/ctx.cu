@@ -707,20 +707,20 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     split_err = dalloc<int>(1);
     CK(cudaMemsetAsync(split_err, 0, sizeof(int), s));
     if (p.precision == MLEGS_PREC_SPLIT) {
-        const int S = p.split_slices > 0 ? p.split_slices : 5;
-        if (!split_supported(g, S) || !split_fold_supported(g, S, d.NRCHOPDIM + 1))
+        const int S = p.split_slices > 0 ? p.split_slices : 6;
+        if (!split_supported(g, S, d.NRCHOPDIM + 1))
             throw ApiError(MLEGS_ERR_ARG, "MLEGS_PREC_SPLIT: needs 3 <= split_slices <= 6, NR <= 256 and the "
-                                          "slice tiles within 227 KB of shared memory");
+                                          "slice stages within 227 KB of shared memory");
         split_S = S;
-        split_img = dalloc<uint8_t>(split_b2p_image_bytes(g, S));
+        split_img = dalloc<uint8_t>(split_image_bytes(g, S, 0, 0));
         split_eA = dalloc<int>((size_t)d.NTCHOPDIM * 2 * 128);
-        k_split_prepare(g, S, split_img, split_eA, s);
+        k_split_prepare(g, S, 0, pf, 0, split_img, split_eA, s);
         const double* W[4] = {pf, V, D, T};
         const int rows[4] = {d.NRCHOPDIM + 1, d.NRCHOPDIM, d.NRCHOPDIM, d.NRCHOPDIM};
         for (int q = 0; q < 4; ++q) {
-            fimg[q] = dalloc<uint8_t>(split_fold_image_bytes(g, S, rows[q]));
+            fimg[q] = dalloc<uint8_t>(split_image_bytes(g, S, 1, rows[q]));
             feA[q] = dalloc<int>((size_t)d.NTCHOPDIM * 2 * 128);
-            k_split_prepare_wt(g, S, W[q], rows[q], fimg[q], feA[q], s);
+            k_split_prepare(g, S, 1, W[q], rows[q], fimg[q], feA[q], s);
         }
     } else if (p.precision != MLEGS_PREC_FP64) {
         throw ApiError(MLEGS_ERR_ARG, "unknown precision");

@@ -86,16 +86,15 @@ void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s);
 void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s);
 
 // Legendre transforms (FP64 and split-BF16 tensor-core forms).
-bool split_supported(const DevGrid& g, int S);
-size_t split_b2p_image_bytes(const DevGrid& g, int S);
-void k_split_prepare(const DevGrid& g, int S, uint8_t* img, int* eA, cudaStream_t s);
+// Split-BF16 tensor-core forms (split_gemm.cu).  mode 0: RTRAN(+1) images from
+// PF; mode 1: fold images from a weight table Wt[m][n][i] with wt_rows rows.
+bool split_supported(const DevGrid& g, int S, int wt_rows);
+size_t split_image_bytes(const DevGrid& g, int S, int mode, int wt_rows);
+void k_split_prepare(const DevGrid& g, int S, int mode, const double* W, int wt_rows, uint8_t* img, int* eA,
+                     cudaStream_t s);
 void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, const double2* a, double2* b,
                  const double* ln, int pad, int* err, cudaStream_t s);
-bool split_fold_supported(const DevGrid& g, int S, int wt_rows);
-size_t split_fold_image_bytes(const DevGrid& g, int S, int wt_rows);
-void k_split_prepare_wt(const DevGrid& g, int S, const double* Wt, int wt_rows, uint8_t* img, int* eA,
-                        cudaStream_t s);
-// Same contract as k_fold_gemm (mode bit 0 = EO/OE, use_w separate), weights given as slice images.
+// Same contract as k_fold_gemm (mode bit 0 = EO/OE, use_w separate).
 void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
                   double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s);
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);

@@ -1,48 +1,57 @@
 // Split-BF16 (Ozaki) Legendre GEMMs on the fifth-generation tensor cores.
 //
-// RTRAN(A, +1) (mod_fft.f90:1264-1336) per m and parity p:
-//     C_p(i, c) = sum_t PF(i, 2t+p) A(2t+p, c),   B(i) = C_0 + C_1, B(NR-1-i) = C_0 - C_1
-// is computed from S slices per operand.  Each row i of PF (per m, p) and each
-// column c of A (per m) is scaled by a power of two into (-1, 1) and written as
-//     v = sum_q a_q 2^{-8(q+1)},  a_q integer, |a_0| <= 256, |a_q| <= 128 (q > 0),
-// each a_q stored in BF16 pre-multiplied by 2^{-8q} (exact).  The products
-// a_qa b_qb with qa + qb <= S-1 go to four FP32 accumulators in tensor memory:
-//     level 0 (qa+qb = 0), level 1, level 2, levels >= 3,
-// so levels 0..2 are exact (every partial sum is a multiple of the level's
-// unit 2^{-8L} and below 2^{24-8L}: K <= 128) and the rounded fourth level
-// sits near 2^-48 of the row x column scale.  The epilogue adds the four in FP64 and
-// applies the two power-of-two scales, the parity butterfly and the
-// (m, k) = (0, 0) log term.
+// Two GEMM families of the path run here when a context is created with
+// MLEGS_PREC_SPLIT:
+//   RTRAN(A, +1)  (mod_fft.f90:1264-1336), per m and parity p of n:
+//       C_p(i, c) = sum_t PF(i, 2t+p) A(2t+p, c),  B(i) = C_0 + C_1,  B(NR-1-i) = C_0 - C_1,
+//       plus the (m, k) = (0, 0) log term;
+//   fold GEMMs    RTRAN(A, -1) (mod_fft.f90:1189-1261) and the EOMUL/OEMUL
+//       products of PROJECT (mod_legops.f90:2497-2535, 2548-2648):
+//       out(n, c) (+)= s(m, k) sum_{i < NRH} Wt(n, i) F(i, c),
+//       F = x(i) +/- x(NR-1-i) (times w_i for RTRAN(-1)); the fold of row n is
+//       parity(n) xor mode.
 //
-// Kernel structure (one CTA = one m and a range of 64-column tiles):
-//   - the PF slices of both parities for this m sit in shared memory for the
-//     whole CTA (one bulk copy per slice, completion on an mbarrier);
-//   - the A-column slices are made by all threads from the FP64 field, 16
-//     K-rows at a time, into a 3-stage ring;
-//   - one thread issues tcgen05.mma (M=128, N=64, K=16, BF16 x BF16 -> F32)
-//     for the S(S+1)/2 slice pairs of each K-chunk and commits them to the
-//     ring stage's mbarrier;
-//   - the epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM
-//     lanes 32w..32w+31 = output rows i).
+// Slicing.  Each row of the weight operand (per m and parity) and each column
+// of the field operand (per m) is scaled by a power of two into (-1, 1) and
+// written as v = sum_q a_q 2^{-8(q+1)}, a_q integer, |a_0| <= 256,
+// |a_q| <= 128 (q > 0); a_q is stored in BF16 pre-multiplied by 2^{-8q}, which
+// is exact.  The products a_qa b_qb with qa + qb <= S-1 go to five FP32
+// accumulators in tensor memory, one per level L = qa + qb for L <= 3 and one
+// for L >= 4.  For K <= 128 every partial sum of levels 0..3 is a multiple of
+// 2^{-8L} below 2^{24-8L}, so those four are exact; only the last level
+// rounds, near 2^-56 of the row x column scale.  The epilogue adds the
+// levels in FP64 and applies the two power-of-two scales.
+//
+// Kernel (persistent, one CTA per SM, 256 threads):
+//   warps 0-3  epilogue: TMEM lane = output row, tcgen05.ld, FP64 combine, stores;
+//   warps 4-6  producers: split 16 K-rows x 48 columns of the FP64 field into
+//              a 4-stage shared-memory ring; thread 0 of warp 4 also brings the
+//              matching weight-slice chunk (one contiguous bulk copy from the
+//              slice image, L2-resident) onto the stage's mbarrier;
+//   warp 7     one thread issues tcgen05.mma (M=128, N=48, K=16, BF16 x BF16
+//              -> F32) for the S(S+1)/2 slice pairs of each chunk and commits
+//              them to the stage's "empty" mbarrier and, at the end of a tile,
+//              to the "tile full" mbarrier the epilogue waits on.
+// Column scales come from a small column-max kernel launched just before.
 // Shared-memory operands use the K-major no-swizzle canonical layout: core
 // matrices of 8 rows x 16 bytes, LBO = 128 B between the two K halves of a
-// K=16 step, SBO between 8-row groups.  Every wait is bounded (1 s); on a
-// timeout the kernel raises *err, drains what it issued and frees its tensor
-// memory before returning.
+// K=16 step, SBO = 256 B between 8-row groups.  Every wait is bounded (1 s);
+// on a timeout the kernel raises *err, lets every role drain, waits (bounded)
+// for what it issued, frees its tensor memory and returns.
 #include "mlegs_internal.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <stdexcept>
 
 namespace mlegs {
 
 namespace {
 
-constexpr int NT = 64;    // output columns per tile (MMA N)
-constexpr int NST = 3;    // B ring stages
-constexpr int NTHR = 128;
 constexpr uint64_t WAIT_NS = 1000000000ull;
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -87,6 +96,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(saddr(dst)),
         "l"(src), "r"(bytes), "r"(saddr(bar))
+        : "memory");
+}
+
+// 2-D tiled TMA load of one box (x = innermost coordinate) onto an mbarrier.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            saddr(dst)),
+        "l"((uint64_t)map), "r"(saddr(bar)), "r"(x), "r"(y)
         : "memory");
 }
 
@@ -175,500 +193,508 @@ __device__ __forceinline__ void split8(double (&x)[8], uint4 (&out)[S]) {
 
 }  // namespace
 
+
 // ---------------------------------------------------------------------------
-// PF slices for RTRAN(+1): image[(m*2+p)][q][rg][kc][row%8][8 bf16], row = i,
-// K index t (n = 2t+p), one row-group slab = KC*128 bytes; eA[(m*2+p)*128+i].
-template <int S>
-__global__ void pf_split_kernel(DevGrid g, uint8_t* img, int* eA, int RG, int KC) {
-    const int m = blockIdx.x, p = blockIdx.y, i = threadIdx.x;
-    if (i >= RG * 8) return;
-    const int ne = g.NRCHOPDIM + 1;
-    const int kt = (ne - p + 1) / 2;
-    const double* pf = g.pf + (size_t)m * ne * g.NRH;
-    double mx = 0.0;
-    if (i < g.NRH)
-        for (int t = 0; t < kt; ++t) mx = fmax(mx, fabs(pf[(size_t)(2 * t + p) * g.NRH + i]));
-    const int e = scale_exp(mx);
-    eA[(m * 2 + p) * 128 + i] = e;
-    const double sc = ldexp(1.0, 8 - e);
-    const size_t sbo = (size_t)KC * 128;
-    uint8_t* base = img + (size_t)(m * 2 + p) * S * RG * sbo;
-    for (int kc = 0; kc < KC; ++kc) {
-        double x[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int t = kc * 8 + u;
-            x[u] = (i < g.NRH && t < kt) ? pf[(size_t)(2 * t + p) * g.NRH + i] * sc : 0.0;
-        }
-        uint4 o[S];
-        split8<S>(x, o);
-#pragma unroll
-        for (int q = 0; q < S; ++q)
-            *(uint4*)(base + (size_t)q * RG * sbo + (size_t)(i >> 3) * sbo + kc * 128 + (i & 7) * 16) = o[q];
-    }
+namespace {
+
+constexpr int NT2 = 32;     // output columns per tile (per slice: the MMA's N is a multiple)
+constexpr int NTH2 = 288;   // 9 warps
+constexpr int NPROD = 128;  // producer threads (warps 4-7)
+constexpr uint32_t BSLICE = (NT2 / 8) * 256;  // one B slice of a chunk
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
 }
 
-struct B2PArgs {
-    const uint8_t* img;
-    const int* eA;
-    const double* in;   // FFF as doubles [m][n][2*NXCHOPDIM]
-    double* out;        // PFF as doubles [m][r][2*NXCHOPDIM]
-    const double* ln;
-    int* err;
-    int pad, RG, KC, tiles_per_cta;
-};
+// Bounded wait that gives up at once when another role has aborted.
+__device__ bool wait_ab(uint64_t* bar, uint32_t parity, volatile int* abort_f) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (!mbar_try(bar, parity)) {
+        if (*abort_f) return false;
+        if (gtimer() - t0 > WAIT_NS) {
+            *abort_f = 1;
+            return false;
+        }
+    }
+    return true;
+}
 
+// Same for 4 values -> S packed half rows (4 BF16 each).
 template <int S>
-__global__ void __launch_bounds__(NTHR, 1) split_b2p_kernel(DevGrid g, B2PArgs P) {
-    extern __shared__ __align__(1024) uint8_t sm[];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m = blockIdx.x;
-    const int ncol = 2 * g.NXCHOPDIM;
-    const int ntiles = (ncol + NT - 1) / NT;
-    const int tile0 = blockIdx.y * P.tiles_per_cta;
-    const int tile1 = min(tile0 + P.tiles_per_cta, ntiles);
-    if (tile0 >= tile1) return;
-
-    const uint32_t SBO_A = P.KC * 128;
-    const uint32_t A_par = S * P.RG * SBO_A;
-    const uint32_t A_tot = ((2 * A_par + (16 - P.RG) * SBO_A) + 1023) & ~1023u;
-    constexpr uint32_t B_slice = (NT / 8) * 256;
-    constexpr uint32_t B_stage = S * B_slice;
-    uint8_t* Asm = sm;
-    uint8_t* Bsm = sm + A_tot;
-    uint64_t* bars = (uint64_t*)(Bsm + NST * B_stage);  // [0] A full, [1..NST] MMA done
-    uint32_t* tslot = (uint32_t*)(bars + 1 + NST);
-    int* abort_f = (int*)(tslot + 1);
-    int* eB = abort_f + 1;                               // [NT]
-    double* cmax = (double*)(((uintptr_t)(eB + NT) + 15) & ~(uintptr_t)15);  // [2][NT]
-
-    int nn = g.NRCHOP + P.pad - m;
-    if (nn < 0) nn = 0;
-    const int kp[2] = {(nn + 1) / 2, nn / 2};
-    const int nch[2] = {(kp[0] + 15) / 16, (kp[1] + 15) / 16};
-    const double* in = P.in + (size_t)m * g.NRCHOPDIM * ncol;
-    double* out = P.out + (size_t)m * g.NR * ncol;
-
-    if (warp == 0) tmem_alloc(tslot, 512);
-    if (tid == 0) {
-        for (int q = 0; q < 1 + NST; ++q) mbar_init(&bars[q], 1);
-        *abort_f = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+__device__ __forceinline__ void split4(double (&x)[4], uint2 (&out)[S]) {
+    uint32_t w[S][2];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        double v = x[u];
+        double sc = 1.0;
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            const double a = rint(v);
+            v = (v - a) * 256.0;
+            const unsigned short b = __bfloat16_as_ushort(__float2bfloat16_rn((float)(a * sc)));
+            sc *= 0.00390625;
+            if (u & 1) w[q][u >> 1] |= (uint32_t)b << 16;
+            else w[q][u >> 1] = b;
+        }
     }
-    __syncthreads();
-    tc_after();
-    const uint32_t tbase = *tslot;
-    bool a_issued = false;
-    if (tid == 0 && nn > 0) {
-        const uint8_t* src = P.img + (size_t)(m * 2) * A_par;
-        mbar_expect_tx(&bars[0], 2 * A_par);
-        for (int q = 0; q < 2 * S; ++q) bulk_g2s(Asm + q * (A_par / S), src + (size_t)q * (A_par / S), A_par / S, &bars[0]);
-        a_issued = true;
-    }
-    bool a_ready = false;
-    uint32_t gchunk = 0;
-    constexpr uint32_t IDESC = idesc_bf16(128, NT);
-    const uint32_t a_base = saddr(Asm), b_base = saddr(Bsm);
+#pragma unroll
+    for (int q = 0; q < S; ++q) out[q] = make_uint2(w[q][0], w[q][1]);
+}
 
-    for (int tile = tile0; tile < tile1; ++tile) {
-        const int c0 = tile * NT;
-        const int j = tid % NT, h = tid / NT;
-        const int col = c0 + j;
-        // column scale over all n < nn of this column (parity h rows by this thread)
-        double mx = 0.0;
-        if (col < ncol)
-            for (int t = 0; t < kp[h]; ++t) mx = fmax(mx, fabs(in[(size_t)(2 * t + h) * ncol + col]));
-        cmax[h * NT + j] = mx;
-        __syncthreads();
-        if (tid < NT) eB[tid] = scale_exp(fmax(cmax[tid], cmax[NT + tid]));
-        __syncthreads();
-        const double bsc = ldexp(1.0, 8 - eB[j]);
-        const int total = nch[0] + nch[1];
-        for (int ci = 0; ci < total; ++ci) {
-            const int p = ci < nch[0] ? 0 : 1;
-            const int c = p ? ci - nch[0] : ci;
-            const uint32_t stage = gchunk % NST, use = gchunk / NST;
-            if (use > 0 && !mbar_wait(&bars[1 + stage], (use - 1) & 1)) atomicExch(abort_f, 1);
-            // B chunk: K rows t = 16c + 8h + u of parity p, column j
+}  // namespace
+
+// Weight slice images, chunk-contiguous:
+//   img[((mp * NCH + c) * S + q) * RG * 256 + rg * 256 + kc2 * 128 + row8 * 16]
+// mp = m * 2 + parity, chunk c = 16 K values, rg = row / 8; eA[mp * 128 + row].
+// MODE 0 (RTRAN +1): rows i < NRH, K index t with n = 2t + parity (table PF).
+// MODE 1 (fold):     rows r with n = 2r + parity < wt_rows, K index i < NRH.
+template <int S, int MODE>
+__global__ void slice_image_kernel(DevGrid g, const double* W, int wt_rows, uint8_t* img, int* eA, int RG,
+                                   int NCH) {
+    const int m = blockIdx.x, p = blockIdx.y, row = threadIdx.x;
+    if (row >= RG * 8) return;
+    const int mp = m * 2 + p;
+    double mx = 0.0;
+    int kt = 0;
+    const double* base = nullptr;
+    bool ok;
+    if (MODE == 0) {
+        const int ne = g.NRCHOPDIM + 1;
+        kt = (ne - p + 1) / 2;
+        base = W + (size_t)m * ne * g.NRH;
+        ok = row < g.NRH;
+        if (ok)
+            for (int t = 0; t < kt; ++t) mx = fmax(mx, fabs(base[(size_t)(2 * t + p) * g.NRH + row]));
+    } else {
+        const int n = 2 * row + p;
+        kt = g.NRH;
+        ok = n < wt_rows;
+        base = W + ((size_t)m * wt_rows + (ok ? n : 0)) * g.NRH;
+        if (ok)
+            for (int i = 0; i < g.NRH; ++i) mx = fmax(mx, fabs(base[i]));
+    }
+    const int e = scale_exp(mx);
+    eA[mp * 128 + row] = e;
+    const double sc = ldexp(1.0, 8 - e);
+    for (int c = 0; c < NCH; ++c)
+        for (int kc2 = 0; kc2 < 2; ++kc2) {
             double x[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const int t = 16 * c + 8 * h + u;
-                x[u] = (t < kp[p] && col < ncol) ? in[(size_t)(2 * t + p) * ncol + col] * bsc : 0.0;
+                const int t = 16 * c + 8 * kc2 + u;
+                double v = 0.0;
+                if (ok && t < kt) v = (MODE == 0) ? base[(size_t)(2 * t + p) * g.NRH + row] : base[t];
+                x[u] = v * sc;
             }
             uint4 o[S];
             split8<S>(x, o);
-            uint8_t* bst = Bsm + stage * B_stage + (j >> 3) * 256 + h * 128 + (j & 7) * 16;
+            uint8_t* dst = img + ((size_t)(mp * NCH + c) * S) * RG * 256 + (row >> 3) * 256 + kc2 * 128 + (row & 7) * 16;
 #pragma unroll
-            for (int q = 0; q < S; ++q) *(uint4*)(bst + q * B_slice) = o[q];
-            fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                if (!a_ready) {
-                    if (!mbar_wait(&bars[0], 0)) atomicExch(abort_f, 1);
-                    a_ready = true;
-                }
-                tc_after();
-                if (*abort_f == 0) {
-                    const uint32_t a_par = a_base + p * A_par + c * 256;
-                    const uint32_t b_stg = b_base + stage * B_stage;
-                    bool first = (c == 0);
-                    uint32_t init_mask = 0;
-                    for (int qa = 0; qa < S; ++qa)
-                        for (int qb = 0; qb + qa < S; ++qb) {
-                            const int lv = min(qa + qb, 3);
-                            const uint32_t d = tbase + (uint32_t)((p * 4 + lv) * NT);
-                            const uint64_t ad = sdesc(a_par + qa * P.RG * SBO_A, 128, SBO_A);
-                            const uint64_t bd = sdesc(b_stg + qb * B_slice, 128, 256);
-                            const uint32_t acc = (!first || (init_mask >> lv) & 1) ? 1u : 0u;
-                            mma_bf16(d, ad, bd, IDESC, acc);
-                            init_mask |= 1u << lv;
-                        }
-                }
-                mma_commit(&bars[1 + stage]);
-            }
-            ++gchunk;
+            for (int q = 0; q < S; ++q) *(uint4*)(dst + (size_t)q * RG * 256) = o[q];
         }
-        // all MMAs of this tile complete
-        if (total > 0) {
-            const uint32_t ls = (gchunk - 1) % NST, lu = (gchunk - 1) / NST;
-            if (!mbar_wait(&bars[1 + ls], lu & 1)) atomicExch(abort_f, 1);
-        }
-        tc_after();
-        __syncthreads();
-        if (*abort_f) break;
-        // epilogue: row i = TMEM lane
-        const int i = warp * 32 + lane;
-        const bool row_ok = i < g.NRH;
-        const int eAe = row_ok ? P.eA[(m * 2 + 0) * 128 + i] : 0;
-        const int eAo = row_ok ? P.eA[(m * 2 + 1) * 128 + i] : 0;
-        const double lnv = (m == 0 && P.ln) ? *P.ln : 0.0;
-        const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
-        for (int cc = 0; cc < NT / 16; ++cc) {
-            double cp[2][16];
-#pragma unroll
-            for (int p = 0; p < 2; ++p) {
-                float a[4][16];
-#pragma unroll
-                for (int lv = 0; lv < 4; ++lv) tmem_ld16(tl + (uint32_t)((p * 4 + lv) * NT + cc * 16), a[lv]);
-                tmem_ld_wait();
-#pragma unroll
-                for (int q = 0; q < 16; ++q)  // level 3 exists only when S > 3
-                    cp[p][q] = nch[p] ? ((double)a[0][q] + (double)a[1][q]) +
-                                            ((double)a[2][q] + (S > 3 ? (double)a[3][q] : 0.0))
-                                      : 0.0;
-            }
-            if (!row_ok) continue;
-#pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int jj = cc * 16 + q;
-                const int cl = c0 + jj;
-                if (cl >= ncol) continue;
-                const double ce = ldexp(cp[0][q], eAe + eB[jj] - 16);
-                const double co = ldexp(cp[1][q], eAo + eB[jj] - 16);
-                double lo = ce + co, hi = ce - co;
-                if (cl == 0 && lnv != 0.0) {
-                    lo += lnv * g.lnx[i];
-                    hi += lnv * g.lnx[g.NR - 1 - i];
-                }
-                out[(size_t)i * ncol + cl] = lo;
-                out[(size_t)(g.NR - 1 - i) * ncol + cl] = hi;
-            }
-        }
-        tc_before();
-        __syncthreads();
-    }
-    // drain: nothing of ours may still be writing shared or tensor memory
-    if (tid == 0) {
-        if (a_issued && !a_ready) mbar_wait(&bars[0], 0);
-        if (*abort_f) atomicExch(P.err, 1);
-    }
-    __syncthreads();
-    if (warp == 0) tmem_dealloc(tbase, 512);
 }
 
-// ---------------------------------------------------------------------------
-// Fold GEMMs: RTRAN(A, -1) (mod_fft.f90:1189-1261) and the EOMUL/OEMUL
-// products of PROJECT (mod_legops.f90:2497-2535, 2548-2648):
-//     out(n, c) (+)= s(m, k) sum_{i < NRH} Wt(n, i) F(i, c),
-//     F = x(i) + x(NR-1-i) (even fold) or x(i) - x(NR-1-i) (odd fold), times w_i
-//     for RTRAN(-1); the fold of row n is parity(n) xor mode.
-// One CTA computes the rows n = 2r + pr (r = TMEM lane) of one parity pr for
-// one m and a group of 64-column tiles, so both operands and the four level
-// accumulators (256 TMEM columns) fit twice per SM.  Wt slices: image
-// [(m*2+pr)][q][rg][kc][r%8][8 bf16] with K = i; eA[(m*2+pr)*128 + r].
-template <int S>
-__global__ void wt_split_kernel(DevGrid g, const double* Wt, int wt_rows, uint8_t* img, int* eA, int RG, int KC) {
-    const int m = blockIdx.x, pr = blockIdx.y, r = threadIdx.x;
-    if (r >= RG * 8) return;
-    const int n = 2 * r + pr;
-    const double* w = Wt + ((size_t)m * wt_rows + n) * g.NRH;
-    const bool ok = n < wt_rows;
-    double mx = 0.0;
-    if (ok)
-        for (int i = 0; i < g.NRH; ++i) mx = fmax(mx, fabs(w[i]));
-    const int e = scale_exp(mx);
-    eA[(m * 2 + pr) * 128 + r] = e;
-    const double sc = ldexp(1.0, 8 - e);
-    const size_t sbo = (size_t)KC * 128;
-    uint8_t* base = img + (size_t)(m * 2 + pr) * S * RG * sbo;
-    for (int kc = 0; kc < KC; ++kc) {
-        double x[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int i = kc * 8 + u;
-            x[u] = (ok && i < g.NRH) ? w[i] * sc : 0.0;
-        }
-        uint4 o[S];
-        split8<S>(x, o);
-#pragma unroll
-        for (int q = 0; q < S; ++q)
-            *(uint4*)(base + (size_t)q * RG * sbo + (size_t)(r >> 3) * sbo + kc * 128 + (r & 7) * 16) = o[q];
-    }
+__device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Collective OR over the 128 producer threads (named barrier 1).
+// Exact 2^e for -1022 <= e <= 1023.
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+__device__ __forceinline__ bool bar_producers_or(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
 }
 
-struct FoldArgs {
+struct SplitArgs {
     const uint8_t* img;
     const int* eA;
-    const double* in;   // PFF as doubles [m][r][2*NXCHOPDIM]
-    double* out;        // FFF as doubles [m][n][2*NXCHOPDIM]
+    const double* in;
+    double* out;
+    const double* ln;  // MODE 0: A%LN of the input (may be null)
     int* err;
-    int pad, RG, KC, tiles_per_cta, mode, scale, accumulate, use_w;
+    int pad, RG, NCH, trows;
+    int mode, scale, accumulate, use_w;  // MODE 1
 };
 
-template <int S>
-__global__ void __launch_bounds__(NTHR, 2) split_fold_kernel(DevGrid g, FoldArgs P) {
+// One work item = (m[, parity of n], 48-column tile).  Per item the producers
+// stage the item's FP64 field columns in shared memory (one bulk copy per
+// row, double-buffered one item ahead), take the column maxima there, and
+// split 16-row chunks into the ring.
+template <int S, int MODE, int NS>
+__global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArgs P,
+                                                            const __grid_constant__ CUtensorMap fmap) {
+    constexpr int NL = S;  // one accumulator per level qa + qb
+    constexpr uint32_t TCOLS = 512;
+    constexpr int NBUF = (MODE == 0) ? 1 : 2;  // accumulator sets in tensor memory (MODE 1: 2 x 240 columns)
+    constexpr uint32_t TROWB = NT2 * 8;  // bytes of one staged field row
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m = blockIdx.x, pr = blockIdx.y & 1;
     const int ncol = 2 * g.NXCHOPDIM;
-    const int ntiles = (ncol + NT - 1) / NT;
-    const int tile0 = (blockIdx.y >> 1) * P.tiles_per_cta;
-    const int tile1 = min(tile0 + P.tiles_per_cta, ntiles);
-    if (tile0 >= tile1) return;
+    const int ntiles = (ncol + NT2 - 1) / NT2;
+    const int nitems = (MODE == 0 ? 1 : 2) * g.NTCHOPDIM * ntiles;
 
-    const uint32_t SBO_A = P.KC * 128;
-    const uint32_t A_img = S * P.RG * SBO_A;
-    const uint32_t A_tot = ((A_img + (16 - P.RG) * SBO_A) + 1023) & ~1023u;
-    constexpr uint32_t B_slice = (NT / 8) * 256;
-    constexpr uint32_t B_stage = S * B_slice;
-    uint8_t* Asm = sm;
-    uint8_t* Bsm = sm + A_tot;
-    uint64_t* bars = (uint64_t*)(Bsm + NST * B_stage);
-    uint32_t* tslot = (uint32_t*)(bars + 1 + NST);
-    int* abort_f = (int*)(tslot + 1);
-    int* eB = abort_f + 1;
-    double* cmax = (double*)(((uintptr_t)(eB + NT) + 15) & ~(uintptr_t)15);
+    const uint32_t SA = (uint32_t)(S * P.RG + 16 - P.RG) * 256;  // A stage incl. tail rows up to 128
+    const uint32_t SB = (uint32_t)S * BSLICE;
+    const uint32_t CB = (uint32_t)S * P.RG * 256;  // one chunk image
+    const uint32_t TB = (uint32_t)P.trows * TROWB;  // one staged field tile
+    uint8_t* tile_s = sm;                           // [2][trows][48] doubles
+    uint8_t* stA = sm + 2 * TB;
+    uint8_t* stB = stA + NS * SA;
+    int* ebs = (int*)(stB + NS * SB);               // [2][32] column exponents
+    double* cmax = (double*)(ebs + 2 * NT2);        // [4][32]
+    double* wsm = cmax + 4 * NT2;                   // [128] Gauss weights
+    uint64_t* full = (uint64_t*)(wsm + 128);
+    uint64_t* empty = full + NS;
+    uint64_t* tfull = empty + NS;     // [2]
+    uint64_t* tempty = tfull + 2;     // [2]
+    uint64_t* done = tempty + 2;
+    uint64_t* tile_full = done + 1;   // [2]
+    uint64_t* eb_ready = tile_full + 2;  // [2]
+    uint64_t* eb_free = eb_ready + 2;    // [2]
+    uint32_t* tslot = (uint32_t*)(eb_free + 2);
+    volatile int* abort_f = (volatile int*)(tslot + 1);
 
-    int nn = g.NRCHOP + P.pad - m;
-    if (nn < 0) nn = 0;
-    const int fold = pr ^ P.mode;  // 0: x_i + x_{NR-1-i}, 1: x_i - x_{NR-1-i}
-    const int nch = (g.NRH + 15) / 16;
-    const bool any_rows = pr < nn;  // some n = 2r + pr < nn
-    const double* x = P.in + (size_t)m * g.NR * ncol;
-    double* out = P.out + (size_t)m * g.NRCHOPDIM * ncol;
-
-    if (warp == 0) tmem_alloc(tslot, 256);
+    if (warp == 0) tmem_alloc(tslot, TCOLS);
     if (tid == 0) {
-        for (int q = 0; q < 1 + NST; ++q) mbar_init(&bars[q], 1);
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], NPROD + 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&tfull[q], 1);
+            mbar_init(&tempty[q], 128);
+        }
+        mbar_init(done, 1);
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&tile_full[q], 1);
+            mbar_init(&eb_ready[q], NPROD);
+            mbar_init(&eb_free[q], 128);
+        }
         *abort_f = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int i = tid; i < g.NRH; i += NTH2) wsm[i] = g.w[i];
     __syncthreads();
     tc_after();
     const uint32_t tbase = *tslot;
-    bool a_issued = false;
-    if (tid == 0 && any_rows) {
-        const uint8_t* src = P.img + (size_t)(m * 2 + pr) * A_img;
-        mbar_expect_tx(&bars[0], A_img);
-        for (int q = 0; q < S; ++q) bulk_g2s(Asm + q * (A_img / S), src + (size_t)q * (A_img / S), A_img / S, &bars[0]);
-        a_issued = true;
-    }
-    bool a_ready = false;
-    uint32_t gchunk = 0;
-    constexpr uint32_t IDESC = idesc_bf16(128, NT);
-    const uint32_t a_base = saddr(Asm), b_base = saddr(Bsm);
 
-    for (int tile = tile0; tile < tile1; ++tile) {
-        const int c0 = tile * NT;
-        const int j = tid % NT, h = tid / NT;
-        const int col = c0 + j;
-        const int total = any_rows ? nch : 0;
-        if (total > 0) {
+    auto item_info = [&](int item, int& m, int& pr, int& tile, int& nn, int& n0, int& n1) {
+        tile = item % ntiles;
+        const int mp = item / ntiles;
+        m = (MODE == 0) ? mp : mp / 2;
+        pr = (MODE == 0) ? 0 : mp % 2;
+        nn = g.NRCHOP + P.pad - m;
+        if (nn < 0) nn = 0;
+        if (MODE == 0) {
+            n0 = ((nn + 1) / 2 + 15) / 16;
+            n1 = (nn / 2 + 15) / 16;
+        } else {
+            n0 = (pr < nn) ? P.NCH : 0;
+            n1 = 0;
+        }
+    };
+
+    if (warp >= 4 && warp < 8) {
+        // ------------------------------------------------------------ producers
+        const int pt = tid - 128, j = pt % NT2, h = pt / NT2;  // h: quarter of the 16 K rows
+        // Stage the field columns of item `it` (local index k) into tile buffer k & 1:
+        // one 2-D TMA box of 48 columns x trows rows (columns past the last are
+        // filled with zeros).  Called by the whole of warp 4.
+        auto issue_tile = [&](int it, int k) {
+            int m, pr, tile, nn, n0, n1;
+            item_info(it, m, pr, tile, nn, n0, n1);
+            const bool any = (MODE == 0) ? nn > 0 : n0 > 0;
+            const int y = m * P.trows;
+            if (lane == 0) {
+                mbar_expect_tx(&tile_full[k & 1], any ? TB : 0u);
+                if (any) tma_load_2d(tile_s + (k & 1) * TB, &fmap, tile * NT2, y, &tile_full[k & 1]);
+            }
+            __syncwarp();
+        };
+        uint32_t gch = 0, issued = 0;
+        int k = 0;
+        if (warp == 4 && (int)blockIdx.x < nitems) issue_tile(blockIdx.x, 0);
+        for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++k) {
+            // all producers are done with item k-1 (its tile buffer is reused below)
+            if (bar_producers_or(*abort_f != 0)) break;
+            const bool ab = *abort_f != 0;
+            int m, pr, tile, nn, n0, n1;
+            item_info(item, m, pr, tile, nn, n0, n1);
+            if (warp == 4 && item + (int)gridDim.x < nitems) issue_tile(item + gridDim.x, k + 1);
+            const double* T = (const double*)(tile_s + (k & 1) * TB);
+            if (!ab) wait_ab(&tile_full[k & 1], (k >> 1) & 1, abort_f);
+            if (k >= 2 && !*abort_f) wait_ab(&eb_free[k & 1], ((k >> 1) - 1) & 1, abort_f);
+            const int col = tile * NT2 + j;
+            const bool cok = col < ncol;
+            const int fp = pr ^ P.mode;
+            // column maxima from the staged tile
             double mx = 0.0;
-            if (col < ncol)
-                for (int i = h; i < g.NRH; i += 2) {
-                    double f = fold ? x[(size_t)i * ncol + col] - x[(size_t)(g.NR - 1 - i) * ncol + col]
-                                    : x[(size_t)i * ncol + col] + x[(size_t)(g.NR - 1 - i) * ncol + col];
-                    if (P.use_w) f *= g.w[i];
-                    mx = fmax(mx, fabs(f));
+            if (cok) {
+                double m1 = 0.0;
+                if (MODE == 0) {
+                    int n = h;
+                    for (; n + 4 < nn; n += 8) {
+                        mx = fmax(mx, fabs(T[n * NT2 + j]));
+                        m1 = fmax(m1, fabs(T[(n + 4) * NT2 + j]));
+                    }
+                    for (; n < nn; n += 4) mx = fmax(mx, fabs(T[n * NT2 + j]));
+                } else if (n0 > 0) {
+                    const double sgn = fp ? -1.0 : 1.0;
+                    int i = h;
+                    for (; i + 4 < g.NRH; i += 8) {
+                        const double w0 = P.use_w ? wsm[i] : 1.0, w1 = P.use_w ? wsm[i + 4] : 1.0;
+                        mx = fmax(mx, fabs((T[i * NT2 + j] + sgn * T[(g.NR - 1 - i) * NT2 + j]) * w0));
+                        m1 = fmax(m1, fabs((T[(i + 4) * NT2 + j] + sgn * T[(g.NR - 5 - i) * NT2 + j]) * w1));
+                    }
+                    for (; i < g.NRH; i += 4) {
+                        const double w0 = P.use_w ? wsm[i] : 1.0;
+                        mx = fmax(mx, fabs((T[i * NT2 + j] + sgn * T[(g.NR - 1 - i) * NT2 + j]) * w0));
+                    }
                 }
-            cmax[h * NT + j] = mx;
-            __syncthreads();
-            if (tid < NT) eB[tid] = scale_exp(fmax(cmax[tid], cmax[NT + tid]));
-            __syncthreads();
-        }
-        const double bsc = ldexp(1.0, 8 - (total > 0 ? eB[j] : 0));
-        for (int c = 0; c < total; ++c) {
-            const uint32_t stage = gchunk % NST, use = gchunk / NST;
-            if (use > 0 && !mbar_wait(&bars[1 + stage], (use - 1) & 1)) atomicExch(abort_f, 1);
-            double xv[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int i = 16 * c + 8 * h + u;
-                double f = 0.0;
-                if (i < g.NRH && col < ncol) {
-                    const double lo = x[(size_t)i * ncol + col], hi = x[(size_t)(g.NR - 1 - i) * ncol + col];
-                    f = fold ? lo - hi : lo + hi;
-                    if (P.use_w) f *= g.w[i];
-                }
-                xv[u] = f * bsc;
+                mx = fmax(mx, m1);
             }
-            uint4 o[S];
-            split8<S>(xv, o);
-            uint8_t* bst = Bsm + stage * B_stage + (j >> 3) * 256 + h * 128 + (j & 7) * 16;
+            cmax[h * NT2 + j] = mx;
+            bar_producers();
+            if (h == 0)
+                ebs[(k & 1) * NT2 + j] =
+                    cok ? scale_exp(fmax(fmax(cmax[j], cmax[NT2 + j]), fmax(cmax[2 * NT2 + j], cmax[3 * NT2 + j]))) : 0;
+            bar_producers();
+            const int eb = ebs[(k & 1) * NT2 + j];
+            mbar_arrive(&eb_ready[k & 1]);
+            const double bsc = ldexp(1.0, 8 - eb);
+            for (int ci = 0; ci < n0 + n1; ++ci) {
+                const int p = (MODE == 0) ? (ci < n0 ? 0 : 1) : pr;
+                const int c = (MODE == 0 && ci >= n0) ? ci - n0 : ci;
+                double x[4];
+                if (MODE == 0) {
+                    const int kp = p ? nn / 2 : (nn + 1) / 2;
 #pragma unroll
-            for (int q = 0; q < S; ++q) *(uint4*)(bst + q * B_slice) = o[q];
-            fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                if (!a_ready) {
-                    if (!mbar_wait(&bars[0], 0)) atomicExch(abort_f, 1);
-                    a_ready = true;
-                }
-                tc_after();
-                if (*abort_f == 0) {
-                    const uint32_t a_k = a_base + c * 256;
-                    const uint32_t b_stg = b_base + stage * B_stage;
-                    uint32_t init_mask = 0;
-                    for (int qa = 0; qa < S; ++qa)
-                        for (int qb = 0; qb + qa < S; ++qb) {
-                            const int lv = min(qa + qb, 3);
-                            const uint64_t ad = sdesc(a_k + qa * P.RG * SBO_A, 128, SBO_A);
-                            const uint64_t bd = sdesc(b_stg + qb * B_slice, 128, 256);
-                            const uint32_t acc = (c > 0 || (init_mask >> lv) & 1) ? 1u : 0u;
-                            mma_bf16(tbase + (uint32_t)(lv * NT), ad, bd, IDESC, acc);
-                            init_mask |= 1u << lv;
-                        }
-                }
-                mma_commit(&bars[1 + stage]);
-            }
-            ++gchunk;
-        }
-        if (total > 0) {
-            const uint32_t ls = (gchunk - 1) % NST, lu = (gchunk - 1) / NST;
-            if (!mbar_wait(&bars[1 + ls], lu & 1)) atomicExch(abort_f, 1);
-        }
-        tc_after();
-        __syncthreads();
-        if (*abort_f) break;
-        // epilogue: TMEM lane r -> row n = 2r + pr
-        const int r = warp * 32 + lane;
-        const int n = 2 * r + pr;
-        const bool row_out = n < g.NRCHOPDIM;
-        const bool row_val = n < nn;
-        const int ea = (row_val && total > 0) ? P.eA[(m * 2 + pr) * 128 + r] : 0;
-        const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
-        for (int cc = 0; cc < NT / 16; ++cc) {
-            float a[4][16];
-            if (total > 0) {
-#pragma unroll
-                for (int lv = 0; lv < 4; ++lv) tmem_ld16(tl + (uint32_t)(lv * NT + cc * 16), a[lv]);
-                tmem_ld_wait();
-            }
-            if (!row_out) continue;
-#pragma unroll
-            for (int q = 0; q < 16; q += 2) {
-                const int cl = c0 + cc * 16 + q;  // even: real part of mode k = cl / 2
-                if (cl >= ncol) continue;
-                double re = 0.0, im = 0.0;
-                if (row_val && total > 0) {
-                    const double s0 = ((double)a[0][q] + (double)a[1][q]) +
-                                      ((double)a[2][q] + (S > 3 ? (double)a[3][q] : 0.0));
-                    const double s1 = ((double)a[0][q + 1] + (double)a[1][q + 1]) +
-                                      ((double)a[2][q + 1] + (S > 3 ? (double)a[3][q + 1] : 0.0));
-                    re = ldexp(s0, ea + eB[cc * 16 + q] - 16);
-                    im = ldexp(s1, ea + eB[cc * 16 + q + 1] - 16);
-                }
-                const int k = cl >> 1;
-                double sr = re, si = im;
-                switch (P.scale) {
-                    case 1: sr = -re; si = -im; break;
-                    case 2: { const double f = -(double)m; sr = -im * f; si = re * f; } break;  // -i m v
-                    case 3: { const double f = g.ak[k]; sr = -im * f; si = re * f; } break;     //  i k v
-                    case 4: { const double f = (double)m * g.ak[k]; sr = re * f; si = im * f; } break;
-                    default: break;
-                }
-                double* dst = out + (size_t)n * ncol + cl;
-                if (!row_val) {
-                    if (!P.accumulate) { dst[0] = 0.0; dst[1] = 0.0; }
-                } else if (P.accumulate) {
-                    dst[0] += sr;
-                    dst[1] += si;
+                    for (int u = 0; u < 4; ++u) {
+                        const int t = 16 * c + 4 * h + u;
+                        x[u] = (cok && t < kp) ? T[(2 * t + p) * NT2 + j] * bsc : 0.0;
+                    }
                 } else {
-                    dst[0] = sr;
-                    dst[1] = si;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int i = 16 * c + 4 * h + u;
+                        double f = 0.0;
+                        if (cok && i < g.NRH) {
+                            const double lo = T[i * NT2 + j], hi = T[(g.NR - 1 - i) * NT2 + j];
+                            f = fp ? lo - hi : lo + hi;
+                            if (P.use_w) f *= wsm[i];
+                        }
+                        x[u] = f * bsc;
+                    }
                 }
+                const uint32_t s = gch % NS, rnd = gch / NS;
+                if (rnd > 0 && !*abort_f) wait_ab(&empty[s], (rnd - 1) & 1, abort_f);
+                if (pt == 0 && !*abort_f) {
+                    mbar_expect_tx(&full[s], CB);
+                    bulk_g2s(stA + s * SA, P.img + (size_t)((m * 2 + p) * P.NCH + c) * CB, CB, &full[s]);
+                    ++issued;
+                }
+                uint2 o[S];
+                split4<S>(x, o);
+                uint8_t* dst = stB + s * SB + (j >> 3) * 256 + (h >> 1) * 128 + (j & 7) * 16 + (h & 1) * 8;
+#pragma unroll
+                for (int q = 0; q < S; ++q) *(uint2*)(dst + q * BSLICE) = o[q];
+                fence_async_smem();
+                mbar_arrive(&full[s]);
+                ++gch;
             }
         }
-        tc_before();
-        __syncthreads();
-    }
-    if (tid == 0) {
-        if (a_issued && !a_ready) mbar_wait(&bars[0], 0);
-        if (*abort_f) atomicExch(P.err, 1);
+        // on an abort, let what this thread issued land before the CTA exits
+        if (pt == 0 && *abort_f) {
+            const uint32_t first = issued > (uint32_t)NS ? issued - NS : 0;
+            for (uint32_t q = first; q < issued; ++q) mbar_wait(&full[q % NS], (q / NS) & 1);
+            for (int q = 0; q < 2; ++q) mbar_wait(&tile_full[(k + q) & 1], ((k + q) >> 1) & 1);
+        }
+    } else if (warp == 8) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t a0 = saddr(stA), b0 = saddr(stB);
+            uint32_t gch = 0, tt = 0;
+            for (int item = blockIdx.x; item < nitems && !*abort_f; item += gridDim.x) {
+                int m, pr, tile, nn, n0, n1;
+                item_info(item, m, pr, tile, nn, n0, n1);
+                const int buf = tt % NBUF;
+                if (tt >= (uint32_t)NBUF && !wait_ab(&tempty[buf], ((tt / NBUF) - 1) & 1, abort_f)) break;
+                tc_after();
+                bool ok = true;
+                for (int ci = 0; ci < n0 + n1; ++ci) {
+                    const int p = (MODE == 0) ? (ci < n0 ? 0 : 1) : 0;
+                    const int c = (MODE == 0 && ci >= n0) ? ci - n0 : ci;
+                    const uint32_t s = gch % NS, rnd = gch / NS;
+                    if (!wait_ab(&full[s], rnd & 1, abort_f)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_after();
+                    // A slice qa against B slices 0..S-1-qa stacked along N: the products
+                    // of levels qa..S-1 land in consecutive accumulators.
+#pragma unroll
+                    for (int qa = 0; qa < S; ++qa) {
+                        const uint64_t ad = sdesc(a0 + s * SA + qa * P.RG * 256, 128, 256);
+                        const uint64_t bd = sdesc(b0 + s * SB, 128, 256);
+                        const uint32_t idesc = idesc_bf16(128, (S - qa) * NT2);
+                        const uint32_t acc = (c > 0 || qa > 0) ? 1u : 0u;
+                        mma_bf16(tbase + (uint32_t)(buf * 256 + (p * NL + qa) * NT2), ad, bd, idesc, acc);
+                    }
+                    mma_commit(&empty[s]);
+                    ++gch;
+                }
+                if (!ok) break;
+                mma_commit(&tfull[buf]);
+                ++tt;
+            }
+            // every MMA issued has completed before the CTA frees its tensor memory
+            mma_commit(done);
+            mbar_wait(done, 0);
+        }
+    } else if (warp < 4) {
+        // ------------------------------------------------------------ epilogue
+        const int r = tid;  // TMEM lane
+        const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
+        uint32_t tt = 0;
+        for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++tt) {
+            if (__any_sync(0xffffffffu, *abort_f != 0)) break;
+            int m, pr, tile, nn, n0, n1;
+            item_info(item, m, pr, tile, nn, n0, n1);
+            const int buf = tt % NBUF;
+            const bool w1 = wait_ab(&tfull[buf], (tt / NBUF) & 1, abort_f);
+            const bool w2 = wait_ab(&eb_ready[tt & 1], (tt >> 1) & 1, abort_f);
+            if (!__all_sync(0xffffffffu, w1 && w2)) break;
+            tc_after();
+            const int c0 = tile * NT2;
+            const int* eb = ebs + (tt & 1) * NT2;
+            if (MODE == 0) {
+                const int i = r;
+                const bool row_ok = i < g.NRH;
+                const double sA0 = pow2((row_ok ? P.eA[(m * 2 + 0) * 128 + i] : 0) - 8);
+                const double sA1 = pow2((row_ok ? P.eA[(m * 2 + 1) * 128 + i] : 0) - 8);
+                const double lnv = (m == 0 && P.ln) ? *P.ln : 0.0;
+                double* out = P.out + (size_t)m * g.NR * ncol;
+                for (int cc = 0; cc < NT2 / 16; ++cc) {
+                    double cp[2][16];
+#pragma unroll
+                    for (int p = 0; p < 2; ++p) {
+                        const int np = p ? n1 : n0;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) cp[p][q] = 0.0;
+                        if (np > 0) {
+                            float a[NL][16];
+#pragma unroll
+                            for (int lv = 0; lv < NL; ++lv) tmem_ld16(tl + (uint32_t)((p * NL + lv) * NT2 + cc * 16), a[lv]);
+                            tmem_ld_wait();
+#pragma unroll
+                            for (int lv = 0; lv < NL; ++lv)
+#pragma unroll
+                                for (int q = 0; q < 16; ++q) cp[p][q] += (double)a[lv][q];
+                        }
+                    }
+                    if (!row_ok) continue;
+                    double lo[16], hi[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const double sb = pow2(eb[cc * 16 + q] - 8);
+                        const double ce = cp[0][q] * sA0 * sb;
+                        const double co = cp[1][q] * sA1 * sb;
+                        lo[q] = ce + co;
+                        hi[q] = ce - co;
+                    }
+                    if (c0 + cc * 16 == 0 && lnv != 0.0) {
+                        lo[0] += lnv * g.lnx[i];
+                        hi[0] += lnv * g.lnx[g.NR - 1 - i];
+                    }
+                    double* o1 = out + (size_t)i * ncol + c0 + cc * 16;
+                    double* o2 = out + (size_t)(g.NR - 1 - i) * ncol + c0 + cc * 16;
+                    const int nq = min(16, ncol - (c0 + cc * 16));
+                    if (nq == 16) {
+#pragma unroll
+                        for (int q = 0; q < 16; q += 2) {
+                            *(double2*)(o1 + q) = make_double2(lo[q], lo[q + 1]);
+                            *(double2*)(o2 + q) = make_double2(hi[q], hi[q + 1]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q)
+                            if (q < nq) {
+                                o1[q] = lo[q];
+                                o2[q] = hi[q];
+                            }
+                    }
+                }
+            } else {
+                const int n = 2 * r + pr;
+                const bool row_out = n < g.NRCHOPDIM, row_val = n < nn;
+                const double sA = pow2(((row_val && n0 > 0) ? P.eA[(m * 2 + pr) * 128 + r] : 0) - 8);
+                double* out = P.out + (size_t)m * g.NRCHOPDIM * ncol;
+                for (int cc = 0; cc < NT2 / 16; ++cc) {
+                    double cp[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) cp[q] = 0.0;
+                    if (n0 > 0) {
+                        float a[NL][16];
+#pragma unroll
+                        for (int lv = 0; lv < NL; ++lv) tmem_ld16(tl + (uint32_t)(buf * 256 + lv * NT2 + cc * 16), a[lv]);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int lv = 0; lv < NL; ++lv)
+#pragma unroll
+                            for (int q = 0; q < 16; ++q) cp[q] += (double)a[lv][q];
+                    }
+                    if (!row_out) continue;
+#pragma unroll
+                    for (int q = 0; q < 16; q += 2) {
+                        const int cl = c0 + cc * 16 + q;  // even: real part of mode k = cl / 2
+                        if (cl >= ncol) continue;
+                        double re = 0.0, im = 0.0;
+                        if (row_val && n0 > 0) {
+                            re = cp[q] * sA * pow2(eb[cc * 16 + q] - 8);
+                            im = cp[q + 1] * sA * pow2(eb[cc * 16 + q + 1] - 8);
+                        }
+                        const int k = cl >> 1;
+                        double sr = re, si = im;
+                        switch (P.scale) {
+                            case 1: sr = -re; si = -im; break;
+                            case 2: { const double f = -(double)m; sr = -im * f; si = re * f; } break;  // -i m v
+                            case 3: { const double f = g.ak[k]; sr = -im * f; si = re * f; } break;     //  i k v
+                            case 4: { const double f = (double)m * g.ak[k]; sr = re * f; si = im * f; } break;
+                            default: break;
+                        }
+                        double2* dst = (double2*)(out + (size_t)n * ncol + cl);
+                        if (!row_val) {
+                            if (!P.accumulate) *dst = make_double2(0.0, 0.0);
+                        } else if (P.accumulate) {
+                            const double2 v = *dst;
+                            *dst = make_double2(v.x + sr, v.y + si);
+                        } else {
+                            *dst = make_double2(sr, si);
+                        }
+                    }
+                }
+            }
+            tc_before();
+            mbar_arrive(&tempty[buf]);
+            mbar_arrive(&eb_free[tt & 1]);
+        }
     }
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tbase, 256);
+    if (tid == 0 && *abort_f) atomicExch(P.err, 1);
+    if (warp == 0) tmem_dealloc(tbase, TCOLS);
 }
 
 // ---------------------------------------------------------------------------
 // Host side.
-
-size_t split_b2p_smem(int S, int RG, int KC) {
-    const size_t sbo = (size_t)KC * 128;
-    const size_t a_par = (size_t)S * RG * sbo;
-    const size_t a_tot = ((2 * a_par + (16 - RG) * sbo) + 1023) & ~(size_t)1023;
-    const size_t b = (size_t)NST * S * (NT / 8) * 256;
-    return a_tot + b + 8 * (1 + NST) + 8 + 4 * NT + 16 + 16 * NT + 64;
-}
-
-void split_geometry(const DevGrid& g, int* RG, int* KC) {
-    const int kt = (g.NRCHOPDIM + 1 + 1) / 2;
-    const int kp = (kt + 15) / 16 * 16;
-    *RG = (g.NRH + 7) / 8;
-    *KC = kp / 8;
-}
-
-size_t split_b2p_image_bytes(const DevGrid& g, int S) {
-    int RG, KC;
-    split_geometry(g, &RG, &KC);
-    return (size_t)g.NTCHOPDIM * 2 * S * RG * KC * 128;
-}
-
-bool split_supported(const DevGrid& g, int S) {
-    if (S < 3 || S > 6 || g.NRH > 128 || g.NRH < 1) return false;
-    int RG, KC;
-    split_geometry(g, &RG, &KC);
-    return split_b2p_smem(S, RG, KC) <= 227 * 1024;
-}
-
-template <int S>
-static void launch_prepare(const DevGrid& g, uint8_t* img, int* eA, cudaStream_t s) {
-    int RG, KC;
-    split_geometry(g, &RG, &KC);
-    pf_split_kernel<S><<<dim3(g.NTCHOPDIM, 2), RG * 8, 0, s>>>(g, img, eA, RG, KC);
-    count_launch();
-}
-
-void k_split_prepare(const DevGrid& g, int S, uint8_t* img, int* eA, cudaStream_t s) {
-    switch (S) {
-        case 3: launch_prepare<3>(g, img, eA, s); break;
-        case 4: launch_prepare<4>(g, img, eA, s); break;
-        case 5: launch_prepare<5>(g, img, eA, s); break;
-        default: launch_prepare<6>(g, img, eA, s); break;
-    }
-}
 
 static int sm_count_split() {
     static int n = 0;
@@ -681,23 +707,140 @@ static int sm_count_split() {
     return n;
 }
 
+// Geometry of one slice image: RG row groups, NCH chunks of 16 K values.
+void split_geometry(const DevGrid& g, int mode, int wt_rows, int* RG, int* NCH) {
+    if (mode == 0) {
+        const int kt = (g.NRCHOPDIM + 2) / 2;  // t < ceil((NRCHOPDIM+1)/2)
+        *RG = (g.NRH + 7) / 8;
+        *NCH = (kt + 15) / 16;
+    } else {
+        *RG = ((wt_rows + 1) / 2 + 7) / 8;
+        *NCH = (g.NRH + 15) / 16;
+    }
+}
+
+static int tile_rows(const DevGrid& g, int mode) { return mode == 0 ? g.NRCHOPDIM : g.NR; }
+
+size_t split_smem(int S, int RG, int trows, int ns) {
+    const size_t sa = (size_t)(S * RG + 16 - RG) * 256, sb = (size_t)S * BSLICE;
+    return 2 * (size_t)trows * NT2 * 8 + ns * (sa + sb) + 2 * NT2 * 4 + 4 * NT2 * 8 + 128 * 8 + 8 * (2 * ns + 11) + 16 +
+           64;
+}
+
+// ring depth per mode: 4 stages where they fit, else 3, else 2
+static int split_stages(const DevGrid& g, int S, int mode, int wt_rows) {
+    int RG, NCH;
+    split_geometry(g, mode, wt_rows, &RG, &NCH);
+    for (int ns = 4; ns >= 2; --ns)
+        if (split_smem(S, RG, tile_rows(g, mode), ns) <= 227 * 1024) return ns;
+    return 0;
+}
+
+size_t split_image_bytes(const DevGrid& g, int S, int mode, int wt_rows) {
+    int RG, NCH;
+    split_geometry(g, mode, wt_rows, &RG, &NCH);
+    return (size_t)g.NTCHOPDIM * 2 * NCH * S * RG * 256;
+}
+
+bool split_supported(const DevGrid& g, int S, int wt_rows) {
+    if (S < 3 || S > 6 || g.NRH > 128 || g.NRH < 1) return false;
+    for (int mode = 0; mode < 2; ++mode) {
+        int RG, NCH;
+        split_geometry(g, mode, wt_rows, &RG, &NCH);
+        if (RG > 16 || split_stages(g, S, mode, wt_rows) == 0) return false;
+    }
+    return true;
+}
+
 template <int S>
-static void launch_b2p(const DevGrid& g, const uint8_t* img, const int* eA, const double2* a, double2* b,
-                       const double* ln, int pad, int* err, cudaStream_t s) {
-    int RG, KC;
-    split_geometry(g, &RG, &KC);
-    // at least 120 KB: one CTA per SM, so no CTA waits in tcgen05.alloc for another's 512 columns
-    const size_t smem = std::max(split_b2p_smem(S, RG, KC), (size_t)120 * 1024);
+static void prep(const DevGrid& g, int mode, const double* W, int wt_rows, uint8_t* img, int* eA, cudaStream_t s) {
+    int RG, NCH;
+    split_geometry(g, mode, wt_rows, &RG, &NCH);
+    if (mode == 0)
+        slice_image_kernel<S, 0><<<dim3(g.NTCHOPDIM, 2), RG * 8, 0, s>>>(g, W, wt_rows, img, eA, RG, NCH);
+    else
+        slice_image_kernel<S, 1><<<dim3(g.NTCHOPDIM, 2), RG * 8, 0, s>>>(g, W, wt_rows, img, eA, RG, NCH);
+    count_launch();
+}
+
+void k_split_prepare(const DevGrid& g, int S, int mode, const double* W, int wt_rows, uint8_t* img, int* eA,
+                     cudaStream_t s) {
+    switch (S) {
+        case 3: prep<3>(g, mode, W, wt_rows, img, eA, s); break;
+        case 4: prep<4>(g, mode, W, wt_rows, img, eA, s); break;
+        case 5: prep<5>(g, mode, W, wt_rows, img, eA, s); break;
+        default: prep<6>(g, mode, W, wt_rows, img, eA, s); break;
+    }
+}
+
+// Tensor map of a field as a 2-D FP64 array (ncol columns x rows), box 48 x box_rows.
+static CUtensorMap field_map(const double* base, int ncol, int rows, int box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)ncol, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ncol * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)NT2, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed for a field operand");
+    return map;
+}
+
+template <int S, int MODE, int NS>
+static void launch_ns(const DevGrid& g, const SplitArgs& A, size_t smem, int grid, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(split_b2p_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(split_gemm_kernel<S, MODE, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024);
         attr = true;
     }
-    const int ntiles = (2 * g.NXCHOPDIM + NT - 1) / NT;
-    int groups = std::max(1, std::min(ntiles, (2 * sm_count_split() + g.NTCHOPDIM - 1) / g.NTCHOPDIM));
-    const int per = (ntiles + groups - 1) / groups;
-    groups = (ntiles + per - 1) / per;
-    B2PArgs P;
+    const CUtensorMap map = field_map(A.in, 2 * g.NXCHOPDIM, g.NTCHOPDIM * A.trows, A.trows);
+    split_gemm_kernel<S, MODE, NS><<<grid, NTH2, smem, s>>>(g, A, map);
+}
+
+template <int S, int MODE>
+static void launch_split(const DevGrid& g, const SplitArgs& P, int wt_rows, cudaStream_t s) {
+    int RG, NCH;
+    split_geometry(g, MODE, wt_rows, &RG, &NCH);
+    const int ns = split_stages(g, S, MODE, wt_rows);
+    SplitArgs A = P;
+    A.RG = RG;
+    A.NCH = NCH;
+    A.trows = tile_rows(g, MODE);
+    // at least 120 KB: one CTA per SM, so no CTA waits in tcgen05.alloc for another's columns
+    const size_t smem = std::max(split_smem(S, RG, A.trows, ns), (size_t)120 * 1024);
+    const int ncol = 2 * g.NXCHOPDIM;
+    const int nitems = (MODE == 0 ? 1 : 2) * g.NTCHOPDIM * ((ncol + NT2 - 1) / NT2);
+    const int grid = std::min(nitems, sm_count_split());
+    if (ns >= 4) launch_ns<S, MODE, 4>(g, A, smem, grid, s);
+    else if (ns == 3) launch_ns<S, MODE, 3>(g, A, smem, grid, s);
+    else launch_ns<S, MODE, 2>(g, A, smem, grid, s);
+    count_launch();
+}
+
+template <int MODE>
+static void launch_any(const DevGrid& g, int S, const SplitArgs& P, int wt_rows, cudaStream_t s) {
+    switch (S) {
+        case 3: launch_split<3, MODE>(g, P, wt_rows, s); break;
+        case 4: launch_split<4, MODE>(g, P, wt_rows, s); break;
+        case 5: launch_split<5, MODE>(g, P, wt_rows, s); break;
+        default: launch_split<6, MODE>(g, P, wt_rows, s); break;
+    }
+}
+
+void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, const double2* a, double2* b,
+                 const double* ln, int pad, int* err, cudaStream_t s) {
+    SplitArgs P{};
     P.img = img;
     P.eA = eA;
     P.in = (const double*)a;
@@ -705,111 +848,23 @@ static void launch_b2p(const DevGrid& g, const uint8_t* img, const int* eA, cons
     P.ln = ln;
     P.err = err;
     P.pad = pad;
-    P.RG = RG;
-    P.KC = KC;
-    P.tiles_per_cta = per;
-    split_b2p_kernel<S><<<dim3(g.NTCHOPDIM, groups), NTHR, smem, s>>>(g, P);
-    count_launch();
+    launch_any<0>(g, S, P, 0, s);
 }
 
-void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, const double2* a, double2* b,
-                 const double* ln, int pad, int* err, cudaStream_t s) {
-    switch (S) {
-        case 3: launch_b2p<3>(g, img, eA, a, b, ln, pad, err, s); break;
-        case 4: launch_b2p<4>(g, img, eA, a, b, ln, pad, err, s); break;
-        case 5: launch_b2p<5>(g, img, eA, a, b, ln, pad, err, s); break;
-        default: launch_b2p<6>(g, img, eA, a, b, ln, pad, err, s); break;
-    }
-}
-
-// ---- fold GEMMs
-void fold_geometry(const DevGrid& g, int wt_rows, int* RG, int* KC) {
-    const int kp = (g.NRH + 15) / 16 * 16;
-    *RG = ((wt_rows + 1) / 2 + 7) / 8;
-    *KC = kp / 8;
-}
-
-size_t split_fold_smem(int S, int RG, int KC) {
-    const size_t sbo = (size_t)KC * 128;
-    const size_t a_tot = (((size_t)S * RG * sbo + (16 - RG) * sbo) + 1023) & ~(size_t)1023;
-    const size_t b = (size_t)NST * S * (NT / 8) * 256;
-    return a_tot + b + 8 * (1 + NST) + 8 + 4 * NT + 16 + 16 * NT + 64;
-}
-
-size_t split_fold_image_bytes(const DevGrid& g, int S, int wt_rows) {
-    int RG, KC;
-    fold_geometry(g, wt_rows, &RG, &KC);
-    return (size_t)g.NTCHOPDIM * 2 * S * RG * KC * 128;
-}
-
-bool split_fold_supported(const DevGrid& g, int S, int wt_rows) {
-    int RG, KC;
-    fold_geometry(g, wt_rows, &RG, &KC);
-    return RG <= 16 && g.NRH <= 128 && split_fold_smem(S, RG, KC) <= 227 * 1024;
-}
-
-template <int S>
-static void launch_wt_prepare(const DevGrid& g, const double* Wt, int wt_rows, uint8_t* img, int* eA,
-                              cudaStream_t s) {
-    int RG, KC;
-    fold_geometry(g, wt_rows, &RG, &KC);
-    wt_split_kernel<S><<<dim3(g.NTCHOPDIM, 2), RG * 8, 0, s>>>(g, Wt, wt_rows, img, eA, RG, KC);
-    count_launch();
-}
-
-void k_split_prepare_wt(const DevGrid& g, int S, const double* Wt, int wt_rows, uint8_t* img, int* eA,
-                        cudaStream_t s) {
-    switch (S) {
-        case 3: launch_wt_prepare<3>(g, Wt, wt_rows, img, eA, s); break;
-        case 4: launch_wt_prepare<4>(g, Wt, wt_rows, img, eA, s); break;
-        case 5: launch_wt_prepare<5>(g, Wt, wt_rows, img, eA, s); break;
-        default: launch_wt_prepare<6>(g, Wt, wt_rows, img, eA, s); break;
-    }
-}
-
-template <int S>
-static void launch_fold(const DevGrid& g, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
-                        double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err,
-                        cudaStream_t s) {
-    int RG, KC;
-    fold_geometry(g, wt_rows, &RG, &KC);
-    // at least 80 KB: at most two CTAs (2 x 256 TMEM columns) per SM
-    const size_t smem = std::max(split_fold_smem(S, RG, KC), (size_t)80 * 1024);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(split_fold_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
-    const int ntiles = (2 * g.NXCHOPDIM + NT - 1) / NT;
-    int groups = std::max(1, std::min(ntiles, (4 * sm_count_split() + 2 * g.NTCHOPDIM - 1) / (2 * g.NTCHOPDIM)));
-    const int per = (ntiles + groups - 1) / groups;
-    groups = (ntiles + per - 1) / per;
-    FoldArgs P;
+void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
+                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s) {
+    SplitArgs P{};
     P.img = img;
     P.eA = eA;
     P.in = (const double*)in;
     P.out = (double*)out;
     P.err = err;
     P.pad = pad;
-    P.RG = RG;
-    P.KC = KC;
-    P.tiles_per_cta = per;
     P.mode = mode & 1;
     P.scale = scale;
     P.accumulate = accumulate;
     P.use_w = use_w;
-    split_fold_kernel<S><<<dim3(g.NTCHOPDIM, 2 * groups), NTHR, smem, s>>>(g, P);
-    count_launch();
-}
-
-void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
-                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s) {
-    switch (S) {
-        case 3: launch_fold<3>(g, img, eA, wt_rows, in, out, mode, scale, accumulate, pad, use_w, err, s); break;
-        case 4: launch_fold<4>(g, img, eA, wt_rows, in, out, mode, scale, accumulate, pad, use_w, err, s); break;
-        case 5: launch_fold<5>(g, img, eA, wt_rows, in, out, mode, scale, accumulate, pad, use_w, err, s); break;
-        default: launch_fold<6>(g, img, eA, wt_rows, in, out, mode, scale, accumulate, pad, use_w, err, s); break;
-    }
+    launch_any<1>(g, S, P, wt_rows, s);
 }
 
 }  // namespace mlegs

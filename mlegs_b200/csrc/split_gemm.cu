@@ -16,51 +16,52 @@
 // written as v = sum_q a_q 2^{-8(q+1)}, a_q integer, |a_0| <= 256,
 // |a_q| <= 128 (q > 0); a_q is stored in BF16 pre-multiplied by 2^{-8q}, which
 // is exact.  The products a_qa b_qb with qa + qb <= S-1 go to five FP32
-// accumulators in tensor memory, one per level L = qa + qb for L <= 3 and one
-// for L >= 4.  For K <= 128 every partial sum of levels 0..3 is a multiple of
-// 2^{-8L} below 2^{24-8L}, so those four are exact; only the last level
-// rounds, near 2^-56 of the row x column scale.  The epilogue adds the
-// levels in FP64 and applies the two power-of-two scales.
+// accumulators in tensor memory, one per level L = qa + qb.  For K <= 128
+// every partial sum of levels 0..3 is a multiple of 2^{-8L} below 2^{24-8L},
+// so those four are exact; levels 4 and 5 round near 2^-56 of the row x
+// column scale.  The epilogue adds the levels in FP64 and applies the two
+// power-of-two scales.
 //
-// Kernel (persistent, one CTA per SM, 256 threads):
+// Kernel (persistent, one CTA per SM, 288 threads):
 //   warps 0-3  epilogue: TMEM lane = output row, tcgen05.ld, FP64 combine, stores;
-//   warps 4-6  producers: split 16 K-rows x 48 columns of the FP64 field into
-//              a 4-stage shared-memory ring; thread 0 of warp 4 also brings the
-//              matching weight-slice chunk (one contiguous bulk copy from the
-//              slice image, L2-resident) onto the stage's mbarrier;
-//   warp 7     one thread issues tcgen05.mma (M=128, N=48, K=16, BF16 x BF16
-//              -> F32) for the S(S+1)/2 slice pairs of each chunk and commits
-//              them to the stage's "empty" mbarrier and, at the end of a tile,
-//              to the "tile full" mbarrier the epilogue waits on.
-// Column scales come from a small column-max kernel launched just before.
+//   warps 4-7  producers: stage the work item's FP64 field columns (32 wide,
+//              all K rows) in shared memory with 16-byte cp.async copies one
+//              item ahead, take the column maxima there, and split 16-row
+//              chunks into a ring of shared-memory stages; in RTRAN(+1) mode
+//              one of them also brings the matching weight-slice chunk (one
+//              contiguous bulk copy of the L2-resident slice image) onto the
+//              stage's mbarrier, in fold mode the weight chunks of one
+//              (m, parity) stay resident across its column tiles;
+//   warp 8     one thread issues tcgen05.mma (M=128, K=16, BF16 x BF16 -> F32):
+//              per chunk and weight slice qa a single MMA against the field
+//              slices 0..S-1-qa stacked along N, whose products land in the
+//              consecutive level accumulators qa..S-1; commits free the ring
+//              stage and, per tile, hand the accumulators to the epilogue
+//              (double-buffered in tensor memory in fold mode).
 // Shared-memory operands use the K-major no-swizzle canonical layout: core
 // matrices of 8 rows x 16 bytes, LBO = 128 B between the two K halves of a
-// K=16 step, SBO = 256 B between 8-row groups.  Every wait is bounded (1 s);
-// on a timeout the kernel raises *err, lets every role drain, waits (bounded)
-// for what it issued, frees its tensor memory and returns.
+// K=16 step, SBO = 256 B between 8-row groups.  Every wait is bounded (about
+// one second of SM cycles); on a timeout the kernel raises *err, lets every
+// role drain, waits (bounded) for what it issued, frees its tensor memory and
+// returns.
 #include "mlegs_internal.h"
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstdint>
-#include <stdexcept>
 
 namespace mlegs {
 
 namespace {
 
-constexpr uint64_t WAIT_NS = 1000000000ull;
+constexpr uint64_t WAIT_NS = 2000000000ull;  // cycles
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint64_t gtimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+// SM cycle counter; the wait limits below are in cycles (2e9 cycles is about
+// one second at the B200's clocks).
+__device__ __forceinline__ uint64_t gtimer() { return (uint64_t)clock64(); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
@@ -83,7 +84,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of `parity` to complete; false after WAIT_NS.
+// Waits for the phase of `parity` to complete; false after WAIT_NS cycles.
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = gtimer();
@@ -99,13 +100,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
-// 2-D tiled TMA load of one box (x = innermost coordinate) onto an mbarrier.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-            saddr(dst)),
-        "l"((uint64_t)map), "r"(saddr(bar)), "r"(x), "r"(y)
-        : "memory");
+// 16-byte asynchronous global -> shared copy (zero fill when src_bytes = 0).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+// Arrive on `bar` once this thread's earlier cp.async copies have landed.
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(saddr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -168,6 +170,21 @@ __device__ __forceinline__ int scale_exp(double mx) {
     return e < -990 ? -990 : e;  // keeps 2^{8-e} finite; such columns hold no significant value
 }
 
+// One slicing step on v (|v| < 256 on entry, an FP64 value): returns the BF16
+// bits of rint(v) * 2^{-8q} and leaves the remainder (v - rint(v)) * 256 in v.
+// Exact arithmetic without conversion instructions: adding 1.5 * 2^52 rounds
+// to the nearest integer and leaves it in the low word of the sum; adding
+// 1.5 * 2^23 to it as a float and subtracting again gives the FP32 value; a
+// value with at most 8 significant bits has its BF16 bits in the FP32's upper half.
+__device__ __forceinline__ uint32_t slice_step(double& v, float sc) {
+    const double t = v + 6755399441055744.0;         // 1.5 * 2^52
+    const double a = t - 6755399441055744.0;         // rint(v)
+    v = (v - a) * 256.0;
+    const int ai = __double2loint(t);                // rint(v) as an integer
+    const float fa = __int_as_float(0x4B400000 + ai) - 12582912.0f;  // (float) ai, exact for |ai| < 2^22
+    return __float_as_uint(fa * sc) >> 16;
+}
+
 // Slices of 8 values (already multiplied by 2^{8-e}, |x| < 256) -> S packed
 // rows of 8 BF16 each; slice q holds a_q 2^{-8q}.
 template <int S>
@@ -176,14 +193,12 @@ __device__ __forceinline__ void split8(double (&x)[8], uint4 (&out)[S]) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
         double v = x[u];
-        double sc = 1.0;
+        float sc = 1.0f;
 #pragma unroll
         for (int q = 0; q < S; ++q) {
-            const double a = rint(v);
-            v = (v - a) * 256.0;
-            const unsigned short b = __bfloat16_as_ushort(__float2bfloat16_rn((float)(a * sc)));
-            sc *= 0.00390625;
-            if (u & 1) w[q][u >> 1] |= (uint32_t)b << 16;
+            const uint32_t b = slice_step(v, sc);
+            sc *= 0.00390625f;
+            if (u & 1) w[q][u >> 1] |= b << 16;
             else w[q][u >> 1] = b;
         }
     }
@@ -227,14 +242,12 @@ __device__ __forceinline__ void split4(double (&x)[4], uint2 (&out)[S]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         double v = x[u];
-        double sc = 1.0;
+        float sc = 1.0f;
 #pragma unroll
         for (int q = 0; q < S; ++q) {
-            const double a = rint(v);
-            v = (v - a) * 256.0;
-            const unsigned short b = __bfloat16_as_ushort(__float2bfloat16_rn((float)(a * sc)));
-            sc *= 0.00390625;
-            if (u & 1) w[q][u >> 1] |= (uint32_t)b << 16;
+            const uint32_t b = slice_step(v, sc);
+            sc *= 0.00390625f;
+            if (u & 1) w[q][u >> 1] |= b << 16;
             else w[q][u >> 1] = b;
         }
     }
@@ -330,8 +343,7 @@ struct SplitArgs {
 // row, double-buffered one item ahead), take the column maxima there, and
 // split 16-row chunks into the ring.
 template <int S, int MODE, int NS>
-__global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArgs P,
-                                                            const __grid_constant__ CUtensorMap fmap) {
+__global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArgs P) {
     constexpr int NL = S;  // one accumulator per level qa + qb
     constexpr uint32_t TCOLS = 512;
     constexpr int NBUF = (MODE == 0) ? 1 : 2;  // accumulator sets in tensor memory (MODE 1: 2 x 240 columns)
@@ -341,14 +353,23 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
     const int ncol = 2 * g.NXCHOPDIM;
     const int ntiles = (ncol + NT2 - 1) / NT2;
     const int nitems = (MODE == 0 ? 1 : 2) * g.NTCHOPDIM * ntiles;
+    // MODE 1: a contiguous item range per CTA, so consecutive items share (m,
+    // parity) and its resident weight chunks; MODE 0: items dealt round-robin.
+    const int per = (nitems + gridDim.x - 1) / gridDim.x;
+    const int ib = (MODE == 1) ? blockIdx.x * per : blockIdx.x;
+    const int ie = (MODE == 1) ? min(nitems, ib + per) : nitems;
+    const int istep = (MODE == 1) ? 1 : gridDim.x;
 
-    const uint32_t SA = (uint32_t)(S * P.RG + 16 - P.RG) * 256;  // A stage incl. tail rows up to 128
+    // MODE 0 streams one weight chunk per ring stage (SA bytes incl. the tail
+    // rows up to 128); MODE 1 keeps all NCH chunks of one (m, parity) resident.
+    const uint32_t SA = (uint32_t)(S * P.RG + 16 - P.RG) * 256;
     const uint32_t SB = (uint32_t)S * BSLICE;
     const uint32_t CB = (uint32_t)S * P.RG * 256;  // one chunk image
     const uint32_t TB = (uint32_t)P.trows * TROWB;  // one staged field tile
-    uint8_t* tile_s = sm;                           // [2][trows][48] doubles
+    uint8_t* tile_s = sm;                           // [2][trows][32] doubles
     uint8_t* stA = sm + 2 * TB;
-    uint8_t* stB = stA + NS * SA;
+    const uint32_t A_bytes = (MODE == 0) ? NS * SA : (uint32_t)P.NCH * CB + (uint32_t)(16 - P.RG) * 256;
+    uint8_t* stB = stA + A_bytes;
     int* ebs = (int*)(stB + NS * SB);               // [2][32] column exponents
     double* cmax = (double*)(ebs + 2 * NT2);        // [4][32]
     double* wsm = cmax + 4 * NT2;                   // [128] Gauss weights
@@ -357,7 +378,9 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
     uint64_t* tfull = empty + NS;     // [2]
     uint64_t* tempty = tfull + 2;     // [2]
     uint64_t* done = tempty + 2;
-    uint64_t* tile_full = done + 1;   // [2]
+    uint64_t* a_full = done + 1;       // MODE 1: resident weight chunks landed
+    uint64_t* a_free = a_full + 1;     // MODE 1: MMAs reading them completed
+    uint64_t* tile_full = a_free + 1;  // [2]
     uint64_t* eb_ready = tile_full + 2;  // [2]
     uint64_t* eb_free = eb_ready + 2;    // [2]
     uint32_t* tslot = (uint32_t*)(eb_free + 2);
@@ -366,7 +389,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
     if (warp == 0) tmem_alloc(tslot, TCOLS);
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
-            mbar_init(&full[s], NPROD + 1);
+            mbar_init(&full[s], MODE == 0 ? NPROD + 1 : NPROD);
             mbar_init(&empty[s], 1);
         }
         for (int q = 0; q < 2; ++q) {
@@ -374,8 +397,10 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
             mbar_init(&tempty[q], 128);
         }
         mbar_init(done, 1);
+        mbar_init(a_full, 1);
+        mbar_init(a_free, 1);
         for (int q = 0; q < 2; ++q) {
-            mbar_init(&tile_full[q], 1);
+            mbar_init(&tile_full[q], NPROD);
             mbar_init(&eb_ready[q], NPROD);
             mbar_init(&eb_free[q], 128);
         }
@@ -407,29 +432,49 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
         // ------------------------------------------------------------ producers
         const int pt = tid - 128, j = pt % NT2, h = pt / NT2;  // h: quarter of the 16 K rows
         // Stage the field columns of item `it` (local index k) into tile buffer k & 1:
-        // one 2-D TMA box of 48 columns x trows rows (columns past the last are
-        // filled with zeros).  Called by the whole of warp 4.
+        // 16-byte cp.async copies by all producers (columns past the last are
+        // zero-filled), completing on tile_full[k & 1].
         auto issue_tile = [&](int it, int k) {
             int m, pr, tile, nn, n0, n1;
             item_info(it, m, pr, tile, nn, n0, n1);
-            const bool any = (MODE == 0) ? nn > 0 : n0 > 0;
-            const int y = m * P.trows;
-            if (lane == 0) {
-                mbar_expect_tx(&tile_full[k & 1], any ? TB : 0u);
-                if (any) tma_load_2d(tile_s + (k & 1) * TB, &fmap, tile * NT2, y, &tile_full[k & 1]);
+            const int rows = (MODE == 0) ? nn : (n0 > 0 ? g.NR : 0);
+            const int c0 = tile * NT2;
+            const double* base = P.in + (size_t)m * P.trows * ncol + c0;
+            uint8_t* dst = tile_s + (k & 1) * TB;
+            for (int idx = pt; idx < rows * (NT2 / 2); idx += NPROD) {
+                const int r = idx / (NT2 / 2), q = idx % (NT2 / 2);
+                const bool ok = c0 + 2 * q < ncol;
+                cp_async16(dst + r * TROWB + q * 16, ok ? (const void*)(base + (size_t)r * ncol + 2 * q) : (const void*)base,
+                           ok ? 16u : 0u);
             }
-            __syncwarp();
+            cp_async_arrive(&tile_full[k & 1]);
         };
         uint32_t gch = 0, issued = 0;
         int k = 0;
-        if (warp == 4 && (int)blockIdx.x < nitems) issue_tile(blockIdx.x, 0);
-        for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++k) {
+        int cur_mp = -1;
+        uint32_t a_loads = 0;
+        if (ib < ie) issue_tile(ib, 0);
+        for (int item = ib; item < ie; item += istep, ++k) {
             // all producers are done with item k-1 (its tile buffer is reused below)
             if (bar_producers_or(*abort_f != 0)) break;
             const bool ab = *abort_f != 0;
             int m, pr, tile, nn, n0, n1;
             item_info(item, m, pr, tile, nn, n0, n1);
-            if (warp == 4 && item + (int)gridDim.x < nitems) issue_tile(item + gridDim.x, k + 1);
+            if (item + istep < ie) issue_tile(item + istep, k + 1);
+            if (MODE == 1 && m * 2 + pr != cur_mp) {
+                // bring the weight chunks of the new (m, parity) once the MMAs on the old ones are done
+                if (warp == 4) {
+                    if (lane == 0 && !ab) {
+                        if (a_loads > 0) wait_ab(a_free, (a_loads - 1) & 1, abort_f);
+                        mbar_expect_tx(a_full, (uint32_t)P.NCH * CB);
+                        const uint8_t* src = P.img + (size_t)((m * 2 + pr) * P.NCH) * CB;
+                        for (int c = 0; c < P.NCH; ++c) bulk_g2s(stA + c * CB, src + (size_t)c * CB, CB, a_full);
+                    }
+                    __syncwarp();
+                }
+                cur_mp = m * 2 + pr;
+                ++a_loads;
+            }
             const double* T = (const double*)(tile_s + (k & 1) * TB);
             if (!ab) wait_ab(&tile_full[k & 1], (k >> 1) & 1, abort_f);
             if (k >= 2 && !*abort_f) wait_ab(&eb_free[k & 1], ((k >> 1) - 1) & 1, abort_f);
@@ -497,7 +542,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
                 }
                 const uint32_t s = gch % NS, rnd = gch / NS;
                 if (rnd > 0 && !*abort_f) wait_ab(&empty[s], (rnd - 1) & 1, abort_f);
-                if (pt == 0 && !*abort_f) {
+                if (MODE == 0 && pt == 0 && !*abort_f) {
                     mbar_expect_tx(&full[s], CB);
                     bulk_g2s(stA + s * SA, P.img + (size_t)((m * 2 + p) * P.NCH + c) * CB, CB, &full[s]);
                     ++issued;
@@ -513,19 +558,27 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
             }
         }
         // on an abort, let what this thread issued land before the CTA exits
+        asm volatile("cp.async.wait_all;" ::: "memory");
         if (pt == 0 && *abort_f) {
             const uint32_t first = issued > (uint32_t)NS ? issued - NS : 0;
             for (uint32_t q = first; q < issued; ++q) mbar_wait(&full[q % NS], (q / NS) & 1);
-            for (int q = 0; q < 2; ++q) mbar_wait(&tile_full[(k + q) & 1], ((k + q) >> 1) & 1);
+            if (MODE == 1 && a_loads > 0) mbar_wait(a_full, (a_loads - 1) & 1);
         }
     } else if (warp == 8) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t a0 = saddr(stA), b0 = saddr(stB);
-            uint32_t gch = 0, tt = 0;
-            for (int item = blockIdx.x; item < nitems && !*abort_f; item += gridDim.x) {
+            uint32_t gch = 0, tt = 0, a_uses = 0;
+            int cur_mp = -1;
+            for (int item = ib; item < ie && !*abort_f; item += istep) {
                 int m, pr, tile, nn, n0, n1;
                 item_info(item, m, pr, tile, nn, n0, n1);
+                if (MODE == 1 && m * 2 + pr != cur_mp) {
+                    if (a_uses > 0) mma_commit(a_free);
+                    if (!wait_ab(a_full, a_uses & 1, abort_f)) break;
+                    cur_mp = m * 2 + pr;
+                    ++a_uses;
+                }
                 const int buf = tt % NBUF;
                 if (tt >= (uint32_t)NBUF && !wait_ab(&tempty[buf], ((tt / NBUF) - 1) & 1, abort_f)) break;
                 tc_after();
@@ -543,7 +596,8 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
                     // of levels qa..S-1 land in consecutive accumulators.
 #pragma unroll
                     for (int qa = 0; qa < S; ++qa) {
-                        const uint64_t ad = sdesc(a0 + s * SA + qa * P.RG * 256, 128, 256);
+                        const uint32_t abase = (MODE == 0) ? a0 + s * SA : a0 + c * CB;
+                        const uint64_t ad = sdesc(abase + qa * P.RG * 256, 128, 256);
                         const uint64_t bd = sdesc(b0 + s * SB, 128, 256);
                         const uint32_t idesc = idesc_bf16(128, (S - qa) * NT2);
                         const uint32_t acc = (c > 0 || qa > 0) ? 1u : 0u;
@@ -565,7 +619,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
         const int r = tid;  // TMEM lane
         const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
         uint32_t tt = 0;
-        for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++tt) {
+        for (int item = ib; item < ie; item += istep, ++tt) {
             if (__any_sync(0xffffffffu, *abort_f != 0)) break;
             int m, pr, tile, nn, n0, n1;
             item_info(item, m, pr, tile, nn, n0, n1);
@@ -721,10 +775,10 @@ void split_geometry(const DevGrid& g, int mode, int wt_rows, int* RG, int* NCH) 
 
 static int tile_rows(const DevGrid& g, int mode) { return mode == 0 ? g.NRCHOPDIM : g.NR; }
 
-size_t split_smem(int S, int RG, int trows, int ns) {
+size_t split_smem(int S, int RG, int NCH, int trows, int ns, int mode) {
     const size_t sa = (size_t)(S * RG + 16 - RG) * 256, sb = (size_t)S * BSLICE;
-    return 2 * (size_t)trows * NT2 * 8 + ns * (sa + sb) + 2 * NT2 * 4 + 4 * NT2 * 8 + 128 * 8 + 8 * (2 * ns + 11) + 16 +
-           64;
+    const size_t a = (mode == 0) ? ns * sa : (size_t)NCH * S * RG * 256 + (size_t)(16 - RG) * 256;
+    return 2 * (size_t)trows * NT2 * 8 + a + ns * sb + 2 * NT2 * 4 + 4 * NT2 * 8 + 128 * 8 + 8 * (2 * ns + 13) + 16 + 64;
 }
 
 // ring depth per mode: 4 stages where they fit, else 3, else 2
@@ -732,7 +786,7 @@ static int split_stages(const DevGrid& g, int S, int mode, int wt_rows) {
     int RG, NCH;
     split_geometry(g, mode, wt_rows, &RG, &NCH);
     for (int ns = 4; ns >= 2; --ns)
-        if (split_smem(S, RG, tile_rows(g, mode), ns) <= 227 * 1024) return ns;
+        if (split_smem(S, RG, NCH, tile_rows(g, mode), ns, mode) <= 227 * 1024) return ns;
     return 0;
 }
 
@@ -773,29 +827,6 @@ void k_split_prepare(const DevGrid& g, int S, int mode, const double* W, int wt_
     }
 }
 
-// Tensor map of a field as a 2-D FP64 array (ncol columns x rows), box 48 x box_rows.
-static CUtensorMap field_map(const double* base, int ncol, int rows, int box_rows) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            throw std::runtime_error("cuTensorMapEncodeTiled is not available");
-        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-    CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)ncol, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)ncol * sizeof(double)};
-    const cuuint32_t box[2] = {(cuuint32_t)NT2, (cuuint32_t)box_rows};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed for a field operand");
-    return map;
-}
-
 template <int S, int MODE, int NS>
 static void launch_ns(const DevGrid& g, const SplitArgs& A, size_t smem, int grid, cudaStream_t s) {
     static bool attr = false;
@@ -804,8 +835,7 @@ static void launch_ns(const DevGrid& g, const SplitArgs& A, size_t smem, int gri
                              227 * 1024);
         attr = true;
     }
-    const CUtensorMap map = field_map(A.in, 2 * g.NXCHOPDIM, g.NTCHOPDIM * A.trows, A.trows);
-    split_gemm_kernel<S, MODE, NS><<<grid, NTH2, smem, s>>>(g, A, map);
+    split_gemm_kernel<S, MODE, NS><<<grid, NTH2, smem, s>>>(g, A);
 }
 
 template <int S, int MODE>
@@ -818,7 +848,7 @@ static void launch_split(const DevGrid& g, const SplitArgs& P, int wt_rows, cuda
     A.NCH = NCH;
     A.trows = tile_rows(g, MODE);
     // at least 120 KB: one CTA per SM, so no CTA waits in tcgen05.alloc for another's columns
-    const size_t smem = std::max(split_smem(S, RG, A.trows, ns), (size_t)120 * 1024);
+    const size_t smem = std::max(split_smem(S, RG, NCH, A.trows, ns, MODE), (size_t)120 * 1024);
     const int ncol = 2 * g.NXCHOPDIM;
     const int nitems = (MODE == 0 ? 1 : 2) * g.NTCHOPDIM * ((ncol + NT2 - 1) / NT2);
     const int grid = std::min(nitems, sm_count_split());

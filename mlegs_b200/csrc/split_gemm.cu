@@ -15,7 +15,7 @@
 // of the field operand (per m) is scaled by a power of two into (-1, 1) and
 // written as v = sum_q a_q 2^{-8(q+1)}, a_q integer, |a_0| <= 256,
 // |a_q| <= 128 (q > 0); a_q is stored in BF16 pre-multiplied by 2^{-8q}, which
-// is exact.  The products a_qa b_qb with qa + qb <= S-1 go to five FP32
+// is exact.  The products a_qa b_qb with qa + qb <= S-1 go to S FP32
 // accumulators in tensor memory, one per level L = qa + qb.  For K <= 128
 // every partial sum of levels 0..3 is a multiple of 2^{-8L} below 2^{24-8L},
 // so those four are exact; levels 4 and 5 round near 2^-56 of the row x

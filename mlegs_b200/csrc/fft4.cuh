@@ -92,6 +92,44 @@ __device__ __forceinline__ void line_fft(double2 (&v)[N1], double2* S, const dou
     __syncwarp();
 }
 
+// Position of entry (k1, n2) of the N1 x N2 transpose tile inside a line slot
+// of exactly N complex values: row-major with the column XOR-swizzled by the
+// row's lane (k1 / U), so that both the column writes of step 3 (fixed k1,
+// lanes t = n2) and the row reads of step 4 (lane t reads rows t U + u) hit
+// distinct 16-byte bank groups.
+template <int N1, int N2>
+__device__ __forceinline__ int swz(int k1, int n2) {
+    constexpr int U = N1 / N2;
+    return k1 * N2 + (n2 ^ ((k1 / U) & (N2 - 1)));
+}
+
+// line_fft with the transpose done in place in the line's own slot L (N
+// complex); L's previous contents must already be consumed by all lanes.
+template <int N1, int N2, int SIGN>
+__device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, const double2* tw, int t,
+                                                 double2 (&o)[N1]) {
+    constexpr int N = N1 * N2, U = N1 / N2;
+    dft<N1, SIGN>(v, tw, N / N1);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+        double2 y = v[k1];
+        if (k1) y = cmul(twid<SIGN>(tw, t * k1), y);
+        L[swz<N1, N2>(k1, t)] = y;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int k1 = t * U + u;
+        double2 w[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = L[swz<N1, N2>(k1, n2)];
+        dft<N2, SIGN>(w, tw, N / N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) o[u * N2 + k2] = w[k2];
+    }
+    __syncwarp();
+}
+
 // Index of o[u * N2 + k2] in the line: k1 + N1 * k2 with k1 = t * U + u.
 template <int N1, int N2>
 __device__ __forceinline__ int out_index(int t, int idx) {

@@ -387,6 +387,179 @@ __global__ void __launch_bounds__(256) theta4_kernel(DevGrid g, PhysArgs A, cons
     }
 }
 
+// ------------------------------------------------------------------------
+// Fused physical stage with in-place line slots (9 slots of N per warp):
+//   round 1: RUR RUP UZ [B]  -> slots 0 1 2 3
+//   round 2: ROR ROP OZ RBR  -> slots 4 5 6 7, then per sample
+//            slot 4 <- N_r, 5 <- N_theta, 6 <- N_z (all terms), 7 <- a1 c1
+//   round 3: RBP BZ          -> slots 3 8, then slot 7 <- N_b
+//   forward: slots 4 5 6 7   -> OUT 0 1 2 3
+// Each group's transposes run inside its own line slot (fft4::swz), so a warp
+// needs 9 N complex of shared memory instead of 11 N plus padded tiles.
+namespace {
+
+// A group with no line in a round still takes part in the warp's barriers:
+// grp_inverse5 and grp_forward5 each execute exactly four __syncwarp().
+__device__ __forceinline__ void idle_group_syncs() {
+    __syncwarp();
+    __syncwarp();
+    __syncwarp();
+    __syncwarp();
+}
+
+// Inverse HORFFT of one PFP row into the natural-order packed samples L[0..N).
+template <int N1, int N2>
+__device__ __forceinline__ void grp_inverse5(const double2* __restrict__ src, bool valid, int md, int ntchop,
+                                             const double2* tw, const double2* twh, double2* L, int t) {
+    constexpr int N = N1 * N2;
+    const int mlim = md < ntchop ? md : ntchop;
+    // coalesced row load into the slot (entries m >= mlim read as zero below)
+    if (valid)
+        for (int m = t; m < mlim; m += N2) L[m] = src[m];
+    __syncwarp();
+    double2 v[N1], o[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        const int m = t + N2 * n1, mc = N - m;
+        double2 xm = make_double2(0.0, 0.0), xc = make_double2(0.0, 0.0);
+        if (valid) {
+            if (m < mlim) xm = L[m];
+            if (mc < mlim) xc = L[mc];
+        }
+        if (m == 0) xm.y = 0.0;
+        xc = fft4::conj(xc);
+        double2 sm = make_double2(xm.x + xc.x, xm.y + xc.y), d = make_double2(xm.x - xc.x, xm.y - xc.y);
+        double2 ed = fft4::cmul(fft4::conj(twh[m]), d);  // e^{+i pi m/N} d
+        v[n1] = make_double2(sm.x - ed.y, sm.y + ed.x);
+    }
+    __syncwarp();
+    fft4::line_fft_inplace<N1, N2, +1>(v, L, tw, t, o);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) L[fft4::out_index<N1, N2>(t, q)] = o[q];
+}
+
+// Forward HORFFT of the natural-order packed samples in L to a PFP row (m < md).
+template <int N1, int N2>
+__device__ __forceinline__ void grp_forward5(double2* L, bool valid, double2* __restrict__ dst, int md, int ntchop,
+                                             const double2* tw, const double2* twh, int t) {
+    constexpr int N = N1 * N2;
+    double2 v[N1], o[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = L[t + N2 * n1];
+    __syncwarp();
+    fft4::line_fft_inplace<N1, N2, -1>(v, L, tw, t, o);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) L[fft4::out_index<N1, N2>(t, q)] = o[q];  // Z_k, natural order
+    __syncwarp();
+    const double sc = 1.0 / (2.0 * N);
+    for (int m = t; m < md; m += N2) {
+        double2 zm = L[m % N], zc = fft4::conj(L[(N - m) % N]);
+        double2 sm = make_double2(zm.x + zc.x, zm.y + zc.y), d = make_double2(zm.x - zc.x, zm.y - zc.y);
+        double2 ed = fft4::cmul(twh[m], d);  // e^{-i pi m/N} d
+        double2 x = make_double2(0.5 * (sm.x + ed.y) * sc, 0.5 * (sm.y - ed.x) * sc);
+        if (m >= ntchop) x = make_double2(0.0, 0.0);
+        if (m == 0) x.y = 0.0;
+        if (valid) dst[m] = x;
+    }
+}
+
+}  // namespace
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, const double2* tw_g,
+                                                     const double2* twh_g) {
+    constexpr int N = N1 * N2, G = 32 / N2;
+    static_assert(G == 4 || G == 2 || G == 8, "4 lines per round need G in {2, 4, 8}");
+    extern __shared__ double2 sm[];
+    double2* tw = sm;
+    double2* twh = tw + (N + 1);
+    for (int q = threadIdx.x; q <= N; q += blockDim.x) {
+        tw[q] = tw_g[q];
+        twh[q] = twh_g[q];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int gid = lane / N2, t = lane % N2;
+    double2* L = twh + (N + 1) + (size_t)warp * 9 * N;
+    const int md = g.NTCHOPDIM;
+    const int nlines = g.NR * g.NX;
+    const double o2 = 2 * A.omega, n2 = A.bv0 * A.bv0;
+    for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
+        const size_t off = (size_t)line * md;
+        const double rr = g.r[line / g.NX];
+        const double ir2 = 1.0 / (rr * rr);
+        // round 1 and 2 (G = 4: one field per group; G = 2: two passes; G = 8: half the groups idle)
+        // round 1: field q (q < 3) or B (q = 3, linear terms only) -> slot q;
+        // round 2: field 3 + q -> slot 4 + q
+        for (int rd = 0; rd < 2; ++rd) {
+            for (int f0 = 0; f0 < 4; f0 += G) {
+                const int q = f0 + gid;
+                if (q < 4) {
+                    const int f = rd ? 3 + q : (q < 3 ? q : 9);
+                    const bool ok = rd || q < 3 || A.linear;
+                    grp_inverse5<N1, N2>(ok ? A.in[f] + off : nullptr, ok, md, g.NTCHOP, tw, twh,
+                                         L + (size_t)(rd ? 4 + q : q) * N, t);
+                } else {
+                    idle_group_syncs();
+                }
+            }
+            __syncwarp();
+        }
+        // round-2 products
+        for (int j = lane; j < N; j += 32) {
+            const double2 a1 = L[j], a2 = L[N + j], a3 = L[2 * N + j];
+            const double2 b1 = L[4 * N + j], b2 = L[5 * N + j], b3 = L[6 * N + j], c1 = L[7 * N + j];
+            double2 nr_ = make_double2(a2.x * b3.x - a3.x * b2.x, a2.y * b3.y - a3.y * b2.y);
+            double2 np_ = make_double2(a3.x * b1.x - a1.x * b3.x, a3.y * b1.y - a1.y * b3.y);
+            double2 nz_ = make_double2((a1.x * b2.x - a2.x * b1.x) * ir2, (a1.y * b2.y - a2.y * b1.y) * ir2);
+            if (A.linear) {
+                const double2 bp = L[3 * N + j];
+                nr_.x += o2 * a2.x;
+                nr_.y += o2 * a2.y;
+                np_.x -= o2 * a1.x;
+                np_.y -= o2 * a1.y;
+                nz_.x -= bp.x;
+                nz_.y -= bp.y;
+            }
+            L[4 * N + j] = nr_;
+            L[5 * N + j] = np_;
+            L[6 * N + j] = nz_;
+            L[7 * N + j] = make_double2(a1.x * c1.x, a1.y * c1.y);
+        }
+        __syncwarp();
+        // round 3
+        for (int f0 = 0; f0 < 4; f0 += G) {
+            const int q = f0 + gid;
+            if (q < 2)  // RBP -> slot 3, BZ -> slot 8
+                grp_inverse5<N1, N2>(A.in[7 + q] + off, true, md, g.NTCHOP, tw, twh, L + (size_t)(q ? 8 : 3) * N, t);
+            else
+                idle_group_syncs();
+        }
+        __syncwarp();
+        for (int j = lane; j < N; j += 32) {
+            const double2 a2 = L[N + j], a3 = L[2 * N + j], c2 = L[3 * N + j], c3 = L[8 * N + j];
+            const double2 bp = L[7 * N + j];
+            double2 bn_ = make_double2(-((bp.x + a2.x * c2.x) * ir2 + a3.x * c3.x),
+                                       -((bp.y + a2.y * c2.y) * ir2 + a3.y * c3.y));
+            if (A.linear) {
+                bn_.x += n2 * a3.x;
+                bn_.y += n2 * a3.y;
+            }
+            L[7 * N + j] = bn_;
+        }
+        __syncwarp();
+        // forward transforms of the four results
+        for (int f0 = 0; f0 < 4; f0 += G) {
+            const int q = f0 + gid;
+            if (q < 4)
+                grp_forward5<N1, N2>(L + (size_t)(4 + q) * N, true, A.out[q] + off, md, g.NTCHOP, tw, twh, t);
+            else
+                idle_group_syncs();
+        }
+        __syncwarp();
+    }
+}
+
 // Single-field HORFFT with the four-step blocks, G lines per warp.  dir +1: PFP -> PPP, -1: PPP -> PFP.
 template <int N1, int N2>
 __global__ void __launch_bounds__(256) horfft4_kernel(DevGrid g, const double2* src, double2* dst,
@@ -577,6 +750,27 @@ static void launch_theta4(const DevGrid& g, const FFTPlan& p, const PhysArgs& A,
 }
 
 template <int N1, int N2>
+static bool launch_theta5(const DevGrid& g, const FFTPlan& p, const PhysArgs& A, cudaStream_t s) {
+    constexpr int N = N1 * N2;
+    const size_t per_warp = (size_t)9 * N * sizeof(double2);
+    const size_t fixed = 2 * (size_t)(N + 1) * sizeof(double2);
+    int warps = (int)((227 * 1024 - fixed) / per_warp);
+    if (warps > 12) warps = 12;
+    if (warps < 1) return false;
+    const size_t sm = fixed + warps * per_warp;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(theta5_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    const int nlines = g.NR * g.NX;
+    const int blocks = std::min((nlines + warps - 1) / warps, sm_count());
+    theta5_kernel<N1, N2><<<blocks, warps * 32, sm, s>>>(g, A, p.tw_t, p.tw_h);
+    count_launch();
+    return true;
+}
+
+template <int N1, int N2>
 static void launch_horfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
                            cudaStream_t s) {
     constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
@@ -607,12 +801,12 @@ void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[1
     A.bv0 = bv0;
     A.linear = linear;
     switch (g.NTH) {
-        case 16: launch_theta4<4, 4>(g, p, A, s); return;
-        case 32: launch_theta4<8, 4>(g, p, A, s); return;
-        case 64: launch_theta4<8, 8>(g, p, A, s); return;
-        case 128: launch_theta4<16, 8>(g, p, A, s); return;
-        case 256: launch_theta4<16, 16>(g, p, A, s); return;
-        case 512: launch_theta4<32, 16>(g, p, A, s); return;
+        case 16: if (launch_theta5<4, 4>(g, p, A, s)) return; launch_theta4<4, 4>(g, p, A, s); return;
+        case 32: if (launch_theta5<8, 4>(g, p, A, s)) return; launch_theta4<8, 4>(g, p, A, s); return;
+        case 64: if (launch_theta5<8, 8>(g, p, A, s)) return; launch_theta4<8, 8>(g, p, A, s); return;
+        case 128: if (launch_theta5<16, 8>(g, p, A, s)) return; launch_theta4<16, 8>(g, p, A, s); return;
+        case 256: if (launch_theta5<16, 16>(g, p, A, s)) return; launch_theta4<16, 16>(g, p, A, s); return;
+        case 512: if (launch_theta5<32, 16>(g, p, A, s)) return; launch_theta4<32, 16>(g, p, A, s); return;
         default: break;
     }
     const int warps = 8;

@@ -1,12 +1,17 @@
 """Benchmark: Boussinesq steps/s on one B200 (or N independent replicas).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--config etd_192x128x256] [--precision fp64|split]
+                [--config etd_192x128x256] [--precision split|fp64] [--slices 6]
 
 Workload: the ETD2AB-CN timestep at NR x NTH x NX = 192 x 128 x 256 (Re 5000,
 hyperviscosity P=2 nu_p=kappa_p=1e-10, Omega 1, N 2, dt 5e-4) from a Gaussian
 q-vortex plus a seeded spectral perturbation (mlegs_b200/inputs.py), one CUDA
 graph replay per step.  Per-GPU work is fixed (replicas only, "weak").
+
+`value` is the mixed-precision step (Legendre GEMMs as split-BF16 slices on
+the tensor cores, everything else FP64); "fp64_comparison" times the plain
+FP64 GPU step beside it and reports the relative field error of the mixed
+path against the FP64 path after --error-steps steps from the same state.
 Every step touches several GB (100 MB physical fields), far above the 126 MB
 L2, so no explicit L2 flush is needed between steps.
 
@@ -37,7 +42,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="etd_192x128x256")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split"])
+    ap.add_argument("--slices", type=int, default=6, help="split-BF16 slices per operand (3..6)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 GPU step and error check")
+    ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     return ap.parse_args()
@@ -195,16 +203,42 @@ def run_reference(args, cfg, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _graph_steps(ctx, stream, steps):
+    """Device time (ms) of `steps` graph-replayed steps on the library stream."""
+    import torch
+    ctx.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.step(steps, graph=True)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _state_after(M, cfg, prec, slices, nsteps, local):
+    """(E, LN) of psi, chi, b after 1 Richardson + nsteps-1 graph steps."""
+    ctx = M.Context(cfg, precision=prec, split_slices=slices, device=local)
+    fs = M.initial_state(ctx)
+    ctx.initialize(*fs)
+    if nsteps > 1:
+        ctx.step(nsteps - 1, graph=True)
+    out = [f.download() for f in fs]
+    ctx.close()
+    return out
+
+
 def run_ours(args, cfg, ws, rank, local):
     import numpy as np
     import torch
 
     import mlegs_b200 as M
-    prec = M.PREC_FP64 if args.precision == "fp64" else M.PREC_SPLIT
-    ctx = M.Context(cfg, precision=prec, device=local)
+    split = args.precision == "split"
+    prec = M.PREC_SPLIT if split else M.PREC_FP64
+    torch.cuda.set_device(local)
+    ctx = M.Context(cfg, precision=prec, split_slices=args.slices if split else 0, device=local)
     psi, chi, b = M.initial_state(ctx)
     ctx.initialize(psi, chi, b)
-    torch.cuda.set_device(local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
     ctx.step(max(args.warmup, 1), graph=True)  # first call captures the graph
     ctx.sync()
@@ -214,15 +248,8 @@ def run_ours(args, cfg, ws, rank, local):
     barrier(ws)
     ctx.reset_launches()
     with Clocks(smi_index) as clk:
-        ctx.sync()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ctx.step(args.steps, graph=True)
-        e1.record(stream)
-        e1.synchronize()
+        ms_total = _graph_steps(ctx, stream, args.steps)
     launches = ctx.launches()
-    ms_total = e0.elapsed_time(e1)
     barrier(ws)
     ms_total = max_over_ranks(ws, ms_total)
     ms_step = ms_total / args.steps
@@ -264,7 +291,10 @@ def run_ours(args, cfg, ws, rank, local):
     pk, pk_kind = peaks()
     kernels = {}
     for name in ctx.KERNELS:
-        ms, by = ctx.kernel_time(name, reps=20)
+        try:
+            ms, by = ctx.kernel_time(name, reps=20)
+        except M.MlegsError:
+            continue  # tensor-core kernels exist only in split contexts
         kernels[name] = {"ms": ms, "bytes": by, "gbs": by / (ms * 1e-3) / 1e9}
     dom = DOMINANT
     tr = traffic_table().get(cfg.name, {}).get(dom)
@@ -272,6 +302,31 @@ def run_ours(args, cfg, ws, rank, local):
     roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": ach / pk["hbm_gbs"], "traffic": tr, "peak_source": pk_kind,
             "algorithmic_bytes_per_launch": kernels[dom]["bytes"], "ms_per_launch": kernels[dom]["ms"]}
+    ctx.close()
+
+    # ---- the plain FP64 GPU step and the error of the mixed path against it
+    compare = None
+    if split and not args.no_compare:
+        c64 = M.Context(cfg, device=local)
+        fs = M.initial_state(c64)
+        c64.initialize(*fs)
+        s64 = torch.cuda.ExternalStream(c64.stream(), device=local)
+        c64.step(max(args.warmup, 1), graph=True)
+        ms64 = _graph_steps(c64, s64, args.steps)
+        c64.close()
+        barrier(ws)
+        ms64 = max_over_ranks(ws, ms64)
+        ref = _state_after(M, cfg, M.PREC_FP64, 0, args.error_steps, local)
+        mix = _state_after(M, cfg, M.PREC_SPLIT, args.slices, args.error_steps, local)
+        errs = {}
+        for name, (E, ln), (R, rl) in zip(("psi", "chi", "b"), mix, ref):
+            errs[name] = float(np.abs(E - R).max() / np.abs(R).max())
+            errs[name + "_ln"] = float(abs(ln - rl) / max(1.0, abs(rl)))
+        fp64_value = ws * args.steps / (ms64 / 1000.0)
+        compare = {"fp64_steps_per_s": fp64_value, "fp64_ms_per_step": ms64 / args.steps,
+                   "mixed_over_fp64": value / fp64_value, "error_steps": args.error_steps,
+                   "rel_error_vs_fp64": errs, "error_bound": 1e-9,
+                   "within_bound": max(errs.values()) <= 1e-9}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -283,23 +338,22 @@ def run_ours(args, cfg, ws, rank, local):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16-split/f32/f64",
+                "vs_baseline": None, "dtype": "f64" if not split else "bf16x%d-split/f32/f64" % args.slices,
                 "data": "synthetic (seeded q-vortex + spectral perturbation)",
                 "config": {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx],
                            "chops": [cfg.nrchop, cfg.ntchop, cfg.nxchop],
                            "scheme": "ETD2AB-CN" if not cfg.adams else "AB2-CN", "dt": cfg.dt,
-                           "precision": args.precision, "graph": True,
-                           "parallelism": "replicas x%d" % ws,
+                           "precision": args.precision, "split_slices": args.slices if split else None,
+                           "graph": True, "parallelism": "replicas x%d" % ws,
                            "l2": "inputs larger than L2 (several GB touched per step)"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * nbytes,
                         "d2h_bytes_per_step": 3 * nbytes},
-                "gpu_launches": int(launches),
+                "gpu_launches": int(launches), "fp64_comparison": compare,
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    ctx.close()
 
 
-DOMINANT = "horfft_b"
+DOMINANT = "phys"
 
 
 def main():

@@ -20,6 +20,8 @@ namespace mlegs {
 
 namespace {
 constexpr int MAXW = 7;  // band width bound (7-band m = 0 systems)
+constexpr int RB = 6;    // rows whose loads are issued together; a multiple of 3 so that
+                         // the 3-row pivot window is indexed by compile-time constants
 }
 
 struct BandRowCtx {
@@ -119,49 +121,77 @@ __global__ void solve_kernel(DevGrid g, double2* A, double* ln_out, int kind, do
 #pragma unroll
         for (int b = 0; b < 4; ++b) U[a][b] = 0.0;
     }
-    for (int r = 0; r < size; ++r) {
-        double w[MAXW];
-        build_row(c, r, w);
-        double2 rhs = col[(size_t)r * st];
-        // eliminate columns r-lo .. r-1 (left to right)
-        for (int d = lo; d >= 1; --d) {
-            int cidx = r - d;
-            if (cidx < 0) continue;
-            const double* u = U[(cidx) % 3];
-            double f = w[3 - d] / u[0];
-            w[3 - d] = 0.0;
-            for (int j = 1; j <= up; ++j) {
-                int q = 3 - d + j;
-                if (q < MAXW) w[q] -= f * u[j];
+    for (int r0 = 0; r0 < size; r0 += RB) {
+        // each row reads only its own right-hand side, so the block's loads go first
+        double2 rb[RB];
+#pragma unroll
+        for (int q = 0; q < RB; ++q) rb[q] = (r0 + q < size) ? col[(size_t)(r0 + q) * st] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int r = r0 + q;  // r0 is a multiple of 3: r % 3 == q % 3
+            if (r >= size) break;
+            double w[MAXW];
+            build_row(c, r, w);
+            double2 rhs = rb[q];
+            // eliminate columns r-lo .. r-1 (left to right)
+#pragma unroll
+            for (int d = 3; d >= 1; --d) {
+                if (d > lo || r - d < 0) continue;
+                const int wi = (q - d + 3) % 3;  // (r - d) % 3
+                const double f = w[3 - d] / U[wi][0];
+                w[3 - d] = 0.0;
+#pragma unroll
+                for (int j = 1; j <= 3; ++j) {
+                    if (j > up) continue;
+                    const int qq = 3 - d + j;
+                    if (qq < MAXW) w[qq] -= f * U[wi][j];
+                }
+                rhs.x -= f * R[wi].x;
+                rhs.y -= f * R[wi].y;
             }
-            double2 pr = R[cidx % 3];
-            rhs.x -= f * pr.x;
-            rhs.y -= f * pr.y;
+            const int wr = q % 3;
+            U[wr][0] = w[3];
+#pragma unroll
+            for (int j = 1; j <= 3; ++j) U[wr][j] = (j <= up) ? w[3 + j] : 0.0;
+            R[wr] = rhs;
+#pragma unroll
+            for (int j = 0; j <= 3; ++j) scratch[((size_t)r * 4 + j) * nsys + t] = U[wr][j];
+            col[(size_t)r * st] = rhs;
         }
-        double* u = U[r % 3];
-        u[0] = w[3];
-        for (int j = 1; j <= 3; ++j) u[j] = (j <= up) ? w[3 + j] : 0.0;
-        R[r % 3] = rhs;
-        for (int j = 0; j <= 3; ++j) scratch[((size_t)r * 4 + j) * nsys + t] = u[j];
-        col[(size_t)r * st] = rhs;
     }
     // back substitution
     double2 x1 = make_double2(0.0, 0.0), x2 = x1, x3 = x1;  // x[r+1], x[r+2], x[r+3]
-    for (int r = size - 1; r >= 0; --r) {
-        double2 v = col[(size_t)r * st];
-        double u1 = scratch[((size_t)r * 4 + 1) * nsys + t];
-        double u2 = scratch[((size_t)r * 4 + 2) * nsys + t];
-        double u3 = scratch[((size_t)r * 4 + 3) * nsys + t];
-        double u0 = scratch[((size_t)r * 4 + 0) * nsys + t];
-        if (r + 1 < size) { v.x -= u1 * x1.x; v.y -= u1 * x1.y; }
-        if (r + 2 < size) { v.x -= u2 * x2.x; v.y -= u2 * x2.y; }
-        if (r + 3 < size) { v.x -= u3 * x3.x; v.y -= u3 * x3.y; }
-        v.x /= u0;
-        v.y /= u0;
-        col[(size_t)r * st] = v;
-        x3 = x2;
-        x2 = x1;
-        x1 = v;
+    for (int r1 = size - 1; r1 >= 0; r1 -= RB) {
+        double2 vb[RB];
+        double ub[RB][4];
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int r = r1 - q;
+            vb[q] = make_double2(0.0, 0.0);
+            ub[q][0] = 1.0;
+            ub[q][1] = ub[q][2] = ub[q][3] = 0.0;
+            if (r >= 0) {
+                vb[q] = col[(size_t)r * st];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) ub[q][j] = scratch[((size_t)r * 4 + j) * nsys + t];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+            const int r = r1 - q;
+            if (r < 0) break;
+            double2 v = vb[q];
+            const double u0 = ub[q][0], u1 = ub[q][1], u2 = ub[q][2], u3 = ub[q][3];
+            if (r + 1 < size) { v.x -= u1 * x1.x; v.y -= u1 * x1.y; }
+            if (r + 2 < size) { v.x -= u2 * x2.x; v.y -= u2 * x2.y; }
+            if (r + 3 < size) { v.x -= u3 * x3.x; v.y -= u3 * x3.y; }
+            v.x /= u0;
+            v.y /= u0;
+            col[(size_t)r * st] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
     }
     if (m == 0 && kind == 2) {
         // A(NN) = 0; A(:NN) = XM(:NN) y  (1310-1316)
@@ -191,7 +221,7 @@ __global__ void solve_kernel(DevGrid g, double2* A, double* ln_out, int kind, do
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln, double ln_in,
                   const double* b_ln, double* scratch, int pad, cudaStream_t s) {
     int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
-    solve_kernel<<<(nsys + 127) / 128, 128, 0, s>>>(g, a, ln_out, kind, alp, has_ln, ln_in, b_ln, scratch, pad);
+    solve_kernel<<<(nsys + 63) / 64, 64, 0, s>>>(g, a, ln_out, kind, alp, has_ln, ln_in, b_ln, scratch, pad);
     count_launch();
 }
 

@@ -104,17 +104,18 @@ __device__ __forceinline__ int swz(int k1, int n2) {
 }
 
 // line_fft with the transpose done in place in the line's own slot L (N
-// complex); L's previous contents must already be consumed by all lanes.
+// complex, element i at L[i * STRIDE]); L's previous contents must already be
+// consumed by all lanes.
 template <int N1, int N2, int SIGN>
 __device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, const double2* tw, int t,
-                                                 double2 (&o)[N1]) {
+                                                 double2 (&o)[N1], int stride = 1) {
     constexpr int N = N1 * N2, U = N1 / N2;
     dft<N1, SIGN>(v, tw, N / N1);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
         double2 y = v[k1];
         if (k1) y = cmul(twid<SIGN>(tw, t * k1), y);
-        L[swz<N1, N2>(k1, t)] = y;
+        L[swz<N1, N2>(k1, t) * stride] = y;
     }
     __syncwarp();
 #pragma unroll
@@ -122,7 +123,7 @@ __device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, c
         const int k1 = t * U + u;
         double2 w[N2];
 #pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) w[n2] = L[swz<N1, N2>(k1, n2)];
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = L[swz<N1, N2>(k1, n2) * stride];
         dft<N2, SIGN>(w, tw, N / N2);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) o[u * N2 + k2] = w[k2];

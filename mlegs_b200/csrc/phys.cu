@@ -639,20 +639,21 @@ void phys_set_attributes() {
 template <int N1, int N2>
 __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* src, double2* dst,
                                                       const double2* tw_g, int dir) {
-    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    constexpr int N = N1 * N2, G = 32 / N2;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int gid = lane / N2, t = lane % N2;
     const int MB = nw * G;
     double2* tw = sm;
-    double2* T = tw + (N + 1);                  // [N][MB + 1]
-    double2* S = T + (size_t)N * (MB + 1) + (size_t)(warp * G + gid) * TILE;
+    double2* T = tw + (N + 1);                  // [N][MB + 1]; column mloc is line m0 + mloc
     for (int q = threadIdx.x; q <= N; q += blockDim.x) tw[q] = tw_g[q];
     const int r = blockIdx.x, m0 = blockIdx.y * MB;
     const int mloc = warp * G + gid, m = m0 + mloc;
     const bool ok = m < g.NTCHOPDIM;
     const int kd = g.NXCHOPDIM, kc = g.NXCHOP, md = g.NTCHOPDIM;
     const int nmb = min(MB, md - m0);
+    double2* col = T + mloc;                    // this group's line, stride MB + 1
+    const int cs = MB + 1;
     double2 v[N1], o[N1];
     if (dir > 0) {  // PFF [m][r][k] -> PFP [r][z][m]
         __syncthreads();
@@ -665,32 +666,33 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
             else if (q >= N - kd + kc) kk = q - (N - kd);
             v[n1] = (ok && kk >= 0) ? line[kk] : make_double2(0.0, 0.0);
         }
-        fft4::line_fft<N1, N2, +1>(v, S, tw, t, o);
+        fft4::line_fft_inplace<N1, N2, +1>(v, col, tw, t, o, cs);
 #pragma unroll
-        for (int q = 0; q < N1; ++q) T[(size_t)fft4::out_index<N1, N2>(t, q) * (MB + 1) + mloc] = o[q];
+        for (int q = 0; q < N1; ++q) col[(size_t)fft4::out_index<N1, N2>(t, q) * cs] = o[q];
         __syncthreads();
         for (int e = threadIdx.x; e < N * nmb; e += blockDim.x) {
             const int z = e / nmb, ml = e - z * nmb;
-            dst[((size_t)r * N + z) * md + m0 + ml] = T[(size_t)z * (MB + 1) + ml];
+            dst[((size_t)r * N + z) * md + m0 + ml] = T[(size_t)z * cs + ml];
         }
     } else {  // PFP [r][z][m] -> PFF [m][r][k], scaled 1/NX, chopped
         __syncthreads();
         for (int e = threadIdx.x; e < N * nmb; e += blockDim.x) {
             const int z = e / nmb, ml = e - z * nmb;
-            T[(size_t)z * (MB + 1) + ml] = src[((size_t)r * N + z) * md + m0 + ml];
+            T[(size_t)z * cs + ml] = src[((size_t)r * N + z) * md + m0 + ml];
         }
         __syncthreads();
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? T[(size_t)(t + N2 * n1) * (MB + 1) + mloc] : make_double2(0.0, 0.0);
-        fft4::line_fft<N1, N2, -1>(v, S, tw, t, o);
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? col[(size_t)(t + N2 * n1) * cs] : make_double2(0.0, 0.0);
+        __syncwarp();
+        fft4::line_fft_inplace<N1, N2, -1>(v, col, tw, t, o, cs);
 #pragma unroll
-        for (int q = 0; q < N1; ++q) S[fft4::out_index<N1, N2>(t, q)] = o[q];
+        for (int q = 0; q < N1; ++q) col[(size_t)fft4::out_index<N1, N2>(t, q) * cs] = o[q];
         __syncwarp();
         const double sc = 1.0 / N;
         double2* line = dst + ((size_t)m * g.NR + r) * kd;
         for (int kk = t; kk < kd; kk += N2) {
             const int q = (kk < kc) ? kk : (N - kd + kk);
-            double2 y = S[q];
+            double2 y = col[(size_t)q * cs];
             if (ok) line[kk] = make_double2(y.x * sc, y.y * sc);
         }
     }
@@ -699,13 +701,13 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
 template <int N1, int N2>
 static void launch_verfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
                            cudaStream_t s) {
-    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
+    constexpr int N = N1 * N2, G = 32 / N2;
     int warps = 8;
     auto need = [&](int w) {
         int MB = w * G;
-        return (size_t)((N + 1) + N * (MB + 1) + MB * TILE) * sizeof(double2);
+        return (size_t)((N + 1) + N * (MB + 1)) * sizeof(double2);
     };
-    while (warps > 1 && need(warps) > 200 * 1024) --warps;
+    while (warps > 1 && need(warps) > 110 * 1024) --warps;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(verfft4_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);

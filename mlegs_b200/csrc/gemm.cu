@@ -102,6 +102,10 @@ __global__ void __launch_bounds__(128) rtran_b2p_kernel(DevGrid g, const double*
 }
 
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
+    if (dmma_supported(g)) {
+        k_rtran_b2p_dmma(g, a, b, ln, pad, s);
+        return;
+    }
     int ncol = 2 * g.NXCHOPDIM;
     dim3 grid((ncol + TN - 1) / TN, (g.NRH + TM - 1) / TM, g.NTCHOPDIM);
     rtran_b2p_kernel<<<grid, 128, 0, s>>>(g, (const double*)a, (double*)b, ln, pad);
@@ -212,6 +216,10 @@ __global__ void __launch_bounds__(128) fold_gemm_kernel(DevGrid g, const double*
 
 void k_fold_gemm(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out, int mode,
                  int scale, int accumulate, int pad, cudaStream_t s) {
+    if (dmma_supported(g)) {
+        k_fold_gemm_dmma(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, s);
+        return;
+    }
     int ncol = 2 * g.NXCHOPDIM;
     int use_w = (mode & 2) ? 1 : 0;
     dim3 grid((ncol + FN - 1) / FN, (g.NRCHOPDIM + FM - 1) / FM, g.NTCHOPDIM);

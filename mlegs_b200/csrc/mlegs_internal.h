@@ -98,6 +98,11 @@ void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, con
 void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
                   double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s);
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
+// FP64 tensor-path (mma.sync m8n8k4.f64) forms used by k_rtran_b2p / k_fold_gemm when supported.
+bool dmma_supported(const DevGrid& g);
+void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
+void k_fold_gemm_dmma(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out, int mode,
+                      int scale, int accumulate, int pad, cudaStream_t s);
 // out[m][n][k] (+)= scale(m,k) * sum_i Wt[m][n][i] * fold(in)(i,k); fold parity per row given by mode
 //   mode 0 (EO): row n even -> even fold, odd -> odd fold;  mode 1 (OE): swapped
 //   scale: 0 -> 1, 1 -> -1, 2 -> -i m, 3 -> i k, 4 -> m k

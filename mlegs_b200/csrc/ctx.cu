@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <initializer_list>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -303,38 +304,43 @@ struct mlegs_ctx {
         k_solve_del2(g, a->data, nullptr, 2, alp, 0, 0.0, nullptr, solve_scr, pad, s);
         chopdo(a, pad);
     }
+    // The fused derivative kernels read row neighbours of their inputs while
+    // writing the outputs, so an output may not share a buffer with an input.
+    static void distinct(std::initializer_list<const Field*> in, std::initializer_list<const Field*> out,
+                         const char* who) {
+        for (const Field* o : out)
+            for (const Field* i : in)
+                if (o->data == i->data)
+                    throw ApiError(MLEGS_ERR_ARG, std::string(who) + ": outputs must be distinct from the inputs");
+    }
     void grad(const Field* a, Field* rr, Field* rp, Field* gz, int pad) {  // 1727-1786
-        xxdx(a, rr, pad);
-        k_mk_combine(g, 4, a->data, nullptr, rp->data, pad, s);
-        k_mk_combine(g, 5, a->data, nullptr, gz->data, pad, s);
-        rp->space = gz->space = MLEGS_FFF;
+        require(a, MLEGS_FFF, "GRAD");
+        distinct({a}, {rr, rp, gz}, "GRAD");
+        k_grad_fused(g, a->data, a->ln, rr->data, rp->data, gz->data, pad, s);
+        rr->space = rp->space = gz->space = MLEGS_FFF;
+        ln_zero(rr);
         ln_zero(rp);
         ln_zero(gz);
     }
     void pc2vel(const Field* psi_, const Field* chi_, Field* rur, Field* rup, Field* uz, int pad) {  // 1789-1853
-        xxdx(chi_, rur, pad);
-        xxdx(psi_, rup, pad);
-        k_mk_combine(g, 0, psi_->data, rur->data, rur->data, pad, s);
-        k_mk_combine(g, 1, chi_->data, rup->data, rup->data, pad, s);
-        delsqh(chi_, uz, pad);
-        Field* W = tmp();
-        mulxm(uz, W, pad);
-        mulxm(W, uz, pad);
-        rel(W);
-        k_mk_combine(g, 6, uz->data, nullptr, uz->data, pad, s);
+        require(psi_, MLEGS_FFF, "PC2VEL");
+        require(chi_, MLEGS_FFF, "PC2VEL");
+        distinct({psi_, chi_}, {rur, rup, uz}, "PC2VEL");
+        k_pc2vel_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, rur->data, rup->data, uz->data, pad, s);
+        rur->space = rup->space = uz->space = MLEGS_FFF;
+        ln_zero(rur);
+        ln_zero(rup);
+        ln_zero(uz);
     }
     void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad) {  // 1856-1919
-        del2(chi_, oz, pad);
-        xxdx(psi_, ror, pad);
-        xxdx(oz, rop, pad);
-        k_mk_combine(g, 2, oz->data, ror->data, ror->data, pad, s);
-        k_mk_combine(g, 3, psi_->data, rop->data, rop->data, pad, s);
-        delsqh(psi_, oz, pad);
-        Field* W = tmp();
-        mulxm(oz, W, pad);
-        mulxm(W, oz, pad);
-        rel(W);
-        k_mk_combine(g, 6, oz->data, nullptr, oz->data, pad, s);
+        require(psi_, MLEGS_FFF, "PC2VOR");
+        require(chi_, MLEGS_FFF, "PC2VOR");
+        distinct({psi_, chi_}, {ror, rop, oz}, "PC2VOR");
+        k_pc2vor_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, ror->data, rop->data, oz->data, pad, s);
+        ror->space = rop->space = oz->space = MLEGS_FFF;
+        ln_zero(ror);
+        ln_zero(rop);
+        ln_zero(oz);
     }
     // PROJECT (mod_legops.f90:2397-2545).  ln_mode: 0 none, 1 value, 2 PSI%LN by reference.
     void project(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_, int ln_mode, double ln) {

@@ -569,4 +569,231 @@ void k_to_ref(const DevGrid& g, int space, const double2* dev, double2* ref, cud
     count_launch();
 }
 
+
+// ---------------------------------------------------------------- fused GRAD, PC2VEL, PC2VOR
+// One thread per FFF element evaluates the whole operator chain as a stencil
+// in n of the (m, k) column, with every intermediate truncated to rows
+// n < NRCHOPS(m) exactly as the chained operators are, so no intermediate
+// field is written:
+//   GRAD   (mod_legops.f90:1727-1786): rr = XXDX(a), rp = i m a, gz = i k a
+//   PC2VEL (1789-1853): rur = i m psi + i k XXDX(chi), rup = -XXDX(psi) - m k chi,
+//                       uz = -XM XM DELSQH(chi)
+//   PC2VOR (1856-1919): oz' = DEL2(chi), ror = -i m oz' + i k XXDX(psi),
+//                       rop = XXDX(oz') - k m psi, oz = -XM XM DELSQH(psi)
+// with the log-term rows of XXDX (742-745), DEL2 (813-817) and DELSQH
+// (128-130) at (m, k) = (0, 0).
+namespace {
+
+struct Col {
+    const double2* p;  // row 0 of the (m, k) column
+    size_t st;         // row stride (NXCHOPDIM)
+    int nn;            // rows kept, NRCHOPS(m)
+    __device__ __forceinline__ double2 at(int j) const {
+        return (j >= 0 && j < nn) ? p[(size_t)j * st] : make_double2(0.0, 0.0);
+    }
+};
+
+// XXDX of column c at row n (zero outside [0, nn)); log rows when ln is given at (0, 0)
+__device__ __forceinline__ double2 xxdx_row(const DevGrid& g, int m, int k, const Col& c, int n, double ln) {
+    if (n < 0 || n >= c.nn) return make_double2(0.0, 0.0);
+    const double* tb = g.xxdx + ((size_t)m * g.NB + n) * 2;
+    double2 v = make_double2(0.0, 0.0);
+    if (n >= 1) {
+        const double2 am = c.p[(size_t)(n - 1) * c.st];
+        v.x += tb[0] * am.x;
+        v.y += tb[0] * am.y;
+    }
+    if (n + 1 < c.nn) {
+        const double2 ap = c.p[(size_t)(n + 1) * c.st];
+        v.x += tb[1] * ap.x;
+        v.y += tb[1] * ap.y;
+    }
+    if (m == 0 && k == 0) {
+        if (n == 0) v.x += ln / g.norm0[0];
+        else if (n == 1) v.x += ln / g.norm0[1];
+    }
+    return v;
+}
+
+// DELSQH of column c at row n (zero outside [0, nn)), log entry at (0, 0, 0)
+__device__ __forceinline__ double2 delsqh_row(const DevGrid& g, int m, int k, const Col& c, int n, double ln) {
+    if (m == 0 && n == 0 && k == 0) return make_double2(ln / g.ELL2 / g.norm0[0], 0.0);
+    if (n < 0 || n >= c.nn) return make_double2(0.0, 0.0);
+    const int N = m + n;
+    return cscale(c.p[(size_t)n * c.st], -(double)(N * (N + 1)) / g.ELL2);
+}
+
+// DEL2 of column c at row n (zero outside [0, nn)), log rows at (0, 0)
+__device__ __forceinline__ double2 del2_row(const DevGrid& g, int m, int k, const Col& c, int n, double ln) {
+    if (n < 0 || n >= c.nn) return make_double2(0.0, 0.0);
+    const double* tb = g.del2h + ((size_t)m * g.NB + n) * 5;
+    double2 v = make_double2(0.0, 0.0);
+    for (int d = 0; d < 5; ++d) {
+        const int j = n + d - 2;
+        if (j < 0 || j >= c.nn) continue;
+        const double2 aj = c.p[(size_t)j * c.st];
+        v.x += tb[d] * aj.x;
+        v.y += tb[d] * aj.y;
+    }
+    const double k2 = g.ak[k] * g.ak[k];
+    const double2 an = c.p[(size_t)n * c.st];
+    v.x -= k2 * an.x;
+    v.y -= k2 * an.y;
+    if (m == 0 && k == 0) {
+        if (n == 0) v.x += 4.0 / 3 * ln / g.ELL2 / g.norm0[0];
+        else if (n == 1) v.x -= 2.0 * ln / g.ELL2 / g.norm0[1];
+        else if (n == 2) v.x += 2.0 / 3 * ln / g.ELL2 / g.norm0[2];
+    }
+    return v;
+}
+
+// -XM XM DELSQH(c) at row n
+__device__ __forceinline__ double2 neg_xm2_delsqh(const DevGrid& g, int m, int k, const Col& c, int n, double ln) {
+    const double* xm = g.xm + (size_t)m * g.NB * 2;
+    double2 d[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) d[q] = delsqh_row(g, m, k, c, n - 2 + q, ln);
+    double2 w[3];  // XM of d at rows n-1, n, n+1
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int j = n - 1 + q;
+        w[q] = make_double2(0.0, 0.0);
+        if (j < 0 || j >= c.nn) continue;
+        double2 v = d[q + 1];
+        if (j >= 1) {
+            v.x += xm[j * 2] * d[q].x;
+            v.y += xm[j * 2] * d[q].y;
+        }
+        if (j + 1 < c.nn) {
+            v.x += xm[j * 2 + 1] * d[q + 2].x;
+            v.y += xm[j * 2 + 1] * d[q + 2].y;
+        }
+        w[q] = v;
+    }
+    double2 v = w[1];
+    if (n >= 1) {
+        v.x += xm[n * 2] * w[0].x;
+        v.y += xm[n * 2] * w[0].y;
+    }
+    if (n + 1 < c.nn) {
+        v.x += xm[n * 2 + 1] * w[2].x;
+        v.y += xm[n * 2 + 1] * w[2].y;
+    }
+    return make_double2(-v.x, -v.y);
+}
+
+__device__ __forceinline__ bool fff_index(const DevGrid& g, size_t t, int& m, int& n, int& k) {
+    const size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t >= total) return false;
+    k = (int)(t % g.NXCHOPDIM);
+    n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    return true;
+}
+
+__device__ __forceinline__ Col column(const DevGrid& g, const double2* a, int m, int k, int pad) {
+    Col c;
+    c.p = a + (size_t)m * g.NRCHOPDIM * g.NXCHOPDIM + k;
+    c.st = g.NXCHOPDIM;
+    c.nn = nrchops(g, m, pad);
+    return c;
+}
+
+}  // namespace
+
+__global__ void grad_fused_kernel(DevGrid g, const double2* a, const double* ln, double2* rr, double2* rp,
+                                  double2* gz, int pad) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int m, n, k;
+    if (!fff_index(g, t, m, n, k)) return;
+    const Col c = column(g, a, m, k, pad);
+    double2 v0 = make_double2(0.0, 0.0), v1 = v0, v2 = v0;
+    if (n < c.nn) {
+        const double2 an = c.p[(size_t)n * c.st];
+        v0 = xxdx_row(g, m, k, c, n, ln ? *ln : 0.0);
+        v1 = cmuli(an, (double)m);
+        v2 = cmuli(an, g.ak[k]);
+    }
+    rr[t] = v0;
+    rp[t] = v1;
+    gz[t] = v2;
+}
+
+__global__ void pc2vel_fused_kernel(DevGrid g, const double2* psi, const double* psi_ln, const double2* chi,
+                                    const double* chi_ln, double2* rur, double2* rup, double2* uz, int pad) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int m, n, k;
+    if (!fff_index(g, t, m, n, k)) return;
+    const Col cp = column(g, psi, m, k, pad), cc = column(g, chi, m, k, pad);
+    double2 v0 = make_double2(0.0, 0.0), v1 = v0, v2 = v0;
+    if (n < cp.nn) {
+        const double lp = psi_ln ? *psi_ln : 0.0, lc = chi_ln ? *chi_ln : 0.0;
+        const double mv = (double)m, kv = g.ak[k];
+        const double2 ps = cp.p[(size_t)n * cp.st], ch = cc.p[(size_t)n * cc.st];
+        const double2 xc = xxdx_row(g, m, k, cc, n, lc);
+        const double2 xp = xxdx_row(g, m, k, cp, n, lp);
+        v0 = cadd(cmuli(ps, mv), cmuli(xc, kv));
+        v1 = make_double2(-xp.x - (mv * kv) * ch.x, -xp.y - (mv * kv) * ch.y);
+        v2 = neg_xm2_delsqh(g, m, k, cc, n, lc);
+    }
+    rur[t] = v0;
+    rup[t] = v1;
+    uz[t] = v2;
+}
+
+__global__ void pc2vor_fused_kernel(DevGrid g, const double2* psi, const double* psi_ln, const double2* chi,
+                                    const double* chi_ln, double2* ror, double2* rop, double2* oz, int pad) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int m, n, k;
+    if (!fff_index(g, t, m, n, k)) return;
+    const Col cp = column(g, psi, m, k, pad), cc = column(g, chi, m, k, pad);
+    double2 v0 = make_double2(0.0, 0.0), v1 = v0, v2 = v0;
+    if (n < cp.nn) {
+        const double lp = psi_ln ? *psi_ln : 0.0, lc = chi_ln ? *chi_ln : 0.0;
+        const double mv = (double)m, kv = g.ak[k];
+        const double2 ps = cp.p[(size_t)n * cp.st];
+        // oz' = DEL2(chi) at rows n-1, n, n+1; XXDX(oz') has no log rows (oz'%LN = 0)
+        const double2 dm = del2_row(g, m, k, cc, n - 1, lc), d0 = del2_row(g, m, k, cc, n, lc),
+                      dp = del2_row(g, m, k, cc, n + 1, lc);
+        const double* tb = g.xxdx + ((size_t)m * g.NB + n) * 2;
+        double2 xo = make_double2(0.0, 0.0);
+        if (n >= 1) {
+            xo.x += tb[0] * dm.x;
+            xo.y += tb[0] * dm.y;
+        }
+        if (n + 1 < cp.nn) {
+            xo.x += tb[1] * dp.x;
+            xo.y += tb[1] * dp.y;
+        }
+        const double2 xp = xxdx_row(g, m, k, cp, n, lp);
+        v0 = cadd(cmuli(d0, -mv), cmuli(xp, kv));
+        v1 = make_double2(xo.x - (kv * mv) * ps.x, xo.y - (kv * mv) * ps.y);
+        v2 = neg_xm2_delsqh(g, m, k, cp, n, lp);
+    }
+    ror[t] = v0;
+    rop[t] = v1;
+    oz[t] = v2;
+}
+
+void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2* rr, double2* rp, double2* gz, int pad,
+                  cudaStream_t s) {
+    const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    grad_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, ln, rr, rp, gz, pad);
+    count_launch();
+}
+
+void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s) {
+    const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    pc2vel_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, rur, rup, uz, pad);
+    count_launch();
+}
+
+void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
+                    double2* ror, double2* rop, double2* oz, int pad, cudaStream_t s) {
+    const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    pc2vor_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, ror, rop, oz, pad);
+    count_launch();
+}
+
 }  // namespace mlegs

@@ -136,6 +136,13 @@ void k_band3(const DevGrid& g, const double2* a, double2* b, int which /*0 xxdx,
 void k_del2(const DevGrid& g, const double2* a, double2* b, int pad, cudaStream_t s);
 void k_logterm_rows(const DevGrid& g, double2* b, const double* ln, int which, double coef, cudaStream_t s);
 void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, double2* out, int pad, cudaStream_t s);
+// GRAD, PC2VEL, PC2VOR each in one pass (kernels.cu); outputs FFF, log terms read from *ln.
+void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2* rr, double2* rp, double2* gz, int pad,
+                  cudaStream_t s);
+void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s);
+void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
+                    double2* ror, double2* rop, double2* oz, int pad, cudaStream_t s);
 void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
 void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
                     const double* explog0, int nn, cudaStream_t s);

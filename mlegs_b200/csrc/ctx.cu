@@ -366,6 +366,11 @@ struct mlegs_ctx {
         ln_zero(chi_);
         if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, explog0, d.NRCHOP, s);
         if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, explog0, d.NRCHOP, s);
+        if (!split_S && dmma_supported(g)) {
+            k_project_dmma(g, V, D, T, rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
+            k_farfield_fix(g, psi_->data, d.NRCHOP, s);
+            return;
+        }
         const int wr = d.NRCHOPDIM;
         // PSI = -(i m) EO(V, RUR) - OE(D, RUP)
         fold(1, V, wr, rur->data, psi_->data, 0, 2, 0, 0);
@@ -1024,55 +1029,72 @@ void mlegs_ctx::rich_etdfe_be() {
     rel(B2);
 }
 
-// STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901).
+// STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901).  The HYPERV filters, the
+// second PC2VEL, CALC_BOUSSI_ETDAB_SUB and the history copies run as one
+// kernel; PROJECT writes the new PSI in place (its inputs do not alias PSI),
+// and the closing R_PI_* -= PC2VEL(PSI, CHI) is one kernel.
 void mlegs_ctx::step_etdab_cn() {
     const double dt = p.dt;
     t += dt;
     n += 1;
+    Field *P0 = nullptr, *C0 = nullptr, *B0 = nullptr;
+    if (p.visc_sw == 1) {  // CALC_BOUSSI_VISC_CN uses the state at the start of the step
+        P0 = tmp();
+        C0 = tmp();
+        B0 = tmp();
+        copy0(P0, psi, 0);
+        copy0(C0, chi, 0);
+        copy0(B0, b, 0);
+    }
     Field *RURN = tmp(), *RUPN = tmp(), *UZN = tmp(), *RORN = tmp(), *ROPN = tmp(), *OZN = tmp(), *BN = tmp();
     pc2vel(psi, chi, RURN, RUPN, UZN, 3);
     pc2vor(psi, chi, RORN, ROPN, OZN, 3);
     nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN);
-    etd_hyperv(RORN, ROPN, OZN, BN, 1.0);
-    Field* B0 = tmp();
-    copy0(B0, b, 0);
-    pc2vel(psi, chi, RURN, RUPN, UZN, 3);
-    k_etd(g, etdE, etdN, dt, 1, RURN->data, RUPN->data, UZN->data, b->data, RORN->data, ROPN->data, OZN->data,
-          BN->data, hist[4]->data, hist[5]->data, hist[6]->data, hist[1]->data, hist[2]->data, hist[3]->data,
-          hist[0]->data, s);
-    const size_t N = fff();
-    k_copy(hist[0]->data, BN->data, N, s);
-    k_copy(hist[1]->data, RORN->data, N, s);
-    k_copy(hist[2]->data, ROPN->data, N, s);
-    k_copy(hist[3]->data, OZN->data, N, s);
+    EtdAbArgs a{};
+    a.E = etdE;
+    a.N = etdN;
+    a.dt = dt;
+    a.hyper = p.visc_sw == 3 ? 1 : 0;
+    for (int q = 0; q < 3; ++q) {
+        a.hv[q] = hv[q];
+        a.hd[q] = hd[q];
+    }
+    a.psi = psi->data;
+    a.chi = chi->data;
+    a.psi_ln = psi->ln;
+    a.chi_ln = chi->ln;
+    a.rur = RURN->data;
+    a.rup = RUPN->data;
+    a.uz = UZN->data;
+    a.b = b->data;
+    a.ror = RORN->data;
+    a.rop = ROPN->data;
+    a.oz = OZN->data;
+    a.bn = BN->data;
+    for (int q = 0; q < 7; ++q) a.hist[q] = hist[q]->data;
+    a.out_ln[0] = RURN->ln;
+    a.out_ln[1] = RUPN->ln;
+    a.out_ln[2] = UZN->ln;
+    k_etd_ab_fused(g, a, s);
+    RURN->space = RUPN->space = UZN->space = MLEGS_FFF;
     rel(BN);
     rel(RORN);
     rel(ROPN);
     rel(OZN);
-    etd_hyperv(RURN, RUPN, UZN, b, 1.0);
-    k_copy(hist[4]->data, RURN->data, N, s);
-    k_copy(hist[5]->data, RUPN->data, N, s);
-    k_copy(hist[6]->data, UZN->data, N, s);
-    Field *P0 = tmp(), *C0 = tmp();
-    copy0(P0, psi, 0);
-    copy0(C0, chi, 0);
-    Field *W = tmp(), *Pn = tmp();
-    project(RURN, RUPN, UZN, Pn, W, 2, 0.0);
-    copy0(psi, Pn, 0);
+    Field* W = tmp();
+    project(RURN, RUPN, UZN, psi, W, 2, 0.0);
     idel2ln(W, chi, 0);
     rel(W);
-    rel(Pn);
-    pc2vel(psi, chi, RURN, RUPN, UZN, 3);
-    k_axpby(hist[4]->data, -1.0, RURN->data, 0.0, nullptr, 1.0, N, s);
-    k_axpby(hist[5]->data, -1.0, RUPN->data, 0.0, nullptr, 1.0, N, s);
-    k_axpby(hist[6]->data, -1.0, UZN->data, 0.0, nullptr, 1.0, N, s);
     rel(RURN);
     rel(RUPN);
     rel(UZN);
-    visc_cn(psi, chi, b, P0, C0, B0);
-    rel(P0);
-    rel(C0);
-    rel(B0);
+    k_pc2vel_fused(g, psi->data, psi->ln, chi->data, chi->ln, hist[4]->data, hist[5]->data, hist[6]->data, 3, s, 1);
+    if (p.visc_sw == 1) {
+        visc_cn(psi, chi, b, P0, C0, B0);
+        rel(P0);
+        rel(C0);
+        rel(B0);
+    }
 }
 
 // ====================================================================== C ABI
@@ -1490,7 +1512,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 12) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 13) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1539,6 +1561,19 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     k_split_fold(g, ctx->split_S, ctx->fimg[0], ctx->feA[0], d.NRCHOPDIM + 1, a->data, b->data, 0,
                                  0, 0, 0, 1, ctx->split_err, s);
                     break;
+                case 13: {  // PROJECT's fold products: f9[0..2] (PFF) -> b, c (FFF)
+                    const int wr = d.NRCHOPDIM;
+                    if (!ctx->split_S && dmma_supported(g)) {
+                        k_project_dmma(g, ctx->V, ctx->D, ctx->T, f9[0]->data, f9[1]->data, f9[2]->data, b->data,
+                                       c->data, s);
+                    } else {
+                        ctx->fold(1, ctx->V, wr, f9[0]->data, b->data, 0, 2, 0, 0);
+                        ctx->fold(2, ctx->D, wr, f9[1]->data, b->data, 1, 1, 1, 0);
+                        ctx->fold(2, ctx->D, wr, f9[0]->data, c->data, 1, 3, 0, 0);
+                        ctx->fold(1, ctx->V, wr, f9[1]->data, c->data, 0, 4, 1, 0);
+                        ctx->fold(3, ctx->T, wr, f9[2]->data, c->data, 0, 1, 1, 0);
+                    }
+                } break;
             }
         };
         const double B16 = 16.0;
@@ -1550,6 +1585,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written
             case 7: bytes = B16 * 2.0 * (double)d.fff(); break;
             case 8: bytes = B16 * 14.0 * (double)d.pfp(); break;  // 10 PFP lines read, 4 written
+            case 13: bytes = B16 * (3.0 * (double)d.pff() + 2.0 * (double)d.fff()); break;
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
         }
         for (int q = 0; q < 3; ++q) launch();  // warm-up

@@ -253,6 +253,135 @@ __global__ void __launch_bounds__(NW * 32) fold_dmma_kernel(DevGrid g, const dou
     }
 }
 
+// PROJECT's five EOMUL/OEMUL products (mod_legops.f90:2497-2535) as two
+// K-concatenated GEMMs per (m, parity of n) and 32-column tile:
+//   PSI = [V | D] . [-i m F0(RUR); -F1(RUP)]                       K = 2 NRH
+//   CHI = [D | V | T] . [i k F1(RUR); m k F0(RUP); -F0(UZ)]         K = 3 NRH
+// F0 / F1 are the EO / OE folds x_i +/- x_{NR-1-i} of the input rows for the
+// output parity; the complex column factors are applied to the folded chunk,
+// before the products (the weights are real).  All 5 NRH / 32 chunks go
+// through one two-stage cp.async ring; PSI is written after the first 2 NRH,
+// CHI at the end, each once and without a read-modify-write.  Segment sg of
+// the K extent: 0 (V, RUR, EO, -i m), 1 (D, RUP, OE, -1), 2 (D, RUR, OE, i k),
+// 3 (V, RUP, EO, m k), 4 (T, UZ, EO, -1).
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32) project_dmma_kernel(DevGrid g, const double* __restrict__ V,
+                                                           const double* __restrict__ D, const double* __restrict__ T,
+                                                           const double* __restrict__ rur,
+                                                           const double* __restrict__ rup,
+                                                           const double* __restrict__ uz, double* __restrict__ psi,
+                                                           double* __restrict__ chi, int RTmax) {
+    extern __shared__ double smd[];
+    const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;
+    const int ncol = 2 * g.NXCHOPDIM;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
+    int nn = g.NRCHOP - m;
+    if (nn < 0) nn = 0;
+    const int rows = (g.NRCHOPDIM - pr + 1) / 2;
+    const int RT = (rows + 7) / 8;
+    const int nch = (g.NRH + KCF - 1) / KCF;
+    const int total = 5 * nch;
+    const size_t stA = (size_t)RTmax * 8 * SAF, stX = (size_t)2 * KCF * SXF;
+    double* Bs = smd + 2 * (stA + stX);  // [KCF][SXF] folded, scaled chunk
+    const size_t wofs = (size_t)m * g.NRCHOPDIM * g.NRH, xofs = (size_t)m * g.NR * ncol;
+
+    auto stage = [&](int gc) {
+        const int sg = gc / nch, i0 = (gc - sg * nch) * KCF;
+        const double* w = (sg == 0 || sg == 3 ? V : (sg == 4 ? T : D)) + wofs;
+        const double* x = (sg == 0 || sg == 2 ? rur : (sg == 4 ? uz : rup)) + xofs;
+        double* As = smd + (gc & 1) * (stA + stX);
+        double* Xs = As + stA;
+        for (int e = tid; e < RT * 8 * (KCF / 2); e += NW * 32) {
+            const int r = e / (KCF / 2), c2 = e - r * (KCF / 2);
+            const int n = 2 * r + pr, i = i0 + 2 * c2;
+            const bool ok = n < nn && i < g.NRH;
+            cp16(As + (size_t)r * SAF + 2 * c2, ok ? w + (size_t)n * g.NRH + i : w, ok);
+        }
+        for (int e = tid; e < 2 * KCF * (CT / 2); e += NW * 32) {
+            const int rr = e / (CT / 2), c2 = e - rr * (CT / 2);
+            const int j = rr % KCF, i = i0 + j;
+            const int src_row = rr < KCF ? i : g.NR - 1 - i;
+            const int c = c0 + 2 * c2;
+            const bool ok = i < g.NRH && c < ncol;
+            cp16(Xs + (size_t)rr * SXF + 2 * c2, ok ? x + (size_t)src_row * ncol + c : x, ok);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    auto epilogue = [&](double (&acc)[MTW][4][2], double* out) {
+        double* o = out + (size_t)m * g.NRCHOPDIM * ncol;
+#pragma unroll
+        for (int t = 0; t < MTW; ++t) {
+            const int r = (warp * MTW + t) * 8 + gq;
+            const int n = 2 * r + pr;
+            if (r >= rows || n >= g.NRCHOPDIM) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = c0 + j * 8 + 2 * q;
+                if (c >= ncol) continue;
+                *(double2*)(o + (size_t)n * ncol + c) =
+                    n < nn ? make_double2(acc[t][j][0], acc[t][j][1]) : make_double2(0.0, 0.0);
+                acc[t][j][0] = acc[t][j][1] = 0.0;
+            }
+        }
+    };
+
+    double acc[MTW][4][2];
+#pragma unroll
+    for (int t = 0; t < MTW; ++t)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
+    stage(0);
+    for (int gc = 0; gc < total; ++gc) {
+        if (gc + 1 < total) {
+            stage(gc + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int sg = gc / nch;
+        const double* As = smd + (gc & 1) * (stA + stX);
+        const double* Xs = As + stA;
+        // fold sign for (parity, EO/OE) and the complex column factor of the segment
+        const double sgn = (pr ^ (sg == 1 || sg == 2 ? 1 : 0)) ? -1.0 : 1.0;
+        for (int e = tid; e < KCF * (CT / 2); e += NW * 32) {
+            const int j = e / (CT / 2), c = 2 * (e - j * (CT / 2));
+            const double re = Xs[(size_t)j * SXF + c] + sgn * Xs[(size_t)(KCF + j) * SXF + c];
+            const double im = Xs[(size_t)j * SXF + c + 1] + sgn * Xs[(size_t)(KCF + j) * SXF + c + 1];
+            const int kk = (c0 + c) >> 1;
+            const double ak = (c0 + c < ncol) ? g.ak[kk] : 0.0;
+            double sr, si;
+            switch (sg) {
+                case 0: sr = im * m; si = -re * m; break;                    // -i m v
+                case 2: sr = -im * ak; si = re * ak; break;                  //  i k v
+                case 3: { const double f = m * ak; sr = re * f; si = im * f; } break;  // m k v
+                default: sr = -re; si = -im; break;                          // -v
+            }
+            Bs[(size_t)j * SXF + c] = sr;
+            Bs[(size_t)j * SXF + c + 1] = si;
+        }
+        __syncthreads();
+        for (int kk = 0; kk < KCF; kk += 4) {
+            const int j = kk + q;
+            double af[MTW], bf[4];
+#pragma unroll
+            for (int t = 0; t < MTW; ++t) {
+                const int mt = warp * MTW + t;
+                af[t] = (mt < RT) ? As[(size_t)(mt * 8 + gq) * SAF + j] : 0.0;
+            }
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SXF + jj * 8 + gq];
+#pragma unroll
+            for (int t = 0; t < MTW; ++t)
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af[t], bf[jj]);
+        }
+        if (gc == 2 * nch - 1) epilogue(acc, psi);
+        if (gc == total - 1) epilogue(acc, chi);
+        __syncthreads();  // the stage is refilled by the next iteration's prefetch
+    }
+}
+
 // ---------------------------------------------------------------------------
 
 static int pad16_8(int v) { return v + ((8 - v % 16) + 16) % 16; }  // smallest >= v that is 8 mod 16
@@ -326,6 +455,46 @@ void k_fold_gemm_dmma(const DevGrid& g, const double* Wt, int wt_rows, const dou
         }
     }
 #undef FOLD_CASE
+}
+
+template <int NW, int MTW>
+static void project_launch(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
+                           const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s) {
+    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
+    const size_t smem = (2 * ((size_t)RT * 8 * SAF + (size_t)2 * KCF * SXF) + (size_t)KCF * SXF) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(project_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    dim3 grid((2 * g.NXCHOPDIM + CT - 1) / CT, 2, g.NTCHOPDIM);
+    project_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, V, D, T, (const double*)rur, (const double*)rup,
+                                                             (const double*)uz, (double*)psi, (double*)chi, RT);
+    count_launch();
+}
+
+void k_project_dmma(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
+                    const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s) {
+    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
+    const int m4 = (RT + 3) / 4, m3 = (RT + 2) / 3;
+    const bool three = 3 * m3 - RT < 4 * m4 - RT && m3 <= 4;
+#define PROJ_CASE(NW, MTW) project_launch<NW, MTW>(g, V, D, T, rur, rup, uz, psi, chi, s)
+    if (three) {
+        switch (m3) {
+            case 1: PROJ_CASE(3, 1); break;
+            case 2: PROJ_CASE(3, 2); break;
+            case 3: PROJ_CASE(3, 3); break;
+            default: PROJ_CASE(3, 4); break;
+        }
+    } else {
+        switch (m4) {
+            case 1: PROJ_CASE(4, 1); break;
+            case 2: PROJ_CASE(4, 2); break;
+            case 3: PROJ_CASE(4, 3); break;
+            default: PROJ_CASE(4, 4); break;
+        }
+    }
+#undef PROJ_CASE
 }
 
 }  // namespace mlegs

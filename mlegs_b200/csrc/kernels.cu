@@ -719,8 +719,9 @@ __global__ void grad_fused_kernel(DevGrid g, const double2* a, const double* ln,
     gz[t] = v2;
 }
 
+// sub = 1: the outputs are decremented by the velocity instead of set to it
 __global__ void pc2vel_fused_kernel(DevGrid g, const double2* psi, const double* psi_ln, const double2* chi,
-                                    const double* chi_ln, double2* rur, double2* rup, double2* uz, int pad) {
+                                    const double* chi_ln, double2* rur, double2* rup, double2* uz, int pad, int sub) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     int m, n, k;
     if (!fff_index(g, t, m, n, k)) return;
@@ -735,6 +736,11 @@ __global__ void pc2vel_fused_kernel(DevGrid g, const double2* psi, const double*
         v0 = cadd(cmuli(ps, mv), cmuli(xc, kv));
         v1 = make_double2(-xp.x - (mv * kv) * ch.x, -xp.y - (mv * kv) * ch.y);
         v2 = neg_xm2_delsqh(g, m, k, cc, n, lc);
+    }
+    if (sub) {
+        v0 = csub(rur[t], v0);
+        v1 = csub(rup[t], v1);
+        v2 = csub(uz[t], v2);
     }
     rur[t] = v0;
     rup[t] = v1;
@@ -775,6 +781,91 @@ __global__ void pc2vor_fused_kernel(DevGrid g, const double2* psi, const double*
     oz[t] = v2;
 }
 
+// The coefficient update of STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901) from
+// the projected nonlinear terms to the new state, in one pass per FFF entry:
+//   HYPERV of the nonlinear terms (1352-1416, at TF = 1, chopped at pad 0),
+//   PC2VEL(PSI, CHI) at pad 3 (mod_legops.f90:1789-1853),
+//   CALC_BOUSSI_ETDAB_SUB (1050-1139), HYPERV of the updated (RUR, RUP, UZ, B),
+//   and the history update N_* <- the filtered nonlinear terms, R_PI_* <- the
+//   filtered velocity.  hyper = 0 (VISC%SW /= 3) skips both filters.
+__global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int m, n, k;
+    if (!fff_index(g, t, m, n, k)) return;
+    if (t < 3) *a.out_ln[t] = 0.0;
+    double fv = 1.0, fd = 1.0;
+    if (a.hyper) {
+        if (n < nrchops(g, m, 0)) {
+            fv = a.hv[0][(size_t)m * g.NRCHOP + n] * a.hv[1][m] * a.hv[2][k];
+            fd = a.hd[0][(size_t)m * g.NRCHOP + n] * a.hd[1][m] * a.hd[2][k];
+        } else {
+            fv = fd = 0.0;
+        }
+    }
+    // PC2VEL(PSI, CHI) at pad 3
+    const Col cp = column(g, a.psi, m, k, 3), cc = column(g, a.chi, m, k, 3);
+    double2 u0 = make_double2(0.0, 0.0), u1 = u0, u2 = u0;
+    if (n < cp.nn) {
+        const double lp = *a.psi_ln, lc = *a.chi_ln;
+        const double mv = (double)m, kv = g.ak[k];
+        const double2 ps = cp.p[(size_t)n * cp.st], ch = cc.p[(size_t)n * cc.st];
+        const double2 xc = xxdx_row(g, m, k, cc, n, lc);
+        const double2 xp = xxdx_row(g, m, k, cp, n, lp);
+        u0 = cadd(cmuli(ps, mv), cmuli(xc, kv));
+        u1 = make_double2(-xp.x - (mv * kv) * ch.x, -xp.y - (mv * kv) * ch.y);
+        u2 = neg_xm2_delsqh(g, m, k, cc, n, lc);
+    }
+    const double2 rn[4] = {cscale(a.ror[t], fv), cscale(a.rop[t], fv), cscale(a.oz[t], fv), cscale(a.bn[t], fd)};
+    double E[16], N[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        E[q] = a.E[q];
+        N[q] = a.N[q];
+    }
+    if (k == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) E[q] = N[q] = 0.0;
+        E[0] = E[5] = 1.0;
+        N[0] = N[5] = a.dt;
+    }
+    const double notm0 = (m == 0) ? 0.0 : 1.0, notk0 = (k == 0) ? 0.0 : 1.0;
+    // history: 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z
+    const double2 ev[4] = {csub(u0, a.hist[4][t]), csub(u1, cscale(a.hist[5][t], notm0)),
+                           csub(u2, cscale(a.hist[6][t], notk0)), a.b[t]};
+    const double2 on[4] = {a.hist[1][t], a.hist[2][t], a.hist[3][t], a.hist[0][t]};
+    double2 cv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double2 x = make_double2(0.0, 0.0), y = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double2 av = csub(cscale(rn[j], 1.5), cscale(on[j], 0.5));
+            x.x += E[i * 4 + j] * ev[j].x;
+            x.y += E[i * 4 + j] * ev[j].y;
+            y.x += N[i * 4 + j] * av.x;
+            y.y += N[i * 4 + j] * av.y;
+        }
+        cv[i] = cscale(cadd(x, y), i < 3 ? fv : fd);
+    }
+    a.rur[t] = cv[0];
+    a.rup[t] = cv[1];
+    a.uz[t] = cv[2];
+    a.b[t] = cv[3];
+    a.hist[0][t] = rn[3];
+    a.hist[1][t] = rn[0];
+    a.hist[2][t] = rn[1];
+    a.hist[3][t] = rn[2];
+    a.hist[4][t] = cv[0];
+    a.hist[5][t] = cv[1];
+    a.hist[6][t] = cv[2];
+}
+
+void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s) {
+    const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    etd_ab_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a);
+    count_launch();
+}
+
 void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2* rr, double2* rp, double2* gz, int pad,
                   cudaStream_t s) {
     const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
@@ -783,9 +874,9 @@ void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2*
 }
 
 void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
-                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s) {
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub) {
     const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
-    pc2vel_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, rur, rup, uz, pad);
+    pc2vel_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, rur, rup, uz, pad, sub);
     count_launch();
 }
 

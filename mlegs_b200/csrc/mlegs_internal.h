@@ -103,6 +103,10 @@ bool dmma_supported(const DevGrid& g);
 void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
 void k_fold_gemm_dmma(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out, int mode,
                       int scale, int accumulate, int pad, cudaStream_t s);
+// PROJECT's five fold products in one launch (FP64 tensor path): PSI and CHI from
+// RUR, RUP, UZ in PFF with the weights V, D, T ([m][n][i], NRCHOPDIM x NRH).
+void k_project_dmma(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
+                    const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s);
 // out[m][n][k] (+)= scale(m,k) * sum_i Wt[m][n][i] * fold(in)(i,k); fold parity per row given by mode
 //   mode 0 (EO): row n even -> even fold, odd -> odd fold;  mode 1 (OE): swapped
 //   scale: 0 -> 1, 1 -> -1, 2 -> -i m, 3 -> i k, 4 -> m k
@@ -140,7 +144,7 @@ void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, 
 void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2* rr, double2* rp, double2* gz, int pad,
                   cudaStream_t s);
 void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
-                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s);
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub = 0);
 void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
                     double2* ror, double2* rop, double2* oz, int pad, cudaStream_t s);
 void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
@@ -175,6 +179,30 @@ void k_etd(const DevGrid& g, const double* E, const double* NL, double dt, int a
            const double2* hr, const double2* hp, const double2* hz,
            const double2* onr, const double2* onp, const double2* onz, const double2* onb,
            cudaStream_t s);
+// One-pass ETD2AB coefficient update of the steady step (kernels.cu).
+struct EtdAbArgs {
+    const double* E;  // 4 x 4 real ETD matrices, row-major
+    const double* N;
+    double dt;
+    int hyper;              // apply the VISC%SW = 3 filters (hv: velocity, hd: buoyancy)
+    const double* hv[3];    // [m][n] (NRCHOP per m), [m], [k]
+    const double* hd[3];
+    const double2* psi;     // state read for PC2VEL
+    const double2* chi;
+    const double* psi_ln;
+    const double* chi_ln;
+    double2* rur;           // out: updated velocity terms
+    double2* rup;
+    double2* uz;
+    double2* b;             // in/out
+    const double2* ror;     // projected nonlinear terms of this step
+    const double2* rop;
+    const double2* oz;
+    const double2* bn;
+    double2* hist[7];       // in/out: 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z
+    double* out_ln[3];      // LN slots of rur, rup, uz: set to 0 (PC2VEL outputs carry no log term)
+};
+void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);
 void k_hyperv(const DevGrid& g, double2* a, const double* hr, const double* ht, const double* hx,
               double tf, int pad, cudaStream_t s);
 void k_finite(const double2* a, size_t n, int* flag, cudaStream_t s);

@@ -43,81 +43,111 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;
 
 }  // namespace
 
-// RTRAN(+1).  smem per parity pass: A [KP][SA] (PF rows t, i contiguous) and
-// B [KP][SBS]; the even-parity products stay in registers during the odd pass.
-template <int MTW>
-__global__ void __launch_bounds__(128) b2p_dmma_kernel(DevGrid g, const double* __restrict__ A,
-                                                       double* __restrict__ out, const double* ln, int pad,
-                                                       int SA, int KPmax) {
+// RTRAN(+1).  Per m, the K rows of both parities (t < kp_p, n = 2t + p) go in
+// chunks of KCB = 16 through a two-stage cp.async ring: A [KCB][SA] (PF rows
+// n, i contiguous) and B [KCB][SBS] (A(n, c0 .. c0+31)).  The even- and
+// odd-parity products accumulate in separate registers; the epilogue forms
+// B(i) = C_0 + C_1 and B(NR-1-i) = C_0 - C_1.  The output-row m-tiles go
+// round-robin over NW warps.
+constexpr int KCB = 16;
+
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const double* __restrict__ A,
+                                                           double* __restrict__ out, const double* ln, int pad,
+                                                           int SA) {
     extern __shared__ double smd[];
-    double* As = smd;                       // [KPmax][SA]
-    double* Bs = smd + (size_t)KPmax * SA;  // [KPmax][SBS]
+    const size_t stg = (size_t)KCB * (SA + SBS);
     const int m = blockIdx.y, c0 = blockIdx.x * CT;
     const int ncol = 2 * g.NXCHOPDIM;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
     const int RT = (g.NRH + 7) / 8;
     int nn = g.NRCHOP + pad - m;
     if (nn < 0) nn = 0;
+    const int kp0 = (nn + 1) / 2, kp1 = nn / 2;
+    const int nc0 = (kp0 + KCB - 1) / KCB, nc1 = (kp1 + KCB - 1) / KCB;
+    const int total = nc0 + nc1;
     const int ne = g.NRCHOPDIM + 1;
     const double* pf = g.pf + (size_t)m * ne * g.NRH;
     const double* a = A + (size_t)m * g.NRCHOPDIM * ncol;
-    double acc[2][MTW][4][2];
-#pragma unroll
-    for (int p = 0; p < 2; ++p)
-#pragma unroll
-        for (int i = 0; i < MTW; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[p][i][j][0] = acc[p][i][j][1] = 0.0;
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-        const int kp = p ? nn / 2 : (nn + 1) / 2;
-        const int KP = (kp + 3) & ~3;
-        if (p) __syncthreads();  // the even pass is done with the buffers
-        // stage A: rows t < KP of PF(:, 2t+p) over i (NRH), zero past kp
-        const int ach = g.NRH / 2;  // 16-byte chunks per row (NRH is even)
-        for (int e = tid; e < KP * ach; e += 128) {
-            const int t = e / ach, ch = e - t * ach;
+    const int ach = g.NRH / 2;  // 16-byte chunks per PF row (NRH is even)
+
+    auto stage = [&](int cidx) {
+        const int p = cidx < nc0 ? 0 : 1;
+        const int t0 = (cidx - (p ? nc0 : 0)) * KCB, kp = p ? kp1 : kp0;
+        double* As = smd + (cidx & 1) * stg;
+        double* Bs = As + (size_t)KCB * SA;
+        for (int e = tid; e < KCB * ach; e += NW * 32) {
+            const int tt = e / ach, ch = e - tt * ach;
+            const int t = t0 + tt;
             const bool ok = t < kp;
-            cp16(As + (size_t)t * SA + 2 * ch, ok ? pf + (size_t)(2 * t + p) * g.NRH + 2 * ch : pf, ok);
+            cp16(As + (size_t)tt * SA + 2 * ch, ok ? pf + (size_t)(2 * t + p) * g.NRH + 2 * ch : pf, ok);
         }
-        // stage B: rows t < KP of A(2t+p, c0 .. c0+31), zero past kp / ncol
-        for (int e = tid; e < KP * (CT / 2); e += 128) {
-            const int t = e / (CT / 2), ch = e - t * (CT / 2);
-            const int c = c0 + 2 * ch;
+        for (int e = tid; e < KCB * (CT / 2); e += NW * 32) {
+            const int tt = e / (CT / 2), ch = e - tt * (CT / 2);
+            const int t = t0 + tt, c = c0 + 2 * ch;
             const bool ok = t < kp && c < ncol;
-            cp16(Bs + (size_t)t * SBS + 2 * ch, ok ? a + (size_t)(2 * t + p) * ncol + c : a, ok);
+            cp16(Bs + (size_t)tt * SBS + 2 * ch, ok ? a + (size_t)(2 * t + p) * ncol + c : a, ok);
         }
-        cp_wait_all();
-        __syncthreads();
-        for (int k = 0; k < KP; k += 4) {
-            double af[MTW], bf[4];
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    auto mma_chunk = [&](double (&acc)[MTW][4][2], const double* As, const double* Bs, int ksteps) {
 #pragma unroll
-            for (int i = 0; i < MTW; ++i) {
-                const int mt = warp * MTW + i;
-                af[i] = (mt < RT) ? As[(size_t)(k + q) * SA + mt * 8 + gq] : 0.0;
+        for (int s4 = 0; s4 < KCB / 4; ++s4) {
+            if (s4 < ksteps) {
+                const int k = 4 * s4 + q;
+                double bf[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bf[j] = Bs[(size_t)k * SBS + j * 8 + gq];
+#pragma unroll
+                for (int i = 0; i < MTW; ++i) {
+                    const int mt = warp + NW * i;
+                    if (mt < RT) {
+                        const double af = As[(size_t)k * SA + mt * 8 + gq];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) dmma(acc[i][j], af, bf[j]);
+                    }
+                }
             }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = Bs[(size_t)(k + q) * SBS + j * 8 + gq];
-#pragma unroll
-            for (int i = 0; i < MTW; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma(acc[p][i][j], af[i], bf[j]);
         }
+    };
+
+    double acc0[MTW][4][2], acc1[MTW][4][2];
+#pragma unroll
+    for (int i = 0; i < MTW; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc0[i][j][0] = acc0[i][j][1] = acc1[i][j][0] = acc1[i][j][1] = 0.0;
+    if (total > 0) stage(0);
+    for (int cidx = 0; cidx < total; ++cidx) {
+        if (cidx + 1 < total) {
+            stage(cidx + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const double* As = smd + (cidx & 1) * stg;
+        const double* Bs = As + (size_t)KCB * SA;
+        const int p = cidx < nc0 ? 0 : 1;
+        const int t0 = (cidx - (p ? nc0 : 0)) * KCB, kp = p ? kp1 : kp0;
+        const int ksteps = (min(KCB, kp - t0) + 3) / 4;
+        if (p == 0) mma_chunk(acc0, As, Bs, ksteps);
+        else mma_chunk(acc1, As, Bs, ksteps);
+        __syncthreads();  // the stage is refilled by the next iteration's prefetch
     }
     // butterfly + log term
     const double lnv = (m == 0 && ln) ? *ln : 0.0;
     double* o = out + (size_t)m * g.NR * ncol;
 #pragma unroll
     for (int i = 0; i < MTW; ++i) {
-        const int row = (warp * MTW + i) * 8 + gq;
+        const int row = (warp + NW * i) * 8 + gq;
         if (row >= g.NRH) continue;
         const int rh = g.NR - 1 - row;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int c = c0 + j * 8 + 2 * q;
             if (c >= ncol) continue;
-            double2 lo = make_double2(acc[0][i][j][0] + acc[1][i][j][0], acc[0][i][j][1] + acc[1][i][j][1]);
-            double2 hi = make_double2(acc[0][i][j][0] - acc[1][i][j][0], acc[0][i][j][1] - acc[1][i][j][1]);
+            double2 lo = make_double2(acc0[i][j][0] + acc1[i][j][0], acc0[i][j][1] + acc1[i][j][1]);
+            double2 hi = make_double2(acc0[i][j][0] - acc1[i][j][0], acc0[i][j][1] - acc1[i][j][1]);
             if (c == 0 && lnv != 0.0) {
                 lo.x += lnv * g.lnx[row];
                 hi.x += lnv * g.lnx[rh];
@@ -128,182 +158,89 @@ __global__ void __launch_bounds__(128) b2p_dmma_kernel(DevGrid g, const double* 
     }
 }
 
-// Fold GEMM for the rows n = 2r + pr of one parity, K-pipelined.  The K rows
-// i < NRH go in chunks of KC = 32; per chunk the CTA stages the weight rows
-// A [RT*8][SAF] (Wt(n, i0..i0+31)) and the input rows x_i and x_{NR-1-i} of its
-// 32 columns in a two-stage cp.async ring; the fold F(i) = (x_i +/- x_{NR-1-i}) w_i
-// of a landed chunk is formed once into a shared B buffer for all warps.
-constexpr int KCF = 32;          // K rows per chunk
-constexpr int SAF = KCF + 4;     // weight row stride (doubles), = 4 mod 16
-constexpr int SXF = CT + 8;      // input row stride (doubles), = 8 mod 16
+// Fold GEMMs: RTRAN(-1) and PROJECT's five EOMUL/OEMUL products.  One CTA
+// computes the output rows n = 2r + pr of one parity, one m and 32 columns,
+// over a K extent of nseg segments of NRH rows each:
+//   out0 = sum_{seg < split} Wt_seg . (s_seg F_seg),  out1 = sum_{seg >= split} ...
+// where F_seg is the EO or OE fold x_i +/- x_{NR-1-i} of the segment's input
+// rows (times w_i for RTRAN(-1)) and s_seg a complex column factor, applied to
+// the folded chunk before the products (the weights are real).  PROJECT
+// (mod_legops.f90:2497-2535) is
+//   PSI = [V | D] . [-i m F0(RUR); -F1(RUP)],
+//   CHI = [D | V | T] . [i k F1(RUR); m k F0(RUP); -F0(UZ)].
+// The K rows go in chunks of KC2 = 16 through a two-stage cp.async ring (the
+// weight rows of the chunk and the input rows x_i, x_{NR-1-i} of the 32
+// columns); the folded, scaled chunk is formed once in shared memory for all
+// warps.  The m-tiles (8 output rows) go round-robin over the warps, and tiles
+// whose rows all lie at n >= NRCHOPS(m) issue no MMAs.  About 49 KB of shared
+// memory lets four CTAs share an SM.
+constexpr int KC2 = 16;       // K rows per chunk
+constexpr int SA2 = KC2 + 4;  // weight row stride (doubles), = 4 mod 16
+constexpr int SX2 = CT + 8;   // input / folded row stride (doubles), = 8 mod 16
 
-template <int NW, int MTW>
-__global__ void __launch_bounds__(NW * 32) fold_dmma_kernel(DevGrid g, const double* __restrict__ Wt, int wt_rows,
-                                                        const double* __restrict__ in, double* __restrict__ out,
-                                                        int mode, int scale, int accumulate, int pad, int use_w,
-                                                        int RTmax) {
-    extern __shared__ double smd[];
-    const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;
-    const int ncol = 2 * g.NXCHOPDIM;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
-    int nn = g.NRCHOP + pad - m;
-    if (nn < 0) nn = 0;
-    const int rows = (g.NRCHOPDIM - pr + 1) / 2;  // output rows n = 2r + pr < NRCHOPDIM
-    const int RT = (rows + 7) / 8;
-    const int nch = (g.NRH + KCF - 1) / KCF;
-    const size_t stA = (size_t)RTmax * 8 * SAF, stX = (size_t)2 * KCF * SXF;
-    double* ws = smd + 2 * (stA + stX);           // [nch*KCF] weights (1 without use_w, 0 past NRH)
-    double* Bs = ws + nch * KCF;                  // [KCF][SXF] folded chunk, shared by the warps
-    const double sgn = (pr ^ mode) ? -1.0 : 1.0;
-    const double* w = Wt + (size_t)m * wt_rows * g.NRH;
-    const double* x = in + (size_t)m * g.NR * ncol;
-    for (int i = tid; i < nch * KCF; i += NW * 32) ws[i] = (i < g.NRH) ? (use_w ? g.w[i] : 1.0) : 0.0;
+struct FoldArgs {
+    const double* w[5];  // weights per segment, [m][wt_rows][NRH]
+    const double* x[5];  // inputs per segment, PFF [m][NR][2 NXCHOPDIM]
+    int mode[5];         // 0: EO fold, 1: OE fold
+    int scale[5];        // 0 none, 1 -v, 2 -i m v, 3 i k v, 4 m k v
+    int nseg, split;     // segments [0, split) -> out0, [split, nseg) -> out1
+    double* out0;
+    double* out1;
+    int wt_rows, pad, use_w, accumulate;
+};
 
-    // chunk ch -> stage ch & 1: A rows r (weights at i0..i0+31), X rows j < 32 (x_{i0+j}),
-    // X rows 32 + j (x_{NR-1-i0-j}); i >= NRH reads as zero
-    auto stage = [&](int ch) {
-        double* As = smd + (ch & 1) * (stA + stX);
-        double* Xs = As + stA;
-        const int i0 = ch * KCF;
-        for (int e = tid; e < RT * 8 * (KCF / 2); e += NW * 32) {
-            const int r = e / (KCF / 2), c2 = e - r * (KCF / 2);
-            const int n = 2 * r + pr, i = i0 + 2 * c2;
-            const bool ok = n < nn && n < wt_rows && i < g.NRH;
-            cp16(As + (size_t)r * SAF + 2 * c2, ok ? w + (size_t)n * g.NRH + i : w, ok);
-        }
-        for (int e = tid; e < 2 * KCF * (CT / 2); e += NW * 32) {
-            const int rr = e / (CT / 2), c2 = e - rr * (CT / 2);
-            const int j = rr % KCF, i = i0 + j;
-            const int src_row = rr < KCF ? i : g.NR - 1 - i;
-            const int c = c0 + 2 * c2;
-            const bool ok = i < g.NRH && c < ncol;
-            cp16(Xs + (size_t)rr * SXF + 2 * c2, ok ? x + (size_t)src_row * ncol + c : x, ok);
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-
-    double acc[MTW][4][2];
+template <class T>
+__device__ __forceinline__ T pick5(const T (&a)[5], int i) {
+    T v = a[0];
 #pragma unroll
-    for (int t = 0; t < MTW; ++t)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
-    stage(0);
-    for (int ch = 0; ch < nch; ++ch) {
-        if (ch + 1 < nch) {
-            stage(ch + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
-        __syncthreads();
-        const double* As = smd + (ch & 1) * (stA + stX);
-        const double* Xs = As + stA;
-        for (int e = tid; e < KCF * CT; e += NW * 32) {
-            const int j = e / CT, c = e - j * CT;
-            Bs[(size_t)j * SXF + c] = (Xs[(size_t)j * SXF + c] + sgn * Xs[(size_t)(KCF + j) * SXF + c]) * ws[ch * KCF + j];
-        }
-        __syncthreads();
-        for (int kk = 0; kk < KCF; kk += 4) {
-            const int j = kk + q;
-            double af[MTW], bf[4];
-#pragma unroll
-            for (int t = 0; t < MTW; ++t) {
-                const int mt = warp * MTW + t;
-                af[t] = (mt < RT) ? As[(size_t)(mt * 8 + gq) * SAF + j] : 0.0;
-            }
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SXF + jj * 8 + gq];
-#pragma unroll
-            for (int t = 0; t < MTW; ++t)
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af[t], bf[jj]);
-        }
-        __syncthreads();  // the stage is refilled by the next iteration's prefetch
-    }
-    double* o = out + (size_t)m * g.NRCHOPDIM * ncol;
-#pragma unroll
-    for (int t = 0; t < MTW; ++t) {
-        const int r = (warp * MTW + t) * 8 + gq;
-        const int n = 2 * r + pr;
-        if (r >= rows || n >= g.NRCHOPDIM) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = c0 + j * 8 + 2 * q;  // even: real part of mode k = c / 2
-            if (c >= ncol) continue;
-            const double re = acc[t][j][0], im = acc[t][j][1];
-            const int kk = c >> 1;
-            double sr = re, si = im;
-            switch (scale) {
-                case 1: sr = -re; si = -im; break;
-                case 2: { const double f = -(double)m; sr = -im * f; si = re * f; } break;  // -i m v
-                case 3: { const double f = g.ak[kk]; sr = -im * f; si = re * f; } break;    //  i k v
-                case 4: { const double f = (double)m * g.ak[kk]; sr = re * f; si = im * f; } break;
-                default: break;
-            }
-            double2* dst = (double2*)(o + (size_t)n * ncol + c);
-            if (n >= nn) {
-                if (!accumulate) *dst = make_double2(0.0, 0.0);
-            } else if (accumulate) {
-                const double2 v = *dst;
-                *dst = make_double2(v.x + sr, v.y + si);
-            } else {
-                *dst = make_double2(sr, si);
-            }
-        }
-    }
+    for (int j = 1; j < 5; ++j)
+        if (i == j) v = a[j];
+    return v;
 }
 
-// PROJECT's five EOMUL/OEMUL products (mod_legops.f90:2497-2535) as two
-// K-concatenated GEMMs per (m, parity of n) and 32-column tile:
-//   PSI = [V | D] . [-i m F0(RUR); -F1(RUP)]                       K = 2 NRH
-//   CHI = [D | V | T] . [i k F1(RUR); m k F0(RUP); -F0(UZ)]         K = 3 NRH
-// F0 / F1 are the EO / OE folds x_i +/- x_{NR-1-i} of the input rows for the
-// output parity; the complex column factors are applied to the folded chunk,
-// before the products (the weights are real).  All 5 NRH / 32 chunks go
-// through one two-stage cp.async ring; PSI is written after the first 2 NRH,
-// CHI at the end, each once and without a read-modify-write.  Segment sg of
-// the K extent: 0 (V, RUR, EO, -i m), 1 (D, RUP, OE, -1), 2 (D, RUR, OE, i k),
-// 3 (V, RUP, EO, m k), 4 (T, UZ, EO, -1).
 template <int NW, int MTW>
-__global__ void __launch_bounds__(NW * 32) project_dmma_kernel(DevGrid g, const double* __restrict__ V,
-                                                           const double* __restrict__ D, const double* __restrict__ T,
-                                                           const double* __restrict__ rur,
-                                                           const double* __restrict__ rup,
-                                                           const double* __restrict__ uz, double* __restrict__ psi,
-                                                           double* __restrict__ chi, int RTmax) {
+__global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, FoldArgs fa, int RTmax) {
     extern __shared__ double smd[];
     const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;
     const int ncol = 2 * g.NXCHOPDIM;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
-    int nn = g.NRCHOP - m;
+    int nn = g.NRCHOP + fa.pad - m;
     if (nn < 0) nn = 0;
-    const int rows = (g.NRCHOPDIM - pr + 1) / 2;
-    const int RT = (rows + 7) / 8;
-    const int nch = (g.NRH + KCF - 1) / KCF;
-    const int total = 5 * nch;
-    const size_t stA = (size_t)RTmax * 8 * SAF, stX = (size_t)2 * KCF * SXF;
-    double* Bs = smd + 2 * (stA + stX);  // [KCF][SXF] folded, scaled chunk
-    const size_t wofs = (size_t)m * g.NRCHOPDIM * g.NRH, xofs = (size_t)m * g.NR * ncol;
+    const int nw = min(nn, fa.wt_rows);                    // rows with weights
+    const int rows = (g.NRCHOPDIM - pr + 1) / 2;           // output rows n = 2r + pr < NRCHOPDIM
+    const int rv = min(rows, max(0, (nw - pr + 1) / 2));   // of them with weights
+    const int RTv = (rv + 7) / 8;
+    const int nch = (g.NRH + KC2 - 1) / KC2;
+    const int total = fa.nseg * nch;
+    const size_t stA = (size_t)RTmax * 8 * SA2, stX = (size_t)2 * KC2 * SX2;
+    double* Bs = smd + 2 * (stA + stX);  // [KC2][SX2] folded, scaled chunk
+    double* ws = Bs + KC2 * SX2;         // [nch * KC2] fold weights (w_i, or 1), 0 past NRH
+    const size_t wofs = (size_t)m * fa.wt_rows * g.NRH, xofs = (size_t)m * g.NR * ncol;
+    for (int i = tid; i < nch * KC2; i += NW * 32) ws[i] = (i < g.NRH) ? (fa.use_w ? g.w[i] : 1.0) : 0.0;
+    // fold pass: thread -> column pair p2 (fixed), rows j = tid / 16 + (NW * 2) t
+    const int p2 = tid & 15;
+    const int cp = c0 + 2 * p2;
+    const double akv = (cp < ncol) ? g.ak[cp >> 1] : 0.0;
 
     auto stage = [&](int gc) {
-        const int sg = gc / nch, i0 = (gc - sg * nch) * KCF;
-        const double* w = (sg == 0 || sg == 3 ? V : (sg == 4 ? T : D)) + wofs;
-        const double* x = (sg == 0 || sg == 2 ? rur : (sg == 4 ? uz : rup)) + xofs;
+        const int sg = gc / nch, i0 = (gc - sg * nch) * KC2;
+        const double* w = pick5(fa.w, sg) + wofs;
+        const double* x = pick5(fa.x, sg) + xofs;
         double* As = smd + (gc & 1) * (stA + stX);
         double* Xs = As + stA;
-        for (int e = tid; e < RT * 8 * (KCF / 2); e += NW * 32) {
-            const int r = e / (KCF / 2), c2 = e - r * (KCF / 2);
+        for (int e = tid; e < RTv * 8 * (KC2 / 2); e += NW * 32) {
+            const int r = e / (KC2 / 2), c2 = e - r * (KC2 / 2);
             const int n = 2 * r + pr, i = i0 + 2 * c2;
-            const bool ok = n < nn && i < g.NRH;
-            cp16(As + (size_t)r * SAF + 2 * c2, ok ? w + (size_t)n * g.NRH + i : w, ok);
+            const bool ok = n < nw && i < g.NRH;
+            cp16(As + (size_t)r * SA2 + 2 * c2, ok ? w + (size_t)n * g.NRH + i : w, ok);
         }
-        for (int e = tid; e < 2 * KCF * (CT / 2); e += NW * 32) {
+        for (int e = tid; e < 2 * KC2 * (CT / 2); e += NW * 32) {
             const int rr = e / (CT / 2), c2 = e - rr * (CT / 2);
-            const int j = rr % KCF, i = i0 + j;
-            const int src_row = rr < KCF ? i : g.NR - 1 - i;
+            const int j = rr % KC2, i = i0 + j;
+            const int src_row = rr < KC2 ? i : g.NR - 1 - i;
             const int c = c0 + 2 * c2;
             const bool ok = i < g.NRH && c < ncol;
-            cp16(Xs + (size_t)rr * SXF + 2 * c2, ok ? x + (size_t)src_row * ncol + c : x, ok);
+            cp16(Xs + (size_t)rr * SX2 + 2 * c2, ok ? x + (size_t)src_row * ncol + c : x, ok);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -311,16 +248,24 @@ __global__ void __launch_bounds__(NW * 32) project_dmma_kernel(DevGrid g, const 
         double* o = out + (size_t)m * g.NRCHOPDIM * ncol;
 #pragma unroll
         for (int t = 0; t < MTW; ++t) {
-            const int r = (warp * MTW + t) * 8 + gq;
+            const int r = (warp + NW * t) * 8 + gq;
             const int n = 2 * r + pr;
             if (r >= rows || n >= g.NRCHOPDIM) continue;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int c = c0 + j * 8 + 2 * q;
-                if (c >= ncol) continue;
-                *(double2*)(o + (size_t)n * ncol + c) =
-                    n < nn ? make_double2(acc[t][j][0], acc[t][j][1]) : make_double2(0.0, 0.0);
+                double2 v = make_double2(acc[t][j][0], acc[t][j][1]);
                 acc[t][j][0] = acc[t][j][1] = 0.0;
+                if (c >= ncol) continue;
+                double2* dst = (double2*)(o + (size_t)n * ncol + c);
+                if (n >= nn) {
+                    if (!fa.accumulate) *dst = make_double2(0.0, 0.0);
+                } else if (fa.accumulate) {
+                    const double2 u = *dst;
+                    *dst = make_double2(u.x + v.x, u.y + v.y);
+                } else {
+                    *dst = v;
+                }
             }
         }
     };
@@ -339,45 +284,44 @@ __global__ void __launch_bounds__(NW * 32) project_dmma_kernel(DevGrid g, const 
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
-        const int sg = gc / nch;
+        const int sg = gc / nch, ch = gc - sg * nch;
         const double* As = smd + (gc & 1) * (stA + stX);
         const double* Xs = As + stA;
-        // fold sign for (parity, EO/OE) and the complex column factor of the segment
-        const double sgn = (pr ^ (sg == 1 || sg == 2 ? 1 : 0)) ? -1.0 : 1.0;
-        for (int e = tid; e < KCF * (CT / 2); e += NW * 32) {
-            const int j = e / (CT / 2), c = 2 * (e - j * (CT / 2));
-            const double re = Xs[(size_t)j * SXF + c] + sgn * Xs[(size_t)(KCF + j) * SXF + c];
-            const double im = Xs[(size_t)j * SXF + c + 1] + sgn * Xs[(size_t)(KCF + j) * SXF + c + 1];
-            const int kk = (c0 + c) >> 1;
-            const double ak = (c0 + c < ncol) ? g.ak[kk] : 0.0;
-            double sr, si;
-            switch (sg) {
-                case 0: sr = im * m; si = -re * m; break;                    // -i m v
-                case 2: sr = -im * ak; si = re * ak; break;                  //  i k v
-                case 3: { const double f = m * ak; sr = re * f; si = im * f; } break;  // m k v
-                default: sr = -re; si = -im; break;                          // -v
+        const double sgn = (pr ^ pick5(fa.mode, sg)) ? -1.0 : 1.0;
+        const int sc = pick5(fa.scale, sg);
+        for (int j = tid >> 4; j < KC2; j += NW * 2) {
+            const double2 top = *(const double2*)(Xs + (size_t)j * SX2 + 2 * p2);
+            const double2 bot = *(const double2*)(Xs + (size_t)(KC2 + j) * SX2 + 2 * p2);
+            const double wv = ws[ch * KC2 + j];
+            const double re = (top.x + sgn * bot.x) * wv, im = (top.y + sgn * bot.y) * wv;
+            double2 v;
+            switch (sc) {
+                case 1: v = make_double2(-re, -im); break;
+                case 2: v = make_double2(im * m, -re * m); break;  // -i m v
+                case 3: v = make_double2(-im * akv, re * akv); break;  // i k v
+                case 4: { const double f = m * akv; v = make_double2(re * f, im * f); } break;  // m k v
+                default: v = make_double2(re, im); break;
             }
-            Bs[(size_t)j * SXF + c] = sr;
-            Bs[(size_t)j * SXF + c + 1] = si;
+            *(double2*)(Bs + (size_t)j * SX2 + 2 * p2) = v;
         }
         __syncthreads();
-        for (int kk = 0; kk < KCF; kk += 4) {
+#pragma unroll
+        for (int kk = 0; kk < KC2; kk += 4) {
             const int j = kk + q;
-            double af[MTW], bf[4];
+            double bf[4];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SX2 + jj * 8 + gq];
 #pragma unroll
             for (int t = 0; t < MTW; ++t) {
-                const int mt = warp * MTW + t;
-                af[t] = (mt < RT) ? As[(size_t)(mt * 8 + gq) * SAF + j] : 0.0;
+                const int mt = warp + NW * t;
+                if (mt < RTv) {
+                    const double af = As[(size_t)(mt * 8 + gq) * SA2 + j];
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af, bf[jj]);
+                }
             }
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SXF + jj * 8 + gq];
-#pragma unroll
-            for (int t = 0; t < MTW; ++t)
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af[t], bf[jj]);
         }
-        if (gc == 2 * nch - 1) epilogue(acc, psi);
-        if (gc == total - 1) epilogue(acc, chi);
+        if (gc == fa.split * nch - 1 || gc == total - 1) epilogue(acc, gc < fa.split * nch ? fa.out0 : fa.out1);
         __syncthreads();  // the stage is refilled by the next iteration's prefetch
     }
 }
@@ -388,113 +332,94 @@ static int pad16_8(int v) { return v + ((8 - v % 16) + 16) % 16; }  // smallest 
 
 bool dmma_supported(const DevGrid& g) { return g.NRH <= 128 && g.NRH % 2 == 0 && g.NRCHOPDIM <= 256; }
 
-template <int MTW>
+template <int NW, int MTW>
 static void b2p_launch(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
     const int SA = pad16_8(((g.NRH + 7) / 8) * 8);
-    const int KPmax = ((g.NRCHOPDIM + 1) / 2 + 3) & ~3;
-    const size_t smem = (size_t)KPmax * (SA + SBS) * sizeof(double);
+    const size_t smem = 2 * (size_t)KCB * (SA + SBS) * sizeof(double);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(b2p_dmma_kernel<MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(b2p_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
     dim3 grid((2 * g.NXCHOPDIM + CT - 1) / CT, g.NTCHOPDIM);
-    b2p_dmma_kernel<MTW><<<grid, 128, smem, s>>>(g, (const double*)a, (double*)b, ln, pad, SA, KPmax);
+    b2p_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, (const double*)a, (double*)b, ln, pad, SA);
     count_launch();
 }
 
+// The NRH / 8 output m-tiles go round-robin over 6 warps.
 void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
     const int RT = (g.NRH + 7) / 8;
-    switch ((RT + 3) / 4) {
-        case 1: b2p_launch<1>(g, a, b, ln, pad, s); break;
-        case 2: b2p_launch<2>(g, a, b, ln, pad, s); break;
-        case 3: b2p_launch<3>(g, a, b, ln, pad, s); break;
-        default: b2p_launch<4>(g, a, b, ln, pad, s); break;
+    switch ((RT + 5) / 6) {
+        case 1: b2p_launch<6, 1>(g, a, b, ln, pad, s); break;
+        default: b2p_launch<6, 2>(g, a, b, ln, pad, s); break;
+        case 3: b2p_launch<6, 3>(g, a, b, ln, pad, s); break;
     }
 }
 
 template <int NW, int MTW>
-static void fold_launch(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out, int mode,
-                        int scale, int accumulate, int pad, int use_w, cudaStream_t s) {
+static void legfold_launch(const DevGrid& g, const FoldArgs& fa, cudaStream_t s) {
     const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
-    const int nch = (g.NRH + KCF - 1) / KCF;
+    const int nch = (g.NRH + KC2 - 1) / KC2;
     const size_t smem =
-        (2 * ((size_t)RT * 8 * SAF + (size_t)2 * KCF * SXF) + (size_t)nch * KCF + (size_t)KCF * SXF) * sizeof(double);
+        (2 * ((size_t)RT * 8 * SA2 + (size_t)2 * KC2 * SX2) + (size_t)KC2 * SX2 + (size_t)nch * KC2) * sizeof(double);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(fold_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(legfold_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
     dim3 grid((2 * g.NXCHOPDIM + CT - 1) / CT, 2, g.NTCHOPDIM);
-    fold_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, Wt, wt_rows, (const double*)in, (double*)out, mode,
-                                                          scale, accumulate, pad, use_w, RT);
+    legfold_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, fa, RT);
     count_launch();
+}
+
+// The output-row m-tiles of one parity go round-robin over 4 warps.
+static void legfold(const DevGrid& g, const FoldArgs& fa, cudaStream_t s) {
+    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
+    switch ((RT + 3) / 4) {
+        case 1: legfold_launch<4, 1>(g, fa, s); break;
+        case 2: legfold_launch<4, 2>(g, fa, s); break;
+        case 3: legfold_launch<4, 3>(g, fa, s); break;
+        default: legfold_launch<4, 4>(g, fa, s); break;
+    }
 }
 
 void k_fold_gemm_dmma(const DevGrid& g, const double* Wt, int wt_rows, const double2* in, double2* out, int mode,
                       int scale, int accumulate, int pad, cudaStream_t s) {
-    // m-tiles of the output rows of one parity split over 3 or 4 warps with the least idle tiles
-    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
-    const int use_w = (mode & 2) ? 1 : 0;
-    const int m4 = (RT + 3) / 4, m3 = (RT + 2) / 3;
-    const bool three = 3 * m3 - RT < 4 * m4 - RT && m3 <= 4;
-#define FOLD_CASE(NW, MTW) fold_launch<NW, MTW>(g, Wt, wt_rows, in, out, mode & 1, scale, accumulate, pad, use_w, s)
-    if (three) {
-        switch (m3) {
-            case 1: FOLD_CASE(3, 1); break;
-            case 2: FOLD_CASE(3, 2); break;
-            case 3: FOLD_CASE(3, 3); break;
-            default: FOLD_CASE(3, 4); break;
-        }
-    } else {
-        switch (m4) {
-            case 1: FOLD_CASE(4, 1); break;
-            case 2: FOLD_CASE(4, 2); break;
-            case 3: FOLD_CASE(4, 3); break;
-            default: FOLD_CASE(4, 4); break;
-        }
-    }
-#undef FOLD_CASE
-}
-
-template <int NW, int MTW>
-static void project_launch(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
-                           const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s) {
-    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
-    const size_t smem = (2 * ((size_t)RT * 8 * SAF + (size_t)2 * KCF * SXF) + (size_t)KCF * SXF) * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(project_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
-    dim3 grid((2 * g.NXCHOPDIM + CT - 1) / CT, 2, g.NTCHOPDIM);
-    project_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, V, D, T, (const double*)rur, (const double*)rup,
-                                                             (const double*)uz, (double*)psi, (double*)chi, RT);
-    count_launch();
+    FoldArgs fa{};
+    fa.w[0] = Wt;
+    fa.x[0] = (const double*)in;
+    fa.mode[0] = mode & 1;
+    fa.scale[0] = scale;
+    fa.nseg = fa.split = 1;
+    fa.out0 = fa.out1 = (double*)out;
+    fa.wt_rows = wt_rows;
+    fa.pad = pad;
+    fa.use_w = (mode & 2) ? 1 : 0;
+    fa.accumulate = accumulate;
+    legfold(g, fa, s);
 }
 
 void k_project_dmma(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
                     const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s) {
-    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
-    const int m4 = (RT + 3) / 4, m3 = (RT + 2) / 3;
-    const bool three = 3 * m3 - RT < 4 * m4 - RT && m3 <= 4;
-#define PROJ_CASE(NW, MTW) project_launch<NW, MTW>(g, V, D, T, rur, rup, uz, psi, chi, s)
-    if (three) {
-        switch (m3) {
-            case 1: PROJ_CASE(3, 1); break;
-            case 2: PROJ_CASE(3, 2); break;
-            case 3: PROJ_CASE(3, 3); break;
-            default: PROJ_CASE(3, 4); break;
-        }
-    } else {
-        switch (m4) {
-            case 1: PROJ_CASE(4, 1); break;
-            case 2: PROJ_CASE(4, 2); break;
-            case 3: PROJ_CASE(4, 3); break;
-            default: PROJ_CASE(4, 4); break;
-        }
+    FoldArgs fa{};
+    const double* w[5] = {V, D, D, V, T};
+    const double2* x[5] = {rur, rup, rur, rup, uz};
+    const int mode[5] = {0, 1, 1, 0, 0}, scale[5] = {2, 1, 3, 4, 1};
+    for (int q = 0; q < 5; ++q) {
+        fa.w[q] = w[q];
+        fa.x[q] = (const double*)x[q];
+        fa.mode[q] = mode[q];
+        fa.scale[q] = scale[q];
     }
-#undef PROJ_CASE
+    fa.nseg = 5;
+    fa.split = 2;
+    fa.out0 = (double*)psi;
+    fa.out1 = (double*)chi;
+    fa.wt_rows = g.NRCHOPDIM;
+    fa.pad = 0;
+    fa.use_w = 0;
+    fa.accumulate = 0;
+    legfold(g, fa, s);
 }
 
 }  // namespace mlegs

@@ -279,8 +279,34 @@ struct mlegs_ctx {
         ln_zero(b);
     }
     // IDEL2 (823-1010): has_ln = 0 -> LN absent.
+    // LU factors per (kind, pad, alp), formed on first use outside graph capture
+    struct SolveFactors {
+        int kind, pad;
+        double alp;
+        double *F5, *F7;
+    };
+    std::vector<SolveFactors> sfac;
+    const SolveFactors* factors(int kind, int pad, double alp) {
+        for (const SolveFactors& f : sfac)
+            if (f.kind == kind && f.pad == pad && f.alp == alp) return &f;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(s, &cs));
+        if (cs != cudaStreamCaptureStatusNone || sfac.size() >= 8 || pad < 0 || d.NRCHOP + pad > d.NRCHOPDIM)
+            return nullptr;
+        size_t n5, n7;
+        solve_factor_sizes(g, &n5, &n7);
+        SolveFactors f{kind, pad, alp, dalloc<double>(n5), dalloc<double>(n7)};
+        k_solve_factor(g, kind, alp, pad, f.F5, f.F7, s);
+        sfac.push_back(f);
+        return &sfac.back();
+    }
     void idel2(const Field* bb, Field* a, int has_ln, double ln, int pad) {
         require(bb, MLEGS_FFF, "IDEL2");
+        if (const SolveFactors* f = factors(1, pad, 0.0)) {
+            k_solve_factored(g, f->F5, f->F7, bb->data, a->data, a->ln, 1, has_ln, ln, pad, 1, s);
+            a->space = MLEGS_FFF;
+            return;
+        }
         copy0(a, bb, pad);
         ln_zero(a);
         k_solve_del2(g, a->data, a->ln, 1, 0.0, has_ln, ln, nullptr, solve_scr, pad, s);
@@ -289,6 +315,11 @@ struct mlegs_ctx {
     }
     void idel2ln(const Field* bb, Field* a, int pad) {  // 1013-1176
         require(bb, MLEGS_FFF, "IDEL2LN");
+        if (const SolveFactors* f = factors(0, pad, 0.0)) {
+            k_solve_factored(g, f->F5, f->F7, bb->data, a->data, a->ln, 0, 0, 0.0, pad, 1, s);
+            a->space = MLEGS_FFF;
+            return;
+        }
         copy0(a, bb, pad);
         ln_zero(a);
         k_solve_del2(g, a->data, a->ln, 0, 0.0, 0, 0.0, nullptr, solve_scr, pad, s);
@@ -301,7 +332,10 @@ struct mlegs_ctx {
         copy0(a, bb, pad);
         k_ln_copy(a->ln, bb->ln, -1.0 / alp, s);      // A%LN = -B%LN/ALP
         k_logterm_rows(g, a->data, a->ln, 2, 1.0, s);  // rhs -= LN * DEL2(log)
-        k_solve_del2(g, a->data, nullptr, 2, alp, 0, 0.0, nullptr, solve_scr, pad, s);
+        if (const SolveFactors* f = factors(2, pad, alp))
+            k_solve_factored(g, f->F5, f->F7, a->data, a->data, nullptr, 2, 0, 0.0, pad, 0, s);
+        else
+            k_solve_del2(g, a->data, nullptr, 2, alp, 0, 0.0, nullptr, solve_scr, pad, s);
         chopdo(a, pad);
     }
     // The fused derivative kernels read row neighbours of their inputs while
@@ -1425,6 +1459,13 @@ int mlegs_solver_init(mlegs_ctx* ctx, mlegs_field* psi, mlegs_field* chi, mlegs_
             ctx->ln_zero(h);
             h->space = MLEGS_FFF;
         }
+        // factors of the steady step's solves, so that a captured step finds them
+        ctx->factors(0, 0, 0.0);
+        if (!ctx->p.adams) ctx->factors(1, 0, 0.0);
+        if (ctx->p.visc_sw == 1) {  // VISC2's Helmholtz shifts (same expression as visc2)
+            ctx->factors(2, 0, 2 / ctx->p.nu / ctx->p.dt);
+            if (ctx->p.kappa != 0.0) ctx->factors(2, 0, 2 / ctx->p.kappa / ctx->p.dt);
+        }
         ctx->mark();
         if (ctx->p.adams) ctx->rich_fe_be();
         else ctx->rich_etdfe_be();
@@ -1540,9 +1581,11 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                                       f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data, b->data,
                                       1.0, 1.0, 1, s);
                     break;
-                case 7:
-                    k_solve_del2(g, a->data, c->ln, 0, 0.0, 0, 0.0, nullptr, ctx->solve_scr, 0, s);
-                    break;
+                case 7: {
+                    const auto* f = ctx->factors(0, 0, 0.0);
+                    if (f) k_solve_factored(g, f->F5, f->F7, a->data, b->data, c->ln, 0, 0, 0.0, 0, 1, s);
+                    else k_solve_del2(g, a->data, c->ln, 0, 0.0, 0, 0.0, nullptr, ctx->solve_scr, 0, s);
+                } break;
                 case 8: {
                     const double2* in[10] = {f9[0]->data, f9[1]->data, f9[2]->data, f9[3]->data, f9[4]->data,
                                              f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data};
@@ -1583,7 +1626,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 2: case 3: bytes = B16 * ((double)d.pff() + (double)d.pfp()); break;
             case 4: case 5: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
             case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written
-            case 7: bytes = B16 * 2.0 * (double)d.fff(); break;
+            case 7: bytes = (B16 * 2.0 + 40.0) * (double)d.fff(); break;  // rhs in, solution out, 5 factors
             case 8: bytes = B16 * 14.0 * (double)d.pfp(); break;  // 10 PFP lines read, 4 written
             case 13: bytes = B16 * (3.0 * (double)d.pff() + 2.0 * (double)d.fff()); break;
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;

@@ -154,6 +154,13 @@ void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode
 // Banded solves (IDEL2LN, IDEL2, IHELM) with per-system elimination scratch.
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln,
                   double ln_in, const double* b_ln, double* scratch, int pad, cudaStream_t s);
+// Factor-once form of the same solves (solve.cu): LU factors of every (m, k)
+// system for one (kind, pad, alp), then substitutions only; src -> dst with
+// rows past the system size zeroed, farfield = 1 adds the CALCAT1 row-0 fix.
+void solve_factor_sizes(const DevGrid& g, size_t* f5, size_t* f7);
+void k_solve_factor(const DevGrid& g, int kind, double alp, int pad, double* F5, double* F7, cudaStream_t s);
+void k_solve_factored(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
+                      double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s);
 // Fixed __device__ solve scratch (solve_static.cu) for the allocation-free
 // IDEL2LN entry point: returns 0 and its address on `device` (the current
 // device), 1 if need_doubles exceeds kStaticSolveBytes, 2 on a CUDA error;

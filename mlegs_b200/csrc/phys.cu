@@ -486,6 +486,17 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
     const double o2 = 2 * A.omega, n2 = A.bv0 * A.bv0;
     for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
         const size_t off = (size_t)line * md;
+        // the warp's next line: lanes 0..9 ask L2 for its ten input rows (md complex each)
+        const int nxt = line + gridDim.x * nw;
+        if (lane < 10 && nxt < nlines && (lane < 9 || A.linear)) {
+            const double2* src = A.in[0];
+#pragma unroll
+            for (int q = 1; q < 10; ++q)
+                if (lane == q) src = A.in[q];
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src + (size_t)nxt * md),
+                         "r"((unsigned)(md * sizeof(double2)))
+                         : "memory");
+        }
         const double rr = g.r[line / g.NX];
         const double ir2 = 1.0 / (rr * rr);
         // round 1 and 2 (G = 4: one field per group; G = 2: two passes; G = 8: half the groups idle)

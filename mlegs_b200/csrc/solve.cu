@@ -218,6 +218,241 @@ __global__ void solve_kernel(DevGrid g, double2* A, double* ln_out, int kind, do
     }
 }
 
+// ---------------------------------------------------------------------------
+// Factor once, solve many.  For a fixed (kind, pad, alp) the system matrices
+// do not change from call to call, so their LU factors (the same unpivoted
+// elimination as solve_kernel, LUDCMPB of mod_bandmat.f90:65-155) are stored
+// once and every later solve is only the substitutions of LUBKSBB (320-401):
+//   F5 [row][5][system]  f2 = L(r, r-2), f1 = L(r, r-1), U(r, r), U(r, r+1), U(r, r+2)
+//                        for the 5-band systems;
+//   F7 [row][7][k]       f3, f2, f1, U(r, r .. r+3) for the 7-band m = 0 systems
+//                        of kinds 1 and 2.
+// The multipliers and pivots are the ones solve_kernel forms, and the
+// substitutions apply them in the same order, so both paths give the same
+// bits.
+__global__ void factor_kernel(DevGrid g, int kind, double alp, int pad, double* F5, double* F7) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nsys) return;
+    const int k = t % g.NXCHOPDIM;
+    const int m = t / g.NXCHOPDIM;
+    int nn = g.NRCHOP + pad - m;
+    if (nn < 0) nn = 0;
+    BandRowCtx c;
+    c.del2h = g.del2h + (size_t)m * g.NB * 5;
+    c.xm = g.xm + (size_t)m * g.NB * 2;
+    c.shift = g.ak[k] * g.ak[k] + ((kind == 2) ? alp : 0.0);
+    c.kind = kind;
+    c.m = m;
+    c.k = k;
+    c.l0 = 4.0 / 3 / g.ELL2;
+    c.l1 = -2 * g.norm0[0] / g.norm0[1] / g.ELL2;
+    c.l2 = 2.0 / 3 * g.norm0[0] / g.norm0[2] / g.ELL2;
+    const bool wide = (m == 0 && kind != 0);
+    const int lo = wide ? 3 : 2, up = wide ? 3 : 2;
+    const int size = (m == 0 && kind == 2) ? nn - 1 : nn;
+    double U[3][4] = {};
+    for (int r = 0; r < size; ++r) {
+        double w[MAXW];
+        build_row(c, r, w);
+        double f[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int d = 3; d >= 1; --d) {
+            if (d > lo || r - d < 0) continue;
+            const int wi = (r - d) % 3;
+            f[d] = w[3 - d] / U[wi][0];
+            w[3 - d] = 0.0;
+            for (int j = 1; j <= 3; ++j) {
+                if (j > up) continue;
+                const int qq = 3 - d + j;
+                if (qq < MAXW) w[qq] -= f[d] * U[wi][j];
+            }
+        }
+        const int wr = r % 3;
+        U[wr][0] = w[3];
+        for (int j = 1; j <= 3; ++j) U[wr][j] = (j <= up) ? w[3 + j] : 0.0;
+        if (wide) {
+            double* o = F7 + (size_t)r * 7 * g.NXCHOPDIM + k;
+            o[0] = f[3];
+            o[(size_t)1 * g.NXCHOPDIM] = f[2];
+            o[(size_t)2 * g.NXCHOPDIM] = f[1];
+            for (int j = 0; j < 4; ++j) o[(size_t)(3 + j) * g.NXCHOPDIM] = U[wr][j];
+        } else {
+            double* o = F5 + (size_t)r * 5 * nsys + t;
+            o[0] = f[2];
+            o[(size_t)1 * nsys] = f[1];
+            for (int j = 0; j < 3; ++j) o[(size_t)(2 + j) * nsys] = U[wr][j];
+        }
+    }
+}
+
+// One thread per (system, real or imaginary part).  Reads the right-hand side
+// from src, writes the solution to dst (rows >= the system size are zeroed),
+// then the per-kind tails of solve_kernel; farfield = 1 also applies the
+// CALCAT1 row-0 correction over n < NRCHOP + pad to the m = 0 columns.
+__global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const double* __restrict__ F5,
+                                                             const double* __restrict__ F7, const double2* src,
+                                                             double2* dst, double* ln_out, int kind, int has_ln,
+                                                             double ln_in, int pad, int farfield) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = u >> 1, comp = u & 1;
+    if (t >= nsys) return;
+    const int k = t % g.NXCHOPDIM;
+    const int m = t / g.NXCHOPDIM;
+    int nn = g.NRCHOP + pad - m;
+    if (nn < 0) nn = 0;
+    const bool wide = (m == 0 && kind != 0);
+    int size = (m == 0 && kind == 2) ? nn - 1 : nn;
+    if (size < 0) size = 0;
+    const size_t cofs = (size_t)m * g.NRCHOPDIM * g.NXCHOPDIM + k;
+    const double* in = (const double*)(src + cofs) + comp;
+    double* col = (double*)(dst + cofs) + comp;
+    const size_t st = 2 * (size_t)g.NXCHOPDIM;
+    // IDEL2 (m = 0, k = 0): right-hand side shifted down one row, row 0 <- the LN condition (929-936)
+    const bool shift = (kind == 1 && m == 0 && k == 0);
+    auto rhs = [&](int r) -> double {
+        if (!shift) return in[(size_t)r * st];
+        if (r == 0) return comp ? 0.0 : (has_ln ? ln_in / g.norm0[0] : 0.0);
+        return in[(size_t)(r - 1) * st];
+    };
+    if (shift) {
+        // the shifted rows are read from src before any row of dst is written (src may be dst)
+        double prev = rhs(0);
+        for (int r = 0; r < size; ++r) {
+            const double cur = (r + 1 < size) ? rhs(r + 1) : 0.0;
+            col[(size_t)r * st] = prev;
+            prev = cur;
+        }
+        in = col;
+    }
+    constexpr int RBF = 8;
+    if (!wide) {
+        double y1 = 0.0, y2 = 0.0;
+        for (int r0 = 0; r0 < size; r0 += RBF) {
+            double rb[RBF], fa[RBF], fb[RBF];
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r0 + q;
+                const bool ok = r < size;
+                rb[q] = ok ? in[(size_t)r * st] : 0.0;
+                fa[q] = ok ? F5[(size_t)r * 5 * nsys + t] : 0.0;
+                fb[q] = ok ? F5[((size_t)r * 5 + 1) * nsys + t] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                if (r0 + q >= size) break;
+                double y = rb[q];
+                y -= fa[q] * y2;
+                y -= fb[q] * y1;
+                col[(size_t)(r0 + q) * st] = y;
+                y2 = y1;
+                y1 = y;
+            }
+        }
+        double x1 = 0.0, x2 = 0.0;
+        for (int r1 = size - 1; r1 >= 0; r1 -= RBF) {
+            double vb[RBF], u0[RBF], u1[RBF], u2[RBF];
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r1 - q;
+                const bool ok = r >= 0;
+                vb[q] = ok ? col[(size_t)r * st] : 0.0;
+                u0[q] = ok ? F5[((size_t)r * 5 + 2) * nsys + t] : 1.0;
+                u1[q] = ok ? F5[((size_t)r * 5 + 3) * nsys + t] : 0.0;
+                u2[q] = ok ? F5[((size_t)r * 5 + 4) * nsys + t] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r1 - q;
+                if (r < 0) break;
+                double v = vb[q];
+                if (r + 1 < size) v -= u1[q] * x1;
+                if (r + 2 < size) v -= u2[q] * x2;
+                v /= u0[q];
+                col[(size_t)r * st] = v;
+                x2 = x1;
+                x1 = v;
+            }
+        }
+    } else {
+        const int NK = g.NXCHOPDIM;
+        double y1 = 0.0, y2 = 0.0, y3 = 0.0;
+        for (int r = 0; r < size; ++r) {
+            const double* f = F7 + (size_t)r * 7 * NK + k;
+            double y = in[(size_t)r * st];
+            y -= f[0] * y3;
+            y -= f[(size_t)NK] * y2;
+            y -= f[(size_t)2 * NK] * y1;
+            col[(size_t)r * st] = y;
+            y3 = y2;
+            y2 = y1;
+            y1 = y;
+        }
+        double x1 = 0.0, x2 = 0.0, x3 = 0.0;
+        for (int r = size - 1; r >= 0; --r) {
+            const double* f = F7 + (size_t)r * 7 * NK + k;
+            double v = col[(size_t)r * st];
+            if (r + 1 < size) v -= f[(size_t)4 * NK] * x1;
+            if (r + 2 < size) v -= f[(size_t)5 * NK] * x2;
+            if (r + 3 < size) v -= f[(size_t)6 * NK] * x3;
+            v /= f[(size_t)3 * NK];
+            col[(size_t)r * st] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
+    }
+    for (int r = size; r < g.NRCHOPDIM; ++r) col[(size_t)r * st] = 0.0;
+    if (m == 0 && kind == 2 && nn > 0) {
+        // A(NN) = 0; A(:NN) = XM(:NN) y  (1310-1316)
+        const double* xm = g.xm;
+        double prev = 0.0;
+        for (int r = 0; r < nn; ++r) {
+            const double cur = col[(size_t)r * st];
+            const double nxt = (r + 1 < nn) ? col[(size_t)(r + 1) * st] : 0.0;
+            double v = cur;
+            if (r >= 1) v += xm[(size_t)r * 2] * prev;
+            if (r + 1 < nn) v += xm[(size_t)r * 2 + 1] * nxt;
+            col[(size_t)r * st] = v;
+            prev = cur;
+        }
+    }
+    if (m == 0 && k == 0 && size > 0) {
+        if (kind == 0) {
+            if (!comp) *ln_out = col[0] * g.norm0[0];
+            col[0] = 0.0;
+        } else if (kind == 1 && !comp && ln_out) {
+            *ln_out = has_ln ? col[0] * g.norm0[0] : 0.0;
+        }
+    }
+    if (farfield && m == 0) {
+        // a(n=0, m=0, k) -= sum_{n < NRCHOP+pad} AT1(n) a(n, 0, k) / AT1(0)
+        const int nr_sum = g.NRCHOP + pad;
+        double sum = 0.0;
+        for (int r = 0; r < nr_sum && r < g.NRCHOPDIM; ++r) sum += g.at1[r] * col[(size_t)r * st];
+        col[0] -= sum / g.at1[0];
+    }
+}
+
+void solve_factor_sizes(const DevGrid& g, size_t* f5, size_t* f7) {
+    *f5 = (size_t)g.NRCHOPDIM * 5 * g.NTCHOPDIM * g.NXCHOPDIM;
+    *f7 = (size_t)g.NRCHOPDIM * 7 * g.NXCHOPDIM;
+}
+
+void k_solve_factor(const DevGrid& g, int kind, double alp, int pad, double* F5, double* F7, cudaStream_t s) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    factor_kernel<<<(nsys + 63) / 64, 64, 0, s>>>(g, kind, alp, pad, F5, F7);
+    count_launch();
+}
+
+void k_solve_factored(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
+                      double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s) {
+    const int n = 2 * g.NTCHOPDIM * g.NXCHOPDIM;
+    solve_factored_kernel<<<(n + 127) / 128, 128, 0, s>>>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad,
+                                                          farfield);
+    count_launch();
+}
+
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln, double ln_in,
                   const double* b_ln, double* scratch, int pad, cudaStream_t s) {
     int nsys = g.NTCHOPDIM * g.NXCHOPDIM;

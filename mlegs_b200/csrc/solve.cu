@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const do
         }
         in = col;
     }
-    constexpr int RBF = 8;
+    constexpr int RBF = 16;
     if (!wide) {
         double y1 = 0.0, y2 = 0.0;
         for (int r0 = 0; r0 < size; r0 += RBF) {
@@ -375,31 +375,61 @@ __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const do
             }
         }
     } else {
-        const int NK = g.NXCHOPDIM;
+        const size_t NK = g.NXCHOPDIM;
         double y1 = 0.0, y2 = 0.0, y3 = 0.0;
-        for (int r = 0; r < size; ++r) {
-            const double* f = F7 + (size_t)r * 7 * NK + k;
-            double y = in[(size_t)r * st];
-            y -= f[0] * y3;
-            y -= f[(size_t)NK] * y2;
-            y -= f[(size_t)2 * NK] * y1;
-            col[(size_t)r * st] = y;
-            y3 = y2;
-            y2 = y1;
-            y1 = y;
+        for (int r0 = 0; r0 < size; r0 += RBF) {
+            double rb[RBF], f3[RBF], f2[RBF], f1[RBF];
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r0 + q;
+                const bool ok = r < size;
+                const double* f = F7 + (size_t)r * 7 * NK + k;
+                rb[q] = ok ? in[(size_t)r * st] : 0.0;
+                f3[q] = ok ? f[0] : 0.0;
+                f2[q] = ok ? f[NK] : 0.0;
+                f1[q] = ok ? f[2 * NK] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                if (r0 + q >= size) break;
+                double y = rb[q];
+                y -= f3[q] * y3;
+                y -= f2[q] * y2;
+                y -= f1[q] * y1;
+                col[(size_t)(r0 + q) * st] = y;
+                y3 = y2;
+                y2 = y1;
+                y1 = y;
+            }
         }
         double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-        for (int r = size - 1; r >= 0; --r) {
-            const double* f = F7 + (size_t)r * 7 * NK + k;
-            double v = col[(size_t)r * st];
-            if (r + 1 < size) v -= f[(size_t)4 * NK] * x1;
-            if (r + 2 < size) v -= f[(size_t)5 * NK] * x2;
-            if (r + 3 < size) v -= f[(size_t)6 * NK] * x3;
-            v /= f[(size_t)3 * NK];
-            col[(size_t)r * st] = v;
-            x3 = x2;
-            x2 = x1;
-            x1 = v;
+        for (int r1 = size - 1; r1 >= 0; r1 -= RBF) {
+            double vb[RBF], u0[RBF], u1[RBF], u2[RBF], u3[RBF];
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r1 - q;
+                const bool ok = r >= 0;
+                const double* f = F7 + (size_t)(ok ? r : 0) * 7 * NK + k;
+                vb[q] = ok ? col[(size_t)r * st] : 0.0;
+                u0[q] = ok ? f[3 * NK] : 1.0;
+                u1[q] = ok ? f[4 * NK] : 0.0;
+                u2[q] = ok ? f[5 * NK] : 0.0;
+                u3[q] = ok ? f[6 * NK] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r1 - q;
+                if (r < 0) break;
+                double v = vb[q];
+                if (r + 1 < size) v -= u1[q] * x1;
+                if (r + 2 < size) v -= u2[q] * x2;
+                if (r + 3 < size) v -= u3[q] * x3;
+                v /= u0[q];
+                col[(size_t)r * st] = v;
+                x3 = x2;
+                x2 = x1;
+                x1 = v;
+            }
         }
     }
     for (int r = size; r < g.NRCHOPDIM; ++r) col[(size_t)r * st] = 0.0;

@@ -260,7 +260,8 @@ class Context:
     KERNELS = {"rtran_b2p": 0, "rtran_p2b": 1, "verfft_b": 2, "verfft_f": 3, "horfft_b": 4,
                "horfft_f": 5, "pointwise": 6, "solve": 7, "phys": 8,
                "horfft_wb": 9, "horfft_wf": 10, "split_b2p": 11,
-               "split_p2b": 12, "project": 13}
+               "split_p2b": 12, "project": 13,
+               "project_fff": 14}
 
     def kernel_time(self, name, reps=20):
         """Mean device ms per launch of one internal kernel (CUDA events on the

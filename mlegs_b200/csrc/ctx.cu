@@ -76,6 +76,7 @@ struct mlegs_ctx {
            *tb_del2h = nullptr;
     double *V = nullptr, *D = nullptr, *T = nullptr;
     double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
+    double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
     double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
     FFTPlan fft;
     std::vector<double> h_x, h_w, h_lognorm;
@@ -416,6 +417,21 @@ struct mlegs_ctx {
         k_farfield_fix(g, psi_->data, d.NRCHOP, s);
     }
 
+    // PROJECT(RUR, RUP, UZ, PSI, CHI) with PSI%LN by reference (ln_mode 2) for
+    // FFF inputs whose LN terms are zero: one composite FFF -> FFF product per m
+    // in FP64 contexts (RUP's (0, 0) column is changed in place by VEL2PLN).
+    void project_fff_ln2(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_) {
+        if (!compV || rur->space != MLEGS_FFF || rup->space != MLEGS_FFF || uz->space != MLEGS_FFF) {
+            project(rur, rup, uz, psi_, chi_, 2, 0.0);
+            return;
+        }
+        psi_->space = chi_->space = MLEGS_FFF;
+        k_project_fff_dmma(g, compV, compD, compT, rur->data, rup->data, uz->data, psi_->data, chi_->data, psi_->ln,
+                           explog0, s);
+        ln_zero(chi_);
+        k_farfield_fix(g, psi_->data, d.NRCHOP, s);
+    }
+
     // ------------------------------------------------------------------ physics
     void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
@@ -624,6 +640,15 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     D = dalloc<double>(vsz);
     T = dalloc<double>(vsz);
     k_tables_project(g, V, D, T, 0, s);
+    if (p.precision == MLEGS_PREC_FP64 && dmma_supported(g)) {
+        const size_t nc = proj_comp_doubles(g);
+        compV = dalloc<double>(nc);
+        compD = dalloc<double>(nc);
+        compT = dalloc<double>(nc);
+        k_proj_comp(g, V, 0, compV, s);
+        k_proj_comp(g, D, 1, compD, s);
+        k_proj_comp(g, T, 0, compT, s);
+    }
 
     // --- FFT twiddles (host long double, rounded once)
     auto lg2 = [](int v) { int l = 0; while ((1 << l) < v) ++l; return l; };
@@ -1116,7 +1141,7 @@ void mlegs_ctx::step_etdab_cn() {
     rel(ROPN);
     rel(OZN);
     Field* W = tmp();
-    project(RURN, RUPN, UZN, psi, W, 2, 0.0);
+    project_fff_ln2(RURN, RUPN, UZN, psi, W);
     idel2ln(W, chi, 0);
     rel(W);
     rel(RURN);
@@ -1553,7 +1578,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 13) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 14) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1604,6 +1629,11 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     k_split_fold(g, ctx->split_S, ctx->fimg[0], ctx->feA[0], d.NRCHOPDIM + 1, a->data, b->data, 0,
                                  0, 0, 0, 1, ctx->split_err, s);
                     break;
+                case 14:  // PROJECT of FFF inputs f9[0..2] -> b, c through the composites
+                    if (!ctx->compV) throw ApiError(MLEGS_ERR_STATE, "needs an FP64 context on the tensor path");
+                    k_project_fff_dmma(g, ctx->compV, ctx->compD, ctx->compT, f9[0]->data, f9[1]->data, f9[2]->data,
+                                       b->data, c->data, c->ln, ctx->explog0, s);
+                    break;
                 case 13: {  // PROJECT's fold products: f9[0..2] (PFF) -> b, c (FFF)
                     const int wr = d.NRCHOPDIM;
                     if (!ctx->split_S && dmma_supported(g)) {
@@ -1629,6 +1659,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 7: bytes = (B16 * 2.0 + 40.0) * (double)d.fff(); break;  // rhs in, solution out, 5 factors
             case 8: bytes = B16 * 14.0 * (double)d.pfp(); break;  // 10 PFP lines read, 4 written
             case 13: bytes = B16 * (3.0 * (double)d.pff() + 2.0 * (double)d.fff()); break;
+            case 14: bytes = B16 * 5.0 * (double)d.fff(); break;
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
         }
         for (int q = 0; q < 3; ++q) launch();  // warm-up

@@ -39,8 +39,6 @@ __device__ __forceinline__ void cp16(void* dst, const void* src, bool ok) {
                  : "memory");
 }
 
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 }  // namespace
 
 // RTRAN(+1).  Per m, the K rows of both parities (t < kp_p, n = 2t + p) go in
@@ -326,6 +324,238 @@ __global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, Fol
     }
 }
 
+// PROJECT of velocity fields given as FFF coefficients, as one FFF -> FFF
+// product per m.  RTRAN(+1) followed by the EO/OE fold is, for output parity
+// pr and fold mode, 2 C_p with p = pr ^ mode (C_p the parity-p half of the
+// RTRAN(+1) product), so each fold product W . F(RTRAN(x)) equals
+//   Comp_W(n, n') x(n'),  Comp_W(n, n') = 2 sum_{i < NRH} W(n, i) PF(n', i),
+// over input rows n' of parity p (n, n' < NRCHOPS(m) at pad 0).  The
+// composite matrices are formed once per context (proj_comp_kernel), stored
+// [m][pr][r][t] for n = 2r + pr, n' = 2t + p; PROJECT then costs a third of
+// the FLOPs of RTRAN(+1) x 3 plus the five fold products and never writes PFF.
+// The complex column factors (-i m, -1, i k, m k, -1) are applied to each B
+// fragment as it is read (a re/im swap and a per-lane real factor).
+__global__ void proj_comp_kernel(DevGrid g, const double* __restrict__ W, int p_flip, double* __restrict__ Cm,
+                                 int RC, int KPC) {
+    const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t total = (size_t)g.NTCHOPDIM * 2 * RC * KPC;
+    if (idx >= total) return;
+    const int t = (int)(idx % KPC);
+    const int r = (int)((idx / KPC) % RC);
+    const int pr = (int)((idx / ((size_t)KPC * RC)) % 2);
+    const int m = (int)(idx / ((size_t)KPC * RC * 2));
+    int nn = g.NRCHOP - m;
+    if (nn < 0) nn = 0;
+    const int n = 2 * r + pr, np = 2 * t + (pr ^ p_flip);
+    double v = 0.0;
+    if (n < nn && n < g.NRCHOPDIM && np < nn) {
+        const double* w = W + ((size_t)m * g.NRCHOPDIM + n) * g.NRH;
+        const double* pf = g.pf + ((size_t)m * (g.NRCHOPDIM + 1) + np) * g.NRH;
+        for (int i = 0; i < g.NRH; ++i) v += w[i] * pf[i];
+        v *= 2.0;
+    }
+    Cm[idx] = v;
+}
+
+struct ProjFffArgs {
+    const double* C[5];  // composite per segment: CV, CD, CD, CV, CT
+    const double* x[5];  // FFF inputs: RUR, RUP, RUR, RUP, UZ
+    double* psi;
+    double* chi;
+};
+
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, ProjFffArgs pa, int RC, int KPC,
+                                                                 int RTmax) {
+    extern __shared__ double smd[];
+    const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;
+    const int ncol = 2 * g.NXCHOPDIM;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
+    int nn = g.NRCHOP - m;
+    if (nn < 0) nn = 0;
+    const int rows = (g.NRCHOPDIM - pr + 1) / 2;
+    const int rv = min(rows, max(0, (nn - pr + 1) / 2));
+    const int RTv = (rv + 7) / 8;
+    // input-row parity of the segments: p = pr for EO (0, 3, 4), pr ^ 1 for OE (1, 2)
+    const int kpS = max(0, (nn - pr + 1) / 2), kpO = max(0, (nn - (pr ^ 1) + 1) / 2);
+    const int nS = (kpS + KC2 - 1) / KC2, nO = (kpO + KC2 - 1) / KC2;
+    const int npsi = nS + nO, total = npsi + nO + 2 * nS;
+    const size_t stA = (size_t)RTmax * 8 * SA2, stB = (size_t)KC2 * SX2;
+    const size_t cofs = (((size_t)m * 2 + pr) * RC) * KPC, xofs = (size_t)m * g.NRCHOPDIM * ncol;
+
+    auto locate = [&](int gc, int& sg, int& ch) {  // chunk -> (segment, chunk in segment)
+        int b = gc;
+        sg = 0;
+        if (b >= nS) {
+            b -= nS;
+            sg = 1;
+            if (b >= nO) {
+                b -= nO;
+                sg = 2;
+                if (b >= nO) {
+                    b -= nO;
+                    sg = 3;
+                    if (b >= nS) {
+                        b -= nS;
+                        sg = 4;
+                    }
+                }
+            }
+        }
+        ch = b;
+    };
+    auto stage = [&](int gc) {
+        int sg, ch;
+        locate(gc, sg, ch);
+        const bool odd = (sg == 1 || sg == 2);
+        const int kp = odd ? kpO : kpS, p = pr ^ (odd ? 1 : 0), t0 = ch * KC2;
+        const double* cm = pick5(pa.C, sg) + cofs;
+        const double* x = pick5(pa.x, sg) + xofs;
+        double* As = smd + (gc & 1) * (stA + stB);
+        double* Bs = As + stA;
+        for (int e = tid; e < RTv * 8 * (KC2 / 2); e += NW * 32) {
+            const int r = e / (KC2 / 2), c2 = e - r * (KC2 / 2);
+            const int t = t0 + 2 * c2;
+            const bool ok = r < rv && t < kp;
+            cp16(As + (size_t)r * SA2 + 2 * c2, ok ? cm + (size_t)r * KPC + t : cm, ok);
+        }
+        for (int e = tid; e < KC2 * (CT / 2); e += NW * 32) {
+            const int tt = e / (CT / 2), c2 = e - tt * (CT / 2);
+            const int t = t0 + tt, c = c0 + 2 * c2;
+            const bool ok = t < kp && c < ncol;
+            cp16(Bs + (size_t)tt * SX2 + 2 * c2, ok ? x + (size_t)(2 * t + p) * ncol + c : x, ok);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    auto epilogue = [&](double (&acc)[MTW][4][2], double* out) {
+        double* o = out + (size_t)m * g.NRCHOPDIM * ncol;
+#pragma unroll
+        for (int t = 0; t < MTW; ++t) {
+            const int r = (warp + NW * t) * 8 + gq;
+            const int n = 2 * r + pr;
+            if (r >= rows || n >= g.NRCHOPDIM) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = c0 + j * 8 + 2 * q;
+                const double2 v = n < nn ? make_double2(acc[t][j][0], acc[t][j][1]) : make_double2(0.0, 0.0);
+                acc[t][j][0] = acc[t][j][1] = 0.0;
+                if (c < ncol) *(double2*)(o + (size_t)n * ncol + c) = v;
+            }
+        }
+    };
+
+    // per-lane B-fragment factors: lane column c = c0 + 8 jj + gq (gq even: real part)
+    double akv[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const int c = c0 + jj * 8 + gq;
+        akv[jj] = (c < ncol) ? g.ak[c >> 1] : 0.0;
+    }
+    const double md = (double)m, ev = (gq & 1) ? -1.0 : 1.0;  // ev: +1 on the real lanes
+
+    double acc[MTW][4][2];
+#pragma unroll
+    for (int t = 0; t < MTW; ++t)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
+    if (npsi == 0) epilogue(acc, pa.psi);
+    if (total == npsi) epilogue(acc, pa.chi);
+    if (total > 0) stage(0);
+    for (int gc = 0; gc < total; ++gc) {
+        if (gc + 1 < total) {
+            stage(gc + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        int sg, ch;
+        locate(gc, sg, ch);
+        const bool odd = (sg == 1 || sg == 2);
+        const int kp = odd ? kpO : kpS;
+        const int ksteps = (min(KC2, kp - ch * KC2) + 3) / 4;
+        // B factor: -i m (swap, +m on real lanes), -1, i k (swap, -k on real lanes), m k, -1
+        const bool swap = (sg == 0 || sg == 2);
+        double f[4];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            switch (sg) {
+                case 0: f[jj] = ev * md; break;
+                case 2: f[jj] = -ev * akv[jj]; break;
+                case 3: f[jj] = md * akv[jj]; break;
+                default: f[jj] = -1.0; break;
+            }
+        }
+        const int bcol = swap ? (gq ^ 1) : gq;
+        const double* As = smd + (gc & 1) * (stA + stB);
+        const double* Bs = As + stA;
+#pragma unroll
+        for (int s4 = 0; s4 < KC2 / 4; ++s4) {
+            if (s4 < ksteps) {
+                const int j = 4 * s4 + q;
+                double bf[4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SX2 + jj * 8 + bcol] * f[jj];
+#pragma unroll
+                for (int t = 0; t < MTW; ++t) {
+                    const int mt = warp + NW * t;
+                    if (mt < RTv) {
+                        const double af = As[(size_t)(mt * 8 + gq) * SA2 + j];
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af, bf[jj]);
+                    }
+                }
+            }
+        }
+        if (gc == npsi - 1) epilogue(acc, pa.psi);
+        if (gc == total - 1) epilogue(acc, pa.chi);
+        __syncthreads();  // the stage is refilled by the next iteration's prefetch
+    }
+}
+
+// The PFF line of RUP at (m, k) = (0, 0), formed from its FFF column as
+// RTRAN(+1) does (real parts), feeds VEL2PLN's far-field extraction
+// (mod_legops.f90:2277-2339); VEL2PLN's subtraction of PLN times the n = 0, 1
+// functions from that line is applied to the FFF column instead (rows 0 and 1
+// += PLN / NORM), which is the same change of the RTRAN(+1) image.
+__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* explog0) {
+    extern __shared__ double sh[];
+    double* be = sh;            // [NRH]
+    double* bo = sh + g.NRH;    // [NRH]
+    double* part = bo + g.NRH;  // [blockDim]
+    const size_t st = g.NXCHOPDIM;  // FFF row stride of the (0, 0) column
+    const int nn = g.NRCHOP;
+    const double* pf = g.pf;  // m = 0: [n][i]
+    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
+        double c0 = 0.0, c1 = 0.0;
+        for (int n = 0; n < nn; n += 2) c0 += pf[(size_t)n * g.NRH + i] * rup[(size_t)n * st].x;
+        for (int n = 1; n < nn; n += 2) c1 += pf[(size_t)n * g.NRH + i] * rup[(size_t)n * st].x;
+        const double lo = c0 + c1, hi = c0 - c1;
+        be[i] = (lo + hi) * g.w[i];
+        bo[i] = (lo - hi) * g.w[i];
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
+        const double* src = (n % 2 == 0) ? be : bo;
+        double s = 0.0;
+        for (int i = 0; i < g.NRH; ++i) s += src[i] * pf[(size_t)n * g.NRH + i];
+        acc += s * explog0[n];
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double pln = -part[0] / 2.0;
+        rup[0].x += pln / g.norm0[0];
+        rup[st].x += pln / g.norm0[1];
+        *psi_ln = pln;
+    }
+}
+
 // ---------------------------------------------------------------------------
 
 static int pad16_8(int v) { return v + ((8 - v % 16) + 16) % 16; }  // smallest >= v that is 8 mod 16
@@ -420,6 +650,58 @@ void k_project_dmma(const DevGrid& g, const double* V, const double* D, const do
     fa.use_w = 0;
     fa.accumulate = 0;
     legfold(g, fa, s);
+}
+
+size_t proj_comp_doubles(const DevGrid& g) {
+    const int RC = (g.NRCHOPDIM + 1) / 2, KPC = (((g.NRCHOP + 1) / 2) + KC2 - 1) / KC2 * KC2;
+    return (size_t)g.NTCHOPDIM * 2 * RC * KPC;
+}
+
+void k_proj_comp(const DevGrid& g, const double* W, int p_flip, double* Cm, cudaStream_t s) {
+    const int RC = (g.NRCHOPDIM + 1) / 2, KPC = (((g.NRCHOP + 1) / 2) + KC2 - 1) / KC2 * KC2;
+    const size_t n = (size_t)g.NTCHOPDIM * 2 * RC * KPC;
+    proj_comp_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, W, p_flip, Cm, RC, KPC);
+    count_launch();
+}
+
+template <int NW, int MTW>
+static void projfff_launch(const DevGrid& g, const ProjFffArgs& pa, cudaStream_t s) {
+    const int RC = (g.NRCHOPDIM + 1) / 2, KPC = (((g.NRCHOP + 1) / 2) + KC2 - 1) / KC2 * KC2;
+    const int RT = (RC + 7) / 8;
+    const size_t smem = 2 * ((size_t)RT * 8 * SA2 + (size_t)KC2 * SX2) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(projfff_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    dim3 grid((2 * g.NXCHOPDIM + CT - 1) / CT, 2, g.NTCHOPDIM);
+    projfff_dmma_kernel<NW, MTW><<<grid, NW * 32, smem, s>>>(g, pa, RC, KPC, RT);
+    count_launch();
+}
+
+void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, const double* CT_, double2* rur,
+                        double2* rup, double2* uz, double2* psi, double2* chi, double* psi_ln, const double* explog0,
+                        cudaStream_t s) {
+    // VEL2PLN on RUP's (0, 0) column first: it changes RUP's input to the products
+    const size_t sm = (2 * (size_t)g.NRH + 128) * sizeof(double);
+    vel2pln_fff_kernel<<<1, 128, sm, s>>>(g, rup, psi_ln, explog0);
+    count_launch();
+    ProjFffArgs pa;
+    const double* C[5] = {CV, CD, CD, CV, CT_};
+    const double2* x[5] = {rur, rup, rur, rup, uz};
+    for (int q = 0; q < 5; ++q) {
+        pa.C[q] = C[q];
+        pa.x[q] = (const double*)x[q];
+    }
+    pa.psi = (double*)psi;
+    pa.chi = (double*)chi;
+    const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
+    switch ((RT + 3) / 4) {
+        case 1: projfff_launch<4, 1>(g, pa, s); break;
+        case 2: projfff_launch<4, 2>(g, pa, s); break;
+        case 3: projfff_launch<4, 3>(g, pa, s); break;
+        default: projfff_launch<4, 4>(g, pa, s); break;
+    }
 }
 
 }  // namespace mlegs

@@ -107,6 +107,17 @@ void k_fold_gemm_dmma(const DevGrid& g, const double* Wt, int wt_rows, const dou
 // RUR, RUP, UZ in PFF with the weights V, D, T ([m][n][i], NRCHOPDIM x NRH).
 void k_project_dmma(const DevGrid& g, const double* V, const double* D, const double* T, const double2* rur,
                     const double2* rup, const double2* uz, double2* psi, double2* chi, cudaStream_t s);
+// PROJECT of FFF velocity fields through per-m composite matrices
+// Comp_W = 2 W . PF^T restricted to one input-row parity (gemm_dmma.cu):
+// k_proj_comp forms one ([m][pr][r][t], proj_comp_doubles entries; p_flip 0
+// for the EO weights V, T, 1 for the OE weight D); k_project_fff_dmma runs
+// VEL2PLN on RUP's (0, 0) column (in place, PSI%LN <- PLN) and then the
+// products.  Input LN terms must be zero.
+size_t proj_comp_doubles(const DevGrid& g);
+void k_proj_comp(const DevGrid& g, const double* W, int p_flip, double* Cm, cudaStream_t s);
+void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, const double* CT, double2* rur,
+                        double2* rup, double2* uz, double2* psi, double2* chi, double* psi_ln, const double* explog0,
+                        cudaStream_t s);
 // out[m][n][k] (+)= scale(m,k) * sum_i Wt[m][n][i] * fold(in)(i,k); fold parity per row given by mode
 //   mode 0 (EO): row n even -> even fold, odd -> odd fold;  mode 1 (OE): swapped
 //   scale: 0 -> 1, 1 -> -1, 2 -> -i m, 3 -> i k, 4 -> m k

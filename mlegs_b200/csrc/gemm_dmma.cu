@@ -513,49 +513,6 @@ __global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, Pro
     }
 }
 
-// The PFF line of RUP at (m, k) = (0, 0), formed from its FFF column as
-// RTRAN(+1) does (real parts), feeds VEL2PLN's far-field extraction
-// (mod_legops.f90:2277-2339); VEL2PLN's subtraction of PLN times the n = 0, 1
-// functions from that line is applied to the FFF column instead (rows 0 and 1
-// += PLN / NORM), which is the same change of the RTRAN(+1) image.
-__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* explog0) {
-    extern __shared__ double sh[];
-    double* be = sh;            // [NRH]
-    double* bo = sh + g.NRH;    // [NRH]
-    double* part = bo + g.NRH;  // [blockDim]
-    const size_t st = g.NXCHOPDIM;  // FFF row stride of the (0, 0) column
-    const int nn = g.NRCHOP;
-    const double* pf = g.pf;  // m = 0: [n][i]
-    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
-        double c0 = 0.0, c1 = 0.0;
-        for (int n = 0; n < nn; n += 2) c0 += pf[(size_t)n * g.NRH + i] * rup[(size_t)n * st].x;
-        for (int n = 1; n < nn; n += 2) c1 += pf[(size_t)n * g.NRH + i] * rup[(size_t)n * st].x;
-        const double lo = c0 + c1, hi = c0 - c1;
-        be[i] = (lo + hi) * g.w[i];
-        bo[i] = (lo - hi) * g.w[i];
-    }
-    __syncthreads();
-    double acc = 0.0;
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
-        const double* src = (n % 2 == 0) ? be : bo;
-        double s = 0.0;
-        for (int i = 0; i < g.NRH; ++i) s += src[i] * pf[(size_t)n * g.NRH + i];
-        acc += s * explog0[n];
-    }
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const double pln = -part[0] / 2.0;
-        rup[0].x += pln / g.norm0[0];
-        rup[st].x += pln / g.norm0[1];
-        *psi_ln = pln;
-    }
-}
-
 // ---------------------------------------------------------------------------
 
 static int pad16_8(int v) { return v + ((8 - v % 16) + 16) % 16; }  // smallest >= v that is 8 mod 16
@@ -683,9 +640,7 @@ void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, co
                         double2* rup, double2* uz, double2* psi, double2* chi, double* psi_ln, const double* explog0,
                         cudaStream_t s) {
     // VEL2PLN on RUP's (0, 0) column first: it changes RUP's input to the products
-    const size_t sm = (2 * (size_t)g.NRH + 128) * sizeof(double);
-    vel2pln_fff_kernel<<<1, 128, sm, s>>>(g, rup, psi_ln, explog0);
-    count_launch();
+    launch_vel2pln_fff(g, rup, psi_ln, explog0, s);
     ProjFffArgs pa;
     const double* C[5] = {CV, CD, CD, CV, CT_};
     const double2* x[5] = {rur, rup, rur, rup, uz};

@@ -258,12 +258,34 @@ void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s) {
 // VEL2PLN (mod_legops.f90:2277-2339) on the (m,k) = (0,0) radial line of a PFF
 // field.  mode 0: PSI%LN <- extracted value; mode 1: PSI%LN <- ln.
 // explog0 (= exp(LOGNORM(:,1))) is passed as g.norm0's sibling table.
+// PLN = -(1/2) sum_{n < nn} EXPLOG0(n) sum_i F(i) PF_0(n, i), F the even (n
+// even) or odd fold of the radial line times the Gauss weights; one warp per
+// n (lanes stride over i), so the block's eight warps share the n range.
+__device__ double vel2pln_sum(const DevGrid& g, const double* be, const double* bo, const double* explog0, int nn,
+                              double* part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double* pf = g.pf;  // m = 0 slice: [n][i]
+    double acc = 0.0;
+    for (int n = warp; n < nn; n += nw) {
+        const double* src = (n % 2 == 0) ? be : bo;
+        double sv = 0.0;
+        for (int i = lane; i < g.NRH; i += 32) sv += src[i] * pf[(size_t)n * g.NRH + i];
+        for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
+        acc += sv * explog0[n];
+    }
+    if (lane == 0) part[warp] = acc;
+    __syncthreads();
+    double tot = 0.0;
+    for (int w = 0; w < nw; ++w) tot += part[w];
+    return -tot / 2.0;
+}
+
 __global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in,
                                const double* explog0, int nn) {
     extern __shared__ double sh[];
     double* be = sh;             // [NRH]
     double* bo = sh + g.NRH;     // [NRH]
-    double* part = bo + g.NRH;   // [blockDim]
+    double* part = bo + g.NRH;   // [warps]
     const size_t st = g.NXCHOPDIM;  // PFF row stride for m = 0 ([0][r][k])
     for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
         double lo = rup[(size_t)i * st].x, hi = rup[(size_t)(g.NR - 1 - i) * st].x;
@@ -271,21 +293,8 @@ __global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode
         bo[i] = (lo - hi) * g.w[i];
     }
     __syncthreads();
-    const double* pf = g.pf;  // m = 0 slice: [n][i]
-    double acc = 0.0;
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
-        const double* src = (n % 2 == 0) ? be : bo;
-        double s = 0.0;
-        for (int i = 0; i < g.NRH; ++i) s += src[i] * pf[(size_t)n * g.NRH + i];
-        acc += s * explog0[n];
-    }
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
-        __syncthreads();
-    }
-    double pln = -part[0] / 2.0;
+    const double pln = vel2pln_sum(g, be, bo, explog0, nn, part);
+    const double* pf = g.pf;
     for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
         double e2 = -pf[i] * pln / g.norm0[0];
         double o2 = -pf[(size_t)g.NRH + i] * pln / g.norm0[1];
@@ -296,8 +305,53 @@ __global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode
 }
 void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
                     const double* explog0, int nn, cudaStream_t s) {
-    size_t sm = (2 * g.NRH + 128) * sizeof(double);
-    vel2pln_kernel<<<1, 128, sm, s>>>(g, rup_pff, psi_ln, mode, ln, explog0, nn);
+    size_t sm = (2 * g.NRH + 8) * sizeof(double);
+    vel2pln_kernel<<<1, 256, sm, s>>>(g, rup_pff, psi_ln, mode, ln, explog0, nn);
+    count_launch();
+}
+
+// The PFF line of RUP at (m, k) = (0, 0), formed from its FFF column as
+// RTRAN(+1) does (real parts), feeds the same far-field extraction; VEL2PLN's
+// subtraction of PLN times the n = 0, 1 functions from that line is applied to
+// the FFF column instead (rows 0 and 1 += PLN / NORM), which is the same change
+// of the RTRAN(+1) image.
+__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* explog0) {
+    extern __shared__ double sh[];
+    const int nn = g.NRCHOP;
+    double* a = sh;             // [nn] real parts of the (0, 0) column
+    double* be = a + nn;        // [NRH]
+    double* bo = be + g.NRH;    // [NRH]
+    double* part = bo + g.NRH;  // [warps]
+    const size_t st = g.NXCHOPDIM;  // FFF row stride of the (0, 0) column
+    const double* pf = g.pf;        // m = 0: [n][i]
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) a[n] = rup[(size_t)n * st].x;
+    __syncthreads();
+    // C_p(i) = sum_{n = p mod 2} PF_0(n, i) a(n): thread (p, i), 8 rows in flight
+    for (int e = threadIdx.x; e < 2 * g.NRH; e += blockDim.x) {
+        const int p = e / g.NRH, i = e - p * g.NRH;
+        double c = 0.0;
+#pragma unroll 8
+        for (int n = p; n < nn; n += 2) c += pf[(size_t)n * g.NRH + i] * a[n];
+        (p ? bo : be)[i] = c;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
+        const double c0 = be[i], c1 = bo[i];
+        const double lo = c0 + c1, hi = c0 - c1;
+        be[i] = (lo + hi) * g.w[i];
+        bo[i] = (lo - hi) * g.w[i];
+    }
+    __syncthreads();
+    const double pln = vel2pln_sum(g, be, bo, explog0, nn, part);
+    if (threadIdx.x == 0) {
+        rup[0].x += pln / g.norm0[0];
+        rup[st].x += pln / g.norm0[1];
+        *psi_ln = pln;
+    }
+}
+void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* explog0, cudaStream_t s) {
+    size_t sm = ((size_t)g.NRCHOP + 2 * g.NRH + 8) * sizeof(double);
+    vel2pln_fff_kernel<<<1, 256, sm, s>>>(g, rup_fff, psi_ln, explog0);
     count_launch();
 }
 

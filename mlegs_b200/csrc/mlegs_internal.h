@@ -161,6 +161,8 @@ void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, 
 void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
 void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
                     const double* explog0, int nn, cudaStream_t s);
+// VEL2PLN (mode 0, nn = NRCHOP) from RUP's FFF (0, 0) column, applied to that column.
+void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* explog0, cudaStream_t s);
 
 // Banded solves (IDEL2LN, IDEL2, IHELM) with per-system elimination scratch.
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln,

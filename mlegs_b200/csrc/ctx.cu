@@ -1583,9 +1583,25 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
         cudaStream_t s = ctx->s;
-        Field *a = ctx->tmp(), *b = ctx->tmp(), *c = ctx->tmp();
+        if ((kernel == 11 || kernel == 12) && !ctx->split_S)
+            throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
+        if (kernel == 14 && !ctx->compV) throw ApiError(MLEGS_ERR_STATE, "needs an FP64 context on the tensor path");
+        // the temporaries go back to the pool however the timing ends
+        struct PoolReturn {
+            mlegs_ctx* c;
+            std::vector<Field*> taken;
+            ~PoolReturn() {
+                for (auto it = taken.rbegin(); it != taken.rend(); ++it) c->rel(*it);
+            }
+        } ret{ctx, {}};
+        auto take = [&]() {
+            Field* f = ctx->tmp();
+            ret.taken.push_back(f);
+            return f;
+        };
+        Field *a = take(), *b = take(), *c = take();
         Field* f9[9];
-        for (auto& q : f9) q = ctx->tmp();
+        for (auto& q : f9) q = take();
         // deterministic non-trivial contents: fill FFF/PPP-sized buffers via axpby of zeros
         // is pointless for timing, so keep whatever the scratch buffers hold (finite zeros
         // after allocation) -- arithmetic cost does not depend on the values.
@@ -1674,10 +1690,6 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
         CK(cudaEventElapsedTime(&ms, e0, e1));
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        for (auto& q : f9) ctx->rel(q);
-        ctx->rel(c);
-        ctx->rel(b);
-        ctx->rel(a);
         if (ms_per_launch) *ms_per_launch = ms / reps;
         if (bytes_per_launch) *bytes_per_launch = bytes;
     });

@@ -77,6 +77,7 @@ struct mlegs_ctx {
     double *V = nullptr, *D = nullptr, *T = nullptr;
     double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
     double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
+    double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
     double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
     FFTPlan fft;
     std::vector<double> h_x, h_w, h_lognorm;
@@ -399,8 +400,8 @@ struct mlegs_ctx {
         psi_->space = chi_->space = MLEGS_FFF;
         ln_zero(psi_);
         ln_zero(chi_);
-        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, explog0, d.NRCHOP, s);
-        if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, explog0, d.NRCHOP, s);
+        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, v2p_pff, s);
+        if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, v2p_pff, s);
         if (!split_S && dmma_supported(g)) {
             k_project_dmma(g, V, D, T, rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
             k_farfield_fix(g, psi_->data, d.NRCHOP, s);
@@ -427,7 +428,7 @@ struct mlegs_ctx {
         }
         psi_->space = chi_->space = MLEGS_FFF;
         k_project_fff_dmma(g, compV, compD, compT, rur->data, rup->data, uz->data, psi_->data, chi_->data, psi_->ln,
-                           explog0, s);
+                           v2p_fff, s);
         ln_zero(chi_);
         k_farfield_fix(g, psi_->data, d.NRCHOP, s);
     }
@@ -640,6 +641,9 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     D = dalloc<double>(vsz);
     T = dalloc<double>(vsz);
     k_tables_project(g, V, D, T, 0, s);
+    v2p_pff = dalloc<double>(d.NR);
+    v2p_fff = dalloc<double>(std::max(d.NRCHOP, 1));
+    k_vel2pln_coef(g, explog0, d.NRCHOP, v2p_pff, v2p_fff, s);
     if (p.precision == MLEGS_PREC_FP64 && dmma_supported(g)) {
         const size_t nc = proj_comp_doubles(g);
         compV = dalloc<double>(nc);
@@ -1648,7 +1652,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                 case 14:  // PROJECT of FFF inputs f9[0..2] -> b, c through the composites
                     if (!ctx->compV) throw ApiError(MLEGS_ERR_STATE, "needs an FP64 context on the tensor path");
                     k_project_fff_dmma(g, ctx->compV, ctx->compD, ctx->compT, f9[0]->data, f9[1]->data, f9[2]->data,
-                                       b->data, c->data, c->ln, ctx->explog0, s);
+                                       b->data, c->data, c->ln, ctx->v2p_fff, s);
                     break;
                 case 13: {  // PROJECT's fold products: f9[0..2] (PFF) -> b, c (FFF)
                     const int wr = d.NRCHOPDIM;

@@ -257,43 +257,59 @@ void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s) {
 
 // VEL2PLN (mod_legops.f90:2277-2339) on the (m,k) = (0,0) radial line of a PFF
 // field.  mode 0: PSI%LN <- extracted value; mode 1: PSI%LN <- ln.
-// explog0 (= exp(LOGNORM(:,1))) is passed as g.norm0's sibling table.
-// PLN = -(1/2) sum_{n < nn} EXPLOG0(n) sum_i F(i) PF_0(n, i), F the even (n
-// even) or odd fold of the radial line times the Gauss weights; one warp per
-// n (lanes stride over i), so the block's eight warps share the n range.
-__device__ double vel2pln_sum(const DevGrid& g, const double* be, const double* bo, const double* explog0, int nn,
-                              double* part) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// VEL2PLN's far-field value (mod_legops.f90:2277-2339) is a fixed linear
+// functional of RUP's (m, k) = (0, 0) line:
+//   PLN = -(1/2) sum_{n < NRCHOP} EXPLOG0(n) sum_i F_n(i) PF_0(n, i),
+// F_n the even (n even) or odd fold of the PFF line times the Gauss weights.
+// Its coefficients are formed once per context, for the PFF line (Lpff, NR
+// entries) and for the FFF column whose RTRAN(+1) image that line is (Lfff,
+// NRCHOP entries; the fold of the image is twice its parity half, so
+// Lfff(n') = -sum_{n = n' mod 2} EXPLOG0(n) sum_i w_i PF_0(n, i) PF_0(n', i)).
+// Each call is then one dot product.
+__global__ void vel2pln_coef_kernel(DevGrid g, const double* explog0, int nn, double* Lpff, double* Lfff) {
     const double* pf = g.pf;  // m = 0 slice: [n][i]
-    double acc = 0.0;
-    for (int n = warp; n < nn; n += nw) {
-        const double* src = (n % 2 == 0) ? be : bo;
-        double sv = 0.0;
-        for (int i = lane; i < g.NRH; i += 32) sv += src[i] * pf[(size_t)n * g.NRH + i];
-        for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
-        acc += sv * explog0[n];
+    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
+        double se = 0.0, so = 0.0;
+        for (int n = 0; n < nn; ++n) {
+            const double v = explog0[n] * pf[(size_t)n * g.NRH + i];
+            if (n % 2 == 0) se += v;
+            else so += v;
+        }
+        Lpff[i] = -0.5 * g.w[i] * (se + so);
+        Lpff[g.NR - 1 - i] = -0.5 * g.w[i] * (se - so);
     }
+    for (int np = threadIdx.x; np < nn; np += blockDim.x) {
+        double acc = 0.0;
+        for (int n = np % 2; n < nn; n += 2) {
+            double gram = 0.0;
+            for (int i = 0; i < g.NRH; ++i) gram += g.w[i] * pf[(size_t)n * g.NRH + i] * pf[(size_t)np * g.NRH + i];
+            acc += explog0[n] * gram;
+        }
+        Lfff[np] = -acc;
+    }
+}
+void k_vel2pln_coef(const DevGrid& g, const double* explog0, int nn, double* Lpff, double* Lfff, cudaStream_t s) {
+    vel2pln_coef_kernel<<<1, 256, 0, s>>>(g, explog0, nn, Lpff, Lfff);
+    count_launch();
+}
+
+// Block-wide sum of sum_j L[j] line[j * st].x over j < n (one block of 256).
+__device__ double vel2pln_dot(const double* L, const double2* line, size_t st, int n, double* part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) acc += L[j] * line[(size_t)j * st].x;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) part[warp] = acc;
     __syncthreads();
     double tot = 0.0;
     for (int w = 0; w < nw; ++w) tot += part[w];
-    return -tot / 2.0;
+    return tot;
 }
 
-__global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in,
-                               const double* explog0, int nn) {
-    extern __shared__ double sh[];
-    double* be = sh;             // [NRH]
-    double* bo = sh + g.NRH;     // [NRH]
-    double* part = bo + g.NRH;   // [warps]
+__global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in, const double* Lpff) {
+    __shared__ double part[8];
     const size_t st = g.NXCHOPDIM;  // PFF row stride for m = 0 ([0][r][k])
-    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
-        double lo = rup[(size_t)i * st].x, hi = rup[(size_t)(g.NR - 1 - i) * st].x;
-        be[i] = (lo + hi) * g.w[i];
-        bo[i] = (lo - hi) * g.w[i];
-    }
-    __syncthreads();
-    const double pln = vel2pln_sum(g, be, bo, explog0, nn, part);
+    const double pln = vel2pln_dot(Lpff, rup, st, g.NR, part);
     const double* pf = g.pf;
     for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
         double e2 = -pf[i] * pln / g.norm0[0];
@@ -303,55 +319,27 @@ __global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode
     }
     if (threadIdx.x == 0) *psi_ln = (mode == 1) ? ln_in : pln;
 }
-void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln,
-                    const double* explog0, int nn, cudaStream_t s) {
-    size_t sm = (2 * g.NRH + 8) * sizeof(double);
-    vel2pln_kernel<<<1, 256, sm, s>>>(g, rup_pff, psi_ln, mode, ln, explog0, nn);
+void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln, const double* Lpff,
+                    cudaStream_t s) {
+    vel2pln_kernel<<<1, 256, 0, s>>>(g, rup_pff, psi_ln, mode, ln, Lpff);
     count_launch();
 }
 
-// The PFF line of RUP at (m, k) = (0, 0), formed from its FFF column as
-// RTRAN(+1) does (real parts), feeds the same far-field extraction; VEL2PLN's
-// subtraction of PLN times the n = 0, 1 functions from that line is applied to
-// the FFF column instead (rows 0 and 1 += PLN / NORM), which is the same change
-// of the RTRAN(+1) image.
-__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* explog0) {
-    extern __shared__ double sh[];
-    const int nn = g.NRCHOP;
-    double* a = sh;             // [nn] real parts of the (0, 0) column
-    double* be = a + nn;        // [NRH]
-    double* bo = be + g.NRH;    // [NRH]
-    double* part = bo + g.NRH;  // [warps]
+// VEL2PLN from RUP's FFF (0, 0) column; the subtraction of PLN times the
+// n = 0, 1 functions from the PFF line is applied to the FFF column instead
+// (rows 0 and 1 += PLN / NORM), the same change of the RTRAN(+1) image.
+__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* Lfff) {
+    __shared__ double part[8];
     const size_t st = g.NXCHOPDIM;  // FFF row stride of the (0, 0) column
-    const double* pf = g.pf;        // m = 0: [n][i]
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) a[n] = rup[(size_t)n * st].x;
-    __syncthreads();
-    // C_p(i) = sum_{n = p mod 2} PF_0(n, i) a(n): thread (p, i), 8 rows in flight
-    for (int e = threadIdx.x; e < 2 * g.NRH; e += blockDim.x) {
-        const int p = e / g.NRH, i = e - p * g.NRH;
-        double c = 0.0;
-#pragma unroll 8
-        for (int n = p; n < nn; n += 2) c += pf[(size_t)n * g.NRH + i] * a[n];
-        (p ? bo : be)[i] = c;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < g.NRH; i += blockDim.x) {
-        const double c0 = be[i], c1 = bo[i];
-        const double lo = c0 + c1, hi = c0 - c1;
-        be[i] = (lo + hi) * g.w[i];
-        bo[i] = (lo - hi) * g.w[i];
-    }
-    __syncthreads();
-    const double pln = vel2pln_sum(g, be, bo, explog0, nn, part);
+    const double pln = vel2pln_dot(Lfff, rup, st, g.NRCHOP, part);
     if (threadIdx.x == 0) {
         rup[0].x += pln / g.norm0[0];
         rup[st].x += pln / g.norm0[1];
         *psi_ln = pln;
     }
 }
-void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* explog0, cudaStream_t s) {
-    size_t sm = ((size_t)g.NRCHOP + 2 * g.NRH + 8) * sizeof(double);
-    vel2pln_fff_kernel<<<1, 256, sm, s>>>(g, rup_fff, psi_ln, explog0);
+void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* Lfff, cudaStream_t s) {
+    vel2pln_fff_kernel<<<1, 256, 0, s>>>(g, rup_fff, psi_ln, Lfff);
     count_launch();
 }
 

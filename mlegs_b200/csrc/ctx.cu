@@ -64,6 +64,10 @@ struct mlegs_ctx {
     Dims d{};
     DevGrid g{};
     cudaStream_t s = nullptr;
+    cudaStream_t s2 = nullptr;         // second stream of the RTRAN(+1) -> VERFFT(+1) pipeline
+    cudaEvent_t evs[64] = {};          // fork/join events, used in rotation
+    int ev_next = 0;
+    double2* pbuf[3] = {};             // PFF images in flight between the two stages
     int dev = 0;
     std::string err;
     int64_t launches = 0;
@@ -242,6 +246,44 @@ struct mlegs_ctx {
         if (f->space == MLEGS_FFF) rtran(f, 1, pad);
         if (f->space == MLEGS_PFF) verfft(f, 1);
         if (f->space == MLEGS_PFP) horfft(f, 1);
+    }
+
+    // TOFP of FFF fields up to PFP (RTRAN(+1) then VERFFT(+1), the reference's
+    // order per field) as a two-stream pipeline: the RTRAN(+1) GEMM of field
+    // i + 1 on s runs beside the VERFFT(+1) of field i on s2, through three
+    // rotating PFF buffers.  Each field ends in its own buffer, in PFP, LN 0.
+    cudaEvent_t next_event() {
+        cudaEvent_t e = evs[ev_next];
+        ev_next = (ev_next + 1) % 64;
+        return e;
+    }
+    void tofp_pipe(Field* const* fs, const int* pads, int n) {
+        for (int i = 0; i < n; ++i) require(fs[i], MLEGS_FFF, "RTRAN");
+        cudaEvent_t e0 = next_event();
+        CK(cudaEventRecord(e0, s));
+        CK(cudaStreamWaitEvent(s2, e0, 0));
+        cudaEvent_t done[3] = {nullptr, nullptr, nullptr};  // last VERFFT reading pbuf[j]
+        for (int i = 0; i < n; ++i) {
+            Field* f = fs[i];
+            double2* buf = pbuf[i % 3];
+            if (done[i % 3]) CK(cudaStreamWaitEvent(s, done[i % 3], 0));
+            if (split_S)
+                k_split_b2p(g, split_S, split_img, split_eA, f->data, buf, f->ln, pads[i], split_err, s);
+            else
+                k_rtran_b2p(g, f->data, buf, f->ln, pads[i], s);
+            ln_zero(f);
+            cudaEvent_t eb = next_event();
+            CK(cudaEventRecord(eb, s));
+            CK(cudaStreamWaitEvent(s2, eb, 0));
+            if (!k_verfft4(g, fft, buf, f->data, +1, s2)) k_verfft_b(g, fft, buf, f->data, s2);
+            cudaEvent_t ev = next_event();
+            CK(cudaEventRecord(ev, s2));
+            done[i % 3] = ev;
+            f->space = MLEGS_PFP;
+        }
+        cudaEvent_t ej = next_event();
+        CK(cudaEventRecord(ej, s2));
+        CK(cudaStreamWaitEvent(s, ej, 0));
     }
 
     // ------------------------------------------------------------------ operators
@@ -500,6 +542,8 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     dev = p.device;
     CK(cudaSetDevice(dev));
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : evs) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     g_launch_counter = &launches;
     fft_set_attributes();
     phys_set_attributes();
@@ -771,6 +815,7 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     lnslots = dalloc<double>(nslots);
     CK(cudaMemsetAsync(lnslots, 0, nslots * sizeof(double), s));
     scratch = dalloc<double2>(d.cap());
+    for (double2*& q : pbuf) q = dalloc<double2>(d.cap());
     size_t nsys = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
     solve_scr = dalloc<double>((size_t)d.NRCHOPDIM * 4 * nsys);
     size_t ref_max = (size_t)d.NDIMR * d.NDIMTH * d.NX;
@@ -813,6 +858,10 @@ void mlegs_ctx::destroy() {
     if (graph) cudaGraphDestroy(graph);
     for (void* q : allocs) cudaFree(q);
     allocs.clear();
+    for (cudaEvent_t& e : evs)
+        if (e) cudaEventDestroy(e);
+    if (s2) cudaStreamDestroy(s2);
+    s2 = nullptr;
     if (s) cudaStreamDestroy(s);
     s = nullptr;
 }
@@ -836,14 +885,13 @@ void mlegs_ctx::force(const Field* PSI, const Field* CHI, const Field* B, Field*
     grad(B, RBR, RBP, BZ, P3);
     pc2vel(PSI, CHI, RUR, RUP, UZ, P3);
     pc2vor(PSI, CHI, ROR, ROP, OZ, P3);
-    // TOFP up to PFP; the HORFFT(+1) of each field happens inside the fused kernel
-    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) {
-        rtran(f, 1, P3);
-        verfft(f, 1);
-    }
     copy0(W, B, 0);  // W = B; TOFP(W) after CHOPSET(-3)
-    rtran(W, 1, 0);
-    verfft(W, 1);
+    // TOFP up to PFP; the HORFFT(+1) of each field happens inside the fused kernel
+    {
+        Field* const fs[10] = {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ, W};
+        const int pads[10] = {P3, P3, P3, P3, P3, P3, P3, P3, P3, 0};
+        tofp_pipe(fs, pads, 10);
+    }
     // VPRODSUB + VDOTPSUB + the linear terms (385-391), then HORFFT(-1) of the results
     Field *NR = tmp(), *NP = tmp(), *NZ = tmp(), *BN = tmp();
     const double2* in[10] = {RUR->data, RUP->data, UZ->data, ROR->data, ROP->data,
@@ -869,9 +917,10 @@ void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field*
                        Field* BN) {
     Field *RBR = tmp(), *RBP = tmp(), *BZ = tmp();
     grad(B, RBR, RBP, BZ, 1);
-    for (Field* f : {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ}) {
-        rtran(f, 1, 0);
-        verfft(f, 1);
+    {
+        Field* const fs[9] = {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ};
+        const int pads[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        tofp_pipe(fs, pads, 9);
     }
     Field *NR = tmp(), *NP = tmp(), *NZ = tmp();
     const double2* in[10] = {RUR->data, RUP->data, UZ->data, ROR->data, ROP->data,

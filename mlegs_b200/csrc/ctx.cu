@@ -100,12 +100,13 @@ struct mlegs_ctx {
     int* feA[4] = {};
     // out (+)= s Wt . fold(in): FP64 kernel, or the split tensor-core kernel when enabled
     void fold(int w, const double* Wt, int wt_rows, const double2* in, double2* out, int mode, int scale,
-              int accumulate, int pad) {
+              int accumulate, int pad, cudaStream_t st = nullptr) {
+        if (!st) st = s;
         if (split_S)
             k_split_fold(g, split_S, fimg[w], feA[w], wt_rows, in, out, mode & 1, scale, accumulate, pad,
-                         (mode & 2) ? 1 : 0, split_err, s);
+                         (mode & 2) ? 1 : 0, split_err, st);
         else
-            k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, s);
+            k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, st);
     }
     double2* staging = nullptr;
     int* dflag = nullptr;
@@ -257,7 +258,7 @@ struct mlegs_ctx {
         ev_next = (ev_next + 1) % 64;
         return e;
     }
-    void tofp_pipe(Field* const* fs, const int* pads, int n) {
+    void tofp_pipe(Field* const* fs, const int* pads, int n, const cudaEvent_t* ready = nullptr) {
         for (int i = 0; i < n; ++i) require(fs[i], MLEGS_FFF, "RTRAN");
         cudaEvent_t e0 = next_event();
         CK(cudaEventRecord(e0, s));
@@ -267,6 +268,7 @@ struct mlegs_ctx {
             Field* f = fs[i];
             double2* buf = pbuf[i % 3];
             if (done[i % 3]) CK(cudaStreamWaitEvent(s, done[i % 3], 0));
+            if (ready && ready[i]) CK(cudaStreamWaitEvent(s, ready[i], 0));  // field made on s2
             if (split_S)
                 k_split_b2p(g, split_S, split_img, split_eA, f->data, buf, f->ln, pads[i], split_err, s);
             else
@@ -391,14 +393,13 @@ struct mlegs_ctx {
                 if (o->data == i->data)
                     throw ApiError(MLEGS_ERR_ARG, std::string(who) + ": outputs must be distinct from the inputs");
     }
-    void grad(const Field* a, Field* rr, Field* rp, Field* gz, int pad) {  // 1727-1786
+    void grad(const Field* a, Field* rr, Field* rp, Field* gz, int pad, cudaStream_t st = nullptr) {  // 1727-1786
         require(a, MLEGS_FFF, "GRAD");
         distinct({a}, {rr, rp, gz}, "GRAD");
-        k_grad_fused(g, a->data, a->ln, rr->data, rp->data, gz->data, pad, s);
+        if (!st) st = s;
+        k_grad_fused(g, a->data, a->ln, rr->data, rp->data, gz->data, pad, st);
         rr->space = rp->space = gz->space = MLEGS_FFF;
-        ln_zero(rr);
-        ln_zero(rp);
-        ln_zero(gz);
+        for (Field* f : {rr, rp, gz}) CK(cudaMemsetAsync(f->ln, 0, sizeof(double), st));
     }
     void pc2vel(const Field* psi_, const Field* chi_, Field* rur, Field* rup, Field* uz, int pad) {  // 1789-1853
         require(psi_, MLEGS_FFF, "PC2VEL");
@@ -410,15 +411,15 @@ struct mlegs_ctx {
         ln_zero(rup);
         ln_zero(uz);
     }
-    void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad) {  // 1856-1919
+    void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad,
+                cudaStream_t st = nullptr) {  // 1856-1919
         require(psi_, MLEGS_FFF, "PC2VOR");
         require(chi_, MLEGS_FFF, "PC2VOR");
         distinct({psi_, chi_}, {ror, rop, oz}, "PC2VOR");
-        k_pc2vor_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, ror->data, rop->data, oz->data, pad, s);
+        if (!st) st = s;
+        k_pc2vor_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, ror->data, rop->data, oz->data, pad, st);
         ror->space = rop->space = oz->space = MLEGS_FFF;
-        ln_zero(ror);
-        ln_zero(rop);
-        ln_zero(oz);
+        for (Field* f : {ror, rop, oz}) CK(cudaMemsetAsync(f->ln, 0, sizeof(double), st));
     }
     // PROJECT (mod_legops.f90:2397-2545).  ln_mode: 0 none, 1 value, 2 PSI%LN by reference.
     void project(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_, int ln_mode, double ln) {
@@ -478,7 +479,7 @@ struct mlegs_ctx {
     // ------------------------------------------------------------------ physics
     void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
-                Field* BN);
+                Field* BN, cudaEvent_t vor_ready = nullptr);
     void visc1(Field* A, double nu, double dt);
     void visc2(Field* A, const Field* AO, double nu, double dt);
     void visc_be(Field* P, Field* C, Field* B, double dt);
@@ -914,13 +915,21 @@ void mlegs_ctx::force(const Field* PSI, const Field* CHI, const Field* B, Field*
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
 // On exit ROR, ROP, OZ hold the projected u x omega in velocity form (FFF).
 void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
-                       Field* BN) {
+                       Field* BN, cudaEvent_t vor_ready) {
     Field *RBR = tmp(), *RBP = tmp(), *BZ = tmp();
-    grad(B, RBR, RBP, BZ, 1);
+    // GRAD(B) on s2, beside the first RTRAN(+1) GEMMs on s; ROR, ROP, OZ may
+    // still be in the making on s2 (vor_ready)
+    cudaEvent_t ef = next_event();
+    CK(cudaEventRecord(ef, s));
+    CK(cudaStreamWaitEvent(s2, ef, 0));
+    grad(B, RBR, RBP, BZ, 1, s2);
+    cudaEvent_t eg = next_event();
+    CK(cudaEventRecord(eg, s2));
     {
         Field* const fs[9] = {RUR, RUP, UZ, ROR, ROP, OZ, RBR, RBP, BZ};
         const int pads[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        tofp_pipe(fs, pads, 9);
+        const cudaEvent_t ready[9] = {nullptr, nullptr, nullptr, vor_ready, vor_ready, vor_ready, eg, eg, eg};
+        tofp_pipe(fs, pads, 9, ready);
     }
     Field *NR = tmp(), *NP = tmp(), *NZ = tmp();
     const double2* in[10] = {RUR->data, RUP->data, UZ->data, ROR->data, ROP->data,
@@ -934,12 +943,22 @@ void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field*
     rel(RBR);
     rel(RBP);
     rel(BZ);
+    // TOFF(BN) (VERFFT(-1), RTRAN(-1)) on s2 beside PROJECT, IDEL2 and PC2VEL on s
+    cudaEvent_t et = next_event();
+    CK(cudaEventRecord(et, s));
+    CK(cudaStreamWaitEvent(s2, et, 0));
+    if (!k_verfft4(g, fft, BN->data, pbuf[0], -1, s2)) k_verfft_f(g, fft, BN->data, pbuf[0], s2);
+    fold(0, pf, d.NRCHOPDIM + 1, pbuf[0], BN->data, 0 | 2, 0, 0, 0, s2);
+    CK(cudaMemsetAsync(BN->ln, 0, sizeof(double), s2));
+    BN->space = MLEGS_FFF;
+    cudaEvent_t eb = next_event();
+    CK(cudaEventRecord(eb, s2));
     Field *PSI = tmp(), *W = tmp(), *CHI = tmp();
     project(NR, NP, NZ, PSI, W, 1, 0.0);
     idel2(W, CHI, 0, 0.0, 0);
     pc2vel(PSI, CHI, ROR, ROP, OZ, 3);
     for (Field* f : {PSI, W, CHI, NR, NP, NZ}) rel(f);
-    toff(BN, 0);
+    CK(cudaStreamWaitEvent(s, eb, 0));
 }
 
 // VISC1 (mod_march.f90:1529-1576): A <- IHELM(-ALP A, ALP), ALP = 1/(NU DT).
@@ -1160,8 +1179,14 @@ void mlegs_ctx::step_etdab_cn() {
     }
     Field *RURN = tmp(), *RUPN = tmp(), *UZN = tmp(), *RORN = tmp(), *ROPN = tmp(), *OZN = tmp(), *BN = tmp();
     pc2vel(psi, chi, RURN, RUPN, UZN, 3);
-    pc2vor(psi, chi, RORN, ROPN, OZN, 3);
-    nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN);
+    // PC2VOR on s2: the RTRAN(+1) of the velocity starts beside it
+    cudaEvent_t ef = next_event();
+    CK(cudaEventRecord(ef, s));
+    CK(cudaStreamWaitEvent(s2, ef, 0));
+    pc2vor(psi, chi, RORN, ROPN, OZN, 3, s2);
+    cudaEvent_t ev = next_event();
+    CK(cudaEventRecord(ev, s2));
+    nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN, ev);
     EtdAbArgs a{};
     a.E = etdE;
     a.N = etdN;

@@ -30,6 +30,27 @@ __device__ __forceinline__ double2 twid(const double2* tw, int q) {
 
 constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
 
+// W_R^e v with W_R = exp(SIGN 2 pi i / R) for an exponent e that is a
+// compile-time constant after unrolling: the multiples of pi/4 and pi/8 are
+// applied with literal constants (a swap for +-i), the rest read tw[e S].
+template <int R, int SIGN>
+__device__ __forceinline__ double2 rot(double2 v, int e, const double2* tw, int S) {
+    constexpr double C4 = 0.70710678118654752440084436210484903928;   // cos(pi/4)
+    constexpr double C8 = 0.92387953251128675612818318939678828682;   // cos(pi/8)
+    constexpr double S8 = 0.38268343236508977172845998403039886676;   // sin(pi/8)
+    double c, sn;  // W = c + i SIGN sn (sn = sin of the angle 2 pi e / R)
+    if (4 * e == R) return SIGN > 0 ? make_double2(-v.y, v.x) : make_double2(v.y, -v.x);
+    if (8 * e == R) { c = C4; sn = C4; }
+    else if (8 * e == 3 * R) { c = -C4; sn = C4; }
+    else if (R == 16 && e == 1) { c = C8; sn = S8; }
+    else if (R == 16 && e == 3) { c = S8; sn = C8; }
+    else if (R == 16 && e == 5) { c = -S8; sn = C8; }
+    else if (R == 16 && e == 7) { c = -C8; sn = S8; }
+    else return cmul(twid<SIGN>(tw, e * S), v);
+    const double si = SIGN > 0 ? sn : -sn;
+    return make_double2(v.x * c - v.y * si, v.x * si + v.y * c);
+}
+
 // In-register DFT of size R (natural order in and out), self-sorting Stockham
 // radix 2: every register index is a function of unrolled loop counters only,
 // so the arrays stay in registers.  S = N / R maps W_R^q to tw[q * S].
@@ -45,7 +66,7 @@ __device__ __forceinline__ void dft(double2 (&v)[R], const double2* tw, int S) {
             const int k = j % Ns;
             double2 v0 = (st & 1) ? b[j] : v[j];
             double2 v1 = (st & 1) ? b[j + R / 2] : v[j + R / 2];
-            if (k) v1 = cmul(twid<SIGN>(tw, (k * (R / (2 * Ns))) * S), v1);
+            if (k) v1 = rot<R, SIGN>(v1, k * (R / (2 * Ns)), tw, S);
             const int base = (j / Ns) * 2 * Ns + k;
             double2 s0 = make_double2(v0.x + v1.x, v0.y + v1.y);
             double2 s1 = make_double2(v0.x - v1.x, v0.y - v1.y);

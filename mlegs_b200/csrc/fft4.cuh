@@ -127,15 +127,25 @@ __device__ __forceinline__ int swz(int k1, int n2) {
 // line_fft with the transpose done in place in the line's own slot L (N
 // complex, element i at L[i * STRIDE]); L's previous contents must already be
 // consumed by all lanes.
+// tw2 (optional): the step-2 twiddles laid out tw2[k1 * N2 + t] = tw[t k1],
+// so that the lanes of a group read consecutive entries (tw[t k1] puts them
+// k1 entries apart, on the same shared-memory banks for even k1).
 template <int N1, int N2, int SIGN>
 __device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, const double2* tw, int t,
-                                                 double2 (&o)[N1], int stride = 1) {
+                                                 double2 (&o)[N1], int stride = 1, const double2* tw2 = nullptr) {
     constexpr int N = N1 * N2, U = N1 / N2;
     dft<N1, SIGN>(v, tw, N / N1);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
         double2 y = v[k1];
-        if (k1) y = cmul(twid<SIGN>(tw, t * k1), y);
+        if (k1) {
+            if (tw2) {
+                const double2 w = tw2[k1 * N2 + t];
+                y = cmul(SIGN > 0 ? conj(w) : w, y);
+            } else {
+                y = cmul(twid<SIGN>(tw, t * k1), y);
+            }
+        }
         L[swz<N1, N2>(k1, t) * stride] = y;
     }
     __syncwarp();

@@ -656,8 +656,10 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
     const int gid = lane / N2, t = lane % N2;
     const int MB = nw * G;
     double2* tw = sm;
-    double2* T = tw + (N + 1);                  // [N][MB + 1]; column mloc is line m0 + mloc
+    double2* tw2 = tw + (N + 1);                // step-2 twiddles, [k1][t]
+    double2* T = tw2 + N;                       // [N][MB + 1]; column mloc is line m0 + mloc
     for (int q = threadIdx.x; q <= N; q += blockDim.x) tw[q] = tw_g[q];
+    for (int q = threadIdx.x; q < N; q += blockDim.x) tw2[q] = tw_g[(q % N2) * (q / N2)];
     const int r = blockIdx.x, m0 = blockIdx.y * MB;
     const int mloc = warp * G + gid, m = m0 + mloc;
     const bool ok = m < g.NTCHOPDIM;
@@ -677,7 +679,7 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
             else if (q >= N - kd + kc) kk = q - (N - kd);
             v[n1] = (ok && kk >= 0) ? line[kk] : make_double2(0.0, 0.0);
         }
-        fft4::line_fft_inplace<N1, N2, +1>(v, col, tw, t, o, cs);
+        fft4::line_fft_inplace<N1, N2, +1>(v, col, tw, t, o, cs, tw2);
 #pragma unroll
         for (int q = 0; q < N1; ++q) col[(size_t)fft4::out_index<N1, N2>(t, q) * cs] = o[q];
         __syncthreads();
@@ -695,7 +697,7 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? col[(size_t)(t + N2 * n1) * cs] : make_double2(0.0, 0.0);
         __syncwarp();
-        fft4::line_fft_inplace<N1, N2, -1>(v, col, tw, t, o, cs);
+        fft4::line_fft_inplace<N1, N2, -1>(v, col, tw, t, o, cs, tw2);
 #pragma unroll
         for (int q = 0; q < N1; ++q) col[(size_t)fft4::out_index<N1, N2>(t, q) * cs] = o[q];
         __syncwarp();
@@ -716,7 +718,7 @@ static void launch_verfft4(const DevGrid& g, const FFTPlan& p, const double2* sr
     int warps = 8;
     auto need = [&](int w) {
         int MB = w * G;
-        return (size_t)((N + 1) + N * (MB + 1)) * sizeof(double2);
+        return (size_t)((N + 1) + N + N * (MB + 1)) * sizeof(double2);
     };
     while (warps > 1 && need(warps) > 110 * 1024) --warps;
     static bool attr = false;

@@ -315,8 +315,10 @@ __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const do
         if (r == 0) return comp ? 0.0 : (has_ln ? ln_in / g.norm0[0] : 0.0);
         return in[(size_t)(r - 1) * st];
     };
-    if (shift) {
-        // the shifted rows are read from src before any row of dst is written (src may be dst)
+    // out of place, the substitution reads the shifted rows directly; in place,
+    // they are shifted first (each row read before it is overwritten)
+    const bool direct = shift && (const void*)src != (const void*)dst;
+    if (shift && !direct) {
         double prev = rhs(0);
         for (int r = 0; r < size; ++r) {
             const double cur = (r + 1 < size) ? rhs(r + 1) : 0.0;
@@ -384,7 +386,7 @@ __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const do
                 const int r = r0 + q;
                 const bool ok = r < size;
                 const double* f = F7 + (size_t)r * 7 * NK + k;
-                rb[q] = ok ? in[(size_t)r * st] : 0.0;
+                rb[q] = ok ? (direct ? rhs(r) : in[(size_t)r * st]) : 0.0;
                 f3[q] = ok ? f[0] : 0.0;
                 f2[q] = ok ? f[NK] : 0.0;
                 f1[q] = ok ? f[2 * NK] : 0.0;

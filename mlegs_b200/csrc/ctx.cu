@@ -273,11 +273,11 @@ struct mlegs_ctx {
                 k_split_b2p(g, split_S, split_img, split_eA, f->data, buf, f->ln, pads[i], split_err, s);
             else
                 k_rtran_b2p(g, f->data, buf, f->ln, pads[i], s);
-            ln_zero(f);
             cudaEvent_t eb = next_event();
             CK(cudaEventRecord(eb, s));
             CK(cudaStreamWaitEvent(s2, eb, 0));
             if (!k_verfft4(g, fft, buf, f->data, +1, s2)) k_verfft_b(g, fft, buf, f->data, s2);
+            CK(cudaMemsetAsync(f->ln, 0, sizeof(double), s2));  // RTRAN zeroes LN (off the GEMM stream)
             cudaEvent_t ev = next_event();
             CK(cudaEventRecord(ev, s2));
             done[i % 3] = ev;
@@ -405,11 +405,9 @@ struct mlegs_ctx {
         require(psi_, MLEGS_FFF, "PC2VEL");
         require(chi_, MLEGS_FFF, "PC2VEL");
         distinct({psi_, chi_}, {rur, rup, uz}, "PC2VEL");
-        k_pc2vel_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, rur->data, rup->data, uz->data, pad, s);
+        double* zl[3] = {rur->ln, rup->ln, uz->ln};  // set to 0 by the kernel
+        k_pc2vel_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, rur->data, rup->data, uz->data, pad, s, 0, zl);
         rur->space = rup->space = uz->space = MLEGS_FFF;
-        ln_zero(rur);
-        ln_zero(rup);
-        ln_zero(uz);
     }
     void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad,
                 cudaStream_t st = nullptr) {  // 1856-1919
@@ -936,17 +934,18 @@ void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field*
                              OZ->data,  RBR->data, RBP->data, BZ->data,  nullptr};
     double2* out[4] = {NR->data, NP->data, NZ->data, BN->data};
     k_theta_fused(g, fft, in, out, 0.0, 0.0, 0, s);
-    for (Field* f : {NR, NP, NZ, BN}) {
-        f->space = MLEGS_PFP;
-        ln_zero(f);
-    }
     rel(RBR);
     rel(RBP);
     rel(BZ);
-    // TOFF(BN) (VERFFT(-1), RTRAN(-1)) on s2 beside PROJECT, IDEL2 and PC2VEL on s
+    // TOFF(BN) (VERFFT(-1), RTRAN(-1)) on s2 beside PROJECT, IDEL2 and PC2VEL on s;
+    // the zero LN of the four results is set there too (nothing on s reads it)
     cudaEvent_t et = next_event();
     CK(cudaEventRecord(et, s));
     CK(cudaStreamWaitEvent(s2, et, 0));
+    for (Field* f : {NR, NP, NZ, BN}) {
+        f->space = MLEGS_PFP;
+        CK(cudaMemsetAsync(f->ln, 0, sizeof(double), s2));
+    }
     if (!k_verfft4(g, fft, BN->data, pbuf[0], -1, s2)) k_verfft_f(g, fft, BN->data, pbuf[0], s2);
     fold(0, pf, d.NRCHOPDIM + 1, pbuf[0], BN->data, 0 | 2, 0, 0, 0, s2);
     CK(cudaMemsetAsync(BN->ln, 0, sizeof(double), s2));

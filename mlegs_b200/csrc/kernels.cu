@@ -763,10 +763,13 @@ __global__ void grad_fused_kernel(DevGrid g, const double2* a, const double* ln,
 
 // sub = 1: the outputs are decremented by the velocity instead of set to it
 __global__ void pc2vel_fused_kernel(DevGrid g, const double2* psi, const double* psi_ln, const double2* chi,
-                                    const double* chi_ln, double2* rur, double2* rup, double2* uz, int pad, int sub) {
+                                    const double* chi_ln, double2* rur, double2* rup, double2* uz, int pad, int sub,
+                                    double* zl0, double* zl1, double* zl2) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     int m, n, k;
     if (!fff_index(g, t, m, n, k)) return;
+    // the outputs' LN slots (PC2VEL results carry no log term); read by no thread here
+    if (t < 3 && zl0) *(t == 0 ? zl0 : (t == 1 ? zl1 : zl2)) = 0.0;
     const Col cp = column(g, psi, m, k, pad), cc = column(g, chi, m, k, pad);
     double2 v0 = make_double2(0.0, 0.0), v1 = v0, v2 = v0;
     if (n < cp.nn) {
@@ -916,9 +919,11 @@ void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2*
 }
 
 void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
-                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub) {
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub, double* const* zero_ln) {
     const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
-    pc2vel_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, rur, rup, uz, pad, sub);
+    pc2vel_fused_kernel<<<nblk(n, 256), 256, 0, s>>>(g, psi, psi_ln, chi, chi_ln, rur, rup, uz, pad, sub,
+                                                     zero_ln ? zero_ln[0] : nullptr, zero_ln ? zero_ln[1] : nullptr,
+                                                     zero_ln ? zero_ln[2] : nullptr);
     count_launch();
 }
 

@@ -155,7 +155,8 @@ void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, 
 void k_grad_fused(const DevGrid& g, const double2* a, const double* ln, double2* rr, double2* rp, double2* gz, int pad,
                   cudaStream_t s);
 void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
-                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub = 0);
+                    double2* rur, double2* rup, double2* uz, int pad, cudaStream_t s, int sub = 0,
+                    double* const* zero_ln = nullptr);
 void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
                     double2* ror, double2* rop, double2* oz, int pad, cudaStream_t s);
 void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);

@@ -439,10 +439,12 @@ struct mlegs_ctx {
             throw ApiError(MLEGS_ERR_TRANSFORM, "PROJECT: bad input space");
         }
         psi_->space = chi_->space = MLEGS_FFF;
-        ln_zero(psi_);
-        ln_zero(chi_);
-        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, v2p_pff, s);
-        if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, v2p_pff, s);
+        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, v2p_pff, s, chi_->ln);
+        else if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, v2p_pff, s, chi_->ln);
+        else {
+            ln_zero(psi_);
+            ln_zero(chi_);
+        }
         if (!split_S && dmma_supported(g)) {
             k_project_dmma(g, V, D, T, rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
             k_farfield_fix(g, psi_->data, d.NRCHOP, s);
@@ -469,8 +471,7 @@ struct mlegs_ctx {
         }
         psi_->space = chi_->space = MLEGS_FFF;
         k_project_fff_dmma(g, compV, compD, compT, rur->data, rup->data, uz->data, psi_->data, chi_->data, psi_->ln,
-                           v2p_fff, s);
-        ln_zero(chi_);
+                           v2p_fff, s, chi_->ln);
         k_farfield_fix(g, psi_->data, d.NRCHOP, s);
     }
 

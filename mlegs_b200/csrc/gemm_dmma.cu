@@ -638,9 +638,9 @@ static void projfff_launch(const DevGrid& g, const ProjFffArgs& pa, cudaStream_t
 
 void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, const double* CT_, double2* rur,
                         double2* rup, double2* uz, double2* psi, double2* chi, double* psi_ln, const double* Lfff,
-                        cudaStream_t s) {
+                        cudaStream_t s, double* chi_ln) {
     // VEL2PLN on RUP's (0, 0) column first: it changes RUP's input to the products
-    launch_vel2pln_fff(g, rup, psi_ln, Lfff, s);
+    launch_vel2pln_fff(g, rup, psi_ln, Lfff, s, chi_ln);
     ProjFffArgs pa;
     const double* C[5] = {CV, CD, CD, CV, CT_};
     const double2* x[5] = {rur, rup, rur, rup, uz};

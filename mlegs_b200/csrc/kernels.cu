@@ -306,7 +306,8 @@ __device__ double vel2pln_dot(const double* L, const double2* line, size_t st, i
     return tot;
 }
 
-__global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in, const double* Lpff) {
+__global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode, double ln_in, const double* Lpff,
+                               double* zero_ln) {
     __shared__ double part[8];
     const size_t st = g.NXCHOPDIM;  // PFF row stride for m = 0 ([0][r][k])
     const double pln = vel2pln_dot(Lpff, rup, st, g.NR, part);
@@ -317,18 +318,21 @@ __global__ void vel2pln_kernel(DevGrid g, double2* rup, double* psi_ln, int mode
         rup[(size_t)i * st].x -= (e2 + o2);
         rup[(size_t)(g.NR - 1 - i) * st].x -= (e2 - o2);
     }
-    if (threadIdx.x == 0) *psi_ln = (mode == 1) ? ln_in : pln;
+    if (threadIdx.x == 0) {
+        *psi_ln = (mode == 1) ? ln_in : pln;
+        if (zero_ln) *zero_ln = 0.0;
+    }
 }
 void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln, const double* Lpff,
-                    cudaStream_t s) {
-    vel2pln_kernel<<<1, 256, 0, s>>>(g, rup_pff, psi_ln, mode, ln, Lpff);
+                    cudaStream_t s, double* zero_ln) {
+    vel2pln_kernel<<<1, 256, 0, s>>>(g, rup_pff, psi_ln, mode, ln, Lpff, zero_ln);
     count_launch();
 }
 
 // VEL2PLN from RUP's FFF (0, 0) column; the subtraction of PLN times the
 // n = 0, 1 functions from the PFF line is applied to the FFF column instead
 // (rows 0 and 1 += PLN / NORM), the same change of the RTRAN(+1) image.
-__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* Lfff) {
+__global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, const double* Lfff, double* zero_ln) {
     __shared__ double part[8];
     const size_t st = g.NXCHOPDIM;  // FFF row stride of the (0, 0) column
     const double pln = vel2pln_dot(Lfff, rup, st, g.NRCHOP, part);
@@ -336,10 +340,12 @@ __global__ void vel2pln_fff_kernel(DevGrid g, double2* rup, double* psi_ln, cons
         rup[0].x += pln / g.norm0[0];
         rup[st].x += pln / g.norm0[1];
         *psi_ln = pln;
+        if (zero_ln) *zero_ln = 0.0;
     }
 }
-void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* Lfff, cudaStream_t s) {
-    vel2pln_fff_kernel<<<1, 256, 0, s>>>(g, rup_fff, psi_ln, Lfff);
+void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* Lfff, cudaStream_t s,
+                        double* zero_ln) {
+    vel2pln_fff_kernel<<<1, 256, 0, s>>>(g, rup_fff, psi_ln, Lfff, zero_ln);
     count_launch();
 }
 

@@ -117,7 +117,7 @@ size_t proj_comp_doubles(const DevGrid& g);
 void k_proj_comp(const DevGrid& g, const double* W, int p_flip, double* Cm, cudaStream_t s);
 void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, const double* CT, double2* rur,
                         double2* rup, double2* uz, double2* psi, double2* chi, double* psi_ln, const double* Lfff,
-                        cudaStream_t s);
+                        cudaStream_t s, double* chi_ln = nullptr);
 // out[m][n][k] (+)= scale(m,k) * sum_i Wt[m][n][i] * fold(in)(i,k); fold parity per row given by mode
 //   mode 0 (EO): row n even -> even fold, odd -> odd fold;  mode 1 (OE): swapped
 //   scale: 0 -> 1, 1 -> -1, 2 -> -i m, 3 -> i k, 4 -> m k
@@ -164,9 +164,11 @@ void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
 // on the PFF line of RUP (Lpff, NR entries), or on RUP's FFF (0, 0) column
 // (Lfff, NRCHOP entries; mode 0, applied to that column).
 void k_vel2pln_coef(const DevGrid& g, const double* explog0, int nn, double* Lpff, double* Lfff, cudaStream_t s);
+// zero_ln (optional): one more LN slot set to 0 by the same launch.
 void launch_vel2pln(const DevGrid& g, double2* rup_pff, double* psi_ln, int mode, double ln, const double* Lpff,
-                    cudaStream_t s);
-void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* Lfff, cudaStream_t s);
+                    cudaStream_t s, double* zero_ln = nullptr);
+void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, const double* Lfff, cudaStream_t s,
+                        double* zero_ln = nullptr);
 
 // Banded solves (IDEL2LN, IDEL2, IHELM) with per-system elimination scratch.
 void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double alp, int has_ln,

@@ -408,13 +408,16 @@ __device__ __forceinline__ void idle_group_syncs() {
 }
 
 // Inverse HORFFT of one PFP row into the natural-order packed samples L[0..N).
+// loaded: the row is already in the slot (an earlier asynchronous copy that
+// the warp has waited for); src is then not read.
 template <int N1, int N2>
 __device__ __forceinline__ void grp_inverse5(const double2* __restrict__ src, bool valid, int md, int ntchop,
-                                             const double2* tw, const double2* twh, double2* L, int t) {
+                                             const double2* tw, const double2* twh, double2* L, int t,
+                                             bool loaded = false) {
     constexpr int N = N1 * N2;
     const int mlim = md < ntchop ? md : ntchop;
     // coalesced row load into the slot (entries m >= mlim read as zero below)
-    if (valid)
+    if (valid && !loaded)
         for (int m = t; m < mlim; m += N2) L[m] = src[m];
     __syncwarp();
     double2 v[N1], o[N1];
@@ -437,6 +440,19 @@ __device__ __forceinline__ void grp_inverse5(const double2* __restrict__ src, bo
 #pragma unroll
     for (int q = 0; q < N1; ++q) L[fft4::out_index<N1, N2>(t, q)] = o[q];
 }
+
+// Asynchronous copy of one PFP row (m < mlim) into a line slot by the group's
+// lanes; completion is waited for with cp.async.wait_group, then __syncwarp.
+template <int N2>
+__device__ __forceinline__ void row_async(const double2* __restrict__ src, int mlim, double2* L, int t) {
+    for (int m = t; m < mlim; m += N2)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(L + m)),
+                     "l"(src + m)
+                     : "memory");
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory"); }
 
 // Forward HORFFT of the natural-order packed samples in L to a PFP row (m < md).
 template <int N1, int N2>
@@ -463,6 +479,65 @@ __device__ __forceinline__ void grp_forward5(double2* L, bool valid, double2* __
     }
 }
 
+// Kernel-argument arrays indexed by a run-time value without copying them to
+// local memory.
+__device__ __forceinline__ const double2* pick_in(const PhysArgs& A, int i) {
+    const double2* p = A.in[0];
+#pragma unroll
+    for (int q = 1; q < 10; ++q)
+        if (i == q) p = A.in[q];
+    return p;
+}
+__device__ __forceinline__ double2* pick_out(const PhysArgs& A, int i) {
+    double2* p = A.out[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+        if (i == q) p = A.out[q];
+    return p;
+}
+
+// After round 2 (slots: 0-2 velocity, 3 B, 4-6 vorticity, 7 RBR): slots 4-6 <-
+// N_r, N_theta, N_z of VPRODSUB (+ the linear terms), slot 7 <- a1 c1.
+template <int N>
+__device__ __forceinline__ void theta_products_r2(double2* L, int lane, double ir2, double o2, int linear) {
+    for (int j = lane; j < N; j += 32) {
+        const double2 a1 = L[j], a2 = L[N + j], a3 = L[2 * N + j];
+        const double2 b1 = L[4 * N + j], b2 = L[5 * N + j], b3 = L[6 * N + j], c1 = L[7 * N + j];
+        double2 nr_ = make_double2(a2.x * b3.x - a3.x * b2.x, a2.y * b3.y - a3.y * b2.y);
+        double2 np_ = make_double2(a3.x * b1.x - a1.x * b3.x, a3.y * b1.y - a1.y * b3.y);
+        double2 nz_ = make_double2((a1.x * b2.x - a2.x * b1.x) * ir2, (a1.y * b2.y - a2.y * b1.y) * ir2);
+        if (linear) {
+            const double2 bp = L[3 * N + j];
+            nr_.x += o2 * a2.x;
+            nr_.y += o2 * a2.y;
+            np_.x -= o2 * a1.x;
+            np_.y -= o2 * a1.y;
+            nz_.x -= bp.x;
+            nz_.y -= bp.y;
+        }
+        L[4 * N + j] = nr_;
+        L[5 * N + j] = np_;
+        L[6 * N + j] = nz_;
+        L[7 * N + j] = make_double2(a1.x * c1.x, a1.y * c1.y);
+    }
+}
+
+// After round 3 (slot 3 RBP, slot 8 BZ): slot 7 <- N_b of VDOTPSUB (+ N^2 u_z).
+template <int N>
+__device__ __forceinline__ void theta_products_r3(double2* L, int lane, double ir2, double n2, int linear) {
+    for (int j = lane; j < N; j += 32) {
+        const double2 a2 = L[N + j], a3 = L[2 * N + j], c2 = L[3 * N + j], c3 = L[8 * N + j];
+        const double2 bp = L[7 * N + j];
+        double2 bn_ = make_double2(-((bp.x + a2.x * c2.x) * ir2 + a3.x * c3.x),
+                                   -((bp.y + a2.y * c2.y) * ir2 + a3.y * c3.y));
+        if (linear) {
+            bn_.x += n2 * a3.x;
+            bn_.y += n2 * a3.y;
+        }
+        L[7 * N + j] = bn_;
+    }
+}
+
 }  // namespace
 
 template <int N1, int N2>
@@ -484,6 +559,70 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
     const int md = g.NTCHOPDIM;
     const int nlines = g.NR * g.NX;
     const double o2 = 2 * A.omega, n2 = A.bv0 * A.bv0;
+    if constexpr (G == 4) {
+        // Rows arrive by cp.async one round ahead: the three (four) round-1
+        // rows of the next line while this line's forward transforms run, the
+        // round-2 rows (and, without the linear terms, the round-3 rows into
+        // the then unused slots 3 and 8) while round 1 computes.
+        const int mlim = md < g.NTCHOP ? md : g.NTCHOP;
+        auto issue_r1 = [&](int ln) {
+            const size_t o = (size_t)ln * md;
+            if (gid < 3) row_async<N2>(pick_in(A, gid) + o, mlim, L + (size_t)gid * N, t);
+            else if (A.linear) row_async<N2>(A.in[9] + o, mlim, L + (size_t)3 * N, t);
+            async_commit();
+        };
+        auto issue_r3 = [&](int ln) {
+            const size_t o = (size_t)ln * md;
+            if (gid < 2) row_async<N2>(pick_in(A, 7 + gid) + o, mlim, L + (size_t)(gid ? 8 : 3) * N, t);
+            async_commit();
+        };
+        const int line0 = blockIdx.x * nw + warp;
+        if (line0 < nlines) issue_r1(line0);
+        for (int line = line0; line < nlines; line += gridDim.x * nw) {
+            const size_t off = (size_t)line * md;
+            const int nxt = line + gridDim.x * nw;
+            if (lane < 10 && nxt < nlines && (lane < 9 || A.linear))
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(pick_in(A, lane) + (size_t)nxt * md),
+                             "r"((unsigned)(md * sizeof(double2)))
+                             : "memory");
+            const double rr = g.r[line / g.NX];
+            const double ir2 = 1.0 / (rr * rr);
+            row_async<N2>(pick_in(A, 3 + gid) + off, mlim, L + (size_t)(4 + gid) * N, t);  // round 2
+            async_commit();
+            if (!A.linear) issue_r3(line);
+            // round 1: fields 0-2 (and B with the linear terms) in slots 0-3
+            if (A.linear) async_wait<1>();
+            else async_wait<2>();
+            __syncwarp();
+            if (gid < 3 || A.linear)
+                grp_inverse5<N1, N2>(nullptr, true, md, g.NTCHOP, tw, twh, L + (size_t)gid * N, t, true);
+            else
+                idle_group_syncs();
+            __syncwarp();
+            // round 2: fields 3-6 in slots 4-7
+            if (A.linear) async_wait<0>();
+            else async_wait<1>();
+            __syncwarp();
+            grp_inverse5<N1, N2>(nullptr, true, md, g.NTCHOP, tw, twh, L + (size_t)(4 + gid) * N, t, true);
+            __syncwarp();
+            theta_products_r2<N>(L, lane, ir2, o2, A.linear);
+            __syncwarp();
+            // round 3: RBP -> slot 3, BZ -> slot 8
+            if (A.linear) issue_r3(line);
+            async_wait<0>();
+            __syncwarp();
+            if (gid < 2)
+                grp_inverse5<N1, N2>(nullptr, true, md, g.NTCHOP, tw, twh, L + (size_t)(gid ? 8 : 3) * N, t, true);
+            else
+                idle_group_syncs();
+            __syncwarp();
+            theta_products_r3<N>(L, lane, ir2, n2, A.linear);
+            __syncwarp();
+            if (nxt < nlines) issue_r1(nxt);  // slots 0-3 are free from here on
+            grp_forward5<N1, N2>(L + (size_t)(4 + gid) * N, true, pick_out(A, gid) + off, md, g.NTCHOP, tw, twh, t);
+            __syncwarp();
+        }
+    } else {
     for (int line = blockIdx.x * nw + warp; line < nlines; line += gridDim.x * nw) {
         const size_t off = (size_t)line * md;
         // the warp's next line: lanes 0..9 ask L2 for its ten input rows (md complex each)
@@ -517,26 +656,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
             __syncwarp();
         }
         // round-2 products
-        for (int j = lane; j < N; j += 32) {
-            const double2 a1 = L[j], a2 = L[N + j], a3 = L[2 * N + j];
-            const double2 b1 = L[4 * N + j], b2 = L[5 * N + j], b3 = L[6 * N + j], c1 = L[7 * N + j];
-            double2 nr_ = make_double2(a2.x * b3.x - a3.x * b2.x, a2.y * b3.y - a3.y * b2.y);
-            double2 np_ = make_double2(a3.x * b1.x - a1.x * b3.x, a3.y * b1.y - a1.y * b3.y);
-            double2 nz_ = make_double2((a1.x * b2.x - a2.x * b1.x) * ir2, (a1.y * b2.y - a2.y * b1.y) * ir2);
-            if (A.linear) {
-                const double2 bp = L[3 * N + j];
-                nr_.x += o2 * a2.x;
-                nr_.y += o2 * a2.y;
-                np_.x -= o2 * a1.x;
-                np_.y -= o2 * a1.y;
-                nz_.x -= bp.x;
-                nz_.y -= bp.y;
-            }
-            L[4 * N + j] = nr_;
-            L[5 * N + j] = np_;
-            L[6 * N + j] = nz_;
-            L[7 * N + j] = make_double2(a1.x * c1.x, a1.y * c1.y);
-        }
+        theta_products_r2<N>(L, lane, ir2, o2, A.linear);
         __syncwarp();
         // round 3
         for (int f0 = 0; f0 < 4; f0 += G) {
@@ -547,17 +667,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
                 idle_group_syncs();
         }
         __syncwarp();
-        for (int j = lane; j < N; j += 32) {
-            const double2 a2 = L[N + j], a3 = L[2 * N + j], c2 = L[3 * N + j], c3 = L[8 * N + j];
-            const double2 bp = L[7 * N + j];
-            double2 bn_ = make_double2(-((bp.x + a2.x * c2.x) * ir2 + a3.x * c3.x),
-                                       -((bp.y + a2.y * c2.y) * ir2 + a3.y * c3.y));
-            if (A.linear) {
-                bn_.x += n2 * a3.x;
-                bn_.y += n2 * a3.y;
-            }
-            L[7 * N + j] = bn_;
-        }
+        theta_products_r3<N>(L, lane, ir2, n2, A.linear);
         __syncwarp();
         // forward transforms of the four results
         for (int f0 = 0; f0 < 4; f0 += G) {
@@ -568,6 +678,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
                 idle_group_syncs();
         }
         __syncwarp();
+    }
     }
 }
 

@@ -191,6 +191,7 @@ int mlegs_check_finite(mlegs_ctx* ctx);
 #define MLEGS_K_SPLIT_P2B  12   /* RTRAN(-1) as split-BF16 tcgen05 GEMM (MLEGS_PREC_SPLIT contexts) */
 #define MLEGS_K_PROJECT    13   /* PROJECT's five EOMUL/OEMUL products, 3 PFF -> 2 FFF */
 #define MLEGS_K_PROJECT_FFF 14  /* PROJECT of FFF velocity fields via composite matrices, 3 FFF -> 2 FFF */
+#define MLEGS_K_PHYS_NONLIN 15  /* MLEGS_K_PHYS as CALC_BOUSSI_NONLIN runs it: 9 inputs, no linear terms */
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
 /* Number of this library's kernel launches issued since the counter was reset. */

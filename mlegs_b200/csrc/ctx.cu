@@ -1656,7 +1656,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 14) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 15) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1677,7 +1677,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             ret.taken.push_back(f);
             return f;
         };
-        Field *a = take(), *b = take(), *c = take();
+        Field *a = take(), *b = take(), *c = take(), *e = take();
         Field* f9[9];
         for (auto& q : f9) q = take();
         // deterministic non-trivial contents: fill FFF/PPP-sized buffers via axpby of zeros
@@ -1710,6 +1710,12 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                                              f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, a->data};
                     double2* out[4] = {b->data, c->data, f9[0]->data, f9[1]->data};
                     k_theta_fused(g, ctx->fft, in, out, 1.0, 1.0, 1, s);
+                } break;
+                case 15: {  // the nonlinear-term form of the step: 9 inputs, no linear terms
+                    const double2* in[10] = {f9[0]->data, f9[1]->data, f9[2]->data, f9[3]->data, f9[4]->data,
+                                             f9[5]->data, f9[6]->data, f9[7]->data, f9[8]->data, nullptr};
+                    double2* out[4] = {a->data, b->data, c->data, e->data};
+                    k_theta_fused(g, ctx->fft, in, out, 0.0, 0.0, 0, s);
                 } break;
                 case 9: k_horfft_warp(g, ctx->fft, a->data, b->data, +1, s); break;
                 case 11:
@@ -1752,6 +1758,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 6: bytes = B16 * 14.0 * (double)d.ppp(); break;  // 10 fields read, 4 written
             case 7: bytes = (B16 * 2.0 + 40.0) * (double)d.fff(); break;  // rhs in, solution out, 5 factors
             case 8: bytes = B16 * 14.0 * (double)d.pfp(); break;  // 10 PFP lines read, 4 written
+            case 15: bytes = B16 * 13.0 * (double)d.pfp(); break;  // 9 read, 4 written
             case 13: bytes = B16 * (3.0 * (double)d.pff() + 2.0 * (double)d.fff()); break;
             case 14: bytes = B16 * 5.0 * (double)d.fff(); break;
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;

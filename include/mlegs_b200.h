@@ -158,6 +158,17 @@ int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field
                        const mlegs_field* b, mlegs_field* psin, mlegs_field* chin,
                        mlegs_field* bn);
 
+/* Energy diagnostics.  CALC_BOUSSI_ENERGY(PSI, CHI, B) (mod_boussinesq.f90:139-232)
+ * without its file output: ke, pe, dke (any may be NULL) receive KE, PE and DKE
+ * per (m >= 0, k >= 0), NTCHOP x NXCHOP doubles each in Fortran order; the
+ * driver's especData_M / especData_K lines are their row / column sums.
+ * MLEGS_ERR_LOGTERM when B%LN is not 0 (the reference aborts there).
+ * CALC_BOUSSI_PE(B) (112-136): pe likewise, at the current chop.  Both
+ * synchronise the context's stream. */
+int mlegs_boussi_energy(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
+                        double* ke, double* pe, double* dke);
+int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe);
+
 /* Solver: SOLVER_T%INITIALIZE (mod_march.f90:171-240, Richardson start-up) and
  * TIME_STEPPING's state update (243-307: STEP_BOUSSI_AB_CN 609 or
  * STEP_BOUSSI_ETDAB_CN 811).  The state fields stay owned by the caller. */

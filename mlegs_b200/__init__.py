@@ -92,6 +92,7 @@ class Context:
         self.lib.mlegs_dims(self.c, d)
         (self.NDIMR, self.NDIMTH, self.NX, self.NRCHOPDIM, self.NTCHOPDIM, self.NXCHOPDIM,
          self.NRH, self.NR, self.NTH) = list(d)
+        self.NTCHOP, self.NXCHOP = int(cfg.ntchop), int(cfg.nxchop)
 
     # ------------------------------------------------------------------
     def close(self):
@@ -233,6 +234,26 @@ class Context:
 
     def CALC_BOUSSI_FORCE(self, psi, chi, b, psin, chin, bn):
         self._ck(self.lib.mlegs_boussi_force(self.c, psi.h, chi.h, b.h, psin.h, chin.h, bn.h))
+
+    # ------------------------------------------------------------ diagnostics
+    def _mk_array(self):
+        return np.zeros((self.NXCHOP, self.NTCHOP), dtype=np.float64)  # Fortran order (NTCHOP, NXCHOP)
+
+    def CALC_BOUSSI_ENERGY(self, psi, chi, b):
+        """CALC_BOUSSI_ENERGY (mod_boussinesq.f90:139-232) without the file
+        output: (KE, PE, DKE), each an (NTCHOP, NXCHOP) array over m >= 0,
+        k >= 0.  The reference's especData_M / especData_K lines are
+        KE.sum(axis=1) / KE.sum(axis=0) (likewise PE, DKE)."""
+        ke, pe, dke = self._mk_array(), self._mk_array(), self._mk_array()
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._ck(self.lib.mlegs_boussi_energy(self.c, psi.h, chi.h, b.h, ptr(ke), ptr(pe), ptr(dke)))
+        return ke.T.copy(), pe.T.copy(), dke.T.copy()
+
+    def CALC_BOUSSI_PE(self, b):
+        """CALC_BOUSSI_PE (mod_boussinesq.f90:112-136): (NTCHOP, NXCHOP) array."""
+        pe = self._mk_array()
+        self._ck(self.lib.mlegs_boussi_pe(self.c, b.h, pe.ctypes.data_as(ctypes.c_void_p)))
+        return pe.T.copy()
 
     # ------------------------------------------------------------ solver
     def initialize(self, psi, chi, b):

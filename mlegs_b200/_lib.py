@@ -73,6 +73,8 @@ SIGNATURES = {
     "mlegs_pc2vor": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_project": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double]),
     "mlegs_boussi_force": (c_int, [c_void_p] + [c_void_p] * 6),
+    "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mlegs_solver_init": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_step": (c_int, [c_void_p, c_int]),
     "mlegs_step_graph": (c_int, [c_void_p, c_int]),

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <algorithm>
 #include <initializer_list>
 #include <memory>
 #include <stdexcept>
@@ -82,6 +83,7 @@ struct mlegs_ctx {
     double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
     double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
     double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
+    double* diag = nullptr;                                         // 4 x [m][k] quadratures (energy)
     double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
     FFTPlan fft;
     std::vector<double> h_x, h_w, h_lognorm;
@@ -477,6 +479,8 @@ struct mlegs_ctx {
 
     // ------------------------------------------------------------------ physics
     void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
+    void energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke);
+    void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
                 Field* BN, cudaEvent_t vor_ready = nullptr);
     void visc1(Field* A, double nu, double dt);
@@ -685,6 +689,7 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     D = dalloc<double>(vsz);
     T = dalloc<double>(vsz);
     k_tables_project(g, V, D, T, 0, s);
+    diag = dalloc<double>((size_t)4 * d.NTCHOPDIM * d.NXCHOPDIM);
     v2p_pff = dalloc<double>(d.NR);
     v2p_fff = dalloc<double>(std::max(d.NRCHOP, 1));
     k_vel2pln_coef(g, explog0, d.NRCHOP, v2p_pff, v2p_fff, s);
@@ -909,6 +914,83 @@ void mlegs_ctx::force(const Field* PSI, const Field* CHI, const Field* B, Field*
     toff(BN, 0);
     copy0(BNout, BN, 0);
     for (Field* f : {Wf, NR, NP, NZ, BN}) rel(f);
+}
+
+// *_MK_HALFK (mod_scalar3.f90:528-554, 808-841) of an [m][k] quadrature array:
+// the m = 0 row halved (the ALLK forms, 523 and 803), then k and -k folded into
+// out(m, k), k < NXCHOP, Fortran order (NTCHOP x NXCHOP); out (+)= sign * that.
+void mlegs_ctx::halfk(const double* all, double sign, double* out, bool accumulate) const {
+    const int nt = d.NTCHOPDIM, nk = d.NXCHOPDIM;
+    for (int kk = 0; kk < d.NXCHOP; ++kk)
+        for (int mm = 0; mm < d.NTCHOP; ++mm) {
+            double v = 0.0;
+            if (mm < nt) {
+                const double h = mm == 0 ? 0.5 : 1.0;
+                const double a = h * all[(size_t)mm * nk + kk];
+                v = kk == 0 ? a : h * all[(size_t)mm * nk + (nk - kk)] + a;
+            }
+            double& o = out[(size_t)kk * d.NTCHOP + mm];
+            o = accumulate ? o + sign * v : sign * v;
+        }
+}
+
+// CALC_BOUSSI_ENERGY(PSI, CHI, B), mod_boussinesq.f90:139-232, without the
+// file output: KE, PE and DKE per (m >= 0, k >= 0), NTCHOP x NXCHOP each
+// (Fortran order); the driver's especData sums are their row / column sums.
+void mlegs_ctx::energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke) {
+    require(PSI, MLEGS_FFF, "CALC_BOUSSI_ENERGY");
+    require(CHI, MLEGS_FFF, "CALC_BOUSSI_ENERGY");
+    require(B, MLEGS_FFF, "CALC_BOUSSI_ENERGY");
+    double bln = 0.0;
+    CK(cudaMemcpyAsync(&bln, B->ln, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (bln != 0.0)
+        throw ApiError(MLEGS_ERR_LOGTERM, "B has non-zero LN, this is not expected in Boussinesq");
+    if (p.bv0 == 0.0) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_ENERGY: BV0 = 0");
+    const int P3 = 3;  // CHOPSET(3) ... CHOPSET(-3)
+    const size_t nmk = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
+    const double scale = 4.0 * 3.141592653589793238462643383279502884 * p.zlen * d.ELL2;
+    Field *W1 = tmp(), *W2 = tmp(), *W3 = tmp();
+    // toroidal: W1 = PSI (LN doubled), W2 = DELSQH(W1); -PRODCT(RTRAN W1, RTRAN W2)
+    copy0(W1, PSI, P3);
+    k_ln_copy(W1->ln, PSI->ln, 2.0, s);
+    delsqh(W1, W2, P3);
+    ln_zero(W1);
+    ln_zero(W2);
+    rtran(W1, 1, P3);
+    rtran(W2, 1, P3);
+    k_prodct_mk(g, W1->data, W2->data, 0, scale, diag, s);
+    // poloidal: W1 = DEL2(CHI), W2 = DELSQH(CHI)
+    del2(CHI, W1, P3);
+    delsqh(CHI, W2, P3);
+    ln_zero(W1);
+    ln_zero(W2);
+    rtran(W1, 1, P3);
+    rtran(W2, 1, P3);
+    k_prodct_mk(g, W1->data, W2->data, 0, scale, diag + nmk, s);
+    // exchange and potential energy from W3 = B
+    copy0(W3, B, P3);
+    ln_zero(W3);
+    rtran(W3, 1, P3);
+    k_prodct_mk(g, W3->data, W2->data, 0, scale, diag + 2 * nmk, s);
+    k_prodct_mk(g, W3->data, nullptr, 1, scale, diag + 3 * nmk, s);
+    rel(W3);
+    rel(W2);
+    rel(W1);
+    std::vector<double> h(4 * nmk);
+    CK(cudaMemcpyAsync(h.data(), diag, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const size_t nout = (size_t)d.NTCHOP * d.NXCHOP;
+    std::vector<double> kev(nout);
+    halfk(h.data(), -1.0, kev.data(), false);
+    halfk(h.data() + nmk, 1.0, kev.data(), true);
+    for (double& v : kev) v /= 2.0;
+    if (ke) std::copy(kev.begin(), kev.end(), ke);
+    if (dke) halfk(h.data() + 2 * nmk, 1.0, dke, false);
+    if (pe) {
+        halfk(h.data() + 3 * nmk, 1.0, pe, false);
+        for (size_t q = 0; q < nout; ++q) pe[q] = pe[q] / 2.0 / (p.bv0 * p.bv0);
+    }
 }
 
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
@@ -1544,6 +1626,47 @@ int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field
         ctx->mark();
         ctx->force(F(psi), F(chi), F(b), F(psin), F(chin), F(bn));
         ctx->restore();
+    });
+}
+
+int mlegs_boussi_energy(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
+                        double* ke, double* pe, double* dke) {
+    return guard(ctx, [&] {
+        ctx->mark();
+        try {
+            ctx->energy(F(psi), F(chi), F(b), ke, pe, dke);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
+        ctx->restore();
+    });
+}
+
+int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe) {
+    return guard(ctx, [&] {
+        // CALC_BOUSSI_PE (mod_boussinesq.f90:112-136): WK = B, LN 0, RTRAN at the
+        // current chop (pad 0), L2NORM_MK_HALFK / 2 / BV0^2
+        const Field* B = F(b);
+        ctx->require(B, MLEGS_FFF, "CALC_BOUSSI_PE");
+        if (ctx->p.bv0 == 0.0) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_PE: BV0 = 0");
+        const Dims& d = ctx->d;
+        const size_t nmk = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
+        ctx->mark();
+        Field* W = ctx->tmp();
+        ctx->copy0(W, B, 0);
+        ctx->ln_zero(W);
+        ctx->rtran(W, 1, 0);
+        k_prodct_mk(ctx->g, W->data, nullptr, 1, 4.0 * 3.141592653589793238462643383279502884 * ctx->p.zlen * d.ELL2,
+                    ctx->diag, ctx->s);
+        ctx->rel(W);
+        ctx->restore();
+        std::vector<double> h(nmk);
+        CK(cudaMemcpyAsync(h.data(), ctx->diag, nmk * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        ctx->halfk(h.data(), 1.0, pe, false);
+        const size_t nout = (size_t)d.NTCHOP * d.NXCHOP;
+        for (size_t q = 0; q < nout; ++q) pe[q] = pe[q] / 2.0 / (ctx->p.bv0 * ctx->p.bv0);
     });
 }
 

@@ -349,6 +349,39 @@ void launch_vel2pln_fff(const DevGrid& g, double2* rup_fff, double* psi_ln, cons
     count_launch();
 }
 
+// PRODCT_MK_ALLK / L2NORM_MK_ALLK (mod_scalar3.f90:470-526, 750-806) before
+// their m = 0 halving: per (m, k) of PFF fields,
+//   mode 0: scale * sum_{r < NR} Re(A conj B)(r) w_r
+//   mode 1: scale * sum_{r < NR} |A(r)|^2 / (1 - x_r)^2 w_r
+// summed in r order like DOT_PRODUCT.  out: [m][k], NTCHOPDIM x NXCHOPDIM.
+__global__ void prodct_mk_kernel(DevGrid g, const double2* A, const double2* B, int mode, double scale,
+                                 double* out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.NTCHOPDIM * g.NXCHOPDIM) return;
+    const int k = t % g.NXCHOPDIM, m = t / g.NXCHOPDIM;
+    const size_t st = g.NXCHOPDIM, base = (size_t)m * g.NR * st + k;
+    double acc = 0.0;
+    if (mode == 0) {
+        for (int r = 0; r < g.NR; ++r) {
+            const double2 a = A[base + (size_t)r * st], b = B[base + (size_t)r * st];
+            acc += (a.x * b.x + a.y * b.y) * g.w[r];
+        }
+    } else {
+        for (int r = 0; r < g.NR; ++r) {
+            const double2 a = A[base + (size_t)r * st];
+            const double om = 1.0 - g.x[r];
+            acc += (a.x * a.x + a.y * a.y) / (om * om) * g.w[r];
+        }
+    }
+    out[t] = scale * acc;
+}
+void k_prodct_mk(const DevGrid& g, const double2* A, const double2* B, int mode, double scale, double* out,
+                 cudaStream_t s) {
+    const int n = g.NTCHOPDIM * g.NXCHOPDIM;
+    prodct_mk_kernel<<<(n + 127) / 128, 128, 0, s>>>(g, A, B, mode, scale, out);
+    count_launch();
+}
+
 // ------------------------------------------------------------ pointwise PPP
 // VPRODSUB + VDOTPSUB (+ linear terms of CALC_BOUSSI_FORCE when linear = 1).
 __global__ void force_pointwise_kernel(int nr, int plane, const double* rad, double2* rur, double2* rup,

@@ -193,6 +193,12 @@ void k_force_pointwise(const DevGrid& g, double2* rur, double2* rup, double2* uz
                        const double2* bz, double2* bn, const double2* bphys, double omega,
                        double bv0, int linear, cudaStream_t s);
 
+// Per-(m, k) quadratures of PFF fields (kernels.cu): mode 0 the PRODCT_MK_ALLK
+// sum of Re(A conj B) w, mode 1 the L2NORM_MK_ALLK sum of |A|^2 w / (1 - x)^2,
+// times scale, into out[m][k] (NTCHOPDIM x NXCHOPDIM, m = 0 not yet halved).
+void k_prodct_mk(const DevGrid& g, const double2* A, const double2* B, int mode, double scale, double* out,
+                 cudaStream_t s);
+
 // FFF-space updates.
 void k_axpby(double2* y, double a, const double2* x1, double b, const double2* x2, double c,
              size_t n, cudaStream_t s);

@@ -227,6 +227,29 @@ def test_project(env, mode):
     assert abs(lnp - P.LN) < 1e-12 * max(1.0, abs(P.LN))
 
 
+def test_boussi_energy(env):
+    """CALC_BOUSSI_ENERGY / CALC_BOUSSI_PE against the oracle (same formulas:
+    DELSQH, DEL2, RTRAN at CHOPSET(3), quadratures per (m, k), k folding)."""
+    from oracle import diagnostics as D
+    M, ctx, g, cfg = env
+    PSI, CHI, B = (random_fff(g, 40 + i, decay=4.0) for i in range(3))
+    PSI.LN, CHI.LN, B.LN = 0.3, -0.2, 0.0
+    fp, fc, fb = up(ctx, PSI), up(ctx, CHI), up(ctx, B)
+    ke, pe, dke = ctx.CALC_BOUSSI_ENERGY(fp, fc, fb)
+    KE, PE, DKE = D.boussi_energy(g, PSI, CHI, B, cfg.bv0)
+    assert ke.shape == KE.shape == (cfg.ntchop, cfg.nxchop)
+    for a, r_ in ((ke, KE), (pe, PE), (dke, DKE)):
+        assert rel(a, r_) < 1e-12
+    assert rel(ctx.CALC_BOUSSI_PE(fb), D.boussi_pe(g, B, cfg.bv0)) < 1e-12
+    # the inputs are left as they were
+    assert rel(fp.download()[0], PSI.E) == 0.0 and fp.download()[1] == PSI.LN
+    # B%LN /= 0 is the reference's SCALAR3_LOGTERM abort, an error code here
+    fb.upload(B.E, 0.5, M.FFF)
+    with pytest.raises(M.MlegsError) as ei:
+        ctx.CALC_BOUSSI_ENERGY(fp, fc, fb)
+    assert ei.value.code == 13
+
+
 def test_qvortex_on_device(env):
     M, ctx, g, cfg = env
     from oracle import layout

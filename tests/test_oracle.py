@@ -175,3 +175,23 @@ def test_inputs_deterministic():
     neg = np.r_[0, np.arange(a.shape[2] - 1, 0, -1)]
     assert np.allclose(a[:, 0, :], np.conj(a[:, 0, neg]))
     assert a[0, 0, 0] == 0
+
+
+def test_pe_matches_physical_integral():
+    """L2NORM_MK_HALFK / CALC_BOUSSI_PE summed over (m, k) equals the
+    physical-space integral of b^2 / (2 N^2) on the collocation grid
+    (Gauss weights with r dr = ELL^2 dx / (1 - x)^2, uniform theta and z)."""
+    from oracle import diagnostics as D
+    from oracle import transforms as T
+    cfg = small_cfg(32, 16, 16, adams=False)
+    g = oracle_grid(cfg)
+    B = random_fff(g, 5, decay=3.0)
+    bv0 = 2.0
+    pe = D.boussi_pe(g, B, bv0)
+    P = B.copy()
+    T.tofp(g, P)
+    f = T.physical_samples(g, P)
+    wr = g.ELL2 * g.W[:g.NR] / (1 - g.X[:g.NR]) ** 2
+    integ = np.einsum("i,isl->", wr, f * f) * (math.pi / g.NTH) * (g.ZLEN / g.NX)
+    assert abs(pe.sum() - integ / 2 / bv0 ** 2) < 1e-13 * integ
+    assert pe.shape == (g.NTCHOP, g.NXCHOP) and (pe >= 0).all()

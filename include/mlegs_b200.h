@@ -158,6 +158,18 @@ int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field
                        const mlegs_field* b, mlegs_field* psin, mlegs_field* chin,
                        mlegs_field* bn);
 
+/* Snapshots in the reference's files (mod_fft.f90:2224-2642), written and
+ * read by one process: global = 1 is MSAVEX / MLOADX (one Fortran unformatted
+ * file: sizes, chops, SPACE, LN, ZLEN, ELL, MINC, MKLINK, E); global = 0 is
+ * MPISAVEX / MPILOADX (path.info with the header records, path with E as raw
+ * COMPLEX(P8)).  E is the field in its space's reference layout.  Loading sets
+ * the field's space and LN from the file; array sizes that differ from this
+ * context's are MLEGS_ERR_DIMMISMATCH (the reference warns on ZLEN, ELL, MINC,
+ * MKLINK and chop mismatches and loads anyway; so does this).  Records over
+ * 2 GiB are not supported. */
+int mlegs_msave(mlegs_ctx* ctx, const mlegs_field* f, const char* path, int global);
+int mlegs_mload(mlegs_ctx* ctx, const char* path, mlegs_field* f, int global);
+
 /* Energy diagnostics.  CALC_BOUSSI_ENERGY(PSI, CHI, B) (mod_boussinesq.f90:139-232)
  * without its file output: ke, pe, dke (any may be NULL) receive KE, PE and DKE
  * per (m >= 0, k >= 0), NTCHOP x NXCHOP doubles each in Fortran order; the

@@ -11,6 +11,7 @@ loaded, construction fails.
 """
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -254,6 +255,16 @@ class Context:
         pe = self._mk_array()
         self._ck(self.lib.mlegs_boussi_pe(self.c, b.h, pe.ctypes.data_as(ctypes.c_void_p)))
         return pe.T.copy()
+
+    # ------------------------------------------------------------ snapshots
+    def MSAVE(self, f, path, glb=True):
+        """MSAVE0(A, FN, GLB) (mod_fft.f90:2224-2301): glb=True writes the global
+        MSAVEX file, glb=False the MPISAVEX pair FN.info + FN (one process)."""
+        self._ck(self.lib.mlegs_msave(self.c, f.h, os.fsencode(path), 1 if glb else 0))
+
+    def MLOAD(self, path, f, glb=True):
+        """MLOAD0(FN, A, GLB) (mod_fft.f90:2390-2633): loads E, SPACE and LN into f."""
+        self._ck(self.lib.mlegs_mload(self.c, os.fsencode(path), f.h, 1 if glb else 0))
 
     # ------------------------------------------------------------ solver
     def initialize(self, psi, chi, b):

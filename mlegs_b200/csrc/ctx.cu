@@ -1496,6 +1496,160 @@ int mlegs_field_download(mlegs_ctx* ctx, const mlegs_field* f, double* host, dou
     });
 }
 
+// ---------------------------------------------------------------- snapshots
+// The reference's snapshot files (mod_fft.f90:2224-2642), little-endian, for
+// one process:
+//   global (MSAVEX / MLOADX): one Fortran unformatted sequential file whose
+//     records are [NR NTH NX] [NRCHOP NTCHOP NXCHOP] [SPACE LN] [ZLEN ELL]
+//     [MINC MKLINK] [SIZE1 SIZE2 SIZE3] [E(:,:,:)], each framed by 4-byte
+//     length markers (INTEGER 4 bytes, REAL(P8) 8, COMPLEX(P8) 16);
+//   MPI form (MPISAVEX / MPILOADX): FN.info with the records [NDIMR NDIMTH
+//     NDIMX] [NRCHOPDIM NTCHOPDIM NXCHOPDIM] [SPACE LN] [ZLEN ELL]
+//     [MINC MKLINK], and FN holding E(:,:,:) as raw COMPLEX(P8), which for
+//     one process is the whole array in Fortran order.
+// E is the field in the reference's layout of its space (SALLOC shapes).
+extern "C++" {
+namespace {
+size_t ref_elems(const Dims& d, int space, int32_t sz[3]) {
+    if (space == MLEGS_FFF) { sz[0] = d.NRCHOPDIM; sz[1] = d.NTCHOPDIM; sz[2] = d.NXCHOPDIM; }
+    else if (space == MLEGS_PFF) { sz[0] = d.NDIMR; sz[1] = d.NTCHOPDIM; sz[2] = d.NXCHOPDIM; }
+    else { sz[0] = d.NDIMR; sz[1] = d.NDIMTH; sz[2] = d.NX; }
+    return (size_t)sz[0] * sz[1] * sz[2];
+}
+struct Bytes {
+    std::vector<unsigned char> b;
+    template <class T>
+    void put(T v) {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+        b.insert(b.end(), p, p + sizeof(T));
+    }
+};
+void write_record(FILE* fp, const void* data, size_t n) {
+    if (n > 0x7fffffffu) throw ApiError(MLEGS_ERR_ARG, "snapshot: records over 2 GiB are not supported");
+    const int32_t len = (int32_t)n;
+    if (fwrite(&len, 4, 1, fp) != 1 || (n && fwrite(data, 1, n, fp) != n) || fwrite(&len, 4, 1, fp) != 1)
+        throw ApiError(MLEGS_ERR_ARG, "snapshot: write failed");
+}
+std::vector<unsigned char> read_record(FILE* fp, size_t expect) {
+    int32_t len = 0, tail = 0;
+    if (fread(&len, 4, 1, fp) != 1 || len < 0) throw ApiError(MLEGS_ERR_ARG, "snapshot: bad record marker");
+    std::vector<unsigned char> v((size_t)len);
+    if ((len && fread(v.data(), 1, (size_t)len, fp) != (size_t)len) || fread(&tail, 4, 1, fp) != 1 || tail != len)
+        throw ApiError(MLEGS_ERR_ARG, "snapshot: truncated record");
+    if (expect && (size_t)len != expect) throw ApiError(MLEGS_ERR_ARG, "snapshot: unexpected record length");
+    return v;
+}
+template <class T>
+T get_at(const std::vector<unsigned char>& v, size_t off) {
+    T x;
+    std::memcpy(&x, v.data() + off, sizeof(T));
+    return x;
+}
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() {
+        if (f) fclose(f);
+    }
+};
+}  // namespace
+}  // extern "C++"
+
+int mlegs_msave(mlegs_ctx* ctx, const mlegs_field* f, const char* path, int global) {
+    if (!f || !path) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        const Dims& d = ctx->d;
+        int32_t sz[3];
+        const int space = F(f)->space;
+        std::vector<double> host(2 * ref_elems(d, space, sz));
+        double ln = 0.0;
+        const int rc = mlegs_field_download(ctx, f, host.data(), &ln);
+        if (rc) throw ApiError(rc, ctx->err);
+        const std::string fn(path);
+        FileCloser hdr{fopen(global ? fn.c_str() : (fn + ".info").c_str(), "wb")};
+        if (!hdr.f) throw ApiError(MLEGS_ERR_ARG, "snapshot: cannot open " + fn);
+        auto rec3 = [&](int32_t a, int32_t b, int32_t c) {
+            Bytes r;
+            r.put(a);
+            r.put(b);
+            r.put(c);
+            write_record(hdr.f, r.b.data(), r.b.size());
+        };
+        if (global) {
+            rec3(d.NR, d.NTH, d.NX);
+            rec3(d.NRCHOP, d.NTCHOP, d.NXCHOP);
+        } else {
+            rec3(d.NDIMR, d.NDIMTH, d.NX);
+            rec3(d.NRCHOPDIM, d.NTCHOPDIM, d.NXCHOPDIM);
+        }
+        {
+            Bytes r;
+            r.put((int32_t)space);
+            r.put(ln);
+            write_record(hdr.f, r.b.data(), r.b.size());
+        }
+        {
+            Bytes r;
+            r.put(ctx->p.zlen);
+            r.put(ctx->p.ell);
+            write_record(hdr.f, r.b.data(), r.b.size());
+        }
+        {
+            Bytes r;
+            r.put((int32_t)1);  // MINC
+            r.put((int32_t)0);  // MKLINK
+            write_record(hdr.f, r.b.data(), r.b.size());
+        }
+        const size_t nbytes = host.size() * sizeof(double);
+        if (global) {
+            rec3(sz[0], sz[1], sz[2]);
+            write_record(hdr.f, host.data(), nbytes);
+        } else {
+            FileCloser raw{fopen(fn.c_str(), "wb")};
+            if (!raw.f) throw ApiError(MLEGS_ERR_ARG, "snapshot: cannot open " + fn);
+            if (fwrite(host.data(), 1, nbytes, raw.f) != nbytes) throw ApiError(MLEGS_ERR_ARG, "snapshot: write failed");
+        }
+    });
+}
+
+int mlegs_mload(mlegs_ctx* ctx, const char* path, mlegs_field* f, int global) {
+    if (!f || !path) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        const Dims& d = ctx->d;
+        const std::string fn(path);
+        FileCloser hdr{fopen(global ? fn.c_str() : (fn + ".info").c_str(), "rb")};
+        if (!hdr.f) throw ApiError(MLEGS_ERR_ARG, "snapshot: cannot open " + fn);
+        read_record(hdr.f, 12);  // NR NTH NX (global) or NDIMR NDIMTH NDIMX
+        read_record(hdr.f, 12);  // chops or chop dims
+        const auto sl = read_record(hdr.f, 12);
+        const int space = get_at<int32_t>(sl, 0);
+        const double ln = get_at<double>(sl, 4);
+        read_record(hdr.f, 16);  // ZLEN ELL: the reference only warns on a mismatch
+        read_record(hdr.f, 8);   // MINC MKLINK: likewise
+        if (space < 0 || space > 3) throw ApiError(MLEGS_ERR_TRANSFORM, "snapshot: unknown SPACE");
+        int32_t sz[3];
+        const size_t n = ref_elems(d, space, sz);
+        std::vector<double> host(2 * n);
+        if (global) {
+            const auto s3 = read_record(hdr.f, 12);
+            if (get_at<int32_t>(s3, 0) != sz[0] || get_at<int32_t>(s3, 4) != sz[1] || get_at<int32_t>(s3, 8) != sz[2])
+                throw ApiError(MLEGS_ERR_DIMMISMATCH, "snapshot: array sizes differ from this context's");
+            const auto e = read_record(hdr.f, n * 16);
+            std::memcpy(host.data(), e.data(), n * 16);
+        } else {
+            FileCloser raw{fopen(fn.c_str(), "rb")};
+            if (!raw.f) throw ApiError(MLEGS_ERR_ARG, "snapshot: cannot open " + fn);
+            if (fread(host.data(), 1, n * 16, raw.f) != n * 16)
+                throw ApiError(MLEGS_ERR_DIMMISMATCH, "snapshot: raw file shorter than this context's array");
+            unsigned char extra;
+            if (fread(&extra, 1, 1, raw.f) == 1)
+                throw ApiError(MLEGS_ERR_DIMMISMATCH,
+                               "snapshot: raw file longer than this context's array (several writers?)");
+        }
+        const int rc = mlegs_field_upload(ctx, f, space, host.data(), ln);
+        if (rc) throw ApiError(rc, ctx->err);
+    });
+}
+
 int mlegs_field_copy(mlegs_ctx* ctx, mlegs_field* dst, const mlegs_field* src, int pad) {
     return guard(ctx, [&] {
         check_pad(ctx, pad);

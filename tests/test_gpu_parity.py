@@ -250,6 +250,42 @@ def test_boussi_energy(env):
     assert ei.value.code == 13
 
 
+def test_snapshot_files(env, tmp_path):
+    """MSAVE / MLOAD through the C ABI against the oracle's restatement of
+    the reference's file formats, both forms, bit for bit."""
+    from oracle import snapshot as S
+    from oracle import transforms as T
+    from oracle.grid import Grid
+    M, ctx, g, cfg = env
+    A = random_fff(g, 50)
+    A.LN = -0.375
+    f = up(ctx, A)
+    for glb in (True, False):
+        p = str(tmp_path / ("fff_%d.dat" % glb))
+        ctx.MSAVE(f, p, glb)
+        E, sp, ln, _ = S.mload(p, glb, shape=A.E.shape)
+        assert sp == M.FFF and ln == A.LN and np.array_equal(E, A.E)
+    # a PFF field written by the oracle, loaded into a field that was FFF
+    P = random_fff(g, 51)
+    T.rtran(g, P, 1)
+    P.LN = 0.0
+    for glb in (True, False):
+        p = str(tmp_path / ("pff_%d.dat" % glb))
+        S.msave(p, g, P, glb)
+        h = ctx.field(M.FFF)
+        ctx.MLOAD(p, h, glb)
+        E, ln = h.download()
+        assert h.space == M.PFF and ln == 0.0 and np.array_equal(E, P.E)
+    # a file from another grid is a dimension mismatch (code 32)
+    g2 = Grid(cfg.nr * 2, cfg.nth, cfg.nx, cfg.nrchop * 2, cfg.ntchop, cfg.nxchop, cfg.ell, cfg.zlen)
+    B2 = g2.alloc()
+    p = str(tmp_path / "other.dat")
+    S.msave(p, g2, B2, True)
+    with pytest.raises(M.MlegsError) as ei:
+        ctx.MLOAD(p, f, True)
+    assert ei.value.code == 32
+
+
 def test_qvortex_on_device(env):
     M, ctx, g, cfg = env
     from oracle import layout

@@ -195,3 +195,31 @@ def test_pe_matches_physical_integral():
     integ = np.einsum("i,isl->", wr, f * f) * (math.pi / g.NTH) * (g.ZLEN / g.NX)
     assert abs(pe.sum() - integ / 2 / bv0 ** 2) < 1e-13 * integ
     assert pe.shape == (g.NTCHOP, g.NXCHOP) and (pe >= 0).all()
+
+
+def test_snapshot_record_layout(tmp_path):
+    """MSAVEX / MPISAVEX restated: the record list and byte layout the
+    reference's reader (tests/postproc/read_binary_info.ipynb) expects, and a
+    round trip of both forms."""
+    import struct
+    from oracle import snapshot as S
+    cfg = small_cfg(32, 16, 16)
+    g = oracle_grid(cfg)
+    A = random_fff(g, 9)
+    A.LN = 0.125
+    p = str(tmp_path / "a.dat")
+    S.msave(p, g, A, glb=True)
+    raw = open(p, "rb").read()
+    assert struct.unpack("<iiiii", raw[:20]) == (12, g.NR, g.NTH, g.NX, 12)
+    off = 20 + 20  # second record: chops
+    assert struct.unpack("<iiiii", raw[20:40]) == (12, g.NRCHOP, g.NTCHOP, g.NXCHOP, 12)
+    assert struct.unpack("<iidi", raw[off:off + 20]) == (12, A.space, A.LN, 12)
+    E, sp, ln, hdr = S.mload(p, glb=True)
+    assert sp == A.space and ln == A.LN and np.array_equal(E, A.E)
+    assert hdr["minc"] == 1 and hdr["mklink"] == 0 and hdr["zlen"] == g.ZLEN
+    q = str(tmp_path / "b.dat")
+    S.msave(q, g, A, glb=False)
+    assert len(open(q, "rb").read()) == A.E.size * 16
+    E2, sp2, ln2, hdr2 = S.mload(q, glb=False, shape=A.E.shape)
+    assert np.array_equal(E2, A.E) and sp2 == A.space and ln2 == A.LN
+    assert hdr2["dims"] == (g.NDIMR, g.NDIMTH, g.NDIMX)

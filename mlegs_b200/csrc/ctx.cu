@@ -482,7 +482,7 @@ struct mlegs_ctx {
     void energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke);
     void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
-                Field* BN, cudaEvent_t vor_ready = nullptr);
+                Field* BN, cudaEvent_t vor_ready = nullptr, Field* PSIN = nullptr, Field* CHIN = nullptr);
     void visc1(Field* A, double nu, double dt);
     void visc2(Field* A, const Field* AO, double nu, double dt);
     void visc_be(Field* P, Field* C, Field* B, double dt);
@@ -996,7 +996,7 @@ void mlegs_ctx::energy(const Field* PSI, const Field* CHI, const Field* B, doubl
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
 // On exit ROR, ROP, OZ hold the projected u x omega in velocity form (FFF).
 void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
-                       Field* BN, cudaEvent_t vor_ready) {
+                       Field* BN, cudaEvent_t vor_ready, Field* PSIN, Field* CHIN) {
     Field *RBR = tmp(), *RBP = tmp(), *BZ = tmp();
     // GRAD(B) on s2, beside the first RTRAN(+1) GEMMs on s; ROR, ROP, OZ may
     // still be in the making on s2 (vor_ready)
@@ -1035,11 +1035,15 @@ void mlegs_ctx::nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field*
     BN->space = MLEGS_FFF;
     cudaEvent_t eb = next_event();
     CK(cudaEventRecord(eb, s2));
-    Field *PSI = tmp(), *W = tmp(), *CHI = tmp();
+    // PSIN, CHIN given: the projected (PSI, CHI) are returned there and the
+    // final PC2VEL into (ROR, ROP, OZ) is left to the caller's ETD kernel
+    Field *PSI = PSIN ? PSIN : tmp(), *W = tmp(), *CHI = CHIN ? CHIN : tmp();
     project(NR, NP, NZ, PSI, W, 1, 0.0);
     idel2(W, CHI, 0, 0.0, 0);
-    pc2vel(PSI, CHI, ROR, ROP, OZ, 3);
-    for (Field* f : {PSI, W, CHI, NR, NP, NZ}) rel(f);
+    if (!PSIN) pc2vel(PSI, CHI, ROR, ROP, OZ, 3);
+    for (Field* f : {W, NR, NP, NZ}) rel(f);
+    if (!PSIN) rel(PSI);
+    if (!CHIN) rel(CHI);
     CK(cudaStreamWaitEvent(s, eb, 0));
 }
 
@@ -1268,7 +1272,8 @@ void mlegs_ctx::step_etdab_cn() {
     pc2vor(psi, chi, RORN, ROPN, OZN, 3, s2);
     cudaEvent_t ev = next_event();
     CK(cudaEventRecord(ev, s2));
-    nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN, ev);
+    Field *PN = tmp(), *CN = tmp();  // projected nonlinear terms as (PSI_N, CHI_N)
+    nonlin(b, RURN, RUPN, UZN, RORN, ROPN, OZN, BN, ev, PN, CN);
     EtdAbArgs a{};
     a.E = etdE;
     a.N = etdN;
@@ -1286,9 +1291,10 @@ void mlegs_ctx::step_etdab_cn() {
     a.rup = RUPN->data;
     a.uz = UZN->data;
     a.b = b->data;
-    a.ror = RORN->data;
-    a.rop = ROPN->data;
-    a.oz = OZN->data;
+    a.npsi = PN->data;
+    a.nchi = CN->data;
+    a.npsi_ln = PN->ln;
+    a.nchi_ln = CN->ln;
     a.bn = BN->data;
     for (int q = 0; q < 7; ++q) a.hist[q] = hist[q]->data;
     a.out_ln[0] = RURN->ln;
@@ -1296,6 +1302,8 @@ void mlegs_ctx::step_etdab_cn() {
     a.out_ln[2] = UZN->ln;
     k_etd_ab_fused(g, a, s);
     RURN->space = RUPN->space = UZN->space = MLEGS_FFF;
+    rel(CN);
+    rel(PN);
     rel(BN);
     rel(RORN);
     rel(ROPN);

@@ -867,11 +867,29 @@ __global__ void pc2vor_fused_kernel(DevGrid g, const double2* psi, const double*
 
 // The coefficient update of STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901) from
 // the projected nonlinear terms to the new state, in one pass per FFF entry:
-//   HYPERV of the nonlinear terms (1352-1416, at TF = 1, chopped at pad 0),
+//   HYPERV of the nonlinear terms (1352-1416, at TF = 1, chopped at pad 0;
+//   given as ROR, ROP, OZ, or formed here as PC2VEL of the projected PSI_N,
+//   CHI_N, the last step of CALC_BOUSSI_NONLIN),
 //   PC2VEL(PSI, CHI) at pad 3 (mod_legops.f90:1789-1853),
 //   CALC_BOUSSI_ETDAB_SUB (1050-1139), HYPERV of the updated (RUR, RUP, UZ, B),
 //   and the history update N_* <- the filtered nonlinear terms, R_PI_* <- the
 //   filtered velocity.  hyper = 0 (VISC%SW /= 3) skips both filters.
+// PC2VEL (mod_legops.f90:1789-1853) of (psi, chi) at one FFF entry (m, n, k).
+__device__ __forceinline__ void pc2vel_at(const DevGrid& g, int m, int n, int k, const double2* psi, double lp,
+                                          const double2* chi, double lc, int pad, double2 (&u)[3]) {
+    const Col cp = column(g, psi, m, k, pad), cc = column(g, chi, m, k, pad);
+    u[0] = u[1] = u[2] = make_double2(0.0, 0.0);
+    if (n < cp.nn) {
+        const double mv = (double)m, kv = g.ak[k];
+        const double2 ps = cp.p[(size_t)n * cp.st], ch = cc.p[(size_t)n * cc.st];
+        const double2 xc = xxdx_row(g, m, k, cc, n, lc);
+        const double2 xp = xxdx_row(g, m, k, cp, n, lp);
+        u[0] = cadd(cmuli(ps, mv), cmuli(xc, kv));
+        u[1] = make_double2(-xp.x - (mv * kv) * ch.x, -xp.y - (mv * kv) * ch.y);
+        u[2] = neg_xm2_delsqh(g, m, k, cc, n, lc);
+    }
+}
+
 __global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     int m, n, k;
@@ -887,19 +905,19 @@ __global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
         }
     }
     // PC2VEL(PSI, CHI) at pad 3
-    const Col cp = column(g, a.psi, m, k, 3), cc = column(g, a.chi, m, k, 3);
-    double2 u0 = make_double2(0.0, 0.0), u1 = u0, u2 = u0;
-    if (n < cp.nn) {
-        const double lp = *a.psi_ln, lc = *a.chi_ln;
-        const double mv = (double)m, kv = g.ak[k];
-        const double2 ps = cp.p[(size_t)n * cp.st], ch = cc.p[(size_t)n * cc.st];
-        const double2 xc = xxdx_row(g, m, k, cc, n, lc);
-        const double2 xp = xxdx_row(g, m, k, cp, n, lp);
-        u0 = cadd(cmuli(ps, mv), cmuli(xc, kv));
-        u1 = make_double2(-xp.x - (mv * kv) * ch.x, -xp.y - (mv * kv) * ch.y);
-        u2 = neg_xm2_delsqh(g, m, k, cc, n, lc);
+    double2 u[3];
+    pc2vel_at(g, m, n, k, a.psi, *a.psi_ln, a.chi, *a.chi_ln, 3, u);
+    const double2 u0 = u[0], u1 = u[1], u2 = u[2];
+    // the projected nonlinear terms in velocity form: read, or PC2VEL of (PSI_N, CHI_N) here
+    double2 w[3];
+    if (a.npsi) {
+        pc2vel_at(g, m, n, k, a.npsi, *a.npsi_ln, a.nchi, *a.nchi_ln, 3, w);
+    } else {
+        w[0] = a.ror[t];
+        w[1] = a.rop[t];
+        w[2] = a.oz[t];
     }
-    const double2 rn[4] = {cscale(a.ror[t], fv), cscale(a.rop[t], fv), cscale(a.oz[t], fv), cscale(a.bn[t], fd)};
+    const double2 rn[4] = {cscale(w[0], fv), cscale(w[1], fv), cscale(w[2], fv), cscale(a.bn[t], fd)};
     double E[16], N[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) {

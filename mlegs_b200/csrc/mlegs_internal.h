@@ -227,9 +227,13 @@ struct EtdAbArgs {
     double2* rup;
     double2* uz;
     double2* b;             // in/out
-    const double2* ror;     // projected nonlinear terms of this step
+    const double2* ror;     // projected nonlinear terms of this step (used when npsi is null)
     const double2* rop;
     const double2* oz;
+    const double2* npsi;    // or: their PSI_N, CHI_N (FFF), PC2VEL formed in the kernel
+    const double2* nchi;
+    const double* npsi_ln;
+    const double* nchi_ln;
     const double2* bn;
     double2* hist[7];       // in/out: 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z
     double* out_ln[3];      // LN slots of rur, rup, uz: set to 0 (PC2VEL outputs carry no log term)

@@ -75,6 +75,9 @@ typedef struct mlegs_params {
     int32_t precision;                /* MLEGS_PREC_*                              */
     int32_t split_slices;             /* slices per operand for MLEGS_PREC_SPLIT   */
     int32_t device;                   /* CUDA device ordinal                        */
+    int32_t rmv_sw;                   /* REMOVE SW: 2 turns on the axial sponge of the
+                                         ETD steps (CALC_BOUSSI_ETD_SPONGE); 0 or 1
+                                         leave the step as it is                      */
 } mlegs_params;
 
 typedef struct mlegs_ctx mlegs_ctx;

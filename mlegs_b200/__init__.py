@@ -84,6 +84,7 @@ class Context:
         p.visc_sw, p.visc_p = cfg.visc_sw, cfg.p
         p.nu, p.nup = cfg.nu, cfg.nup
         p.precision, p.split_slices, p.device = precision, split_slices, device
+        p.rmv_sw = int(getattr(cfg, "rmv_sw", 0))
         h = ctypes.c_void_p()
         rc = self.lib.mlegs_create(ctypes.byref(p), ctypes.byref(h))
         if rc != 0:

@@ -32,7 +32,7 @@ class Params(ctypes.Structure):
         ("visc_sw", ctypes.c_int32), ("visc_p", ctypes.c_int32),
         ("nu", c_double), ("nup", c_double),
         ("precision", ctypes.c_int32), ("split_slices", ctypes.c_int32),
-        ("device", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("rmv_sw", ctypes.c_int32),
     ]
 
 

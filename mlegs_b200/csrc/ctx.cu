@@ -84,6 +84,7 @@ struct mlegs_ctx {
     double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
     double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
     double* diag = nullptr;                                         // 4 x [m][k] quadratures (energy)
+    double *sp_damp = nullptr, *sp_damp_h = nullptr;                // sponge factors for DT and DT/2 (RMV%SW = 2)
     double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
     FFTPlan fft;
     std::vector<double> h_x, h_w, h_lognorm;
@@ -489,6 +490,7 @@ struct mlegs_ctx {
     void visc_cn(Field* P, Field* C, Field* B, const Field* PO, const Field* CO, const Field* BO);
     void hyperv3(Field* P, Field* C, Field* B, double tf);
     void etd_hyperv(Field* R, Field* Pp, Field* Z, Field* B, double tf);
+    void sponge(Field* UZ, Field* B, double dt);
     void rich_fe_be();
     void step_ab_cn();
     void etdfe_be(Field* P, Field* C, Field* B, const double* E, const double* NL, double dt, bool store);
@@ -690,6 +692,23 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     T = dalloc<double>(vsz);
     k_tables_project(g, V, D, T, 0, s);
     diag = dalloc<double>((size_t)4 * d.NTCHOPDIM * d.NXCHOPDIM);
+    if (p.rmv_sw == 2 && !p.adams) {
+        // SPNGINIT (mod_march.f90:2292-2323): N_TAU = 10, RATIO_L = 0.86,
+        // RATIO_S = 0.04; T(z) = TOPHAT(Z - ZLEN/2, ZLEN RATIO_L/2, ZLEN RATIO_S)
+        // (3704-3712); the damping over DT is exp(-(1 - T(z))/TAU DT), TAU = N_TAU DT
+        const double hw = p.zlen * 0.86 / 2.0, st = p.zlen * 0.04, tau = 10 * p.dt;
+        auto damp = [&](double dt) {
+            std::vector<double> h(d.NX);
+            for (int q = 0; q < d.NX; ++q) {
+                const double z = p.zlen * q / d.NX - p.zlen / 2.0;
+                const double th = 0.5 * (std::tanh((z + hw) / st) - std::tanh((z - hw) / st));
+                h[q] = std::exp(-(1.0 - th) / tau * dt);
+            }
+            return up(h);
+        };
+        sp_damp = damp(p.dt);
+        sp_damp_h = damp(p.dt * 0.5);
+    }
     v2p_pff = dalloc<double>(d.NR);
     v2p_fff = dalloc<double>(std::max(d.NRCHOP, 1));
     k_vel2pln_coef(g, explog0, d.NRCHOP, v2p_pff, v2p_fff, s);
@@ -1097,6 +1116,23 @@ void mlegs_ctx::etd_hyperv(Field* R, Field* Pp, Field* Z, Field* B, double tf) {
     k_hyperv(g, B->data, hd[0], hd[1], hd[2], tf, 0, s);
 }
 
+// CALC_BOUSSI_ETD_SPONGE(UZ, B, DT), mod_march.f90:1436-1469: UZ and B to PFP
+// (RTRAN, VERFFT), damped per z-plane with the m = 0 modes made real, back to
+// FFF (TOFF) at the current chop.  The state field B's buffer is swapped an
+// even number of times, so it ends in its own buffer.
+void mlegs_ctx::sponge(Field* UZ, Field* B, double dt) {
+    if (p.rmv_sw != 2 || p.adams) return;
+    const double* damp = (dt == p.dt) ? sp_damp : (dt == p.dt * 0.5 ? sp_damp_h : nullptr);
+    if (!damp) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_ETD_SPONGE: DT other than TIM%DT or TIM%DT/2");
+    for (Field* f : {UZ, B}) {
+        require(f, MLEGS_FFF, "SPONGE: INPUT MUST BE IN FFF_SPACE");
+        rtran(f, 1, 0);
+        verfft(f, 1);
+        k_sponge(g, f->data, damp, s);
+        toff(f, 0);
+    }
+}
+
 // RICH_BOUSSI_FE_BE (mod_march.f90:535-606).  hist: 0 N_PSI, 1 N_CHI, 2 N_B.
 void mlegs_ctx::rich_fe_be() {
     const double dt = p.dt, hdt = dt * 0.5;
@@ -1186,6 +1222,7 @@ void mlegs_ctx::etdfe_be(Field* P, Field* C, Field* B, const double* E, const do
     pc2vel(P, C, RURN, RUPN, UZN, 3);
     k_etd(g, E, NL, dt, 0, RURN->data, RUPN->data, UZN->data, B->data, RORN->data, ROPN->data, OZN->data,
           BN->data, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, s);
+    sponge(UZN, B, dt);
     etd_hyperv(RURN, RUPN, UZN, B, dt / p.dt);
     if (store) {
         const size_t N = fff();
@@ -1300,8 +1337,18 @@ void mlegs_ctx::step_etdab_cn() {
     a.out_ln[0] = RURN->ln;
     a.out_ln[1] = RUPN->ln;
     a.out_ln[2] = UZN->ln;
+    const bool sp = (p.rmv_sw == 2);
+    a.raw_out = sp ? 1 : 0;
     k_etd_ab_fused(g, a, s);
     RURN->space = RUPN->space = UZN->space = MLEGS_FFF;
+    if (sp) {  // CALC_BOUSSI_ETD_SPONGE, then the filters and R_PI_* (mod_march.f90:864-866)
+        sponge(UZN, b, dt);
+        etd_hyperv(RURN, RUPN, UZN, b, 1.0);
+        const size_t N = fff();
+        k_copy(hist[4]->data, RURN->data, N, s);
+        k_copy(hist[5]->data, RUPN->data, N, s);
+        k_copy(hist[6]->data, UZN->data, N, s);
+    }
     rel(CN);
     rel(PN);
     rel(BN);

@@ -947,7 +947,7 @@ __global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
             y.x += N[i * 4 + j] * av.x;
             y.y += N[i * 4 + j] * av.y;
         }
-        cv[i] = cscale(cadd(x, y), i < 3 ? fv : fd);
+        cv[i] = a.raw_out ? cadd(x, y) : cscale(cadd(x, y), i < 3 ? fv : fd);
     }
     a.rur[t] = cv[0];
     a.rup[t] = cv[1];
@@ -957,9 +957,28 @@ __global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
     a.hist[1][t] = rn[0];
     a.hist[2][t] = rn[1];
     a.hist[3][t] = rn[2];
-    a.hist[4][t] = cv[0];
-    a.hist[5][t] = cv[1];
-    a.hist[6][t] = cv[2];
+    if (!a.raw_out) {
+        a.hist[4][t] = cv[0];
+        a.hist[5][t] = cv[1];
+        a.hist[6][t] = cv[2];
+    }
+}
+
+// The damping of CALC_BOUSSI_ETD_SPONGE (mod_march.f90:1455-1464) on a PFP
+// field ([r][z][m]): every z-plane times damp[z], the m = 0 modes made real.
+__global__ void sponge_kernel(DevGrid g, double2* a, const double* damp) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t md = g.NTCHOPDIM, total = (size_t)g.NR * g.NX * md;
+    if (t >= total) return;
+    const int m = (int)(t % md), z = (int)((t / md) % g.NX);
+    double2 v = cscale(a[t], damp[z]);
+    if (m == 0) v.y = 0.0;
+    a[t] = v;
+}
+void k_sponge(const DevGrid& g, double2* a, const double* damp, cudaStream_t s) {
+    const size_t n = (size_t)g.NR * g.NX * g.NTCHOPDIM;
+    sponge_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, damp);
+    count_launch();
 }
 
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s) {

@@ -237,7 +237,10 @@ struct EtdAbArgs {
     const double2* bn;
     double2* hist[7];       // in/out: 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z
     double* out_ln[3];      // LN slots of rur, rup, uz: set to 0 (PC2VEL outputs carry no log term)
+    int raw_out;            // 1: outputs unfiltered and R_PI_* not written (the sponge comes between)
 };
+// CALC_BOUSSI_ETD_SPONGE's damping of one PFP field by damp[z] (NX entries).
+void k_sponge(const DevGrid& g, double2* a, const double* damp, cudaStream_t s);
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);
 void k_hyperv(const DevGrid& g, double2* a, const double* hr, const double* ht, const double* hx,
               double tf, int pad, cudaStream_t s);

@@ -45,6 +45,7 @@ class Config:
     nup: float = 0.0
     kappap: float = 0.0
     p: int = 2
+    rmv_sw: int = 0          # REMOVE SW (2: axial sponge in the ETD steps)
     amp: float = 1e-3
     mmax: int = 4
     kmax: int = 4

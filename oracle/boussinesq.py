@@ -33,7 +33,7 @@ import numpy as np
 from .grid import FFF, PPP
 from .legops import (del2, grad, idel2, idel2ln, ihelm, pc2vel, pc2vor, project,
                      vdotpsub, vprodsub)
-from .transforms import toff, tofp
+from .transforms import rtran, toff, tofp, verfft
 
 
 @dataclass
@@ -49,6 +49,7 @@ class Physics:
     nu: float = 0.0
     nup: float = 0.0
     p: int = 2
+    rmv_sw: int = 0
 
 
 # ----------------------------------------------------------------------
@@ -410,6 +411,27 @@ class Solver:
         self.psi, self.chi, self.b = PSI, CHI, B
 
     # -- ETD2AB-CN ----------------------------------------------------
+    def _etd_sponge(self, UZ, B, dt):
+        """CALC_BOUSSI_ETD_SPONGE(UZ, B, DT), mod_march.f90:1436-1469, with the
+        SPNGINIT profile (2292-2323): N_TAU = 10, RATIO_L = 0.86, RATIO_S = 0.04;
+        each z-plane of UZ and B in PFP is scaled by exp(-(1 - T(z))/TAU DT),
+        T = TOPHAT(Z - ZLEN/2, ZLEN RATIO_L/2, ZLEN RATIO_S) (3704-3712); the
+        m = 0 modes are made real; both go back to FFF."""
+        if self.ph.rmv_sw != 2:
+            return
+        g = self.g
+        z = g.Z[:g.NX] - g.ZLEN / 2.0
+        hw, st = g.ZLEN * 0.86 / 2.0, g.ZLEN * 0.04
+        tophat = 0.5 * (np.tanh((z + hw) / st) - np.tanh((z - hw) / st))
+        tau = 10 * self.ph.dt
+        damp = np.exp(-(1.0 - tophat) / tau * dt)
+        for F in (UZ, B):
+            rtran(g, F, 1)
+            verfft(g, F, 1)
+            F.E[:, :, :g.NX] *= damp[None, None, :]
+            F.E[:, 0, :] = F.E[:, 0, :].real
+            toff(g, F)
+
     def _etdfe_be(self, PSI, CHI, B, E, NL, dt, store):
         """STEP_BOUSSI_ETDFE_BE, mod_march.f90:664-753 (returns new PSI, CHI)."""
         g = self.g
@@ -423,6 +445,7 @@ class Solver:
         RURN, RUPN, UZN = pc2vel(g, PSI, CHI)
         g.chopset(-3)
         calc_boussi_etdfe_sub(E, NL, B, RURN, RUPN, UZN, BN, RORN, ROPN, OZN, dt)
+        self._etd_sponge(UZN, B, dt)
         self._etd_hyperv(RURN, RUPN, UZN, B, dt)
         if store:
             self.n_b = BN.copy()
@@ -481,6 +504,7 @@ class Solver:
         calc_boussi_etdab_sub(self, B, RURN, RUPN, UZN, BN, RORN, ROPN, OZN, dt)
         self.n_b = BN.copy()
         self.r_n_r, self.r_n_p, self.n_z = RORN.copy(), ROPN.copy(), OZN.copy()
+        self._etd_sponge(UZN, B, dt)
         self._etd_hyperv(RURN, RUPN, UZN, B, dt)
         self.r_pi_r, self.r_pi_p, self.pi_z = RURN.copy(), RUPN.copy(), UZN.copy()
         PSI0, CHI0 = g.copy0(PSI), g.copy0(CHI)

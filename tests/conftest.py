@@ -57,7 +57,8 @@ def oracle_grid(cfg):
 def oracle_physics(cfg):
     from oracle.boussinesq import Physics
     return Physics(dt=cfg.dt, omega=cfg.omega, bv0=cfg.bv0, kappa=cfg.kappa, kappap=cfg.kappap,
-                   adams=cfg.adams, visc_sw=cfg.visc_sw, nu=cfg.nu, nup=cfg.nup, p=cfg.p)
+                   adams=cfg.adams, visc_sw=cfg.visc_sw, nu=cfg.nu, nup=cfg.nup, p=cfg.p,
+                   rmv_sw=getattr(cfg, "rmv_sw", 0))
 
 
 def random_fff(g, seed, decay=6.0, pad=0, hermitian=True):

@@ -361,6 +361,17 @@ def test_steps_small(lib_built, adams):
         assert abs(ln - R.LN) < 1e-10 * max(1.0, abs(R.LN))
 
 
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_etd_steps_with_sponge(lib_built, graph):
+    """REMOVE SW = 2: CALC_BOUSSI_ETD_SPONGE in the Richardson start-up and the
+    steady ETD steps (the unfused update, sponge, filters, history path)."""
+    cfg = small_cfg(32, 16, 16, adams=False, rmv_sw=2)
+    out, ref = _run_pair(cfg, 6, graph=graph)
+    for (E, ln), R in zip(out, ref):
+        assert rel(E, R.E) < 1e-10
+        assert abs(ln - R.LN) < 1e-10 * max(1.0, abs(R.LN))
+
+
 def test_ab2_config_100_steps(lib_built):
     """The AB2-CN IVP configuration, 1 Richardson + 99 AB2 steps, <= 1e-9 per field."""
     from mlegs_b200.inputs import CONFIGS

@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 import scipy.linalg as sl
 
-from conftest import oracle_grid, random_fff, rel, small_cfg
+from conftest import oracle_grid, oracle_physics, random_fff, rel, small_cfg
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "legendre_golden.npz")
 
@@ -223,3 +223,32 @@ def test_snapshot_record_layout(tmp_path):
     E2, sp2, ln2, hdr2 = S.mload(q, glb=False, shape=A.E.shape)
     assert np.array_equal(E2, A.E) and sp2 == A.space and ln2 == A.LN
     assert hdr2["dims"] == (g.NDIMR, g.NDIMTH, g.NDIMX)
+
+
+def test_sponge_profile_and_k0_kat():
+    """CALC_BOUSSI_ETD_SPONGE restated: the damping is 1 in the middle of the
+    axial domain, symmetric, and between exp(-DT/TAU) = exp(-0.1) and 1
+    (TAU = 10 DT), strongest at the ends; a
+    field with only k = 0 content keeps its k = 0 coefficients scaled by the
+    z-average of the damping (the m = 0 modes real)."""
+    from oracle import boussinesq as BQ
+    cfg = small_cfg(32, 16, 16, adams=False, rmv_sw=2)
+    g = oracle_grid(cfg)
+    ph = oracle_physics(cfg)
+    s = BQ.Solver.__new__(BQ.Solver)
+    s.g, s.ph = g, ph
+    z = g.Z[:g.NX] - g.ZLEN / 2.0
+    hw, st = g.ZLEN * 0.86 / 2.0, g.ZLEN * 0.04
+    damp = np.exp(-(1.0 - 0.5 * (np.tanh((z + hw) / st) - np.tanh((z - hw) / st))) / (10 * ph.dt) * ph.dt)
+    assert abs(damp[g.NX // 2] - 1.0) < 1e-9
+    assert (damp >= math.exp(-0.1)).all() and (damp <= 1.0).all()
+    assert np.abs(damp[1:] - damp[1:][::-1]).max() < 1e-15      # symmetric about ZLEN/2
+    assert damp[0] < 0.91                                        # damped at the ends
+    B = random_fff(g, 12)
+    B.E[:, :, 1:] = 0.0
+    B.E[:, 0, 0] = B.E[:, 0, 0].real
+    U = g.alloc()
+    ref = B.E[:, :, 0].copy()
+    s._etd_sponge(U, B, ph.dt)
+    assert np.abs(B.E[:, :, 0] - damp.mean() * ref).max() < 1e-12 * np.abs(ref).max()
+    assert np.abs(U.E).max() == 0.0

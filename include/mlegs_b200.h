@@ -183,6 +183,14 @@ int mlegs_mload(mlegs_ctx* ctx, const char* path, mlegs_field* f, int global);
 int mlegs_boussi_energy(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
                         double* ke, double* pe, double* dke);
 int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe);
+/* DIAGNOST(PSI, CHI) (mod_march.f90:1689-1966) without its printing and
+ * stored initial values: out[11] = VALVOR, VALZMO, VALANG, VALENE, VALHEL,
+ * the spread over k of |CALCAT1(PSI)| and |CALCAT1(CHI)|, the norm check's
+ * |Im PSI(2,1,1) + Im CHI(2,1,1)|, and CALCXY's (1967-2047) <X>, <Y>, <R>.  The dealiasing and divergence checks
+ * return MLEGS_ERR_DEALIASING / MLEGS_ERR_DIVERGENCE where the reference
+ * aborts.  VALANG integrates the RTRAN(+1) image that INTEG_P forms (the
+ * reference reads past its FFF argument there).  Synchronises the stream. */
+int mlegs_diagnost(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, double* out);
 
 /* Solver: SOLVER_T%INITIALIZE (mod_march.f90:171-240, Richardson start-up) and
  * TIME_STEPPING's state update (243-307: STEP_BOUSSI_AB_CN 609 or

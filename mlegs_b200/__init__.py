@@ -251,6 +251,17 @@ class Context:
         self._ck(self.lib.mlegs_boussi_energy(self.c, psi.h, chi.h, b.h, ptr(ke), ptr(pe), ptr(dke)))
         return ke.T.copy(), pe.T.copy(), dke.T.copy()
 
+    DIAGNOST_KEYS = ("VALVOR", "VALZMO", "VALANG", "VALENE", "VALHEL", "PAT1_SPREAD", "CAT1_SPREAD", "NORM_CHECK",
+                     "VALX", "VALY", "VALR")
+
+    def DIAGNOST(self, psi, chi):
+        """DIAGNOST(PSI, CHI) (mod_march.f90:1689-1917) values as a dict (see
+        mlegs_diagnost); raises MlegsError 11 / 12 on the dealiasing /
+        divergence checks."""
+        out = np.zeros(len(self.DIAGNOST_KEYS))
+        self._ck(self.lib.mlegs_diagnost(self.c, psi.h, chi.h, out.ctypes.data_as(ctypes.c_void_p)))
+        return dict(zip(self.DIAGNOST_KEYS, out.tolist()))
+
     def CALC_BOUSSI_PE(self, b):
         """CALC_BOUSSI_PE (mod_boussinesq.f90:112-136): (NTCHOP, NXCHOP) array."""
         pe = self._mk_array()

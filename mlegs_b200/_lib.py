@@ -75,6 +75,7 @@ SIGNATURES = {
     "mlegs_boussi_force": (c_int, [c_void_p] + [c_void_p] * 6),
     "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mlegs_diagnost": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_msave": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_int]),
     "mlegs_mload": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_int]),
     "mlegs_solver_init": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -481,6 +481,7 @@ struct mlegs_ctx {
     // ------------------------------------------------------------------ physics
     void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
     void energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke);
+    void diagnost(const Field* PSI, const Field* CHI, double out[11]);
     void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
                 Field* BN, cudaEvent_t vor_ready = nullptr, Field* PSIN = nullptr, Field* CHIN = nullptr);
@@ -1010,6 +1011,156 @@ void mlegs_ctx::energy(const Field* PSI, const Field* CHI, const Field* B, doubl
         halfk(h.data() + 3 * nmk, 1.0, pe, false);
         for (size_t q = 0; q < nout; ++q) pe[q] = pe[q] / 2.0 / (p.bv0 * p.bv0);
     }
+}
+
+// DIAGNOST(PSI, CHI), mod_march.f90:1689-1966, without the printing and the
+// stored initial values: the norm, dealiasing and divergence checks
+// (1726-1787) and, under CHOPSET(3), VALVOR = INTEG(OZH), VALZMO = INTEG(UZH)
+// (OZH, UZH the 'H' forms -DELSQH(PSI), -DELSQH(CHI) of PC2VOR/PC2VEL),
+// VALANG = -INTEG_P(XXDX(PSI with LN 0)), VALENE = -ENE1 + ENE2, VALHEL, the
+// spread of CALCAT1(PSI), CALCAT1(CHI) over k, and CALCXY's enstrophy-weighted
+// <X>, <Y>, <R>.  INTEG_P (3649-3682) reads F%E(:NR,1,1) of its FFF argument,
+// whose first dimension is NRCHOPDIM < NR; the RTRAN(+1) image F_COPY that it
+// forms is used here instead.
+// out: VALVOR, VALZMO, VALANG, VALENE, VALHEL, PAT1MAX-PAT1MIN, CAT1MAX-CAT1MIN,
+// |Im PSI(2,1,1) + Im CHI(2,1,1)| (the norm check's quantity), <X>, <Y>, <R>.
+void mlegs_ctx::diagnost(const Field* PSI, const Field* CHI, double out[11]) {
+    require(PSI, MLEGS_FFF, "DIAGNOST");
+    require(CHI, MLEGS_FFF, "DIAGNOST");
+    const int nk = d.NXCHOPDIM, nrd = d.NRCHOPDIM;
+    const size_t slab = (size_t)nrd * nk;
+    const int mm6 = std::min(6, d.NTCHOPDIM);
+    std::vector<double2> ps((size_t)mm6 * slab), cs(slab);
+    double lnp = 0.0, lnc = 0.0;
+    CK(cudaMemcpyAsync(ps.data(), PSI->data, ps.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(cs.data(), CHI->data, cs.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&lnp, PSI->ln, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&lnc, CHI->ln, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    auto at = [&](const std::vector<double2>& v, int m, int n, int k) { return v[((size_t)m * nrd + n) * nk + k]; };
+    auto nrchops = [&](int m, int pad) { return std::max(std::min(d.NRCHOP + pad, d.NRCHOP + pad - m), 0); };
+    out[7] = (nrd > 1) ? std::fabs(at(ps, 0, 1, 0).y + at(cs, 0, 1, 0).y) : 0.0;
+    // dealiasing check: radial modes past NRCHOPS of m = 0, 1 must be zero
+    double chk = 0.0;
+    for (int mm = 0; mm < std::min(2, d.NTCHOPDIM); ++mm) {
+        double mx = 0.0;
+        for (int n = nrchops(mm, 0); n < nrd; ++n)
+            for (int k = 0; k < nk; ++k) mx = std::max(mx, std::hypot(at(ps, mm, n, k).x, at(ps, mm, n, k).y));
+        chk += mx;
+    }
+    if (chk > 1.0e-12) throw ApiError(MLEGS_ERR_DEALIASING, "DIAG: DEALIASING INCOMPLETE");
+    // divergence check on the first coefficients
+    for (int kk = 0; kk < std::min(5, nk); ++kk)
+        for (int mm = 1; mm < mm6; ++mm)
+            for (int n = 0; n < std::min(5, d.NRCHOP); ++n)
+                if (std::hypot(at(ps, mm, n, kk).x, at(ps, mm, n, kk).y) > 100.0)
+                    throw ApiError(MLEGS_ERR_DIVERGENCE, "DIAG: DIVERGENCE");
+    const int P3 = 3;  // CHOPSET(3) ... CHOPSET(-3)
+    const double pi = 3.141592653589793238462643383279502884;
+    const double n00 = std::sqrt(0.5);  // TFM%NORM(1,1)
+    auto coef000 = [&](const Field* f) {
+        double2 v;
+        CK(cudaMemcpyAsync(&v, f->data, sizeof(double2), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return v.x;
+    };
+    const size_t nmk = (size_t)d.NTCHOPDIM * nk;
+    const double scale = 4.0 * pi * p.zlen * d.ELL2;
+    auto prodct = [&](const Field* A, const Field* B) {  // PRODCT: the sum of the halved ALLK array
+        k_prodct_mk(g, A->data, B->data, 0, scale, diag, s);
+        std::vector<double> h(nmk);
+        CK(cudaMemcpyAsync(h.data(), diag, nmk * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double sum = 0.0;
+        for (size_t q = 0; q < nmk; ++q) sum += (q < (size_t)nk ? 0.5 : 1.0) * h[q];
+        return sum;
+    };
+    Field *W1 = tmp(), *W2 = tmp(), *W3 = tmp();
+    // VALVOR = INTEG(-DELSQH(PSI)), VALZMO = INTEG(-DELSQH(CHI)) (INTEG, mod_scalar3.f90:312-353)
+    delsqh(PSI, W1, P3);
+    out[0] = 4.0 * pi * p.zlen * d.ELL2 * (-coef000(W1)) * n00;
+    delsqh(CHI, W1, P3);
+    out[1] = 4.0 * pi * p.zlen * d.ELL2 * (-coef000(W1)) * n00;
+    // VALANG = -INTEG_P(XXDX(PSI with LN 0))
+    copy0(W1, PSI, P3);
+    ln_zero(W1);
+    xxdx(W1, W2, P3);
+    rtran(W2, 1, P3);
+    {
+        std::vector<double2> line(d.NR);
+        CK(cudaMemcpy2DAsync(line.data(), sizeof(double2), W2->data, (size_t)nk * sizeof(double2), sizeof(double2),
+                             d.NR, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double acc = 0.0;
+        for (int r = 0; r < d.NR; ++r) {
+            const double om = 1.0 - h_x[r];
+            acc += line[r].x / (om * om) * h_w[r];
+        }
+        out[2] = -(2.0 * pi * p.zlen * d.ELL2 * acc);
+    }
+    // ENE1 = PRODCT(RTRAN DELSQH(PSI with LN doubled), RTRAN(PSI with LN 0))
+    copy0(W1, PSI, P3);
+    k_ln_copy(W1->ln, PSI->ln, 2.0, s);
+    delsqh(W1, W2, P3);
+    rtran(W2, 1, P3);
+    copy0(W1, PSI, P3);
+    ln_zero(W1);
+    rtran(W1, 1, P3);
+    const double ene1 = prodct(W2, W1);
+    // ENE2 = PRODCT(RTRAN DELSQH(CHI), RTRAN DEL2(CHI)); HEL1 = PRODCT(RTRAN DELSQH(PSI), RTRAN DEL2(CHI))
+    del2(CHI, W3, P3);
+    ln_zero(W3);
+    rtran(W3, 1, P3);
+    delsqh(CHI, W1, P3);
+    rtran(W1, 1, P3);
+    const double ene2 = prodct(W1, W3);
+    out[3] = -ene1 + ene2;
+    delsqh(PSI, W1, P3);
+    rtran(W1, 1, P3);
+    out[4] = 2.0 * prodct(W1, W3);
+    // CALCXY(ROR, ROP, OZ) (1967-2047): OZH times (1-x)^2 by the two MULXM of
+    // 1953-1955 is PC2VOR's OZ; TOFP, ABSVEC2 into OZ, then INTEG(TOFF(.)) of
+    // the enstrophy weighted by 1, R cos(th), R sin(th), R^2.
+    Field* W4 = tmp();
+    pc2vor(PSI, CHI, W1, W2, W3, P3);
+    tofp(W1, P3);
+    tofp(W2, P3);
+    tofp(W3, P3);
+    k_absvec2(g, W1->data, W2->data, W3->data, W3->data, s);
+    double mom[4];
+    for (int mode = 0; mode < 4; ++mode) {
+        k_mulr(g, W3->data, W4->data, mode, s);
+        W4->space = MLEGS_PPP;
+        ln_zero(W4);
+        toff(W4, P3);
+        mom[mode] = 4.0 * pi * p.zlen * d.ELL2 * coef000(W4) * n00;
+    }
+    out[8] = mom[1] / mom[0];
+    out[9] = mom[2] / mom[0];
+    out[10] = std::sqrt(mom[3] / mom[0]);
+    rel(W4);
+    rel(W3);
+    rel(W2);
+    rel(W1);
+    // CALCAT1 (mod_scalar3.f90:286-310) of PSI and CHI per k, at CHOPSET(3)
+    auto at1range = [&](const std::vector<double2>& v) {
+        double mx = 0.0, mn = 1e300;
+        const int nsum = std::min(d.NRCHOP + P3, nrd);
+        for (int k = 0; k < nk; ++k) {
+            double sx = 0.0, sy = 0.0;
+            for (int n = 0; n < nsum; ++n) {
+                const double a1 = std::sqrt((2 * n + 1) / 2.0);
+                sx += a1 * at(v, 0, n, k).x;
+                sy += a1 * at(v, 0, n, k).y;
+            }
+            const double av = std::hypot(sx, sy);
+            mx = std::max(mx, av);
+            mn = std::min(mn, av);
+        }
+        return mx - mn;
+    };
+    out[5] = at1range(ps);
+    out[6] = at1range(cs);
 }
 
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
@@ -1844,6 +1995,20 @@ int mlegs_boussi_energy(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_fiel
         ctx->mark();
         try {
             ctx->energy(F(psi), F(chi), F(b), ke, pe, dke);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
+        ctx->restore();
+    });
+}
+
+int mlegs_diagnost(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, double* out) {
+    if (!out) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        ctx->mark();
+        try {
+            ctx->diagnost(F(psi), F(chi), out);
         } catch (...) {
             ctx->restore();
             throw;

@@ -890,7 +890,10 @@ __device__ __forceinline__ void pc2vel_at(const DevGrid& g, int m, int n, int k,
     }
 }
 
-__global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
+// Three 256-thread blocks per SM (at most 80 registers; a few bytes spill):
+// the kernel is bound by memory-level parallelism, and this beats the 98-register
+// form at two blocks per SM.
+__global__ void __launch_bounds__(256, 3) etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     int m, n, k;
     if (!fff_index(g, t, m, n, k)) return;
@@ -918,34 +921,30 @@ __global__ void etd_ab_fused_kernel(DevGrid g, EtdAbArgs a) {
         w[2] = a.oz[t];
     }
     const double2 rn[4] = {cscale(w[0], fv), cscale(w[1], fv), cscale(w[2], fv), cscale(a.bn[t], fd)};
-    double E[16], N[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        E[q] = a.E[q];
-        N[q] = a.N[q];
-    }
-    if (k == 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) E[q] = N[q] = 0.0;
-        E[0] = E[5] = 1.0;
-        N[0] = N[5] = a.dt;
-    }
     const double notm0 = (m == 0) ? 0.0 : 1.0, notk0 = (k == 0) ? 0.0 : 1.0;
     // history: 0 N_B, 1 R_N_R, 2 R_N_P, 3 N_Z, 4 R_PI_R, 5 R_PI_P, 6 PI_Z
     const double2 ev[4] = {csub(u0, a.hist[4][t]), csub(u1, cscale(a.hist[5][t], notm0)),
                            csub(u2, cscale(a.hist[6][t], notk0)), a.b[t]};
     const double2 on[4] = {a.hist[1][t], a.hist[2][t], a.hist[3][t], a.hist[0][t]};
+    double2 av[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) av[j] = csub(cscale(rn[j], 1.5), cscale(on[j], 0.5));
+    // E and N are read from the parameter bank in the sums (no register copies);
+    // at k = 0 rows 0 and 1 are the identity and dt times it.
     double2 cv[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         double2 x = make_double2(0.0, 0.0), y = make_double2(0.0, 0.0);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const double2 av = csub(cscale(rn[j], 1.5), cscale(on[j], 0.5));
-            x.x += E[i * 4 + j] * ev[j].x;
-            x.y += E[i * 4 + j] * ev[j].y;
-            y.x += N[i * 4 + j] * av.x;
-            y.y += N[i * 4 + j] * av.y;
+            x.x += a.E[i * 4 + j] * ev[j].x;
+            x.y += a.E[i * 4 + j] * ev[j].y;
+            y.x += a.N[i * 4 + j] * av[j].x;
+            y.y += a.N[i * 4 + j] * av[j].y;
+        }
+        if (i < 2 && k == 0) {
+            x = ev[i];
+            y = cscale(av[i], a.dt);
         }
         cv[i] = a.raw_out ? cadd(x, y) : cscale(cadd(x, y), i < 3 ? fv : fd);
     }
@@ -978,6 +977,55 @@ __global__ void sponge_kernel(DevGrid g, double2* a, const double* damp) {
 void k_sponge(const DevGrid& g, double2* a, const double* damp, cudaStream_t s) {
     const size_t n = (size_t)g.NR * g.NX * g.NTCHOPDIM;
     sponge_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, damp);
+    count_launch();
+}
+
+// ABSVEC2(U, V, W, A) of CALCXY (mod_march.f90:2050-2099) on PPP [r][z][j]:
+// A = ((RU^2 + RV^2)/R^2 + W^2) / (1-x)^2 per packed sample (re and im apart).
+// A may alias W.
+__global__ void absvec2_kernel(DevGrid g, const double2* u, const double2* v, const double2* w, double2* a) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t plane = (size_t)g.NX * g.NTH;
+    if (t >= (size_t)g.NR * plane) return;
+    const int i = (int)(t / plane);
+    const double r = g.r[i], om = 1.0 - g.x[i], f = om * om, r2 = r * r;
+    const double2 uu = u[t], vv = v[t], ww = w[t];
+    a[t] = make_double2(((uu.x * uu.x + vv.x * vv.x) / r2 + ww.x * ww.x) / f,
+                        ((uu.y * uu.y + vv.y * vv.y) / r2 + ww.y * ww.y) / f);
+}
+void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const double2* w, double2* a, cudaStream_t s) {
+    const size_t n = (size_t)g.NR * g.NX * g.NTH;
+    absvec2_kernel<<<nblk(n, 256), 256, 0, s>>>(g, u, v, w, a);
+    count_launch();
+}
+
+// dst = src * {1, R cos(th), R sin(th), R^2}[mode] on PPP [r][z][j], the re
+// sample at THR(j) = 2 pi j / NTH and the im sample at THI(j) = 2 pi (j + 1/2) / NTH
+// (MULRCOSTH / MULRSINTH / MULR2, mod_march.f90:2102-2225; TFM%THR/THI, mod_fft.f90:323-324).
+__global__ void mulr_kernel(DevGrid g, const double2* src, double2* dst, int mode) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t plane = (size_t)g.NX * g.NTH;
+    if (t >= (size_t)g.NR * plane) return;
+    const int i = (int)(t / plane), j = (int)(t % g.NTH);
+    const double r = g.r[i];
+    const double pi = 3.141592653589793238462643383279502884;
+    const double thr = 2.0 * pi / g.NTH * j, thi = 2.0 * pi / g.NTH * (j + 0.5);
+    double fr = 1.0, fi = 1.0;
+    if (mode == 1) {
+        fr = r * cos(thr);
+        fi = r * cos(thi);
+    } else if (mode == 2) {
+        fr = r * sin(thr);
+        fi = r * sin(thi);
+    } else if (mode == 3) {
+        fr = fi = r * r;
+    }
+    const double2 a = src[t];
+    dst[t] = make_double2(fr * a.x, fi * a.y);
+}
+void k_mulr(const DevGrid& g, const double2* src, double2* dst, int mode, cudaStream_t s) {
+    const size_t n = (size_t)g.NR * g.NX * g.NTH;
+    mulr_kernel<<<nblk(n, 256), 256, 0, s>>>(g, src, dst, mode);
     count_launch();
 }
 

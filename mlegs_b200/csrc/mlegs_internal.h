@@ -241,6 +241,8 @@ struct EtdAbArgs {
 };
 // CALC_BOUSSI_ETD_SPONGE's damping of one PFP field by damp[z] (NX entries).
 void k_sponge(const DevGrid& g, double2* a, const double* damp, cudaStream_t s);
+void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const double2* w, double2* a, cudaStream_t s);
+void k_mulr(const DevGrid& g, const double2* src, double2* dst, int mode, cudaStream_t s);
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);
 void k_hyperv(const DevGrid& g, double2* a, const double* hr, const double* ht, const double* hx,
               double tf, int pad, cudaStream_t s);

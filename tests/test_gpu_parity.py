@@ -250,6 +250,30 @@ def test_boussi_energy(env):
     assert ei.value.code == 13
 
 
+def test_diagnost(env):
+    """DIAGNOST values and checks against the oracle (DELSQH, XXDX, DEL2,
+    RTRAN, INTEG, INTEG_P, PRODCT, CALCAT1 at CHOPSET(3))."""
+    from oracle import diagnostics as D
+    M, ctx, g, cfg = env
+    PSI, CHI = (random_fff(g, 70 + i, decay=4.0) for i in range(2))
+    PSI.LN, CHI.LN = 0.3, -0.2
+    fp, fc = up(ctx, PSI), up(ctx, CHI)
+    got = ctx.DIAGNOST(fp, fc)
+    ref = D.diagnost(g, PSI, CHI)
+    for key in D.DIAGNOST_KEYS:
+        assert abs(got[key] - ref[key]) <= 1e-12 * max(1.0, abs(ref[key])), key
+    assert rel(fp.download()[0], PSI.E) == 0.0 and fp.download()[1] == PSI.LN
+    for (n, m, k, val, code) in ((g.NRCHOPS[1], 1, 2, 1e-9, 11), (3, 2, 1, 150.0, 12)):
+        bad = PSI.copy()
+        bad.E[n, m, k] = val
+        fb = up(ctx, bad)
+        with pytest.raises(M.MlegsError) as ei:
+            ctx.DIAGNOST(fb, fc)
+        assert ei.value.code == code
+        with pytest.raises(D.DiagnostError):
+            D.diagnost(g, bad, CHI)
+
+
 def test_snapshot_files(env, tmp_path):
     """MSAVE / MLOAD through the C ABI against the oracle's restatement of
     the reference's file formats, both forms, bit for bit."""

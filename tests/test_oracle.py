@@ -197,6 +197,45 @@ def test_pe_matches_physical_integral():
     assert pe.shape == (g.NTCHOP, g.NXCHOP) and (pe >= 0).all()
 
 
+def test_diagnost_known_answers():
+    """DIAGNOST restated: the n = 0 row of DELSQH is the log term alone, so
+    VALVOR = -4 pi ZLEN PSI%LN and VALZMO = -4 pi ZLEN CHI%LN; VALENE is twice
+    the kinetic energy that CALC_BOUSSI_ENERGY sums over (m, k); the
+    dealiasing and divergence checks raise the reference's abort codes; CALCXY
+    finds the centre of an off-axis q-vortex."""
+    from oracle import diagnostics as D
+    cfg = small_cfg(32, 16, 16, adams=False)
+    g = oracle_grid(cfg)
+    PSI, CHI, B = (random_fff(g, 60 + i, decay=4.0) for i in range(3))
+    PSI.LN, CHI.LN = 0.3, -0.2
+    v = D.diagnost(g, PSI, CHI)
+    assert abs(v["VALVOR"] + 4 * math.pi * g.ZLEN * PSI.LN) < 1e-13
+    assert abs(v["VALZMO"] + 4 * math.pi * g.ZLEN * CHI.LN) < 1e-13
+    ke, _, _ = D.boussi_energy(g, PSI, CHI, B, 1.0)
+    assert abs(v["VALENE"] - 2 * ke.sum()) < 1e-12 * abs(v["VALENE"])
+    assert v["NORM_CHECK"] == abs(PSI.E[1, 0, 0].imag + CHI.E[1, 0, 0].imag)
+    assert g.NRCHOP == cfg.nrchop  # CHOPSET(3) undone
+    bad = PSI.copy()
+    bad.E[g.NRCHOPS[1], 1, 2] = 1e-9
+    with pytest.raises(D.DiagnostError) as ei:
+        D.diagnost(g, bad, CHI)
+    assert ei.value.code == 11
+    bad = PSI.copy()
+    bad.E[3, 2, 1] = 150.0
+    with pytest.raises(D.DiagnostError) as ei:
+        D.diagnost(g, bad, CHI)
+    assert ei.value.code == 12
+    # CALCXY: the enstrophy of a Gaussian q-vortex at (xc, yc) with core R0 is
+    # a Gaussian of variance R0^2/4 per axis, so <X> = xc, <Y> = yc and
+    # <R>^2 = xc^2 + yc^2 + R0^2/2.
+    from oracle import layout
+    g = oracle_grid(small_cfg(64, 32, 32))
+    psi, chi = layout.qvortex(g, xc=0.4, yc=-0.3)
+    v = D.diagnost(g, psi, chi)
+    assert abs(v["VALX"] - 0.4) < 1e-10 and abs(v["VALY"] + 0.3) < 1e-10
+    assert abs(v["VALR"] - math.sqrt(0.4 ** 2 + 0.3 ** 2 + 0.5)) < 1e-10
+
+
 def test_snapshot_record_layout(tmp_path):
     """MSAVEX / MPISAVEX restated: the record list and byte layout the
     reference's reader (tests/postproc/read_binary_info.ipynb) expects, and a

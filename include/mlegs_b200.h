@@ -192,6 +192,27 @@ int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe);
  * reference reads past its FFF argument there).  Synchronises the stream. */
 int mlegs_diagnost(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, double* out);
 
+/* Adaptive hyperviscosity (VISC%ADJSW /= 0 with VISC%SW = 3).
+ * ENEMON(PSI, CHI, EM, EK) (mod_march.f90:2585-2617) at CHOPSET(pad):
+ * em[NTCHOP] and ek[NXCHOP] (either may be NULL).  Synchronises the stream. */
+int mlegs_enemon(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, int pad, double* em,
+                 double* ek);
+/* HYP3ADJ(PSI, CHI, B) (mod_march.f90:3000-3182) followed by the stepper's two
+ * HYP3SET calls (283-288): updates NUP_R/T/X (and KAPPAP_R/T/X when b is not
+ * NULL) and rewrites the HYPERV / HYPERD tables that the steps (and captured
+ * step graphs) read.  The controller history persists in the context. */
+int mlegs_hyp3adj(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b);
+/* out[6] = NUP_R, NUP_T, NUP_X, KAPPAP_R, KAPPAP_T, KAPPAP_X. */
+int mlegs_hyp3_coeffs(mlegs_ctx* ctx, double* out);
+/* The host-side pieces of HYP3ADJ (no context, no device):
+ * SPECURV(ESPEC(1:n), USE_RATIO) (2619-2698), SPESLOP(ESPEC(1:n), RATIO)
+ * (2700-2774) and PDAJUST(COEFF, CURRENT, PREVIOUS, BASELINE, PARAMS[4]
+ * [, OVERDAMP_THRESHOLD]) (2776-2812; has_threshold = PRESENT(...)). */
+int mlegs_specurv(const double* espec, int n, double use_ratio, double* curv);
+int mlegs_speslop(const double* espec, int n, double ratio, double* slope);
+int mlegs_pdajust(double* coeff, double current, double previous, double baseline, const double* params,
+                  int has_threshold, double threshold);
+
 /* Solver: SOLVER_T%INITIALIZE (mod_march.f90:171-240, Richardson start-up) and
  * TIME_STEPPING's state update (243-307: STEP_BOUSSI_AB_CN 609 or
  * STEP_BOUSSI_ETDAB_CN 811).  The state fields stay owned by the caller. */

@@ -262,6 +262,23 @@ class Context:
         self._ck(self.lib.mlegs_diagnost(self.c, psi.h, chi.h, out.ctypes.data_as(ctypes.c_void_p)))
         return dict(zip(self.DIAGNOST_KEYS, out.tolist()))
 
+    def ENEMON(self, psi, chi, pad=0):
+        """ENEMON(PSI, CHI, EM, EK) (mod_march.f90:2585-2617) at CHOPSET(pad): (EM, EK)."""
+        em, ek = np.zeros(self.NTCHOP), np.zeros(self.NXCHOP)
+        self._ck(self.lib.mlegs_enemon(self.c, psi.h, chi.h, pad, em.ctypes.data_as(ctypes.c_void_p),
+                                       ek.ctypes.data_as(ctypes.c_void_p)))
+        return em, ek
+
+    def HYP3ADJ(self, psi, chi, b=None):
+        """HYP3ADJ(PSI, CHI[, B]) and the stepper's two HYP3SET (mod_march.f90:283-288)."""
+        self._ck(self.lib.mlegs_hyp3adj(self.c, psi.h, chi.h, b.h if b is not None else None))
+
+    def hyp3_coeffs(self):
+        """(NUP_R, NUP_T, NUP_X), (KAPPAP_R, KAPPAP_T, KAPPAP_X)."""
+        out = np.zeros(6)
+        self._ck(self.lib.mlegs_hyp3_coeffs(self.c, out.ctypes.data_as(ctypes.c_void_p)))
+        return tuple(out[:3]), tuple(out[3:])
+
     def CALC_BOUSSI_PE(self, b):
         """CALC_BOUSSI_PE (mod_boussinesq.f90:112-136): (NTCHOP, NXCHOP) array."""
         pe = self._mk_array()
@@ -316,6 +333,38 @@ class Context:
         return ms.value, by.value
 
 
+def _spectrum_call(name, espec, ratio):
+    e = np.ascontiguousarray(espec, dtype=np.float64)
+    out = ctypes.c_double(0.0)
+    rc = getattr(_lib.load(), name)(e.ctypes.data_as(ctypes.c_void_p), e.size, float(ratio), ctypes.byref(out))
+    if rc != 0:
+        raise MlegsError(rc, name)
+    return out.value
+
+
+def SPECURV(espec, use_ratio=1.0 / 3.0):
+    """SPECURV(ESPEC, USE_RATIO), mod_march.f90:2619-2698 (host code, no device)."""
+    return _spectrum_call("mlegs_specurv", espec, use_ratio)
+
+
+def SPESLOP(espec, ratio=1.0 / 3.0):
+    """SPESLOP(ESPEC, RATIO), mod_march.f90:2700-2774 (host code, no device)."""
+    return _spectrum_call("mlegs_speslop", espec, ratio)
+
+
+def PDAJUST(coeff, current, previous, baseline, params, overdamp_threshold=None):
+    """PDAJUST(COEFF, CURRENT, PREVIOUS, BASELINE, PARAMS[, OVERDAMP_THRESHOLD]),
+    mod_march.f90:2776-2812; returns the updated COEFF (host code, no device)."""
+    c = ctypes.c_double(coeff)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    rc = _lib.load().mlegs_pdajust(ctypes.byref(c), float(current), float(previous), float(baseline),
+                                   prm.ctypes.data_as(ctypes.c_void_p), int(overdamp_threshold is not None),
+                                   float(overdamp_threshold or 0.0))
+    if rc != 0:
+        raise MlegsError(rc, "mlegs_pdajust")
+    return c.value
+
+
 def qvortex(ctx, q=1.0, r0=1.0, xc=0.0, yc=0.0):
     """QVORTEX (mod_layout.f90:449-609) for one vortex with H = 0, on the device.
 
@@ -362,4 +411,5 @@ def initial_state(ctx, cfg=None):
 
 
 __all__ = ["Context", "Field", "MlegsError", "qvortex", "initial_state", "CONFIGS", "Config",
+           "SPECURV", "SPESLOP", "PDAJUST",
            "PPP", "FFF", "PFP", "PFF", "PREC_FP64", "PREC_SPLIT"]

@@ -76,6 +76,12 @@ SIGNATURES = {
     "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mlegs_diagnost": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_enemon": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "mlegs_hyp3adj": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_hyp3_coeffs": (c_int, [c_void_p, c_void_p]),
+    "mlegs_specurv": (c_int, [c_void_p, c_int, c_double, c_void_p]),
+    "mlegs_speslop": (c_int, [c_void_p, c_int, c_double, c_void_p]),
+    "mlegs_pdajust": (c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_int, c_double]),
     "mlegs_msave": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_int]),
     "mlegs_mload": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_int]),
     "mlegs_solver_init": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

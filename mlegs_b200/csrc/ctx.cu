@@ -81,6 +81,11 @@ struct mlegs_ctx {
            *tb_del2h = nullptr;
     double *V = nullptr, *D = nullptr, *T = nullptr;
     double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
+    // HYP3SET masks (VISC%MASK_R/T/X) and the adaptive state of VISC
+    // (mod_march.f90:70-86): NUP_R/T/X, KAPPAP_R/T/X, the controllers' history.
+    std::vector<double> h3_mr, h3_mt, h3_mx, h3_ak;
+    double nup3[3] = {0, 0, 0}, kap3[3] = {0, 0, 0};
+    Hyp3State adj;
     double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
     double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
     double* diag = nullptr;                                         // 4 x [m][k] quadratures (energy)
@@ -482,6 +487,10 @@ struct mlegs_ctx {
     void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
     void energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke);
     void diagnost(const Field* PSI, const Field* CHI, double out[11]);
+    void boussi_pe(const Field* B, double* pe);
+    void enemon(const Field* PSI, const Field* CHI, int pad, double* em, double* ek);
+    void hyp3set(const double nu[3], double** tables);
+    void hyp3adj(const Field* PSI, const Field* CHI, const Field* B);
     void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
                 Field* BN, cudaEvent_t vor_ready = nullptr, Field* PSIN = nullptr, Field* CHIN = nullptr);
@@ -776,28 +785,17 @@ void mlegs_ctx::init(const mlegs_params& prm) {
             for (int q = 0; q < d.NXCHOPDIM; ++q) kx[q] = std::fabs(h_ak[q]);
             mx = mask(kx, d.NXCHOPDIM, 2.0 / 3.0, 2.0);
         }
-        const int ph2 = p.visc_p / 2;
-        auto ipow = [](double v, int e) { double r2 = 1.0; for (int q = 0; q < e; ++q) r2 *= v; return r2; };
-        double k2r = 1.5 * 1.5 * (double)((nrc - 1) * nrc) / d.ELL2;
-        double k2t = (double)((d.NTCHOPDIM - 1) * (d.NTCHOPDIM - 1));
-        double k2x = 0.0;
-        for (double v : h_ak) k2x = std::max(k2x, v * v);
-        auto set = [&](double nu, double** outp) {
-            std::vector<double> hr((size_t)nrc * d.NTCHOPDIM), ht(d.NTCHOPDIM), hx(d.NXCHOPDIM);
-            for (int m = 0; m < d.NTCHOPDIM; ++m) {
-                ht[m] = std::exp(-nu * mt[m] * ipow((double)(m * m) / k2t, ph2));
-                for (int nn = 1; nn <= nrc; ++nn)
-                    hr[(size_t)m * nrc + nn - 1] =
-                        std::exp(-nu * mr[(size_t)m * nrc + nn - 1] *
-                                 ipow(1.5 * 1.5 * (double)((nn - 1) * nn) / d.ELL2 / k2r, ph2));
-            }
-            for (int q = 0; q < d.NXCHOPDIM; ++q) hx[q] = std::exp(-nu * mx[q] * ipow(h_ak[q] * h_ak[q] / k2x, ph2));
-            outp[0] = up(hr);
-            outp[1] = up(ht);
-            outp[2] = up(hx);
-        };
-        set(p.nup, hv);
-        set(p.kappap, hd);
+        h3_mr = mr;
+        h3_mt = mt;
+        h3_mx = mx;
+        h3_ak = h_ak;
+        // HYP3INIT (3464-3480)
+        for (int q = 0; q < 3; ++q) {
+            nup3[q] = p.nup;
+            kap3[q] = p.kappap;
+        }
+        hyp3set(nup3, hv);
+        hyp3set(kap3, hd);
     }
 
     // --- ETD operators (CALC_BOUSSI_ETD_OP, mod_march.f90:906-945; host FP64)
@@ -1161,6 +1159,126 @@ void mlegs_ctx::diagnost(const Field* PSI, const Field* CHI, double out[11]) {
     };
     out[5] = at1range(ps);
     out[6] = at1range(cs);
+}
+
+// CALC_BOUSSI_PE(B), mod_boussinesq.f90:112-136: WK = B, LN 0, RTRAN at the
+// current chop (pad 0), L2NORM_MK_HALFK / 2 / BV0^2 into pe (NTCHOP x NXCHOP).
+void mlegs_ctx::boussi_pe(const Field* B, double* pe) {
+    require(B, MLEGS_FFF, "CALC_BOUSSI_PE");
+    if (p.bv0 == 0.0) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_PE: BV0 = 0");
+    const size_t nmk = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
+    Field* W = tmp();
+    copy0(W, B, 0);
+    ln_zero(W);
+    rtran(W, 1, 0);
+    k_prodct_mk(g, W->data, nullptr, 1, 4.0 * 3.141592653589793238462643383279502884 * p.zlen * d.ELL2, diag, s);
+    rel(W);
+    std::vector<double> h(nmk);
+    CK(cudaMemcpyAsync(h.data(), diag, nmk * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    halfk(h.data(), 1.0, pe, false);
+    const size_t nout = (size_t)d.NTCHOP * d.NXCHOP;
+    for (size_t q = 0; q < nout; ++q) pe[q] = pe[q] / 2.0 / (p.bv0 * p.bv0);
+}
+
+// HYP3SET(NU_R, NU_T, NU_X, HYPER_R, HYPER_T, HYPER_X), mod_march.f90:3320-3368
+// (without hyperv.dat): exp(-NU * MASK * (k^2 / K2MAX)^(P/2)) per direction, with
+// the masks of the first call.  The device tables are allocated once and
+// rewritten in place afterwards, so captured step graphs read the new values.
+void mlegs_ctx::hyp3set(const double nu[3], double** tables) {
+    const int nrc = d.NRCHOP, ph2 = p.visc_p / 2;
+    auto ipow = [](double v, int e) { double r2 = 1.0; for (int q = 0; q < e; ++q) r2 *= v; return r2; };
+    const double k2r = 1.5 * 1.5 * (double)((nrc - 1) * nrc) / d.ELL2;
+    const double k2t = (double)((d.NTCHOPDIM - 1) * (d.NTCHOPDIM - 1));
+    double k2x = 0.0;
+    for (double v : h3_ak) k2x = std::max(k2x, v * v);
+    std::vector<double> hr((size_t)nrc * d.NTCHOPDIM), ht(d.NTCHOPDIM), hx(d.NXCHOPDIM);
+    for (int m = 0; m < d.NTCHOPDIM; ++m) {
+        ht[m] = std::exp(-nu[1] * h3_mt[m] * ipow((double)(m * m) / k2t, ph2));
+        for (int nn = 1; nn <= nrc; ++nn)
+            hr[(size_t)m * nrc + nn - 1] = std::exp(-nu[0] * h3_mr[(size_t)m * nrc + nn - 1] *
+                                                    ipow(1.5 * 1.5 * (double)((nn - 1) * nn) / d.ELL2 / k2r, ph2));
+    }
+    for (int q = 0; q < d.NXCHOPDIM; ++q) hx[q] = std::exp(-nu[2] * h3_mx[q] * ipow(h3_ak[q] * h3_ak[q] / k2x, ph2));
+    const std::vector<double>* hs[3] = {&hr, &ht, &hx};
+    for (int q = 0; q < 3; ++q) {
+        if (!tables[q]) tables[q] = dalloc<double>(hs[q]->size());
+        CK(cudaMemcpyAsync(tables[q], hs[q]->data(), hs[q]->size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+}
+
+// ENEMON(PSI, CHI, EM, EK), mod_march.f90:2585-2617, at CHOPSET(pad):
+// EM(m) = sum_k, EK(k) = sum_m of -PRODCT_MK_HALFK(RTRAN DELSQH(PSI, 2 LN),
+// RTRAN(PSI, LN 0)) + PRODCT_MK_HALFK(RTRAN DELSQH(CHI), RTRAN DEL2(CHI)).
+void mlegs_ctx::enemon(const Field* PSI, const Field* CHI, int pad, double* em, double* ek) {
+    require(PSI, MLEGS_FFF, "ENEMON");
+    require(CHI, MLEGS_FFF, "ENEMON");
+    const size_t nmk = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
+    const double scale = 4.0 * 3.141592653589793238462643383279502884 * p.zlen * d.ELL2;
+    Field *W1 = tmp(), *W2 = tmp();
+    copy0(W1, PSI, pad);
+    k_ln_copy(W1->ln, PSI->ln, 2.0, s);
+    delsqh(W1, W2, pad);
+    rtran(W2, 1, pad);
+    copy0(W1, PSI, pad);
+    ln_zero(W1);
+    rtran(W1, 1, pad);
+    k_prodct_mk(g, W2->data, W1->data, 0, scale, diag, s);
+    del2(CHI, W1, pad);
+    rtran(W1, 1, pad);
+    delsqh(CHI, W2, pad);
+    rtran(W2, 1, pad);
+    k_prodct_mk(g, W2->data, W1->data, 0, scale, diag + nmk, s);
+    rel(W2);
+    rel(W1);
+    std::vector<double> h(2 * nmk);
+    CK(cudaMemcpyAsync(h.data(), diag, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int nt = d.NTCHOP, nx = d.NXCHOP;
+    std::vector<double> mk((size_t)nt * nx);  // (NTCHOP, NXCHOP), m fastest
+    halfk(h.data(), -1.0, mk.data(), false);
+    halfk(h.data() + nmk, 1.0, mk.data(), true);
+    for (int m = 0; m < nt; ++m) {
+        double a = 0.0;
+        for (int k = 0; k < nx; ++k) a += mk[(size_t)k * nt + m];
+        if (em) em[m] = a;
+    }
+    for (int k = 0; k < nx; ++k) {
+        double a = 0.0;
+        for (int m = 0; m < nt; ++m) a += mk[(size_t)k * nt + m];
+        if (ek) ek[k] = a;
+    }
+}
+
+// HYP3ADJ(PSI, CHI, B), mod_march.f90:3000-3182, then the two HYP3SET of the
+// stepper (283-288).  ENEMON at CHOPSET(2); the spectra metrics and the
+// controllers are host code (hyperadj.cu); B (optional) adds the
+// hyperdiffusivity controller from CALC_BOUSSI_PE at the current chop.
+void mlegs_ctx::hyp3adj(const Field* PSI, const Field* CHI, const Field* B) {
+    const int nt = d.NTCHOP, nx = d.NXCHOP;
+    std::vector<double> em(nt), ek(nx);
+    enemon(PSI, CHI, 2, em.data(), ek.data());
+    std::vector<double> pm, pk;
+    if (B) {
+        require(B, MLEGS_FFF, "HYP3ADJ");
+        if (p.bv0 == 0.0) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_PE: BV0 = 0");
+        std::vector<double> pe((size_t)nt * nx);
+        boussi_pe(B, pe.data());
+        pm.assign(std::max(nt - 2, 0), 0.0);
+        pk.assign(nx, 0.0);
+        for (int m = 0; m < nt; ++m)  // pe is (NTCHOP, NXCHOP), m fastest
+            for (int k = 0; k < nx; ++k) {
+                if (m < nt - 2) pm[m] += pe[(size_t)k * nt + m];
+                pk[k] += pe[(size_t)k * nt + m];
+            }
+    }
+    hyp3adj_update(adj, em.data(), std::max(nt - 2, 0), ek.data(), nx, nup3, B ? pm.data() : nullptr,
+                   (int)pm.size(), B ? pk.data() : nullptr, (int)pk.size(), kap3);
+    if (p.visc_sw == 3) {
+        hyp3set(nup3, hv);
+        hyp3set(kap3, hd);
+    }
 }
 
 // CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314.
@@ -2019,28 +2137,51 @@ int mlegs_diagnost(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* ch
 
 int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe) {
     return guard(ctx, [&] {
-        // CALC_BOUSSI_PE (mod_boussinesq.f90:112-136): WK = B, LN 0, RTRAN at the
-        // current chop (pad 0), L2NORM_MK_HALFK / 2 / BV0^2
-        const Field* B = F(b);
-        ctx->require(B, MLEGS_FFF, "CALC_BOUSSI_PE");
-        if (ctx->p.bv0 == 0.0) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_PE: BV0 = 0");
-        const Dims& d = ctx->d;
-        const size_t nmk = (size_t)d.NTCHOPDIM * d.NXCHOPDIM;
         ctx->mark();
-        Field* W = ctx->tmp();
-        ctx->copy0(W, B, 0);
-        ctx->ln_zero(W);
-        ctx->rtran(W, 1, 0);
-        k_prodct_mk(ctx->g, W->data, nullptr, 1, 4.0 * 3.141592653589793238462643383279502884 * ctx->p.zlen * d.ELL2,
-                    ctx->diag, ctx->s);
-        ctx->rel(W);
+        try {
+            ctx->boussi_pe(F(b), pe);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
         ctx->restore();
-        std::vector<double> h(nmk);
-        CK(cudaMemcpyAsync(h.data(), ctx->diag, nmk * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaStreamSynchronize(ctx->s));
-        ctx->halfk(h.data(), 1.0, pe, false);
-        const size_t nout = (size_t)d.NTCHOP * d.NXCHOP;
-        for (size_t q = 0; q < nout; ++q) pe[q] = pe[q] / 2.0 / (ctx->p.bv0 * ctx->p.bv0);
+    });
+}
+
+int mlegs_enemon(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, int pad, double* em, double* ek) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        ctx->mark();
+        try {
+            ctx->enemon(F(psi), F(chi), pad, em, ek);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
+        ctx->restore();
+    });
+}
+
+int mlegs_hyp3adj(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b) {
+    return guard(ctx, [&] {
+        ctx->mark();
+        try {
+            ctx->hyp3adj(F(psi), F(chi), b ? F(b) : nullptr);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
+        ctx->restore();
+    });
+}
+
+int mlegs_hyp3_coeffs(mlegs_ctx* ctx, double* out) {
+    if (!out) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        for (int q = 0; q < 3; ++q) {
+            out[q] = ctx->nup3[q];
+            out[3 + q] = ctx->kap3[q];
+        }
     });
 }
 

@@ -241,6 +241,18 @@ struct EtdAbArgs {
 };
 // CALC_BOUSSI_ETD_SPONGE's damping of one PFP field by damp[z] (NX entries).
 void k_sponge(const DevGrid& g, double2* a, const double* damp, cudaStream_t s);
+// Adaptive hyperviscosity state of VISC (mod_march.f90:74-76) and its host code (hyperadj.cu).
+struct Hyp3State {
+    double nupb = -1.0, kappapb = -1.0;
+    double hist[4] = {0, 0, 0, 0};    // CURVMO CURVKO SLOPMO SLOPKO
+    double phist[4] = {0, 0, 0, 0};   // PCURVMO PCURVKO PSLOPMO PSLOPKO
+};
+double specurv(const double* e, int size, double use_ratio);
+double speslop(const double* e, int size, double ratio);
+double pdajust(double coeff, double current, double previous, double baseline, const double params[4],
+               bool has_threshold, double threshold);
+void hyp3adj_update(Hyp3State& st, const double* em, int nm, const double* ek, int nk, double nup[3],
+                    const double* pm, int npm, const double* pk, int npk, double kap[3]);
 void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const double2* w, double2* a, cudaStream_t s);
 void k_mulr(const DevGrid& g, const double2* src, double2* dst, int mode, cudaStream_t s);
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);

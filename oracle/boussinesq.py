@@ -179,20 +179,31 @@ class Hyperv3:
                                           ratio=0.5, steep=2.0)
         self.mask_t = hyp3mask(g.M.astype(float), g.NTCHOPDIM, steep=2.0)
         self.mask_x = hyp3mask(np.abs(g.AK[0, :]), g.NXCHOPDIM, steep=2.0)
-        self.hv = self._set(g, ph, ph.nup)
-        self.hd = self._set(g, ph, ph.kappap)
+        # HYP3INIT (3464-3480): NUP_R/T/X = NUP, KAPPAP_R/T/X = KAPPAP
+        self.nup = [ph.nup] * 3
+        self.kappap = [ph.kappap] * 3
+        self.hv = self._set(g, ph, *self.nup)
+        self.hd = self._set(g, ph, *self.kappap)
 
-    def _set(self, g, ph, nu):
+    def _set(self, g, ph, nu_r, nu_t=None, nu_x=None):
+        """HYP3SET(NU_R, NU_T, NU_X, ...), mod_march.f90:3320-3368 (without hyperv.dat)."""
+        nu_t = nu_r if nu_t is None else nu_t
+        nu_x = nu_r if nu_x is None else nu_x
         nrchop = g.NRCHOP
         ph2 = ph.p // 2
         k2r = 1.5 ** 2 * float((nrchop - 1) * nrchop) / g.ELL2
         k2t = float(np.max(g.M ** 2))
         k2x = float(np.max(g.AK[0, :] ** 2))
-        ht = np.exp(-nu * self.mask_t * (g.M.astype(float) ** 2 / k2t) ** ph2)
+        ht = np.exp(-nu_t * self.mask_t * (g.M.astype(float) ** 2 / k2t) ** ph2)
         nn = np.arange(1, nrchop + 1)
-        hr = np.exp(-nu * self.mask_r * ((1.5 ** 2 * ((nn - 1) * nn).astype(float) / g.ELL2 / k2r) ** ph2)[:, None])
-        hx = np.exp(-nu * self.mask_x * (g.AK[0, :] ** 2 / k2x) ** ph2)
+        hr = np.exp(-nu_r * self.mask_r * ((1.5 ** 2 * ((nn - 1) * nn).astype(float) / g.ELL2 / k2r) ** ph2)[:, None])
+        hx = np.exp(-nu_x * self.mask_x * (g.AK[0, :] ** 2 / k2x) ** ph2)
         return hr, ht, hx
+
+    def reset(self, g, ph):
+        """The two HYP3SET calls after HYP3ADJ in the stepper (mod_march.f90:286-287)."""
+        self.hv = self._set(g, ph, *self.nup)
+        self.hd = self._set(g, ph, *self.kappap)
 
     @staticmethod
     def _apply(g, A, filt, tf):

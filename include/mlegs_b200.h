@@ -192,6 +192,19 @@ int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe);
  * reference reads past its FFF argument there).  Synchronises the stream. */
 int mlegs_diagnost(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, double* out);
 
+/* One vortex of QPAIR (read.input's vortex list, mod_init.f90): centre X, Y;
+ * strengths Q (toroidal) and H, decay B (poloidal); the z-waviness DX, DY
+ * with axial wavenumber K and phase DP (degrees); core R with its modulation
+ * DR, wavenumber RK and phase RP (degrees).  K and RK count periods per ZLEN. */
+typedef struct mlegs_vortex {
+    double x, y, q, h, b, dx, dy, k, dp, r, dr, rk, rp;
+} mlegs_vortex;
+
+/* QVORTEX(PSI, CHI) (mod_layout.f90:449-609) with NOISE = 0, on the device:
+ * LAY(A, GAUS, 2) of every vortex (Q -> 2Q, B -> 1 for PSI; Q -> H, B for
+ * CHI), TOFF, A = -A with LN 0, IDELSQH.  psi and chi end in FFF.  n >= 1. */
+int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, mlegs_field* psi, mlegs_field* chi);
+
 /* Adaptive hyperviscosity (VISC%ADJSW /= 0 with VISC%SW = 3).
  * ENEMON(PSI, CHI, EM, EK) (mod_march.f90:2585-2617) at CHOPSET(pad):
  * em[NTCHOP] and ek[NXCHOP] (either may be NULL).  Synchronises the stream. */

@@ -365,31 +365,30 @@ def PDAJUST(coeff, current, previous, baseline, params, overdamp_threshold=None)
     return c.value
 
 
-def qvortex(ctx, q=1.0, r0=1.0, xc=0.0, yc=0.0):
-    """QVORTEX (mod_layout.f90:449-609) for one vortex with H = 0, on the device.
+VORTEX_DEFAULTS = dict(x=0.0, y=0.0, q=1.0, h=0.0, b=1.0, dx=0.0, dy=0.0, k=0.0, dp=0.0,
+                       r=1.0, dr=0.0, rk=0.0, rp=0.0)
 
-    omega_z = 2Q exp(-((x-xc)^2 + (y-yc)^2)/R0^2)/R0^2 is laid out at the
-    collocation points divided by (1-x)^2 (LAY with IPIN = 2, 64-117), taken
-    to FFF by TOFF, negated with its log term muted, and inverted by IDELSQH.
-    Returns (psi, chi) Fields; chi = 0.
-    """
-    x, _, r = ctx.grid()
-    nth = ctx.NTH
-    th = np.pi / nth * np.arange(2 * nth)
-    X = r[:, None] * np.cos(th)[None, :]
-    Y = r[:, None] * np.sin(th)[None, :]
-    val = 2.0 * q / r0 ** 2 * np.exp(-1.0 * ((X - xc) ** 2 + (Y - yc) ** 2) / r0 ** 2)
-    val = val / ((1 - x[:, None]) ** 2)
-    E = np.zeros(ctx.shape(PPP), dtype=np.complex128)
-    E[:ctx.NR, :nth, :] = (val[:, 0::2] + 1j * val[:, 1::2])[:, :, None]
-    A = ctx.field(PPP, E, 0.0)
-    ctx.TOFF(A)
-    ctx.AXPBY(A, -1.0, A)
-    ctx.SET_LN(A, 0.0)
-    psi = ctx.field(FFF)
-    ctx.IDELSQH(A, psi)
-    chi = ctx.field(FFF)
+
+def QVORTEX(ctx, vortices):
+    """QVORTEX(PSI, CHI) (mod_layout.f90:449-609, NOISE = 0) on the device for a
+    QPAIR list: each entry a dict with any of the keys of VORTEX_DEFAULTS (X, Y,
+    Q, H, B, DX, DY, K, DP, R, DR, RK, RP in lower case).  Returns (psi, chi)."""
+    arr = (_lib.Vortex * len(vortices))()
+    for i, v in enumerate(vortices):
+        unknown = set(v) - set(VORTEX_DEFAULTS)
+        if unknown:
+            raise ValueError("unknown vortex keys %s" % sorted(unknown))
+        full = dict(VORTEX_DEFAULTS, **v)
+        for key, val in full.items():
+            setattr(arr[i], key, float(val))
+    psi, chi = ctx.field(FFF), ctx.field(FFF)
+    ctx._ck(ctx.lib.mlegs_qvortex(ctx.c, arr, len(vortices), psi.h, chi.h))
     return psi, chi
+
+
+def qvortex(ctx, q=1.0, r0=1.0, xc=0.0, yc=0.0, h=0.0, b=1.0):
+    """One Gaussian q-vortex (QVORTEX with a single QPAIR entry) on the device."""
+    return QVORTEX(ctx, [dict(q=q, r=r0, x=xc, y=yc, h=h, b=b)])
 
 
 def initial_state(ctx, cfg=None):
@@ -410,6 +409,6 @@ def initial_state(ctx, cfg=None):
     return psi, chi, b
 
 
-__all__ = ["Context", "Field", "MlegsError", "qvortex", "initial_state", "CONFIGS", "Config",
+__all__ = ["Context", "Field", "MlegsError", "qvortex", "QVORTEX", "initial_state", "CONFIGS", "Config",
            "SPECURV", "SPESLOP", "PDAJUST",
            "PPP", "FFF", "PFP", "PFF", "PREC_FP64", "PREC_SPLIT"]

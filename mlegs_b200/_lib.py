@@ -20,6 +20,11 @@ c_char_p = ctypes.c_char_p
 dptr = ctypes.POINTER(ctypes.c_double)
 
 
+class Vortex(ctypes.Structure):
+    """mlegs_vortex (include/mlegs_b200.h): one QPAIR entry."""
+    _fields_ = [(k, ctypes.c_double) for k in ("x", "y", "q", "h", "b", "dx", "dy", "k", "dp", "r", "dr", "rk", "rp")]
+
+
 class Params(ctypes.Structure):
     """mlegs_params (include/mlegs_b200.h)."""
     _fields_ = [
@@ -76,6 +81,7 @@ SIGNATURES = {
     "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mlegs_diagnost": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_qvortex": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "mlegs_enemon": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "mlegs_hyp3adj": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_hyp3_coeffs": (c_int, [c_void_p, c_void_p]),

@@ -490,6 +490,7 @@ struct mlegs_ctx {
     void boussi_pe(const Field* B, double* pe);
     void enemon(const Field* PSI, const Field* CHI, int pad, double* em, double* ek);
     void hyp3set(const double nu[3], double** tables);
+    void qvortex(const mlegs_vortex* v, int n, Field* PSI, Field* CHI);
     void hyp3adj(const Field* PSI, const Field* CHI, const Field* B);
     void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
@@ -1159,6 +1160,45 @@ void mlegs_ctx::diagnost(const Field* PSI, const Field* CHI, double out[11]) {
     };
     out[5] = at1range(ps);
     out[6] = at1range(cs);
+}
+
+// QVORTEX(PSI, CHI), mod_layout.f90:449-609 (NOISE = 0): for PSI, LAY with
+// GAUSDATA%Q = 2 QPAIR%Q and B = 1 for every vortex; for CHI, Q = QPAIR%H and
+// B = QPAIR%B; each then TOFF, negated with LN 0, and inverted by IDELSQH.
+void mlegs_ctx::qvortex(const mlegs_vortex* v, int n, Field* PSI, Field* CHI) {
+    if (!v || n < 1) throw ApiError(MLEGS_ERR_ARG, "QVORTEX: no vortices");
+    for (int i = 0; i < n; ++i)  // R0 = R + DR sin(.) must stay positive on every plane
+        if (!(v[i].r > std::fabs(v[i].dr)))
+            throw ApiError(MLEGS_ERR_ARG, "QVORTEX: the core radius R must be larger than |DR|");
+    // vortex list and per-field strengths / decays in one device buffer
+    const size_t vb = (size_t)n * sizeof(mlegs_vortex);
+    std::vector<double> qb(4 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        qb[i] = 2.0 * v[i].q;
+        qb[n + i] = 1.0;
+        qb[2 * n + i] = v[i].h;
+        qb[3 * n + i] = v[i].b;
+    }
+    uint8_t* dbuf = nullptr;
+    CK(cudaMallocAsync((void**)&dbuf, vb + qb.size() * sizeof(double), s));
+    CK(cudaMemcpyAsync(dbuf, v, vb, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dbuf + vb, qb.data(), qb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    const mlegs_vortex* dv = (const mlegs_vortex*)dbuf;
+    const double* dq = (const double*)(dbuf + vb);
+    Field* A = tmp(MLEGS_PPP);
+    Field* out[2] = {PSI, CHI};
+    for (int f = 0; f < 2; ++f) {
+        A->space = MLEGS_PPP;
+        k_fill(A->data, d.ppp(), s);
+        k_lay_gaus(g, p.zlen, dv, n, dq + 2 * f * n, dq + (2 * f + 1) * n, A->data, s);
+        toff(A, 0);
+        k_axpby(A->data, -1.0, A->data, 0.0, nullptr, 0.0, fff(), s);
+        ln_zero(A);
+        idelsqh(A, out[f], 0);
+    }
+    rel(A);
+    CK(cudaFreeAsync(dbuf, s));
+    CK(cudaStreamSynchronize(s));
 }
 
 // CALC_BOUSSI_PE(B), mod_boussinesq.f90:112-136: WK = B, LN 0, RTRAN at the
@@ -2140,6 +2180,20 @@ int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe) {
         ctx->mark();
         try {
             ctx->boussi_pe(F(b), pe);
+        } catch (...) {
+            ctx->restore();
+            throw;
+        }
+        ctx->restore();
+    });
+}
+
+int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, mlegs_field* psi, mlegs_field* chi) {
+    return guard(ctx, [&] {
+        if (F(psi)->data == F(chi)->data) throw ApiError(MLEGS_ERR_ARG, "QVORTEX: PSI and CHI must be distinct");
+        ctx->mark();
+        try {
+            ctx->qvortex(vortices, n, F(psi), F(chi));
         } catch (...) {
             ctx->restore();
             throw;

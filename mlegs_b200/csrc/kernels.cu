@@ -999,6 +999,46 @@ void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const doubl
     count_launch();
 }
 
+// LAY(A, GAUS, IP = 2) (mod_layout.f90:64-117) for a list of vortices at once:
+// A += GAUS(R, THR/THI, Z) / (1-x)^2 per vortex, GAUS (640-672) a Gaussian of
+// strength Q / R0^2 and decay B around a centre displaced by DX, DY sin(AK1 Z - DP)
+// with core R0 = R + DR sin(RK Z - RP); Z = ZLEN (z) / NX.  PPP [r][z][j].
+__global__ void lay_gaus_kernel(DevGrid g, double zlen, const mlegs_vortex* v, int nv, const double* q, const double* b,
+                                double2* a) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t plane = (size_t)g.NX * g.NTH;
+    if (t >= (size_t)g.NR * plane) return;
+    const int i = (int)(t / plane), z = (int)((t / g.NTH) % g.NX), j = (int)(t % g.NTH);
+    const double pi = 3.141592653589793238462643383279502884;
+    const double r = g.r[i], om = 1.0 - g.x[i], f = om * om;
+    const double zz = zlen * z / g.NX;
+    const double th[2] = {2.0 * pi / g.NTH * j, 2.0 * pi / g.NTH * (j + 0.5)};
+    double2 acc = a[t];
+    for (int p = 0; p < nv; ++p) {
+        const double ak1 = 2.0 * pi * v[p].k / zlen, rk = 2.0 * pi * v[p].rk / zlen;
+        const double dp = pi / 180.0 * v[p].dp, rp = pi / 180.0 * v[p].rp;
+        const double xc = v[p].x + v[p].dx * sin(ak1 * zz - dp);
+        const double yc = v[p].y + v[p].dy * sin(ak1 * zz - dp);
+        const double r0 = v[p].r + v[p].dr * sin(rk * zz - rp);
+        double val[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const double x = r * cos(th[h]), y = r * sin(th[h]);
+            const double r2 = ((x - xc) * (x - xc) + (y - yc) * (y - yc)) / (r0 * r0);
+            val[h] = q[p] / (r0 * r0) * exp(-b[p] * r2);
+        }
+        acc.x += val[0] / f;
+        acc.y += val[1] / f;
+    }
+    a[t] = acc;
+}
+void k_lay_gaus(const DevGrid& g, double zlen, const mlegs_vortex* v, int nv, const double* q, const double* b,
+                double2* a, cudaStream_t s) {
+    const size_t n = (size_t)g.NR * g.NX * g.NTH;
+    lay_gaus_kernel<<<nblk(n, 256), 256, 0, s>>>(g, zlen, v, nv, q, b, a);
+    count_launch();
+}
+
 // dst = src * {1, R cos(th), R sin(th), R^2}[mode] on PPP [r][z][j], the re
 // sample at THR(j) = 2 pi j / NTH and the im sample at THI(j) = 2 pi (j + 1/2) / NTH
 // (MULRCOSTH / MULRSINTH / MULR2, mod_march.f90:2102-2225; TFM%THR/THI, mod_fft.f90:323-324).

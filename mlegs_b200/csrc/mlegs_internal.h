@@ -253,6 +253,8 @@ double pdajust(double coeff, double current, double previous, double baseline, c
                bool has_threshold, double threshold);
 void hyp3adj_update(Hyp3State& st, const double* em, int nm, const double* ek, int nk, double nup[3],
                     const double* pm, int npm, const double* pk, int npk, double kap[3]);
+void k_lay_gaus(const DevGrid& g, double zlen, const mlegs_vortex* v, int nv, const double* q, const double* b,
+                double2* a, cudaStream_t s);
 void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const double2* w, double2* a, cudaStream_t s);
 void k_mulr(const DevGrid& g, const double2* src, double2* dst, int mode, cudaStream_t s);
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);

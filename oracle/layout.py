@@ -3,7 +3,8 @@
 Restates:
   mod_layout.f90:64-117   LAY      (analytic field at collocation points, /(1-x)^IP)
   mod_layout.f90:449-609  QVORTEX  (omega_z = 2Q exp(-B r^2/R0^2)/R0^2 -> psi via IDELSQH)
-  mod_layout.f90:640-672  GAUS
+  mod_layout.f90:640-672  GAUS (with the z-waviness DX, DY, K, DP and the core
+                          modulation DR, RK, RP of a QPAIR entry)
 The seeded spectral perturbation that the benchmark configurations add on
 top of the vortex is synthetic input data, generated by the caller and
 passed in as FFF coefficient arrays.
@@ -35,6 +36,58 @@ def gaus_ppp(g, q, b=1.0, r0=1.0, xc=0.0, yc=0.0, ip=2):
     A.E[:g.NR, :g.NTH, :] = (vr + 1j * vi)[:, :, None]
     g.chopdo(A)
     return A
+
+
+VORTEX_KEYS = ("x", "y", "q", "h", "b", "dx", "dy", "k", "dp", "r", "dr", "rk", "rp")
+
+
+def vortex(**kw):
+    """One QPAIR entry with the reference's defaults (Q = 1, B = 1, R = 1, rest 0)."""
+    v = dict(x=0.0, y=0.0, q=1.0, h=0.0, b=1.0, dx=0.0, dy=0.0, k=0.0, dp=0.0, r=1.0, dr=0.0, rk=0.0, rp=0.0)
+    v.update(kw)
+    return v
+
+
+def lay_gaus(g, A, q, b, v):
+    """A += LAY(GAUS, IP = 2) of one vortex with GAUSDATA%Q = q, %B = b and the
+    centre / core modulation of v (GAUS, mod_layout.f90:640-672; Z = ZLEN (KK-1) / NX)."""
+    r = g.R[:g.NR, None, None]
+    f = (1 - g.X[:g.NR, None, None]) ** 2
+    z = g.Z[None, None, :g.NX]
+    ak1 = 2 * np.pi * v["k"] / g.ZLEN
+    rk = 2 * np.pi * v["rk"] / g.ZLEN
+    dp = np.pi / 180.0 * v["dp"]
+    rp = np.pi / 180.0 * v["rp"]
+    xc = v["x"] + v["dx"] * np.sin(ak1 * z - dp)
+    yc = v["y"] + v["dy"] * np.sin(ak1 * z - dp)
+    r0 = v["r"] + v["dr"] * np.sin(rk * z - rp)
+
+    def gaus(th):
+        x = r * np.cos(th)[None, :, None]
+        y = r * np.sin(th)[None, :, None]
+        r2 = ((x - xc) ** 2.0 + (y - yc) ** 2.0) / r0 ** 2.0
+        return q / r0 ** 2.0 * np.exp(-b * r2)
+
+    A.E[:g.NR, :g.NTH, :g.NX] += gaus(g.THR[:g.NTH]) / f + 1j * (gaus(g.THI[:g.NTH]) / f)
+    return A
+
+
+def qvortex_list(g, vortices):
+    """QVORTEX(PSI, CHI), mod_layout.f90:449-609, NOISE = 0, for a QPAIR list."""
+    out = []
+    for field in ("psi", "chi"):
+        A = g.alloc(PPP)
+        for v in vortices:
+            if field == "psi":
+                lay_gaus(g, A, 2.0 * v["q"], 1.0, v)
+            else:
+                lay_gaus(g, A, v["h"], v["b"], v)
+        g.chopdo(A)
+        toff(g, A)
+        A.E = -A.E
+        A.LN = 0.0
+        out.append(idelsqh(g, A))
+    return out[0], out[1]
 
 
 def qvortex(g, q=1.0, h=0.0, b=1.0, r0=1.0, xc=0.0, yc=0.0):

@@ -322,6 +322,30 @@ def test_qvortex_on_device(env):
     assert rel(E, P.E) < 1e-12
 
 
+def test_qvortex_list_on_device(env):
+    """QVORTEX for a QPAIR list with every GAUS parameter in use (H, B, the
+    z-waviness DX, DY, K, DP and the core modulation DR, RK, RP): LAY on the
+    device, TOFF, IDELSQH, against the oracle."""
+    M, ctx, g, cfg = env
+    from oracle import layout
+    vs = [dict(x=0.4, y=-0.2, q=1.0, h=0.3, b=1.5, dx=0.05, dy=-0.03, k=1.0, dp=30.0, r=1.0, dr=0.1, rk=2.0,
+               rp=-45.0),
+          dict(x=-0.5, y=0.6, q=-0.7, h=-0.2, b=0.8, r=0.8)]
+    psi, chi = M.QVORTEX(ctx, vs)
+    P, C = layout.qvortex_list(g, [layout.vortex(**v) for v in vs])
+    for f, R in ((psi, P), (chi, C)):
+        E, ln = f.download()
+        assert rel(E, R.E) < 1e-12
+        assert abs(ln - R.LN) < 1e-12 * max(1.0, abs(R.LN))
+    # the log term is the circulation: -(sum of Q) / 2 for PSI, -(sum of H / B) / 4 for CHI
+    tol = 1e-12 if cfg.nr >= 64 else 1e-6
+    assert abs(psi.download()[1] + 0.5 * (1.0 - 0.7)) < tol
+    assert abs(chi.download()[1] + (0.3 / 1.5 - 0.2 / 0.8) / 4.0) < tol
+    with pytest.raises(M.MlegsError) as ei:   # R0 = R + DR sin(.) would reach zero
+        M.QVORTEX(ctx, [dict(r=0.1, dr=0.2)])
+    assert ei.value.code == 101
+
+
 def test_boussi_force(env):
     from oracle import boussinesq as BQ
     from oracle import layout

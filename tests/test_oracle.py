@@ -97,6 +97,24 @@ def test_qvortex_logterm(xc):
     assert chi.LN == 0.0
 
 
+def test_qvortex_list_logterms():
+    """QVORTEX over a QPAIR list: PSI%LN = -sum(Q)/2 and CHI%LN = -sum(H/B)/4
+    (the circulations 2 pi Q and pi H / B of the Gaussians over 4 pi), with the
+    z-waviness and core modulation in use; a one-entry list equals the
+    single-vortex form."""
+    from oracle import layout
+    g = oracle_grid(small_cfg(64, 32, 32))
+    vs = [layout.vortex(x=0.4, y=-0.2, q=1.0, h=0.3, b=1.5, dx=0.05, dy=-0.03, k=1.0, dp=30.0, dr=0.1,
+                        rk=2.0, rp=-45.0),
+          layout.vortex(x=-0.5, y=0.6, q=-0.7, h=-0.2, b=0.8, r=0.8)]
+    psi, chi = layout.qvortex_list(g, vs)
+    assert abs(psi.LN + 0.5 * 0.3) < 1e-12
+    assert abs(chi.LN + (0.3 / 1.5 - 0.2 / 0.8) / 4.0) < 1e-12
+    p1, c1 = layout.qvortex(g, q=1.0, h=0.5, b=2.0, r0=1.2, xc=0.3, yc=-0.1)
+    p2, c2 = layout.qvortex_list(g, [layout.vortex(q=1.0, h=0.5, b=2.0, r=1.2, x=0.3, y=-0.1)])
+    assert np.array_equal(p1.E, p2.E) and np.array_equal(c1.E, c2.E) and p1.LN == p2.LN
+
+
 def test_etd_matches_expm():
     from oracle.boussinesq import calc_boussi_diag, calc_boussi_etd_op
     J, S, Si = calc_boussi_diag(2.0, 1.0)

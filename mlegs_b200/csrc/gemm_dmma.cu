@@ -42,12 +42,15 @@ __device__ __forceinline__ void cp16(void* dst, const void* src, bool ok) {
 }  // namespace
 
 // RTRAN(+1).  Per m, the K rows of both parities (t < kp_p, n = 2t + p) go in
-// chunks of KCB = 16 through a two-stage cp.async ring: A [KCB][SA] (PF rows
+// chunks of KCB = 16 through an NST_B2P-stage cp.async ring: A [KCB][SA] (PF rows
 // n, i contiguous) and B [KCB][SBS] (A(n, c0 .. c0+31)).  The even- and
 // odd-parity products accumulate in separate registers; the epilogue forms
 // B(i) = C_0 + C_1 and B(NR-1-i) = C_0 - C_1.  The output-row m-tiles go
 // round-robin over NW warps.
 constexpr int KCB = 16;
+constexpr int NST_B2P = 2;   // ring stages of b2p_dmma_kernel
+constexpr int NST_FOLD = 2;  // ring stages of legfold_dmma_kernel
+constexpr int NST_PFFF = 2;  // ring stages of projfff_dmma_kernel
 
 template <int NW, int MTW>
 __global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const double* __restrict__ A,
@@ -72,7 +75,7 @@ __global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const doub
     auto stage = [&](int cidx) {
         const int p = cidx < nc0 ? 0 : 1;
         const int t0 = (cidx - (p ? nc0 : 0)) * KCB, kp = p ? kp1 : kp0;
-        double* As = smd + (cidx & 1) * stg;
+        double* As = smd + (cidx % NST_B2P) * stg;
         double* Bs = As + (size_t)KCB * SA;
         for (int e = tid; e < KCB * ach; e += NW * 32) {
             const int tt = e / ach, ch = e - tt * ach;
@@ -114,16 +117,19 @@ __global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const doub
     for (int i = 0; i < MTW; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc0[i][j][0] = acc0[i][j][1] = acc1[i][j][0] = acc1[i][j][1] = 0.0;
-    if (total > 0) stage(0);
+    // ring: NST_B2P - 1 chunks in flight ahead of the one computed; every
+    // iteration commits one group (empty past the end), so the wait count is fixed
+#pragma unroll
+    for (int c = 0; c < NST_B2P - 1; ++c) {
+        if (c < total) stage(c);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int cidx = 0; cidx < total; ++cidx) {
-        if (cidx + 1 < total) {
-            stage(cidx + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
+        if (cidx + NST_B2P - 1 < total) stage(cidx + NST_B2P - 1);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NST_B2P - 1) : "memory");
         __syncthreads();
-        const double* As = smd + (cidx & 1) * stg;
+        const double* As = smd + (cidx % NST_B2P) * stg;
         const double* Bs = As + (size_t)KCB * SA;
         const int p = cidx < nc0 ? 0 : 1;
         const int t0 = (cidx - (p ? nc0 : 0)) * KCB, kp = p ? kp1 : kp0;
@@ -211,7 +217,7 @@ __global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, Fol
     const int nch = (g.NRH + KC2 - 1) / KC2;
     const int total = fa.nseg * nch;
     const size_t stA = (size_t)RTmax * 8 * SA2, stX = (size_t)2 * KC2 * SX2;
-    double* Bs = smd + 2 * (stA + stX);  // [KC2][SX2] folded, scaled chunk
+    double* Bs = smd + NST_FOLD * (stA + stX);  // [KC2][SX2] folded, scaled chunk
     double* ws = Bs + KC2 * SX2;         // [nch * KC2] fold weights (w_i, or 1), 0 past NRH
     const size_t wofs = (size_t)m * fa.wt_rows * g.NRH, xofs = (size_t)m * g.NR * ncol;
     for (int i = tid; i < nch * KC2; i += NW * 32) ws[i] = (i < g.NRH) ? (fa.use_w ? g.w[i] : 1.0) : 0.0;
@@ -224,7 +230,7 @@ __global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, Fol
         const int sg = gc / nch, i0 = (gc - sg * nch) * KC2;
         const double* w = pick5(fa.w, sg) + wofs;
         const double* x = pick5(fa.x, sg) + xofs;
-        double* As = smd + (gc & 1) * (stA + stX);
+        double* As = smd + (gc % NST_FOLD) * (stA + stX);
         double* Xs = As + stA;
         for (int e = tid; e < RTv * 8 * (KC2 / 2); e += NW * 32) {
             const int r = e / (KC2 / 2), c2 = e - r * (KC2 / 2);
@@ -273,17 +279,18 @@ __global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, Fol
     for (int t = 0; t < MTW; ++t)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
-    stage(0);
+#pragma unroll
+    for (int c = 0; c < NST_FOLD - 1; ++c) {
+        if (c < total) stage(c);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int gc = 0; gc < total; ++gc) {
-        if (gc + 1 < total) {
-            stage(gc + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
+        if (gc + NST_FOLD - 1 < total) stage(gc + NST_FOLD - 1);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NST_FOLD - 1) : "memory");
         __syncthreads();
         const int sg = gc / nch, ch = gc - sg * nch;
-        const double* As = smd + (gc & 1) * (stA + stX);
+        const double* As = smd + (gc % NST_FOLD) * (stA + stX);
         const double* Xs = As + stA;
         const double sgn = (pr ^ pick5(fa.mode, sg)) ? -1.0 : 1.0;
         const int sc = pick5(fa.scale, sg);
@@ -411,7 +418,7 @@ __global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, Pro
         const int kp = odd ? kpO : kpS, p = pr ^ (odd ? 1 : 0), t0 = ch * KC2;
         const double* cm = pick5(pa.C, sg) + cofs;
         const double* x = pick5(pa.x, sg) + xofs;
-        double* As = smd + (gc & 1) * (stA + stB);
+        double* As = smd + (gc % NST_PFFF) * (stA + stB);
         double* Bs = As + stA;
         for (int e = tid; e < RTv * 8 * (KC2 / 2); e += NW * 32) {
             const int r = e / (KC2 / 2), c2 = e - r * (KC2 / 2);
@@ -460,14 +467,15 @@ __global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, Pro
         for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
     if (npsi == 0) epilogue(acc, pa.psi);
     if (total == npsi) epilogue(acc, pa.chi);
-    if (total > 0) stage(0);
+#pragma unroll
+    for (int c = 0; c < NST_PFFF - 1; ++c) {
+        if (c < total) stage(c);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int gc = 0; gc < total; ++gc) {
-        if (gc + 1 < total) {
-            stage(gc + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
+        if (gc + NST_PFFF - 1 < total) stage(gc + NST_PFFF - 1);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NST_PFFF - 1) : "memory");
         __syncthreads();
         int sg, ch;
         locate(gc, sg, ch);
@@ -487,7 +495,7 @@ __global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, Pro
             }
         }
         const int bcol = swap ? (gq ^ 1) : gq;
-        const double* As = smd + (gc & 1) * (stA + stB);
+        const double* As = smd + (gc % NST_PFFF) * (stA + stB);
         const double* Bs = As + stA;
 #pragma unroll
         for (int s4 = 0; s4 < KC2 / 4; ++s4) {
@@ -522,7 +530,7 @@ bool dmma_supported(const DevGrid& g) { return g.NRH <= 128 && g.NRH % 2 == 0 &&
 template <int NW, int MTW>
 static void b2p_launch(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
     const int SA = pad16_8(((g.NRH + 7) / 8) * 8);
-    const size_t smem = 2 * (size_t)KCB * (SA + SBS) * sizeof(double);
+    const size_t smem = NST_B2P * (size_t)KCB * (SA + SBS) * sizeof(double);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(b2p_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -548,7 +556,7 @@ static void legfold_launch(const DevGrid& g, const FoldArgs& fa, cudaStream_t s)
     const int RT = ((g.NRCHOPDIM + 1) / 2 + 7) / 8;
     const int nch = (g.NRH + KC2 - 1) / KC2;
     const size_t smem =
-        (2 * ((size_t)RT * 8 * SA2 + (size_t)2 * KC2 * SX2) + (size_t)KC2 * SX2 + (size_t)nch * KC2) * sizeof(double);
+        (NST_FOLD * ((size_t)RT * 8 * SA2 + (size_t)2 * KC2 * SX2) + (size_t)KC2 * SX2 + (size_t)nch * KC2) * sizeof(double);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(legfold_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -625,7 +633,7 @@ template <int NW, int MTW>
 static void projfff_launch(const DevGrid& g, const ProjFffArgs& pa, cudaStream_t s) {
     const int RC = (g.NRCHOPDIM + 1) / 2, KPC = (((g.NRCHOP + 1) / 2) + KC2 - 1) / KC2 * KC2;
     const int RT = (RC + 7) / 8;
-    const size_t smem = 2 * ((size_t)RT * 8 * SA2 + (size_t)KC2 * SX2) * sizeof(double);
+    const size_t smem = NST_PFFF * ((size_t)RT * 8 * SA2 + (size_t)KC2 * SX2) * sizeof(double);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(projfff_dmma_kernel<NW, MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);

@@ -200,10 +200,14 @@ typedef struct mlegs_vortex {
     double x, y, q, h, b, dx, dy, k, dp, r, dr, rk, rp;
 } mlegs_vortex;
 
-/* QVORTEX(PSI, CHI) (mod_layout.f90:449-609) with NOISE = 0, on the device:
- * LAY(A, GAUS, 2) of every vortex (Q -> 2Q, B -> 1 for PSI; Q -> H, B for
- * CHI), TOFF, A = -A with LN 0, IDELSQH.  psi and chi end in FFF.  n >= 1. */
-int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, mlegs_field* psi, mlegs_field* chi);
+/* QVORTEX(PSI, CHI) (mod_layout.f90:449-609) on the device: LAY(A, GAUS, 2)
+ * of every vortex (Q -> 2Q, B -> 1 for PSI; Q -> H, B for CHI), TOFF, A = -A
+ * with LN 0, IDELSQH.  psi and chi end in FFF.  n >= 1.
+ * noise_seeds: NULL for QPAIR%NOISE = 0; else NOISE = 1 with the two RAN0
+ * seeds ISEED (>= 0) for PSI and CHI, which the reference draws from
+ * RANDOM_NUMBER (mod_layout.f90:175-177) and which are explicit here. */
+int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, const int32_t* noise_seeds,
+                  mlegs_field* psi, mlegs_field* chi);
 
 /* Adaptive hyperviscosity (VISC%ADJSW /= 0 with VISC%SW = 3).
  * ENEMON(PSI, CHI, EM, EK) (mod_march.f90:2585-2617) at CHOPSET(pad):

@@ -369,10 +369,11 @@ VORTEX_DEFAULTS = dict(x=0.0, y=0.0, q=1.0, h=0.0, b=1.0, dx=0.0, dy=0.0, k=0.0,
                        r=1.0, dr=0.0, rk=0.0, rp=0.0)
 
 
-def QVORTEX(ctx, vortices):
-    """QVORTEX(PSI, CHI) (mod_layout.f90:449-609, NOISE = 0) on the device for a
-    QPAIR list: each entry a dict with any of the keys of VORTEX_DEFAULTS (X, Y,
-    Q, H, B, DX, DY, K, DP, R, DR, RK, RP in lower case).  Returns (psi, chi)."""
+def QVORTEX(ctx, vortices, noise_seeds=None):
+    """QVORTEX(PSI, CHI) (mod_layout.f90:449-609) on the device for a QPAIR
+    list: each entry a dict with any of the keys of VORTEX_DEFAULTS (X, Y, Q, H,
+    B, DX, DY, K, DP, R, DR, RK, RP in lower case).  noise_seeds: None for
+    NOISE = 0, or the two RAN0 seeds (PSI, CHI) of NOISE = 1.  Returns (psi, chi)."""
     arr = (_lib.Vortex * len(vortices))()
     for i, v in enumerate(vortices):
         unknown = set(v) - set(VORTEX_DEFAULTS)
@@ -382,7 +383,10 @@ def QVORTEX(ctx, vortices):
         for key, val in full.items():
             setattr(arr[i], key, float(val))
     psi, chi = ctx.field(FFF), ctx.field(FFF)
-    ctx._ck(ctx.lib.mlegs_qvortex(ctx.c, arr, len(vortices), psi.h, chi.h))
+    seeds = None
+    if noise_seeds is not None:
+        seeds = (ctypes.c_int32 * 2)(*[int(x) for x in noise_seeds])
+    ctx._ck(ctx.lib.mlegs_qvortex(ctx.c, arr, len(vortices), seeds, psi.h, chi.h))
     return psi, chi
 
 

@@ -81,7 +81,7 @@ SIGNATURES = {
     "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mlegs_diagnost": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
-    "mlegs_qvortex": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "mlegs_qvortex": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "mlegs_enemon": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "mlegs_hyp3adj": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_hyp3_coeffs": (c_int, [c_void_p, c_void_p]),

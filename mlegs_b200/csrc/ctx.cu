@@ -490,7 +490,7 @@ struct mlegs_ctx {
     void boussi_pe(const Field* B, double* pe);
     void enemon(const Field* PSI, const Field* CHI, int pad, double* em, double* ek);
     void hyp3set(const double nu[3], double** tables);
-    void qvortex(const mlegs_vortex* v, int n, Field* PSI, Field* CHI);
+    void qvortex(const mlegs_vortex* v, int n, const int32_t* seeds, Field* PSI, Field* CHI);
     void hyp3adj(const Field* PSI, const Field* CHI, const Field* B);
     void halfk(const double* all, double sign, double* out, bool accumulate) const;
     void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
@@ -1162,10 +1162,12 @@ void mlegs_ctx::diagnost(const Field* PSI, const Field* CHI, double out[11]) {
     out[6] = at1range(cs);
 }
 
-// QVORTEX(PSI, CHI), mod_layout.f90:449-609 (NOISE = 0): for PSI, LAY with
-// GAUSDATA%Q = 2 QPAIR%Q and B = 1 for every vortex; for CHI, Q = QPAIR%H and
-// B = QPAIR%B; each then TOFF, negated with LN 0, and inverted by IDELSQH.
-void mlegs_ctx::qvortex(const mlegs_vortex* v, int n, Field* PSI, Field* CHI) {
+// QVORTEX(PSI, CHI), mod_layout.f90:449-609: for PSI, LAY with GAUSDATA%Q =
+// 2 QPAIR%Q and B = 1 for every vortex; for CHI, Q = QPAIR%H and B = QPAIR%B;
+// each then TOFF, negated with LN 0, and inverted by IDELSQH.  With seeds (the
+// NOISE = 1 path, 550-559 / 585-594), before IDELSQH: B = A, NOISE(A, 0.02)
+// with ISEED = seeds[field], TOFP of both, FLATTEN(A, B), TOFF(A).
+void mlegs_ctx::qvortex(const mlegs_vortex* v, int n, const int32_t* seeds, Field* PSI, Field* CHI) {
     if (!v || n < 1) throw ApiError(MLEGS_ERR_ARG, "QVORTEX: no vortices");
     for (int i = 0; i < n; ++i)  // R0 = R + DR sin(.) must stay positive on every plane
         if (!(v[i].r > std::fabs(v[i].dr)))
@@ -1194,6 +1196,21 @@ void mlegs_ctx::qvortex(const mlegs_vortex* v, int n, Field* PSI, Field* CHI) {
         toff(A, 0);
         k_axpby(A->data, -1.0, A->data, 0.0, nullptr, 0.0, fff(), s);
         ln_zero(A);
+        if (seeds) {
+            Field* Bc = tmp();
+            copy0(Bc, A, 0);
+            const double akmax0 = 2.0 * 3.141592653589793238462643383279502884 / p.zlen * (d.NXCHOP - 1);
+            k_maxabs(A->data, fff(), 0, diag, s);
+            k_noise(g, A->data, diag, 0.02, akmax0 == 0.0 ? 1.0 : akmax0,
+                    (long long)(((uint32_t)seeds[f]) ^ 123459876u), s);
+            chopdo(A, 0);
+            tofp(A, 0);
+            tofp(Bc, 0);
+            k_maxabs(A->data, d.ppp(), 1, diag, s);
+            k_flatten(g, A->data, Bc->data, diag, s);
+            toff(A, 0);
+            rel(Bc);
+        }
         idelsqh(A, out[f], 0);
     }
     rel(A);
@@ -2188,12 +2205,15 @@ int mlegs_boussi_pe(mlegs_ctx* ctx, const mlegs_field* b, double* pe) {
     });
 }
 
-int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, mlegs_field* psi, mlegs_field* chi) {
+int mlegs_qvortex(mlegs_ctx* ctx, const mlegs_vortex* vortices, int n, const int32_t* noise_seeds, mlegs_field* psi,
+                  mlegs_field* chi) {
     return guard(ctx, [&] {
         if (F(psi)->data == F(chi)->data) throw ApiError(MLEGS_ERR_ARG, "QVORTEX: PSI and CHI must be distinct");
+        if (noise_seeds && (noise_seeds[0] < 0 || noise_seeds[1] < 0))
+            throw ApiError(MLEGS_ERR_ARG, "QVORTEX: noise seeds must be non-negative");
         ctx->mark();
         try {
-            ctx->qvortex(vortices, n, F(psi), F(chi));
+            ctx->qvortex(vortices, n, noise_seeds, F(psi), F(chi));
         } catch (...) {
             ctx->restore();
             throw;

@@ -1039,6 +1039,92 @@ void k_lay_gaus(const DevGrid& g, double zlen, const mlegs_vortex* v, int nv, co
     count_launch();
 }
 
+// max over n values of |a| (mode 0) or |Re a| (mode 1) into *out (zeroed by the
+// caller); non-negative doubles order like their bit patterns.
+__global__ void maxabs_kernel(const double2* a, size_t n, int mode, unsigned long long* out) {
+    double mx = 0.0;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = a[t];
+        mx = fmax(mx, mode ? fabs(v.x) : hypot(v.x, v.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
+void k_maxabs(const double2* a, size_t n, int mode, double* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(double), s);
+    int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    if (blocks < 1) blocks = 1;
+    maxabs_kernel<<<blocks, 256, 0, s>>>(a, n, mode, (unsigned long long*)out);
+    count_launch();
+}
+
+// NOISE(A, ALEVEL), mod_layout.f90:165-226, on the FFF layout [m][n][k]: for
+// m < NTCHOP, n < NRCHOPS(m) (pad 0), all k, in the reference's loop order
+// (m, n, k) the call pair (2j, 2j+1) of RAN0 (196-214) gives X and Y; RAN0's
+// state is the Park-Miller sequence v_{j+1} = 16807 v_j mod (2^31 - 1) from
+// v_0 = ISEED xor 123459876, output v_{j+1} / (2^31 - 1), so element j jumps
+// ahead by modular powers.  FAC = 0.1 exp(-12 ((AK/AKMAX)^2 + (N/NRCHOP)^2))
+// with the reference's default-real literal 0.1 and FLOAT(N)/NRCHOP in single
+// precision; CMPLX(X, Y) rounds X, Y to single precision before the product with
+// REFVAL = ALEVEL max|A| (refmax holds max|A|).
+__device__ __forceinline__ unsigned long long powmod_ia(unsigned long long e) {
+    const unsigned long long IM = 2147483647ull;
+    unsigned long long r = 1, b = 16807;
+    while (e) {
+        if (e & 1) r = r * b % IM;
+        b = b * b % IM;
+        e >>= 1;
+    }
+    return r;
+}
+__global__ void noise_kernel(DevGrid g, double2* a, const double* refmax, double alevel, double akmax, long long v0) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int m, n, k;
+    if (!fff_index(g, t, m, n, k)) return;
+    const int mlim = g.NTCHOP < g.NTCHOPDIM ? g.NTCHOP : g.NTCHOPDIM;
+    if (m >= mlim || n >= nrchops(g, m, 0)) return;
+    long long row = n;  // rows before (m, n) in the (m, n) loop order
+    for (int mm = 0; mm < m; ++mm) row += nrchops(g, mm, 0);
+    const unsigned long long j = 2ull * ((unsigned long long)row * g.NXCHOPDIM + k);
+    const unsigned long long IM = 2147483647ull;
+    const double AM = 1.0 / 2147483647.0;
+    const unsigned long long vx = powmod_ia(j + 1) * (unsigned long long)v0 % IM;
+    const unsigned long long vy = vx * 16807ull % IM;
+    const double akr = g.ak[k] / akmax;
+    const float q = (float)(m + n) / (float)g.NRCHOP;
+    const float q2 = q * q;
+    const double fac = (double)0.1f * exp(-12.0 * (akr * akr + (double)q2));
+    const float x = (float)(fac * (AM * (double)vx)), y = (float)(fac * (AM * (double)vy));
+    const double refval = alevel * *refmax;
+    double2 v = a[t];
+    v.x += (double)x * refval;
+    v.y += (double)y * refval;
+    a[t] = v;
+}
+void k_noise(const DevGrid& g, double2* a, const double* refmax, double alevel, double akmax, long long v0,
+             cudaStream_t s) {
+    const size_t n = g.NTCHOPDIM * (size_t)g.NRCHOPDIM * g.NXCHOPDIM;
+    noise_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, refmax, alevel, akmax, v0);
+    count_launch();
+}
+
+// FLATTEN(A, B), mod_layout.f90:228-278, on PPP: A = B + (A - B) tanh(20 B / REFVAL)^2
+// per packed sample, REFVAL = max |Re A| (1 if zero; refmax holds it).
+__global__ void flatten_kernel(DevGrid g, double2* a, const double2* b, const double* refmax) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= (size_t)g.NR * g.NX * g.NTH) return;
+    double refval = *refmax;
+    if (refval == 0.0) refval = 1.0;
+    const double2 rb = b[t], av = a[t];
+    const double fr = tanh(rb.x / refval * 20.0), fi = tanh(rb.y / refval * 20.0);
+    a[t] = make_double2(rb.x + (av.x - rb.x) * (fr * fr), rb.y + (av.y - rb.y) * (fi * fi));
+}
+void k_flatten(const DevGrid& g, double2* a, const double2* b, const double* refmax, cudaStream_t s) {
+    const size_t n = (size_t)g.NR * g.NX * g.NTH;
+    flatten_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, b, refmax);
+    count_launch();
+}
+
 // dst = src * {1, R cos(th), R sin(th), R^2}[mode] on PPP [r][z][j], the re
 // sample at THR(j) = 2 pi j / NTH and the im sample at THI(j) = 2 pi (j + 1/2) / NTH
 // (MULRCOSTH / MULRSINTH / MULR2, mod_march.f90:2102-2225; TFM%THR/THI, mod_fft.f90:323-324).

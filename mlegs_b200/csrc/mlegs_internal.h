@@ -255,6 +255,10 @@ void hyp3adj_update(Hyp3State& st, const double* em, int nm, const double* ek, i
                     const double* pm, int npm, const double* pk, int npk, double kap[3]);
 void k_lay_gaus(const DevGrid& g, double zlen, const mlegs_vortex* v, int nv, const double* q, const double* b,
                 double2* a, cudaStream_t s);
+void k_maxabs(const double2* a, size_t n, int mode, double* out, cudaStream_t s);
+void k_noise(const DevGrid& g, double2* a, const double* refmax, double alevel, double akmax, long long v0,
+             cudaStream_t s);
+void k_flatten(const DevGrid& g, double2* a, const double2* b, const double* refmax, cudaStream_t s);
 void k_absvec2(const DevGrid& g, const double2* u, const double2* v, const double2* w, double2* a, cudaStream_t s);
 void k_mulr(const DevGrid& g, const double2* src, double2* dst, int mode, cudaStream_t s);
 void k_etd_ab_fused(const DevGrid& g, const EtdAbArgs& a, cudaStream_t s);

@@ -5,6 +5,7 @@ Restates:
   mod_layout.f90:449-609  QVORTEX  (omega_z = 2Q exp(-B r^2/R0^2)/R0^2 -> psi via IDELSQH)
   mod_layout.f90:640-672  GAUS (with the z-waviness DX, DY, K, DP and the core
                           modulation DR, RK, RP of a QPAIR entry)
+  mod_layout.f90:165-278  NOISE, RAN0, FLATTEN (QPAIR%NOISE = 1, seeds explicit)
 The seeded spectral perturbation that the benchmark configurations add on
 top of the vortex is synthetic input data, generated by the caller and
 passed in as FFF coefficient arrays.
@@ -16,7 +17,7 @@ import numpy as np
 
 from .grid import FFF, PPP
 from .legops import idelsqh
-from .transforms import toff
+from .transforms import toff, tofp
 
 
 def gaus_ppp(g, q, b=1.0, r0=1.0, xc=0.0, yc=0.0, ip=2):
@@ -72,10 +73,67 @@ def lay_gaus(g, A, q, b, v):
     return A
 
 
-def qvortex_list(g, vortices):
-    """QVORTEX(PSI, CHI), mod_layout.f90:449-609, NOISE = 0, for a QPAIR list."""
+class Ran0:
+    """RAN0(IDUM), mod_layout.f90:196-214: Park-Miller minimal standard by
+    Schrage's method, with the XOR mask applied around each call."""
+    IA, IM, IQ, IR, MASK = 16807, 2147483647, 127773, 2836, 123459876
+
+    def __init__(self, iseed):
+        self.idum = int(iseed)
+
+    def __call__(self):
+        idum = self.idum ^ self.MASK
+        k = int(idum / self.IQ)                 # Fortran integer division truncates
+        idum = self.IA * (idum - k * self.IQ) - self.IR * k
+        if idum < 0:
+            idum += self.IM
+        val = (1.0 / self.IM) * idum
+        self.idum = idum ^ self.MASK
+        return val
+
+
+def noise(g, A, alevel, iseed):
+    """NOISE(A, ALEVEL), mod_layout.f90:165-226, on an FFF field with an explicit
+    ISEED.  Precision as written: the literal 0.1 and FLOAT(N)/NRCHOP are default
+    (single-precision) reals, and CMPLX(X, Y) rounds X and Y to single precision."""
+    ran = Ran0(iseed)
+    refval = alevel * np.abs(A.E).max()
+    akmax = np.abs(g.AK[:g.NTCHOP, :g.NXCHOP]).max()
+    if akmax == 0.0:
+        akmax = 1.0
+    c01 = np.float64(np.float32(0.1))
+    for mm in range(min(g.NTCHOP, A.E.shape[1])):
+        for nn in range(int(g.NRCHOPS[mm])):
+            n = int(g.M[mm]) + nn
+            q = np.float32(n) / np.float32(g.NRCHOP)
+            q2 = np.float64(np.float32(q * q))
+            for kk in range(A.E.shape[2]):
+                akr = g.AK[mm, kk] / akmax
+                fac = c01 * np.exp(-12.0 * (akr * akr + q2))
+                x = np.float64(np.float32(fac * ran()))
+                y = np.float64(np.float32(fac * ran()))
+                A.E[nn, mm, kk] += complex(x * refval, y * refval)
+    g.chopdo(A)
+    return A
+
+
+def flatten(g, A, B):
+    """FLATTEN(A, B), mod_layout.f90:228-278 (PPP): A = B + (A - B) tanh(20 B / REFVAL)^2,
+    REFVAL = max |Re A| (1 if zero), real and imaginary samples apart."""
+    refval = np.abs(A.E.real).max()
+    if refval == 0.0:
+        refval = 1.0
+    fr = np.tanh(B.E.real / refval * 20) ** 2
+    fi = np.tanh(B.E.imag / refval * 20) ** 2
+    A.E = (B.E.real + (A.E.real - B.E.real) * fr) + 1j * (B.E.imag + (A.E.imag - B.E.imag) * fi)
+    return A
+
+
+def qvortex_list(g, vortices, noise_seeds=None):
+    """QVORTEX(PSI, CHI), mod_layout.f90:449-609, for a QPAIR list; NOISE = 1
+    when noise_seeds gives the two RAN0 seeds (PSI, CHI)."""
     out = []
-    for field in ("psi", "chi"):
+    for f, field in enumerate(("psi", "chi")):
         A = g.alloc(PPP)
         for v in vortices:
             if field == "psi":
@@ -86,6 +144,13 @@ def qvortex_list(g, vortices):
         toff(g, A)
         A.E = -A.E
         A.LN = 0.0
+        if noise_seeds is not None:
+            B = g.copy0(A)
+            noise(g, A, 0.02, noise_seeds[f])
+            tofp(g, A)
+            tofp(g, B)
+            flatten(g, A, B)
+            toff(g, A)
         out.append(idelsqh(g, A))
     return out[0], out[1]
 

@@ -341,6 +341,14 @@ def test_qvortex_list_on_device(env):
     tol = 1e-12 if cfg.nr >= 64 else 1e-6
     assert abs(psi.download()[1] + 0.5 * (1.0 - 0.7)) < tol
     assert abs(chi.download()[1] + (0.3 / 1.5 - 0.2 / 0.8) / 4.0) < tol
+    # QPAIR%NOISE = 1 with explicit RAN0 seeds: NOISE, TOFP, FLATTEN, TOFF before IDELSQH
+    psn, chn = M.QVORTEX(ctx, vs, noise_seeds=(4242, 777))
+    Pn, Cn = layout.qvortex_list(g, [layout.vortex(**v) for v in vs], noise_seeds=(4242, 777))
+    for f, R, R0 in ((psn, Pn, P), (chn, Cn, C)):
+        E, ln = f.download()
+        assert rel(E, R.E) < 1e-9          # X, Y pass through single precision (CMPLX)
+        assert rel(R.E, R0.E) > 1e-5       # the noise is there
+        assert abs(ln - R.LN) < 1e-9 * max(1.0, abs(R.LN))
     with pytest.raises(M.MlegsError) as ei:   # R0 = R + DR sin(.) would reach zero
         M.QVORTEX(ctx, [dict(r=0.1, dr=0.2)])
     assert ei.value.code == 101

@@ -115,6 +115,40 @@ def test_qvortex_list_logterms():
     assert np.array_equal(p1.E, p2.E) and np.array_equal(c1.E, c2.E) and p1.LN == p2.LN
 
 
+def test_ran0_and_noise():
+    """RAN0 is the Park-Miller minimal standard behind an XOR mask: from state 1
+    the 10000th state is 1043618065 (Park & Miller's check value).  NOISE touches
+    only n < NRCHOPS(m), m < NTCHOP, with |dE| <= 0.1 ALEVEL max|A| per part;
+    FLATTEN keeps B where B is zero and A where |B| is large."""
+    from oracle import layout
+    r = layout.Ran0(1 ^ layout.Ran0.MASK)
+    for _ in range(10000):
+        r()
+    assert r.idum ^ layout.Ran0.MASK == 1043618065
+    g = oracle_grid(small_cfg(32, 16, 16))
+    psi, _ = layout.qvortex(g)
+    A = g.copy0(psi)
+    A0 = A.E.copy()
+    layout.noise(g, A, 0.02, 4242)
+    d = A.E - A0
+    ref = 0.02 * np.abs(A0).max()
+    assert np.abs(d.real).max() <= 0.1 * ref and np.abs(d.imag).max() <= 0.1 * ref and np.abs(d).max() > 0
+    for mm in range(g.NTCHOPDIM):
+        assert not np.any(d[int(g.NRCHOPS[mm]):, mm, :])
+    from oracle.grid import PPP
+    B = g.alloc(PPP)
+    B.E[:g.NR, :g.NTH, :] = 1.0 + 1.0j
+    B.E[0, 0, 0] = 0.0
+    C = g.alloc(PPP)
+    C.E[:] = 0.5
+    layout.flatten(g, C, B)
+    # REFVAL = max |Re A| = 0.5: where B = 0 the result is B; where B = 1 + i it is
+    # B + (A - B) tanh(20 / 0.5)^2 per part
+    t2 = np.tanh(40.0) ** 2
+    expect = (1.0 + (0.5 - 1.0) * t2) + 1j * (1.0 + (0.0 - 1.0) * t2)
+    assert C.E[0, 0, 0] == 0.0 and abs(C.E[1, 1, 1] - expect) < 1e-15
+
+
 def test_etd_matches_expm():
     from oracle.boussinesq import calc_boussi_diag, calc_boussi_etd_op
     J, S, Si = calc_boussi_diag(2.0, 1.0)

@@ -135,6 +135,11 @@ __device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, c
                                                  double2 (&o)[N1], int stride = 1, const double2* tw2 = nullptr) {
     constexpr int N = N1 * N2, U = N1 / N2;
     dft<N1, SIGN>(v, tw, N / N1);
+    // step 2 without tw2: W^{t k1} as running powers of W^t (one table read per
+    // lane instead of N1 - 1 reads that share banks), at most N1 - 2 rounded
+    // products away from the table value
+    const double2 w1 = twid<SIGN>(tw, t);
+    double2 wk = w1;
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
         double2 y = v[k1];
@@ -143,7 +148,8 @@ __device__ __forceinline__ void line_fft_inplace(double2 (&v)[N1], double2* L, c
                 const double2 w = tw2[k1 * N2 + t];
                 y = cmul(SIGN > 0 ? conj(w) : w, y);
             } else {
-                y = cmul(twid<SIGN>(tw, t * k1), y);
+                if (k1 > 1) wk = cmul(wk, w1);
+                y = cmul(wk, y);
             }
         }
         L[swz<N1, N2>(k1, t) * stride] = y;

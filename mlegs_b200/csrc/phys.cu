@@ -407,7 +407,19 @@ __device__ __forceinline__ void idle_group_syncs() {
     __syncwarp();
 }
 
-// Inverse HORFFT of one PFP row into the natural-order packed samples L[0..N).
+// Position of physical sample k inside a line slot.  The inverse transform's
+// lanes store samples U t + u + N1 k2 (stride U = N1/N2) and the forward
+// transform's lanes load samples t + N2 n1; with N2 = 8, flipping the low
+// log2(U) bits by the next ones puts both on distinct 16-byte bank groups.
+// The pointwise products see the same permutation in every slot.
+template <int N1, int N2>
+__device__ __forceinline__ int phys_pos(int k) {
+    constexpr int U = N1 / N2;
+    if constexpr (N2 == 8 && U > 1) return k ^ ((k >> 3) & (U - 1));
+    else return k;
+}
+
+// Inverse HORFFT of one PFP row into the packed samples L[phys_pos(0..N))
 // loaded: the row is already in the slot (an earlier asynchronous copy that
 // the warp has waited for); src is then not read.
 template <int N1, int N2>
@@ -438,7 +450,7 @@ __device__ __forceinline__ void grp_inverse5(const double2* __restrict__ src, bo
     __syncwarp();
     fft4::line_fft_inplace<N1, N2, +1>(v, L, tw, t, o);
 #pragma unroll
-    for (int q = 0; q < N1; ++q) L[fft4::out_index<N1, N2>(t, q)] = o[q];
+    for (int q = 0; q < N1; ++q) L[phys_pos<N1, N2>(fft4::out_index<N1, N2>(t, q))] = o[q];
 }
 
 // Asynchronous copy of one PFP row (m < mlim) into a line slot by the group's
@@ -454,14 +466,14 @@ __device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_g
 template <int K>
 __device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory"); }
 
-// Forward HORFFT of the natural-order packed samples in L to a PFP row (m < md).
+// Forward HORFFT of the packed samples L[phys_pos(0..N))] to a PFP row (m < md).
 template <int N1, int N2>
 __device__ __forceinline__ void grp_forward5(double2* L, bool valid, double2* __restrict__ dst, int md, int ntchop,
                                              const double2* tw, const double2* twh, int t) {
     constexpr int N = N1 * N2;
     double2 v[N1], o[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = L[t + N2 * n1];
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = L[phys_pos<N1, N2>(t + N2 * n1)];
     __syncwarp();
     fft4::line_fft_inplace<N1, N2, -1>(v, L, tw, t, o);
 #pragma unroll

@@ -812,9 +812,17 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
         }
     } else {  // PFP [r][z][m] -> PFF [m][r][k], scaled 1/NX, chopped
         __syncthreads();
-        for (int e = threadIdx.x; e < N * nmb; e += blockDim.x) {
-            const int z = e / nmb, ml = e - z * nmb;
-            T[(size_t)z * cs + ml] = src[((size_t)r * N + z) * md + m0 + ml];
+        // the tile [z][m0 .. m0 + nmb) by cp.async: every thread keeps its column
+        // ml and issues all its rows before waiting (MB divides the block size)
+        {
+            const int ml = threadIdx.x % MB;
+            if (ml < nmb)
+                for (int z = threadIdx.x / MB; z < N; z += blockDim.x / MB)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(T + (size_t)z * cs + ml)),
+                                 "l"(src + ((size_t)r * N + z) * md + m0 + ml)
+                                 : "memory");
+            asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
 #pragma unroll

@@ -71,17 +71,27 @@ __global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const doub
     const double* pf = g.pf + (size_t)m * ne * g.NRH;
     const double* a = A + (size_t)m * g.NRCHOPDIM * ncol;
     const int ach = g.NRH / 2;  // 16-byte chunks per PF row (NRH is even)
+    // (row, chunk) of this thread's first PF element and the step per pass, so
+    // the staging loop needs no division
+    const int tt0 = tid / ach, ch0 = tid - tt0 * ach;
+    const int dtt = (NW * 32) / ach, dch = (NW * 32) - dtt * ach;
 
     auto stage = [&](int cidx) {
         const int p = cidx < nc0 ? 0 : 1;
         const int t0 = (cidx - (p ? nc0 : 0)) * KCB, kp = p ? kp1 : kp0;
         double* As = smd + (cidx % NST_B2P) * stg;
         double* Bs = As + (size_t)KCB * SA;
+        int tt = tt0, ch = ch0;
         for (int e = tid; e < KCB * ach; e += NW * 32) {
-            const int tt = e / ach, ch = e - tt * ach;
             const int t = t0 + tt;
             const bool ok = t < kp;
             cp16(As + (size_t)tt * SA + 2 * ch, ok ? pf + (size_t)(2 * t + p) * g.NRH + 2 * ch : pf, ok);
+            tt += dtt;
+            ch += dch;
+            if (ch >= ach) {
+                ch -= ach;
+                ++tt;
+            }
         }
         for (int e = tid; e < KCB * (CT / 2); e += NW * 32) {
             const int tt = e / (CT / 2), ch = e - tt * (CT / 2);

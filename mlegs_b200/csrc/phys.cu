@@ -783,7 +783,7 @@ __global__ void __launch_bounds__(256) verfft4_kernel(DevGrid g, const double2* 
     double2* T = tw2 + N;                       // [N][MB + 1]; column mloc is line m0 + mloc
     for (int q = threadIdx.x; q <= N; q += blockDim.x) tw[q] = tw_g[q];
     for (int q = threadIdx.x; q < N; q += blockDim.x) tw2[q] = tw_g[(q % N2) * (q / N2)];
-    const int r = blockIdx.x, m0 = blockIdx.y * MB;
+    const int r = blockIdx.y, m0 = blockIdx.x * MB;  // the m-blocks of one r run together
     const int mloc = warp * G + gid, m = m0 + mloc;
     const bool ok = m < g.NTCHOPDIM;
     const int kd = g.NXCHOPDIM, kc = g.NXCHOP, md = g.NTCHOPDIM;
@@ -858,7 +858,7 @@ static void launch_verfft4(const DevGrid& g, const FFTPlan& p, const double2* sr
         attr = true;
     }
     const int MB = warps * G;
-    dim3 grid(g.NR, (g.NTCHOPDIM + MB - 1) / MB);
+    dim3 grid((g.NTCHOPDIM + MB - 1) / MB, g.NR);
     verfft4_kernel<N1, N2><<<grid, warps * 32, need(warps), s>>>(g, src, dst, p.tw_x, dir);
     count_launch();
 }

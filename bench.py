@@ -26,6 +26,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -100,7 +101,9 @@ class Clocks:
 
     def __init__(self, index):
         self.index = index
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+        # the raw samples: MLEGS_CLOCKS_CSV, else the system temporary directory
+        self.path = os.environ.get("MLEGS_CLOCKS_CSV") or os.path.join(tempfile.gettempdir(),
+                                                                       "mlegs_clocks_bench.csv")
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
         self.proc = None
 

@@ -3,7 +3,7 @@
 FP64 GPU path vs FP64 oracle: per-operator relative error (max|d|/max|ref|)
 below 1e-12 (transforms, band operators, projection) and 1e-10 for the
 banded solves; whole steps below 1e-9 per field after the stated number of
-steps (the north_star tolerance).
+steps (the solver's stated field tolerance).
 """
 
 import numpy as np

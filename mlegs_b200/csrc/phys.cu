@@ -846,7 +846,9 @@ template <int N1, int N2>
 static void launch_verfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
                            cudaStream_t s) {
     constexpr int N = N1 * N2, G = 32 / N2;
-    int warps = 4;  // MB = 4 G lines per CTA: more, smaller CTAs per SM overlap their load, FFT and store phases
+    // (+1): MB = 4 G lines per CTA, more and smaller CTAs per SM overlapping their
+    // load, FFT and store phases; (-1): 8 warps, longer tile rows per cp.async pass
+    int warps = dir > 0 ? 4 : 8;
     auto need = [&](int w) {
         int MB = w * G;
         return (size_t)((N + 1) + N + N * (MB + 1)) * sizeof(double2);

@@ -553,11 +553,14 @@ static void b2p_launch(const DevGrid& g, const double2* a, double2* b, const dou
 
 // The NRH / 8 output m-tiles go round-robin over 6 warps.
 void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
+    // 4 warps per CTA: the small CTAs (about 140 registers a thread, 36 KB of
+    // shared memory) run three to an SM; the m-tiles go round-robin over the warps
     const int RT = (g.NRH + 7) / 8;
-    switch ((RT + 5) / 6) {
-        case 1: b2p_launch<6, 1>(g, a, b, ln, pad, s); break;
-        default: b2p_launch<6, 2>(g, a, b, ln, pad, s); break;
-        case 3: b2p_launch<6, 3>(g, a, b, ln, pad, s); break;
+    switch ((RT + 3) / 4) {
+        case 1: b2p_launch<4, 1>(g, a, b, ln, pad, s); break;
+        case 2: b2p_launch<4, 2>(g, a, b, ln, pad, s); break;
+        case 3: b2p_launch<4, 3>(g, a, b, ln, pad, s); break;
+        default: b2p_launch<4, 4>(g, a, b, ln, pad, s); break;
     }
 }
 

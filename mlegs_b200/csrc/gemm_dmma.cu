@@ -382,7 +382,7 @@ struct ProjFffArgs {
 };
 
 template <int NW, int MTW>
-__global__ void __launch_bounds__(NW * 32, 4) projfff_dmma_kernel(DevGrid g, ProjFffArgs pa, int RC, int KPC,
+__global__ void __launch_bounds__(NW * 32, 5) projfff_dmma_kernel(DevGrid g, ProjFffArgs pa, int RC, int KPC,
                                                                  int RTmax) {
     extern __shared__ double smd[];
     const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;

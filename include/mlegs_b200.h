@@ -229,6 +229,11 @@ int mlegs_specurv(const double* espec, int n, double use_ratio, double* curv);
 int mlegs_speslop(const double* espec, int n, double ratio, double* slope);
 int mlegs_pdajust(double* coeff, double current, double previous, double baseline, const double* params,
                   int has_threshold, double threshold);
+/* One field's HYP3ADJ controller (mod_march.f90:3025-3101) on given spectra,
+ * no context: em[nm] (EM without its last two entries), ek[nk]; state[5] =
+ * NUPB (negative before the first call), CURVMO, CURVKO, SLOPMO, SLOPKO, updated
+ * in place; coef[3] = NUP_R, NUP_T, NUP_X, updated in place. */
+int mlegs_hyp3_controller(const double* em, int nm, const double* ek, int nk, double* state, double* coef);
 
 /* Solver: SOLVER_T%INITIALIZE (mod_march.f90:171-240, Richardson start-up) and
  * TIME_STEPPING's state update (243-307: STEP_BOUSSI_AB_CN 609 or

@@ -390,6 +390,23 @@ def QVORTEX(ctx, vortices, noise_seeds=None):
     return psi, chi
 
 
+def HYP3_CONTROLLER(em, ek, state, coef):
+    """One field's HYP3ADJ controller (mod_march.f90:3025-3101) on given spectra
+    (host code, no device).  state: [NUPB, CURVMO, CURVKO, SLOPMO, SLOPKO]
+    (NUPB < 0 before the first call); coef: [R, T, X].  Returns the updated
+    (state, coef) as new arrays."""
+    e_m = np.ascontiguousarray(em, dtype=np.float64)
+    e_k = np.ascontiguousarray(ek, dtype=np.float64)
+    st = np.array(state, dtype=np.float64)
+    cf = np.array(coef, dtype=np.float64)
+    rc = _lib.load().mlegs_hyp3_controller(e_m.ctypes.data_as(ctypes.c_void_p), e_m.size,
+                                           e_k.ctypes.data_as(ctypes.c_void_p), e_k.size,
+                                           st.ctypes.data_as(ctypes.c_void_p), cf.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise MlegsError(rc, "mlegs_hyp3_controller")
+    return st, cf
+
+
 def qvortex(ctx, q=1.0, r0=1.0, xc=0.0, yc=0.0, h=0.0, b=1.0):
     """One Gaussian q-vortex (QVORTEX with a single QPAIR entry) on the device."""
     return QVORTEX(ctx, [dict(q=q, r=r0, x=xc, y=yc, h=h, b=b)])
@@ -414,5 +431,5 @@ def initial_state(ctx, cfg=None):
 
 
 __all__ = ["Context", "Field", "MlegsError", "qvortex", "QVORTEX", "initial_state", "CONFIGS", "Config",
-           "SPECURV", "SPESLOP", "PDAJUST",
+           "SPECURV", "SPESLOP", "PDAJUST", "HYP3_CONTROLLER",
            "PPP", "FFF", "PFP", "PFF", "PREC_FP64", "PREC_SPLIT"]

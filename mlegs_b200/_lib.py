@@ -88,6 +88,7 @@ SIGNATURES = {
     "mlegs_specurv": (c_int, [c_void_p, c_int, c_double, c_void_p]),
     "mlegs_speslop": (c_int, [c_void_p, c_int, c_double, c_void_p]),
     "mlegs_pdajust": (c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_int, c_double]),
+    "mlegs_hyp3_controller": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "mlegs_msave": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_int]),
     "mlegs_mload": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_int]),
     "mlegs_solver_init": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -151,6 +151,17 @@ int mlegs_speslop(const double* espec, int n, double ratio, double* slope) {
     return MLEGS_OK;
 }
 
+int mlegs_hyp3_controller(const double* em, int nm, const double* ek, int nk, double* state, double* coef) {
+    if (!em || !ek || !state || !coef || nm < 1 || nk < 1) return MLEGS_ERR_ARG;
+    mlegs::Hyp3State st;
+    st.nupb = state[0];
+    for (int q = 0; q < 4; ++q) st.hist[q] = state[1 + q];
+    mlegs::hyp3adj_update(st, em, nm, ek, nk, coef, nullptr, 0, nullptr, 0, nullptr);
+    state[0] = st.nupb;
+    for (int q = 0; q < 4; ++q) state[1 + q] = st.hist[q];
+    return MLEGS_OK;
+}
+
 int mlegs_pdajust(double* coeff, double current, double previous, double baseline, const double* params,
                   int has_threshold, double threshold) {
     if (!coeff || !params) return MLEGS_ERR_ARG;

@@ -82,6 +82,31 @@ def test_pdajust_known_answers(lib_built):
             assert abs(M.PDAJUST(c, cur, prev, base, prm, thr) - H.pdajust(c, cur, prev, base, prm, thr)) < 1e-14
 
 
+def test_hyp3_controller_sequence_matches_oracle(lib_built):
+    """The library's HYP3ADJ controller (host code) against the oracle over a
+    sequence of calls with evolving history: spectra from shallow to steep
+    power laws with noise, so the curvature, slope, over-damping and clamp
+    branches all occur."""
+    import mlegs_b200 as M
+    from oracle import hyperadj as H
+    rng = np.random.default_rng(11)
+    state = np.array([-1.0, 0.0, 0.0, 0.0, 0.0])
+    coef = np.array([0.3, 0.3, 0.3])
+    nupb, hist, ref = -1.0, [0.0] * 4, [0.3, 0.3, 0.3]
+    for step, p in enumerate((1.0, 2.5, 4.0, 6.0, 9.0, 3.0, 0.5, 12.0)):
+        em = np.arange(1, 84, dtype=float) ** -p * np.exp(0.3 * rng.standard_normal(83))
+        ek = np.arange(1, 86, dtype=float) ** -(p + 0.5) * np.exp(0.3 * rng.standard_normal(85))
+        state, coef = M.HYP3_CONTROLLER(em, ek, state, coef)
+        met = H.Hyp3Adj._metrics(em, ek)
+        if nupb < 0.0:
+            hist, nupb = list(met), H.BASELINE_NUP
+        ref = H.Hyp3Adj._control(ref, met, hist, nupb)
+        hist = list(met)
+        assert np.abs(coef - np.array(ref)).max() < 1e-12 * max(1.0, np.abs(ref).max()), step
+        assert np.abs(state[1:] - np.array(hist)).max() < 1e-12 and state[0] == nupb
+        assert coef.min() >= nupb and coef[0] <= 2.0
+
+
 def test_hyp3adj_controller_first_call():
     """First HYP3ADJ: the history takes the current metrics, NUPB = 0.8 and every
     coefficient ends at or above it, NUP_R at most 2."""

@@ -49,25 +49,30 @@ def vortex(**kw):
     return v
 
 
-def lay_gaus(g, A, q, b, v):
-    """A += LAY(GAUS, IP = 2) of one vortex with GAUSDATA%Q = q, %B = b and the
-    centre / core modulation of v (GAUS, mod_layout.f90:640-672; Z = ZLEN (KK-1) / NX)."""
-    r = g.R[:g.NR, None, None]
-    f = (1 - g.X[:g.NR, None, None]) ** 2
-    z = g.Z[None, None, :g.NX]
-    ak1 = 2 * np.pi * v["k"] / g.ZLEN
-    rk = 2 * np.pi * v["rk"] / g.ZLEN
+def gaus_value(v, q, b, x, y, z, zlen):
+    """GAUS(R, TH, Z), mod_layout.f90:640-672, at Cartesian (x, y) and axial z
+    (broadcasting): strength q / R0^2, decay b, the centre displaced by
+    DX, DY sin(AK1 Z - DP) and the core R0 = R + DR sin(RK Z - RP)."""
+    ak1 = 2 * np.pi * v["k"] / zlen
+    rk = 2 * np.pi * v["rk"] / zlen
     dp = np.pi / 180.0 * v["dp"]
     rp = np.pi / 180.0 * v["rp"]
     xc = v["x"] + v["dx"] * np.sin(ak1 * z - dp)
     yc = v["y"] + v["dy"] * np.sin(ak1 * z - dp)
     r0 = v["r"] + v["dr"] * np.sin(rk * z - rp)
+    r2 = ((x - xc) ** 2.0 + (y - yc) ** 2.0) / r0 ** 2.0
+    return q / r0 ** 2.0 * np.exp(-b * r2)
+
+
+def lay_gaus(g, A, q, b, v):
+    """A += LAY(GAUS, IP = 2) of one vortex with GAUSDATA%Q = q, %B = b and the
+    centre / core modulation of v (mod_layout.f90:64-117; Z = ZLEN (KK-1) / NX)."""
+    r = g.R[:g.NR, None, None]
+    f = (1 - g.X[:g.NR, None, None]) ** 2
+    z = g.Z[None, None, :g.NX]
 
     def gaus(th):
-        x = r * np.cos(th)[None, :, None]
-        y = r * np.sin(th)[None, :, None]
-        r2 = ((x - xc) ** 2.0 + (y - yc) ** 2.0) / r0 ** 2.0
-        return q / r0 ** 2.0 * np.exp(-b * r2)
+        return gaus_value(v, q, b, r * np.cos(th)[None, :, None], r * np.sin(th)[None, :, None], z, g.ZLEN)
 
     A.E[:g.NR, :g.NTH, :g.NX] += gaus(g.THR[:g.NTH]) / f + 1j * (gaus(g.THI[:g.NTH]) / f)
     return A

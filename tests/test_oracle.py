@@ -97,6 +97,22 @@ def test_qvortex_logterm(xc):
     assert chi.LN == 0.0
 
 
+def test_gaus_matches_reference_notebook():
+    """The oracle's GAUS against the reference's own Python restatement of it
+    (tests/init/visualize_gaussian.ipynb), golden values from
+    tests/golden/make_gaus_golden.py, with the waviness and core modulation."""
+    import os
+    from oracle import layout
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "gaus_golden.npz"))
+    keys = [str(k) for k in d["keys"]]
+    for prm, ref in zip(d["params"], d["vals"]):
+        p = dict(zip(keys, prm))
+        v = layout.vortex(x=p["XC"], y=p["YC"], dx=p["DX"], dy=p["DY"], k=p["K"], dp=p["DP"], r=p["R"],
+                          dr=p["DR"], rk=p["RK"], rp=p["RP"])
+        got = layout.gaus_value(v, p["Q"], p["B"], d["x"], d["y"], d["z"], p["ZLEN"])
+        assert np.abs(got - ref).max() <= 1e-15 * max(1.0, np.abs(ref).max())
+
+
 def test_qvortex_list_logterms():
     """QVORTEX over a QPAIR list: PSI%LN = -sum(Q)/2 and CHI%LN = -sum(H/B)/4
     (the circulations 2 pi Q and pi H / B of the Gaussians over 4 pi), with the

@@ -1063,10 +1063,10 @@ void k_maxabs(const double2* a, size_t n, int mode, double* out, cudaStream_t s)
 // (m, n, k) the call pair (2j, 2j+1) of RAN0 (196-214) gives X and Y; RAN0's
 // state is the Park-Miller sequence v_{j+1} = 16807 v_j mod (2^31 - 1) from
 // v_0 = ISEED xor 123459876, output v_{j+1} / (2^31 - 1), so element j jumps
-// ahead by modular powers.  FAC = 0.1 exp(-12 ((AK/AKMAX)^2 + (N/NRCHOP)^2))
-// with the reference's default-real literal 0.1 and FLOAT(N)/NRCHOP in single
-// precision; CMPLX(X, Y) rounds X, Y to single precision before the product with
-// REFVAL = ALEVEL max|A| (refmax holds max|A|).
+// ahead by modular powers.  FAC = 0.1 exp(-12 ((AK/AKMAX)^2 + (N/NRCHOP)^2)),
+// and A += (X, Y) REFVAL with REFVAL = ALEVEL max|A| (refmax holds max|A|); the
+// reference is built with default REAL of 8 bytes (-r8 / -fdefault-real-8), so
+// the literals, FLOAT and CMPLX are all double precision.
 __device__ __forceinline__ unsigned long long powmod_ia(unsigned long long e) {
     const unsigned long long IM = 2147483647ull;
     unsigned long long r = 1, b = 16807;
@@ -1091,14 +1091,13 @@ __global__ void noise_kernel(DevGrid g, double2* a, const double* refmax, double
     const unsigned long long vx = powmod_ia(j + 1) * (unsigned long long)v0 % IM;
     const unsigned long long vy = vx * 16807ull % IM;
     const double akr = g.ak[k] / akmax;
-    const float q = (float)(m + n) / (float)g.NRCHOP;
-    const float q2 = q * q;
-    const double fac = (double)0.1f * exp(-12.0 * (akr * akr + (double)q2));
-    const float x = (float)(fac * (AM * (double)vx)), y = (float)(fac * (AM * (double)vy));
+    const double q = (double)(m + n) / (double)g.NRCHOP;
+    const double fac = 0.1 * exp(-12.0 * (akr * akr + q * q));
+    const double x = fac * (AM * (double)vx), y = fac * (AM * (double)vy);
     const double refval = alevel * *refmax;
     double2 v = a[t];
-    v.x += (double)x * refval;
-    v.y += (double)y * refval;
+    v.x += x * refval;
+    v.y += y * refval;
     a[t] = v;
 }
 void k_noise(const DevGrid& g, double2* a, const double* refmax, double alevel, double akmax, long long v0,

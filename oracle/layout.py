@@ -99,24 +99,23 @@ class Ran0:
 
 def noise(g, A, alevel, iseed):
     """NOISE(A, ALEVEL), mod_layout.f90:165-226, on an FFF field with an explicit
-    ISEED.  Precision as written: the literal 0.1 and FLOAT(N)/NRCHOP are default
-    (single-precision) reals, and CMPLX(X, Y) rounds X and Y to single precision."""
+    ISEED.  The reference is compiled with default REAL of 8 bytes (-r8 or
+    -fdefault-real-8 in its Makefile), so the literal 0.1, FLOAT(N) and
+    CMPLX(X, Y) are double precision."""
     ran = Ran0(iseed)
     refval = alevel * np.abs(A.E).max()
     akmax = np.abs(g.AK[:g.NTCHOP, :g.NXCHOP]).max()
     if akmax == 0.0:
         akmax = 1.0
-    c01 = np.float64(np.float32(0.1))
     for mm in range(min(g.NTCHOP, A.E.shape[1])):
         for nn in range(int(g.NRCHOPS[mm])):
             n = int(g.M[mm]) + nn
-            q = np.float32(n) / np.float32(g.NRCHOP)
-            q2 = np.float64(np.float32(q * q))
+            q = float(n) / g.NRCHOP
             for kk in range(A.E.shape[2]):
                 akr = g.AK[mm, kk] / akmax
-                fac = c01 * np.exp(-12.0 * (akr * akr + q2))
-                x = np.float64(np.float32(fac * ran()))
-                y = np.float64(np.float32(fac * ran()))
+                fac = 0.1 * np.exp(-12.0 * (akr * akr + q * q))
+                x = fac * ran()
+                y = fac * ran()
                 A.E[nn, mm, kk] += complex(x * refval, y * refval)
     g.chopdo(A)
     return A

@@ -346,9 +346,9 @@ def test_qvortex_list_on_device(env):
     Pn, Cn = layout.qvortex_list(g, [layout.vortex(**v) for v in vs], noise_seeds=(4242, 777))
     for f, R, R0 in ((psn, Pn, P), (chn, Cn, C)):
         E, ln = f.download()
-        assert rel(E, R.E) < 1e-9          # X, Y pass through single precision (CMPLX)
+        assert rel(E, R.E) < 1e-10
         assert rel(R.E, R0.E) > 1e-5       # the noise is there
-        assert abs(ln - R.LN) < 1e-9 * max(1.0, abs(R.LN))
+        assert abs(ln - R.LN) < 1e-10 * max(1.0, abs(R.LN))
     with pytest.raises(M.MlegsError) as ei:   # R0 = R + DR sin(.) would reach zero
         M.QVORTEX(ctx, [dict(r=0.1, dr=0.2)])
     assert ei.value.code == 101

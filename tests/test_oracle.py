@@ -302,6 +302,10 @@ def test_diagnost_known_answers():
     v = D.diagnost(g, psi, chi)
     assert abs(v["VALX"] - 0.4) < 1e-10 and abs(v["VALY"] + 0.3) < 1e-10
     assert abs(v["VALR"] - math.sqrt(0.4 ** 2 + 0.3 ** 2 + 0.5)) < 1e-10
+    # two equal, well separated vortices: the enstrophy-weighted centre is their midpoint
+    psi, chi = layout.qvortex_list(g, [layout.vortex(x=1.5, y=0.5), layout.vortex(x=-1.0, y=-0.5)])
+    v = D.diagnost(g, psi, chi)
+    assert abs(v["VALX"] - 0.25) < 1e-8 and abs(v["VALY"]) < 1e-8
 
 
 def test_snapshot_record_layout(tmp_path):

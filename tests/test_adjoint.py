@@ -1,0 +1,84 @@
+"""Adjoints of the transform and nonlinear-term maps (oracle/adjoint.py),
+checked by the dot-product identity <y, F(x)> = <F^T(y), x> on random inputs
+that fill every entry of each space (padding and chopped entries included,
+so the projections are checked too), and the product adjoint by central
+finite differences."""
+
+import numpy as np
+import pytest
+
+from conftest import oracle_grid, small_cfg
+
+
+def _rand(g, space, seed):
+    from oracle.grid import Field
+    rng = np.random.default_rng(seed)
+    shape = g.shape(space)
+    return Field(rng.standard_normal(shape) + 1j * rng.standard_normal(shape), space, float(rng.standard_normal()))
+
+
+def _dot(a, b):
+    return float(np.sum(a.real * b.real + a.imag * b.imag))
+
+
+def _check(fwd, adj, x, y, with_ln=False):
+    fx = fwd(x.copy())
+    aty = adj(y)
+    lhs = _dot(y.E, fx.E)
+    rhs = _dot(aty.E, x.E) + (aty.LN * x.LN if with_ln else 0.0)
+    assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs))
+
+
+@pytest.mark.parametrize("dims", [(32, 16, 16), (24, 12, 8)])
+def test_transform_adjoints(dims):
+    from oracle import adjoint as AD
+    from oracle import transforms as T
+    from oracle.grid import FFF, PFF, PFP, PPP
+    g = oracle_grid(small_cfg(*dims))
+    cases = [
+        (lambda a: T.rtran(g, a, 1), lambda y: AD.rtran_T(g, y, 1), FFF, PFF, True),
+        (lambda a: T.rtran(g, a, -1), lambda y: AD.rtran_T(g, y, -1), PFF, FFF, False),
+        (lambda a: T.verfft(g, a, 1), lambda y: AD.verfft_T(g, y, 1), PFF, PFP, False),
+        (lambda a: T.verfft(g, a, -1), lambda y: AD.verfft_T(g, y, -1), PFP, PFF, False),
+        (lambda a: T.horfft(g, a, 1), lambda y: AD.horfft_T(g, y, 1), PFP, PPP, False),
+        (lambda a: T.horfft(g, a, -1), lambda y: AD.horfft_T(g, y, -1), PPP, PFP, False),
+        (lambda a: T.tofp(g, a), lambda y: AD.tofp_T(g, y), FFF, PPP, True),
+        (lambda a: T.toff(g, a), lambda y: AD.toff_T(g, y), PPP, FFF, False),
+    ]
+    for i, (fwd, adj, sin, sout, ln) in enumerate(cases):
+        x = _rand(g, sin, 10 + i)
+        if not ln:
+            x.LN = 0.0
+        y = _rand(g, sout, 50 + i)
+        y.LN = 0.0
+        _check(fwd, adj, x, y, with_ln=ln)
+
+
+def test_product_adjoint_matches_finite_differences():
+    from oracle import adjoint as AD
+    from oracle.grid import PPP
+    from oracle.legops import vprodsub
+    g = oracle_grid(small_cfg(24, 12, 8))
+    U = [_rand(g, PPP, 100 + q) for q in range(3)]
+    W = [_rand(g, PPP, 200 + q) for q in range(3)]
+    Y = [_rand(g, PPP, 300 + q).E for q in range(3)]
+
+    def J(Us, Ws):
+        Wc = [w.copy() for w in Ws]
+        vprodsub(g, *[u.copy() for u in Us], *Wc)
+        sl = (slice(0, g.NR), slice(0, g.NTH), slice(None))
+        return sum(_dot(Y[q][sl], Wc[q].E[sl]) for q in range(3))
+
+    ub, wb = AD.vprodsub_T(g, [u.E for u in U], [w.E for w in W], Y)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        du = [_rand(g, PPP, int(rng.integers(1 << 30))) for _ in range(3)]
+        dw = [_rand(g, PPP, int(rng.integers(1 << 30))) for _ in range(3)]
+        h = 1e-6
+        Up = [type(u)(u.E + h * d.E, PPP, 0.0) for u, d in zip(U, du)]
+        Um = [type(u)(u.E - h * d.E, PPP, 0.0) for u, d in zip(U, du)]
+        Wp = [type(w)(w.E + h * d.E, PPP, 0.0) for w, d in zip(W, dw)]
+        Wm = [type(w)(w.E - h * d.E, PPP, 0.0) for w, d in zip(W, dw)]
+        fd = (J(Up, Wp) - J(Um, Wm)) / (2 * h)
+        an = sum(_dot(ub[q], du[q].E) + _dot(wb[q], dw[q].E) for q in range(3))
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an))

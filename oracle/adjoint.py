@@ -13,9 +13,12 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   verfft_T(g, Y, IS)  VERFFT(A, IS), mod_fft.f90:928-1113
   horfft_T(g, Y, IS)  HORFFT(A, IS), mod_fft.f90:771-926
   tofp_T / toff_T     TOFP / TOFF, mod_fft.f90:1342-1398 (reverse order)
-  vprodsub_T          VPRODSUB (mod_legops.f90:1972-2133) with VDOTPSUB
-                      (2136-2232) as the nonlinear term of CALC_BOUSSI_NONLIN
-                      forms them, pointwise in PPP
+  vprodsub_T          the VPRODSUB cross products (mod_legops.f90:2105-2130),
+                      pointwise in PPP
+  mulxm_T, xxdx_T, delsqh_T, del2_T   MULXM (371-428), XXDX (680-748), DELSQH
+                      (76-133), DEL2 (751-820), log-term rows included
+  grad_T, pc2vel_T, pc2vor_T          GRAD (1727-1786), PC2VEL (1789-1853),
+                      PC2VOR (1856-1919)
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -159,3 +162,126 @@ def vprodsub_T(g, U, OM, NB_bar):
             out_u[q][sl] += f * du[q]
             out_w[q][sl] += f * dw[q]
     return out_u, out_w
+
+
+# ----------------------------------------------------------------------
+# FFF operators (mod_legops.f90).  Per (m, k) column each is a real band
+# matrix M acting on the rows n < NRCHOPS(m), so the adjoint applies M^T; the
+# (m, k) = (0, 0) log-term rows give LN_bar = sum_rows coef * Re Y(row, 0, 0).
+
+def _band_T(g, Y, make_band, c):
+    from .bandmat import band_to_full
+    y = _field(Y.E, FFF)
+    g.chopdo(y)
+    A = g.alloc(FFF)
+    for mm in range(A.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        full = band_to_full(make_band(nn, mm), c, nn)
+        A.E[:nn, mm, :] = full.T @ y.E[:nn, mm, :]
+    return A, y
+
+
+def mulxm_T(g, Y):
+    """Adjoint of MULXM (371-428)."""
+    from .bandmat import band_xm
+    A, _ = _band_T(g, Y, lambda nn, mm: band_xm(nn, g.M[mm], g.LOGNORM[:, mm]), 1)
+    return A
+
+
+def xxdx_T(g, Y):
+    """Adjoint of XXDX (680-748) with its log-term rows (742-745)."""
+    from .bandmat import band_xxdx
+    A, y = _band_T(g, Y, lambda nn, mm: band_xxdx(nn, g.M[mm], g.LOGNORM[:, mm]), 1)
+    A.LN = float(y.E[0, 0, 0].real / g.NORM0[0] + y.E[1, 0, 0].real / g.NORM0[1])
+    return A
+
+
+def delsqh_T(g, Y):
+    """Adjoint of DELSQH (76-133): the diagonal -n(n+1)/L^2, and B(0,0,0) = LN / L^2 / NORM(1,1)."""
+    y = _field(Y.E, FFF)
+    g.chopdo(y)
+    A = g.alloc(FFF)
+    for mm in range(A.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        n = g.M[mm] + np.arange(nn)
+        A.E[:nn, mm, :] = -y.E[:nn, mm, :] * (n * (n + 1) / g.ELL2)[:, None]
+    A.E[0, 0, 0] = 0.0                      # the forward overwrites B(0, 0, 0)
+    A.LN = float(y.E[0, 0, 0].real / g.ELL2 / g.NORM0[0])
+    return A
+
+
+def del2_T(g, Y):
+    """Adjoint of DEL2 (751-820): band del^2_h minus k^2, log-term rows 813-817."""
+    from .bandmat import band_del2h, band_to_full
+    y = _field(Y.E, FFF)
+    g.chopdo(y)
+    A = g.alloc(FFF)
+    for mm in range(A.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        full = band_to_full(band_del2h(nn, g.M[mm], g.ELL, g.LOGNORM[:, mm]), 2, nn)
+        A.E[:nn, mm, :] = full.T @ y.E[:nn, mm, :] - (g.AK[mm, :] ** 2)[None, :] * y.E[:nn, mm, :]
+    A.LN = float((4.0 / 3 * y.E[0, 0, 0].real / g.NORM0[0] - 2.0 * y.E[1, 0, 0].real / g.NORM0[1]
+                  + 2.0 / 3 * y.E[2, 0, 0].real / g.NORM0[2]) / g.ELL2)
+    return A
+
+
+def _scale_T(g, Y, fac):
+    """Adjoint of A -> fac(m, k) A on rows n < NRCHOPS(m): multiply by conj(fac)."""
+    A = g.alloc(FFF)
+    for mm in range(A.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        A.E[:nn, mm, :] = np.conj(fac(mm))[None, :] * Y.E[:nn, mm, :]
+    return A
+
+
+def _add(*fs):
+    out = fs[0].copy()
+    for f in fs[1:]:
+        out.E = out.E + f.E
+        out.LN = out.LN + f.LN
+    return out
+
+
+def grad_T(g, RR, RP, GZ):
+    """Adjoint of GRAD (1727-1786) -> A_bar (FFF, with LN_bar)."""
+    a = xxdx_T(g, RR)
+    b = _scale_T(g, RP, lambda mm: 1j * g.M[mm] * np.ones(g.NXCHOPDIM))
+    c = _scale_T(g, GZ, lambda mm: 1j * g.AK[mm, :])
+    return _add(a, b, c)
+
+
+def _neg(F):
+    out = F.copy()
+    out.E = -out.E
+    out.LN = -out.LN
+    return out
+
+
+def pc2vel_T(g, RUR, RUP, UZ):
+    """Adjoint of PC2VEL (1789-1853) -> (PSI_bar, CHI_bar)."""
+    kv = lambda mm: g.AK[mm, :]
+    mv = lambda mm: g.M[mm] * np.ones(g.NXCHOPDIM)
+    # RUR = i m PSI + i k XXDX(CHI);  RUP = -XXDX(PSI) - m k CHI;  UZ = -MULXM(MULXM(DELSQH(CHI)))
+    psi = _add(_scale_T(g, RUR, lambda mm: 1j * mv(mm)), _neg(xxdx_T(g, _field(RUP.E, FFF))))
+    chi = _add(xxdx_T(g, _scale_T(g, RUR, lambda mm: 1j * kv(mm))),
+               _scale_T(g, RUP, lambda mm: -mv(mm) * kv(mm)),
+               delsqh_T(g, mulxm_T(g, mulxm_T(g, _neg(_field(UZ.E, FFF))))))
+    return psi, chi
+
+
+def pc2vor_T(g, ROR, ROP, OZ):
+    """Adjoint of PC2VOR (1856-1919) -> (PSI_bar, CHI_bar)."""
+    kv = lambda mm: g.AK[mm, :]
+    mv = lambda mm: g.M[mm] * np.ones(g.NXCHOPDIM)
+    # W = DEL2(CHI); ROR = -i m W + i k XXDX(PSI); ROP = XXDX(W) - k m PSI;
+    # OZ = -MULXM(MULXM(DELSQH(PSI)))
+    w_bar = _add(_scale_T(g, ROR, lambda mm: -1j * mv(mm)), xxdx_T(g, _field(ROP.E, FFF)))
+    chi = del2_T(g, w_bar)
+    psi = _add(xxdx_T(g, _scale_T(g, ROR, lambda mm: 1j * kv(mm))),
+               _scale_T(g, ROP, lambda mm: -kv(mm) * mv(mm)),
+               delsqh_T(g, mulxm_T(g, mulxm_T(g, _neg(_field(OZ.E, FFF))))))
+    return psi, chi

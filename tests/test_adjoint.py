@@ -82,3 +82,41 @@ def test_product_adjoint_matches_finite_differences():
         fd = (J(Up, Wp) - J(Um, Wm)) / (2 * h)
         an = sum(_dot(ub[q], du[q].E) + _dot(wb[q], dw[q].E) for q in range(3))
         assert abs(fd - an) <= 1e-6 * max(1.0, abs(an))
+
+
+@pytest.mark.parametrize("dims", [(32, 16, 16), (24, 12, 8)])
+def test_operator_adjoints(dims):
+    """MULXM, XXDX, DELSQH, DEL2 (log-term rows included), GRAD, PC2VEL and
+    PC2VOR against their transposes."""
+    from oracle import adjoint as AD
+    from oracle import legops as LO
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(*dims))
+    unary = [(LO.mulxm, AD.mulxm_T, False), (LO.xxdx, AD.xxdx_T, True),
+             (LO.delsqh, AD.delsqh_T, True), (LO.del2, AD.del2_T, True)]
+    for i, (f, ft, ln) in enumerate(unary):
+        x = _rand(g, FFF, 400 + i)
+        if not ln:
+            x.LN = 0.0
+        y = _rand(g, FFF, 500 + i)
+        fx = f(g, x.copy())
+        at = ft(g, y)
+        lhs = _dot(y.E, fx.E)
+        rhs = _dot(at.E, x.E) + at.LN * x.LN
+        assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs)), f.__name__
+    # GRAD: one input, three outputs
+    x = _rand(g, FFF, 600)
+    ys = [_rand(g, FFF, 610 + q) for q in range(3)]
+    outs = LO.grad(g, x.copy())
+    at = AD.grad_T(g, *ys)
+    lhs = sum(_dot(y.E, o.E) for y, o in zip(ys, outs))
+    assert abs(lhs - (_dot(at.E, x.E) + at.LN * x.LN)) <= 1e-12 * max(1.0, abs(lhs))
+    # PC2VEL / PC2VOR: two inputs, three outputs
+    for f, ft, s0 in ((LO.pc2vel, AD.pc2vel_T, 700), (LO.pc2vor, AD.pc2vor_T, 800)):
+        p, c = _rand(g, FFF, s0), _rand(g, FFF, s0 + 1)
+        ys = [_rand(g, FFF, s0 + 10 + q) for q in range(3)]
+        outs = f(g, p.copy(), c.copy())
+        pb, cb = ft(g, *ys)
+        lhs = sum(_dot(y.E, o.E) for y, o in zip(ys, outs))
+        rhs = _dot(pb.E, p.E) + pb.LN * p.LN + _dot(cb.E, c.E) + cb.LN * c.LN
+        assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs)), f.__name__

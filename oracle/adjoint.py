@@ -19,6 +19,10 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
                       (76-133), DEL2 (751-820), log-term rows included
   grad_T, pc2vel_T, pc2vor_T          GRAD (1727-1786), PC2VEL (1789-1853),
                       PC2VOR (1856-1919)
+  vdotpsub_T          VDOTPSUB (2136-2232), pointwise in PPP
+  project_T           PROJECT (2397-2545) of PFF inputs without the log term,
+                      with EOMUL/OEMUL (2548-2648) and the far-field fix
+                      (farfield_T, CALCAT1 of mod_scalar3.f90:286-310)
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -285,3 +289,79 @@ def pc2vor_T(g, ROR, ROP, OZ):
                _scale_T(g, ROP, lambda mm: -kv(mm) * mv(mm)),
                delsqh_T(g, mulxm_T(g, mulxm_T(g, _neg(_field(OZ.E, FFF))))))
     return psi, chi
+
+
+def vdotpsub_T(g, A, B, Y):
+    """Adjoint of VDOTPSUB (2136-2232), out = (a1 b1 + a2 b2)/r^2 + a3 b3 per
+    packed part: returns (A_bar, B_bar), lists of three PPP arrays."""
+    r2 = (g.R[:g.NR] ** 2)[:, None, None]
+    sl = (slice(0, g.NR), slice(0, g.NTH), slice(None))
+    out_a = [np.zeros_like(A[0]) for _ in range(3)]
+    out_b = [np.zeros_like(A[0]) for _ in range(3)]
+    for part, f in ((0, 1.0), (1, 1j)):
+        pick = (lambda a: a.real) if part == 0 else (lambda a: a.imag)
+        a = [pick(x[sl]) for x in A]
+        b = [pick(x[sl]) for x in B]
+        y = pick(Y[sl])
+        w = [y / r2, y / r2, y]
+        for q in range(3):
+            out_a[q][sl] += f * (w[q] * b[q])
+            out_b[q][sl] += f * (w[q] * a[q])
+    return out_a, out_b
+
+
+def _fold_T(A, Cbar, nj, odd_first):
+    """Adjoint of EOMUL (odd_first False) / OEMUL (True) with respect to B:
+    C = A[0::2] . (even or odd fold of B), C[1::2] = A[1::2] . (the other)."""
+    njh = A.shape[1]
+    x0 = A[0::2].T @ Cbar[0::2]
+    x1 = A[1::2].T @ Cbar[1::2] if A.shape[0] > 1 else np.zeros_like(x0)
+    be_bar, bo_bar = (x1, x0) if odd_first else (x0, x1)
+    Bbar = np.zeros((nj,) + Cbar.shape[1:], dtype=np.complex128)
+    Bbar[:njh] = be_bar + bo_bar
+    Bbar[nj - 1:njh - 1:-1] = be_bar - bo_bar
+    return Bbar
+
+
+def farfield_T(g, Y):
+    """Adjoint of the far-field fix PSI(1,1,:) -= CALCAT1(PSI)/AT1(1)
+    (mod_legops.f90:2540; CALCAT1 mod_scalar3.f90:286-310) on a chopped field:
+    row 0 of m = 0 becomes -sum_{1 <= n < NRCHOP} AT1(n)/AT1(0) row n."""
+    X = _field(Y.E, FFF, Y.LN)
+    nr = g.NRCHOP
+    y0 = np.array(Y.E[0, 0, :])
+    X.E[1:nr, 0, :] = Y.E[1:nr, 0, :] - (g.AT1[1:nr] / g.AT1[0])[:, None] * y0[None, :]
+    X.E[0, 0, :] = 0.0
+    return X
+
+
+def project_T(g, PSI_bar, CHI_bar):
+    """Adjoint of PROJECT (2397-2545) of PFF inputs without log-term handling
+    (LN absent): returns (RUR_bar, RUP_bar, UZ_bar) in PFF."""
+    from .legops import project_weights
+    nr = g.NR
+    ps = farfield_T(g, PSI_bar)
+    g.chopdo(ps)
+    ch = _field(CHI_bar.E, FFF)
+    g.chopdo(ch)
+    out = [g.alloc(PFF) for _ in range(3)]
+    for mm in range(ps.E.shape[1]):
+        mv = int(g.M[mm])
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        V, D, T = project_weights(g, mm)
+        kv = g.AK[mm, :][None, :]
+        yp = ps.E[:nn, mm, :]
+        yc = ch.E[:nn, mm, :]
+        # PSI = -(i m) EO(V, rur) - OE(D, rup);  CHI = (i k) OE(D, rur) + m k EO(V, rup) - EO(T, uz)
+        rur = _fold_T(D, np.conj(1j * kv) * yc, nr, True)
+        rup = _fold_T(D, -yp, nr, True)
+        if mv != 0:
+            rur = rur + _fold_T(V, np.conj(-1j * mv) * yp, nr, False)
+            rup = rup + _fold_T(V, (mv * kv) * yc, nr, False)
+        uz = _fold_T(T, -yc, nr, False)
+        out[0].E[:nr, mm, :] = rur
+        out[1].E[:nr, mm, :] = rup
+        out[2].E[:nr, mm, :] = uz
+    return out

@@ -120,3 +120,42 @@ def test_operator_adjoints(dims):
         lhs = sum(_dot(y.E, o.E) for y, o in zip(ys, outs))
         rhs = _dot(pb.E, p.E) + pb.LN * p.LN + _dot(cb.E, c.E) + cb.LN * c.LN
         assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs)), f.__name__
+
+
+def test_vdotpsub_and_project_adjoints():
+    """VDOTPSUB (finite differences) and PROJECT of PFF inputs with the
+    far-field fix (dot product)."""
+    from oracle import adjoint as AD
+    from oracle import legops as LO
+    from oracle.grid import FFF, PFF, PPP
+    g = oracle_grid(small_cfg(32, 16, 16))
+    A = [_rand(g, PPP, 900 + q).E for q in range(3)]
+    B = [_rand(g, PPP, 910 + q).E for q in range(3)]
+    Y = _rand(g, PPP, 920).E
+    sl = (slice(0, g.NR), slice(0, g.NTH), slice(None))
+
+    def J(As, Bs):
+        from oracle.grid import Field
+        out = LO.vdotpsub(g, *[Field(a, PPP, 0.0) for a in As], *[Field(b, PPP, 0.0) for b in Bs])
+        return _dot(Y[sl], out[sl])
+
+    ab, bb = AD.vdotpsub_T(g, A, B, Y)
+    rng = np.random.default_rng(3)
+    da = [rng.standard_normal(A[0].shape) + 1j * rng.standard_normal(A[0].shape) for _ in range(3)]
+    db = [rng.standard_normal(A[0].shape) + 1j * rng.standard_normal(A[0].shape) for _ in range(3)]
+    h = 1e-6
+    fd = (J([a + h * d for a, d in zip(A, da)], [b + h * d for b, d in zip(B, db)])
+          - J([a - h * d for a, d in zip(A, da)], [b - h * d for b, d in zip(B, db)])) / (2 * h)
+    an = sum(_dot(ab[q], da[q]) + _dot(bb[q], db[q]) for q in range(3))
+    assert abs(fd - an) <= 1e-6 * max(1.0, abs(an))
+    # PROJECT of PFF inputs: three inputs, two outputs
+    xs = [_rand(g, PFF, 930 + q) for q in range(3)]
+    for x in xs:
+        x.LN = 0.0
+        x.E[g.NR:] = 0.0          # PFF padding rows do not take part
+    ys = [_rand(g, FFF, 940 + q) for q in range(2)]
+    P, C = LO.project(g, *[x.copy() for x in xs])
+    lhs = _dot(ys[0].E, P.E) + _dot(ys[1].E, C.E)
+    bars = AD.project_T(g, *ys)
+    rhs = sum(_dot(b.E, x.E) for b, x in zip(bars, xs))
+    assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs))

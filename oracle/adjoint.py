@@ -365,3 +365,48 @@ def project_T(g, PSI_bar, CHI_bar):
         out[1].E[:nr, mm, :] = rup
         out[2].E[:nr, mm, :] = uz
     return out
+
+
+def _solve_T_column(band, c, nn, y):
+    """x with M^T x = y, M the dense form of a (nn x nn) band (the transposed
+    banded solve; the forward runs the unpivoted band LU of M)."""
+    from .bandmat import band_to_full
+    return np.linalg.solve(band_to_full(band[:nn], c, nn).T, y)
+
+
+def idel2ln_T(g, A_bar):
+    """Adjoint of IDEL2LN(B, A) (mod_legops.f90:1013-1176) as the map
+    B -> (A, A%LN): the far-field fix, CHOPDO, the transposed m >= 1 penta-band
+    solves, A%LN = Re A(1,1,1) NORM(1,1) with A(1,1,1) then zeroed, and the
+    transposed m = 0 solves (the (m, k) = (0, 0) system carries the log column
+    of 1091-1107).  B%LN does not enter, so B_bar%LN = 0."""
+    from .bandmat import band_del2h
+    y = farfield_T(g, A_bar)
+    g.chopdo(y)
+    Bb = g.alloc(FFF)
+    K = y.E.shape[2]
+    n0 = g.NORM0
+    for mm in range(1, y.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        band0 = band_del2h(nn, g.M[mm], g.ELL, g.LOGNORM[:, mm])
+        for kk in range(K):
+            band = band0.copy()
+            band[:, 2] -= g.AK[mm, kk] ** 2
+            Bb.E[:nn, mm, kk] = _solve_T_column(band, 2, nn, y.E[:nn, mm, kk])
+    nn = int(g.NRCHOPS[0])
+    d0 = band_del2h(nn + 1, g.M[0], g.ELL, g.LOGNORM[:, 0])
+    x_bar = np.array(y.E[:nn, 0, :])
+    x_bar[0, 0] = A_bar.LN * n0[0]            # A(1,1,1) was replaced by the log term
+    for kk in range(K):
+        band = d0.copy()
+        band[:, 2] -= g.AK[0, kk] ** 2
+        if kk == 0:
+            band[0, 2] += 4.0 / 3 / g.ELL2
+            band[1, 1] -= 2 * n0[0] / n0[1] / g.ELL2
+            band[2, 0] += 2.0 / 3 * n0[0] / n0[2] / g.ELL2
+        Bb.E[:nn, 0, kk] = _solve_T_column(band, 2, nn, x_bar[:, kk])
+    g.chopdo(Bb)
+    Bb.LN = 0.0
+    return Bb

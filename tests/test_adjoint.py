@@ -159,3 +159,20 @@ def test_vdotpsub_and_project_adjoints():
     bars = AD.project_T(g, *ys)
     rhs = sum(_dot(b.E, x.E) for b, x in zip(bars, xs))
     assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs))
+
+
+def test_idel2ln_adjoint():
+    """IDEL2LN as B -> (A, A%LN) against its transpose (dot product, log term
+    and far-field fix included)."""
+    from oracle import adjoint as AD
+    from oracle import legops as LO
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(32, 16, 16))
+    x = _rand(g, FFF, 960)
+    x.LN = 0.0
+    y = _rand(g, FFF, 961)
+    A = LO.idel2ln(g, x.copy())
+    lhs = _dot(y.E, A.E) + y.LN * A.LN
+    bt = AD.idel2ln_T(g, y)
+    rhs = _dot(bt.E, x.E)
+    assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs))

@@ -410,3 +410,79 @@ def idel2ln_T(g, A_bar):
     g.chopdo(Bb)
     Bb.LN = 0.0
     return Bb
+
+
+def idel2_T(g, A_bar):
+    """Adjoint of IDEL2(B, A) without LN (mod_legops.f90:823-1010): the
+    far-field fix, CHOPDO, the transposed m >= 1 penta-band solves and the
+    transposed m = 0 7-band solves, where (m, k) = (0, 0) carries the log
+    column and solves the right-hand side shifted down one row (917-936)."""
+    from .bandmat import band_del2h
+    y = farfield_T(g, A_bar)
+    g.chopdo(y)
+    Bb = g.alloc(FFF)
+    K = y.E.shape[2]
+    n0 = g.NORM0
+    for mm in range(1, y.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        band0 = band_del2h(nn, g.M[mm], g.ELL, g.LOGNORM[:, mm])
+        for kk in range(K):
+            band = band0.copy()
+            band[:, 2] -= g.AK[mm, kk] ** 2
+            Bb.E[:nn, mm, kk] = _solve_T_column(band, 2, nn, y.E[:nn, mm, kk])
+    nn = int(g.NRCHOPS[0])
+    np_ = nn + 1
+    d0 = np.zeros((np_, 7))
+    d0[:, 1:6] = band_del2h(np_, g.M[0], g.ELL, g.LOGNORM[:, 0])
+    for kk in range(K):
+        o = d0.copy()
+        o[:, 3] -= g.AK[0, kk] ** 2
+        if kk == 0:
+            o[0, 3] += 4.0 / 3 / g.ELL2
+            o[1, 2] -= 2 * n0[0] / n0[1] / g.ELL2
+            o[2, 1] += 2.0 / 3 * n0[0] / n0[2] / g.ELL2
+            o[1:np_, 0:5] = o[0:np_ - 1, 1:6].copy()
+            o[:, 5:7] = 0
+            o[0, :] = 0
+            o[0, 3] = 1
+        b_bar = _solve_T_column(o, 3, nn, y.E[:nn, 0, kk])
+        if kk == 0:           # the right-hand side was shifted down one row, row 0 <- 0
+            shifted = np.zeros_like(b_bar)
+            shifted[:nn - 1] = b_bar[1:nn]
+            b_bar = shifted
+        Bb.E[:nn, 0, kk] = b_bar
+    g.chopdo(Bb)
+    Bb.LN = 0.0
+    return Bb
+
+
+def _vel2pln_vectors(g):
+    """VEL2PLN (2277-2339) as line -> line - v (c . Re line) on the (m, k) =
+    (0, 0) PFF line: c gives PSI%LN = c . Re line, v the removed -LN (1 + x)."""
+    nr, nrh = g.NR, g.NRH
+    w = g.W[:nrh]
+    nn = int(g.NRCHOPS[0])
+    pf = g.PF[:nrh, :, 0]
+    e = np.exp(g.LOGNORM[:nn, 0])
+    se = pf[:, 0:nn:2] @ e[0:nn:2]
+    so = pf[:, 1:nn:2] @ e[1:nn:2]
+    c = np.zeros(nr)
+    c[:nrh] = -0.5 * w * (se + so)
+    c[nr - 1:nrh - 1:-1] = -0.5 * w * (se - so)
+    v = np.zeros(nr)
+    v[:nrh] = -(pf[:, 0] / g.NORM0[0] + pf[:, 1] / g.NORM0[1])
+    v[nr - 1:nrh - 1:-1] = -(pf[:, 0] / g.NORM0[0] - pf[:, 1] / g.NORM0[1])
+    return c, v
+
+
+def vel2pln_T(g, RUP_bar):
+    """Adjoint of the in-place VEL2PLN update of RUP (PFF) with LN given: only
+    the real part of the (0, 0) line changes, line - v (c . Re line)."""
+    c, v = _vel2pln_vectors(g)
+    out = _field(RUP_bar.E, PFF)
+    nr = g.NR
+    y = out.E[:nr, 0, 0]
+    out.E[:nr, 0, 0] = (y.real - c * np.dot(v, y.real)) + 1j * y.imag
+    return out

@@ -176,3 +176,27 @@ def test_idel2ln_adjoint():
     bt = AD.idel2ln_T(g, y)
     rhs = _dot(bt.E, x.E)
     assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs))
+
+
+def test_idel2_and_vel2pln_adjoints():
+    from oracle import adjoint as AD
+    from oracle import legops as LO
+    from oracle.grid import FFF, PFF
+    g = oracle_grid(small_cfg(32, 16, 16))
+    x = _rand(g, FFF, 970)
+    x.LN = 0.0
+    y = _rand(g, FFF, 971)
+    y.LN = 0.0
+    A = LO.idel2(g, x.copy())
+    lhs = _dot(y.E, A.E)
+    assert abs(lhs - _dot(AD.idel2_T(g, y).E, x.E)) <= 1e-10 * max(1.0, abs(lhs))
+    # VEL2PLN with LN given: the update of RUP is linear in RUP
+    r = _rand(g, PFF, 972)
+    r.E[g.NR:] = 0.0
+    yb = _rand(g, PFF, 973)
+    yb.E[g.NR:] = 0.0
+    rr = r.copy()
+    P = g.alloc(FFF)
+    LO.vel2pln(g, rr, P, 0.0)
+    lhs = _dot(yb.E, rr.E)
+    assert abs(lhs - _dot(AD.vel2pln_T(g, yb).E, r.E)) <= 1e-12 * max(1.0, abs(lhs))

@@ -486,3 +486,52 @@ def vel2pln_T(g, RUP_bar):
     y = out.E[:nr, 0, 0]
     out.E[:nr, 0, 0] = (y.real - c * np.dot(v, y.real)) + 1j * y.imag
     return out
+
+
+def project_ppp_ln0_T(g, PSI_bar, W_bar):
+    """Adjoint of PROJECT(ROR, ROP, OZ, PSI, W, 0.0) on PPP inputs, as
+    CALC_BOUSSI_NONLIN calls it (mod_boussinesq.f90:283): PLNFFT(-1) of the
+    three inputs (HORFFT(-1) then VERFFT(-1)), VEL2PLN with LN = 0 on RUP, the
+    fold products and the far-field fix.  PSI%LN is set to 0, so it has no
+    cotangent."""
+    bars = project_T(g, PSI_bar, W_bar)
+    bars[1] = vel2pln_T(g, bars[1])
+    return [horfft_T(g, verfft_T(g, b, -1), -1) for b in bars]
+
+
+def boussi_nonlin_vjp(g, B, RUR, RUP, UZ, ROR, ROP, OZ, BN_bar, NR_bar, NP_bar, NZ_bar):
+    """Vector-Jacobian product of CALC_BOUSSI_NONLIN (mod_boussinesq.f90:235-314,
+    oracle/boussinesq.calc_boussi_nonlin): inputs B and the FFF velocity and
+    vorticity, outputs BN and the velocity form (NR, NP, NZ) of the projected
+    u x omega.  Returns the cotangents (B, RUR, RUP, UZ, ROR, ROP, OZ), FFF with LN."""
+    from .legops import grad, idel2, project, vdotpsub, vprodsub
+    from .transforms import tofp
+    # forward, keeping what the products need
+    g.chopset(1)
+    G = grad(g, B)
+    g.chopset(-1)
+    U = [tofp(g, F.copy()) for F in (RUR, RUP, UZ)]
+    Wv = [tofp(g, F.copy()) for F in (ROR, ROP, OZ)]
+    Gp = [tofp(g, F) for F in G]
+    Nv = [F.copy() for F in Wv]
+    vprodsub(g, *[F.copy() for F in U], *Nv)
+    PSI, W = project(g, *[F.copy() for F in Nv], 0.0)
+    # reverse
+    g.chopset(3)
+    psi_bar, chi_bar = pc2vel_T(g, NR_bar, NP_bar, NZ_bar)
+    g.chopset(-3)
+    w_bar = idel2_T(g, chi_bar)
+    nv_bar = project_ppp_ln0_T(g, psi_bar, w_bar)
+    bn_ppp_bar = toff_T(g, BN_bar)
+    u_bar1, w_bar1 = vprodsub_T(g, [F.E for F in U], [F.E for F in Wv], [F.E for F in nv_bar])
+    u_bar2, g_bar = vdotpsub_T(g, [F.E for F in U], [F.E for F in Gp], -bn_ppp_bar.E)
+    ins = []
+    for q in range(3):
+        ins.append(tofp_T(g, _field(u_bar1[q] + u_bar2[q], PPP)))
+    for q in range(3):
+        ins.append(tofp_T(g, _field(w_bar1[q], PPP)))
+    g_fff = [tofp_T(g, _field(gb, PPP)) for gb in g_bar]
+    g.chopset(1)
+    b_bar = grad_T(g, *g_fff)
+    g.chopset(-1)
+    return [b_bar] + ins

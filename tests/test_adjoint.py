@@ -200,3 +200,47 @@ def test_idel2_and_vel2pln_adjoints():
     LO.vel2pln(g, rr, P, 0.0)
     lhs = _dot(yb.E, rr.E)
     assert abs(lhs - _dot(AD.vel2pln_T(g, yb).E, r.E)) <= 1e-12 * max(1.0, abs(lhs))
+
+
+def test_boussi_nonlin_vjp_matches_finite_differences():
+    """The whole nonlinear term of the ETD step (GRAD, TOFP, VPRODSUB,
+    VDOTPSUB, PROJECT with VEL2PLN, IDEL2, PC2VEL, TOFF) against central
+    differences of the oracle's CALC_BOUSSI_NONLIN along random directions."""
+    from oracle import adjoint as AD
+    from oracle.boussinesq import calc_boussi_nonlin
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(24, 12, 8, adams=False))
+
+    def rnd(seed, ln=True):
+        F = _rand(g, FFF, seed)
+        g.chopdo(F)
+        F.E *= 0.1
+        if not ln:
+            F.LN = 0.0
+        return F
+
+    X = [rnd(1000, ln=False)] + [rnd(1001 + q) for q in range(6)]
+    Y = [rnd(1100 + q, ln=False) for q in range(4)]
+
+    def J(Xs):
+        outs = calc_boussi_nonlin(g, *[F.copy() for F in Xs])
+        return sum(_dot(y.E, o.E) for y, o in zip(Y, outs))
+
+    bars = AD.boussi_nonlin_vjp(g, *X, *Y)
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        D = [rnd(int(rng.integers(1 << 30)), ln=(q > 0)) for q in range(7)]
+        h = 1e-5
+
+        def shift(s):
+            out = []
+            for x, d in zip(X, D):
+                F = x.copy()
+                F.E = x.E + s * h * d.E
+                F.LN = x.LN + s * h * d.LN
+                out.append(F)
+            return out
+
+        fd = (J(shift(1)) - J(shift(-1))) / (2 * h)
+        an = sum(_dot(b.E, d.E) + b.LN * d.LN for b, d in zip(bars, D))
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)

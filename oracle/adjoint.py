@@ -23,6 +23,12 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   project_T           PROJECT (2397-2545) of PFF inputs without the log term,
                       with EOMUL/OEMUL (2548-2648) and the far-field fix
                       (farfield_T, CALCAT1 of mod_scalar3.f90:286-310)
+  vel2pln_T           VEL2PLN's update of RUP (2277-2339)
+  idel2ln_T, idel2_T  IDEL2LN (1013-1176), IDEL2 (823-1010): transposed banded
+                      solves with their log columns, row shift and far field
+  boussi_nonlin_vjp   CALC_BOUSSI_NONLIN (mod_boussinesq.f90:235-314)
+  etdab_cn_step_vjp   one steady STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901)
+                      as a map of the whole state (psi, chi, b, history)
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -535,3 +541,103 @@ def boussi_nonlin_vjp(g, B, RUR, RUP, UZ, ROR, ROP, OZ, BN_bar, NR_bar, NP_bar, 
     b_bar = grad_T(g, *g_fff)
     g.chopset(-1)
     return [b_bar] + ins
+
+
+HISTORY = ("r_pi_r", "r_pi_p", "pi_z", "r_n_r", "r_n_p", "n_z", "n_b")
+
+
+def etdab_cn_step_vjp(s, bars):
+    """Vector-Jacobian product of one steady STEP_BOUSSI_ETDAB_CN
+    (mod_march.f90:811-901, oracle Solver._step_etdab_cn with VISC%SW = 3 and
+    no sponge) as the map of the state (psi, chi, b and the seven history
+    fields) to the next state.  s: an oracle Solver holding the state before
+    the step (not changed); bars: dict of output cotangents keyed "psi", "chi",
+    "b" and HISTORY (FFF Fields; psi and chi with LN).  Returns the input
+    cotangents in a dict with the same keys."""
+    from .boussinesq import calc_boussi_etdab_sub, calc_boussi_nonlin, _etd_mats
+    from .legops import idel2ln, pc2vel, pc2vor, project
+    g, ph, dt = s.g, s.ph, s.ph.dt
+    tf = 1.0
+    hyp = s.hyp
+
+    def filt(F, which):
+        out = _field(F.E, FFF, F.LN)
+        if hyp is not None:
+            hyp._apply(g, out, hyp.hv if which == "v" else hyp.hd, tf)
+        return out
+
+    # ---- forward, keeping the intermediates
+    PSI, CHI, B = s.psi, s.chi, s.b
+    g.chopset(3)
+    V = pc2vel(g, PSI, CHI)
+    Om = pc2vor(g, PSI, CHI)
+    g.chopset(-3)
+    BN, NR_, NP_, NZ_ = calc_boussi_nonlin(g, B.copy(), *[F.copy() for F in V], *[F.copy() for F in Om])
+    Nf = [filt(F, "v") for F in (NR_, NP_, NZ_)] + [filt(BN, "d")]
+    Vw = [F.copy() for F in V]
+    Bw = B.copy()
+    calc_boussi_etdab_sub(s, Bw, *Vw, Nf[3], Nf[0], Nf[1], Nf[2], dt)
+    Vf = [filt(F, "v") for F in Vw]
+    Bf = filt(Bw, "d")
+    PSI1, W = project(g, *[F.copy() for F in Vf], "psi")
+    CHI1 = idel2ln(g, W)
+
+    # ---- reverse
+    psi1_bar = _field(bars["psi"].E, FFF, bars["psi"].LN)
+    chi1_bar = _field(bars["chi"].E, FFF, bars["chi"].LN)
+    g.chopset(3)
+    p_h, c_h = pc2vel_T(g, *[_neg(bars[k]) for k in ("r_pi_r", "r_pi_p", "pi_z")])
+    g.chopset(-3)
+    psi1_bar = _add(psi1_bar, p_h)
+    chi1_bar = _add(chi1_bar, c_h)
+    w_bar = idel2ln_T(g, chi1_bar)
+    pb = project_T(g, psi1_bar, w_bar)
+    c, _ = _vel2pln_vectors(g)
+    pb[1] = vel2pln_T(g, pb[1])
+    pb[1].E[:g.NR, 0, 0] += c * psi1_bar.LN                       # PSI%LN = c . Re line
+    vf_bar = [_add(_field(bars[k].E, FFF), rtran_T(g, b_, 1))
+              for k, b_ in zip(("r_pi_r", "r_pi_p", "pi_z"), pb)]
+    for F in vf_bar:
+        F.LN = 0.0
+    # the filters after the update
+    vw_bar = [filt(F, "v") for F in vf_bar]
+    bw_bar = filt(_field(bars["b"].E, FFF), "d")
+    # CALC_BOUSSI_ETDAB_SUB: cv = Er ev + Nr av per k
+    K = B.E.shape[2]
+    notm0 = np.ones(B.E.shape[1])
+    notm0[0] = 0.0
+    ev_bar = [np.zeros_like(B.E) for _ in range(4)]
+    av_bar = [np.zeros_like(B.E) for _ in range(4)]
+    cvb = [vw_bar[0].E, vw_bar[1].E, vw_bar[2].E, bw_bar.E]
+    for kk in range(K):
+        Er, Nr = _etd_mats(s.etd_e, s.etd_nl, dt, kk == 0)
+        cv = np.stack([x[:, :, kk] for x in cvb])
+        e_ = np.einsum("ji,j...->i...", Er, cv)
+        a_ = np.einsum("ji,j...->i...", Nr, cv)
+        for q in range(4):
+            ev_bar[q][:, :, kk] = e_[q]
+            av_bar[q][:, :, kk] = a_[q]
+    notk0 = np.ones(K)
+    notk0[0] = 0.0
+    out = {}
+    out["r_pi_r"] = _field(-ev_bar[0], FFF)
+    out["r_pi_p"] = _field(-ev_bar[1] * notm0[None, :, None], FFF)
+    out["pi_z"] = _field(-ev_bar[2] * notk0[None, None, :], FFF)
+    for k, q in zip(("r_n_r", "r_n_p", "n_z", "n_b"), range(4)):
+        out[k] = _field(-0.5 * av_bar[q], FFF)
+    v_bar = [_field(ev_bar[q], FFF) for q in range(3)]
+    b_bar = _field(ev_bar[3], FFF)
+    nf_bar = [_field(1.5 * av_bar[q], FFF) for q in range(4)]
+    for q, k in enumerate(("r_n_r", "r_n_p", "n_z", "n_b")):
+        nf_bar[q].E = nf_bar[q].E + bars[k].E
+    n_bar = [filt(nf_bar[q], "v") for q in range(3)] + [filt(nf_bar[3], "d")]
+    nl = boussi_nonlin_vjp(g, B, *V, *Om, n_bar[3], n_bar[0], n_bar[1], n_bar[2])
+    b_bar = _add(b_bar, nl[0])
+    g.chopset(3)
+    p1, c1 = pc2vel_T(g, *[_add(v_bar[q], nl[1 + q]) for q in range(3)])
+    p2, c2 = pc2vor_T(g, *nl[4:7])
+    g.chopset(-3)
+    out["psi"] = _add(p1, p2)
+    out["chi"] = _add(c1, c2)
+    out["b"] = b_bar
+    return out

@@ -244,3 +244,68 @@ def test_boussi_nonlin_vjp_matches_finite_differences():
         fd = (J(shift(1)) - J(shift(-1))) / (2 * h)
         an = sum(_dot(b.E, d.E) + b.LN * d.LN for b, d in zip(bars, D))
         assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+
+
+def test_etd_step_vjp_matches_finite_differences():
+    """One steady ETD2AB-CN step of the oracle (PC2VEL, PC2VOR, the nonlinear
+    term, HYPERV3 filters, CALC_BOUSSI_ETDAB_SUB, PROJECT with the extracted
+    log term, IDEL2LN, the history update) as a map of the whole state:
+    its VJP against central differences along random directions."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=False, nup=0.3, kappap=0.3)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    s.step()
+    keys = ("psi", "chi", "b") + AD.HISTORY
+
+    def get(sv, k):
+        return getattr(sv, k)
+
+    def run(state):
+        s2 = copy.deepcopy(s)
+        for k in keys:
+            setattr(s2, k, state[k].copy())
+        s2._step_etdab_cn()
+        return {k: get(s2, k) for k in keys}
+
+    rng = np.random.default_rng(21)
+
+    def rnd(ln):
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        F.LN = F.LN if ln else 0.0
+        return F
+
+    Y = {k: rnd(k in ("psi", "chi")) for k in keys}
+    x0 = {k: get(s, k).copy() for k in keys}
+
+    def J(state):
+        out = run(state)
+        return sum(_dot(Y[k].E, out[k].E) + (Y[k].LN * out[k].LN if k in ("psi", "chi") else 0.0) for k in keys)
+
+    bars = AD.etdab_cn_step_vjp(s, Y)
+    scale = max(np.abs(x0[k].E).max() for k in keys)
+    for _ in range(2):
+        D = {k: rnd(k in ("psi", "chi")) for k in keys}
+        h = 1e-6 * scale
+
+        def shifted(sg):
+            st = {}
+            for k in keys:
+                F = x0[k].copy()
+                F.E = F.E + sg * h * D[k].E
+                F.LN = F.LN + sg * h * D[k].LN
+                st[k] = F
+            return st
+
+        fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+        an = sum(_dot(bars[k].E, D[k].E) + (bars[k].LN * D[k].LN if k in ("psi", "chi") else 0.0) for k in keys)
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)

@@ -29,6 +29,7 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   boussi_nonlin_vjp   CALC_BOUSSI_NONLIN (mod_boussinesq.f90:235-314)
   etdab_cn_step_vjp   one steady STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901)
                       as a map of the whole state (psi, chi, b, history)
+  etd_trajectory_grad reverse accumulation of the step VJPs over a trajectory
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -641,3 +642,25 @@ def etdab_cn_step_vjp(s, bars):
     out["chi"] = _add(c1, c2)
     out["b"] = b_bar
     return out
+
+
+STATE = ("psi", "chi", "b") + HISTORY
+
+
+def etd_trajectory_grad(s, nsteps, objective_grad):
+    """Reverse-mode gradient through nsteps steady ETD2AB-CN steps from the
+    oracle Solver s (not changed): forward with every state kept, then the
+    step VJPs in reverse.  objective_grad(final_state) returns the cotangents
+    of the objective with respect to the final state (dict over STATE).
+    Returns the gradient with respect to the state s holds."""
+    import copy
+    traj = [copy.deepcopy(s)]
+    for _ in range(nsteps):
+        nxt = copy.deepcopy(traj[-1])
+        nxt._step_etdab_cn()
+        traj.append(nxt)
+    final = {k: getattr(traj[-1], k) for k in STATE}
+    bars = objective_grad(final)
+    for i in range(nsteps - 1, -1, -1):
+        bars = etdab_cn_step_vjp(traj[i], bars)
+    return bars

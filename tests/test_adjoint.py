@@ -309,3 +309,68 @@ def test_etd_step_vjp_matches_finite_differences():
         fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
         an = sum(_dot(bars[k].E, D[k].E) + (bars[k].LN * D[k].LN if k in ("psi", "chi") else 0.0) for k in keys)
         assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+
+
+def test_trajectory_gradient_matches_finite_differences():
+    """Gradient of J = 1/2 |b|^2 + 1/2 |psi|^2 + 1/2 psi%LN^2 after three ETD
+    steps with respect to the whole initial state (reverse accumulation of
+    the step VJPs) against central differences: <= 1e-6 relative."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF, Field
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=False, nup=0.3, kappap=0.3)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    s.step()
+    n = 3
+
+    def objective(st):
+        return 0.5 * (_dot(st["b"].E, st["b"].E) + _dot(st["psi"].E, st["psi"].E) + st["psi"].LN ** 2)
+
+    def objective_grad(st):
+        bars = {k: Field(np.zeros(g.shape(FFF), dtype=np.complex128), FFF, 0.0) for k in AD.STATE}
+        bars["b"] = Field(st["b"].E.copy(), FFF, 0.0)
+        bars["psi"] = Field(st["psi"].E.copy(), FFF, st["psi"].LN)
+        return bars
+
+    grad = AD.etd_trajectory_grad(s, n, objective_grad)
+
+    def J(state):
+        s2 = copy.deepcopy(s)
+        for k in AD.STATE:
+            setattr(s2, k, state[k].copy())
+        for _ in range(n):
+            s2._step_etdab_cn()
+        return objective({k: getattr(s2, k) for k in AD.STATE})
+
+    x0 = {k: getattr(s, k).copy() for k in AD.STATE}
+    rng = np.random.default_rng(8)
+    for _ in range(2):
+        D = {}
+        for k in AD.STATE:
+            F = _rand(g, FFF, int(rng.integers(1 << 30)))
+            g.chopdo(F)
+            F.E *= np.abs(x0[k].E).max() + 1e-30
+            F.LN = F.LN * abs(x0[k].LN) if k in ("psi", "chi") else 0.0
+            D[k] = F
+        h = 1e-6
+
+        def shifted(sg):
+            out = {}
+            for k in AD.STATE:
+                F = x0[k].copy()
+                F.E = F.E + sg * h * D[k].E
+                F.LN = F.LN + sg * h * D[k].LN
+                out[k] = F
+            return out
+
+        fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+        an = sum(_dot(grad[k].E, D[k].E) + (grad[k].LN * D[k].LN if k in ("psi", "chi") else 0.0)
+                 for k in AD.STATE)
+        assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)

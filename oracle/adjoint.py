@@ -29,7 +29,10 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   boussi_nonlin_vjp   CALC_BOUSSI_NONLIN (mod_boussinesq.f90:235-314)
   etdab_cn_step_vjp   one steady STEP_BOUSSI_ETDAB_CN (mod_march.f90:811-901)
                       as a map of the whole state (psi, chi, b, history)
-  etd_trajectory_grad reverse accumulation of the step VJPs over a trajectory
+  ihelm_T, visc2_T    IHELM (1204-1354), VISC2 (mod_march.f90:1579-1636)
+  boussi_force_vjp    CALC_BOUSSI_FORCE (mod_boussinesq.f90:317-410)
+  ab_cn_step_vjp      one steady STEP_BOUSSI_AB_CN (mod_march.f90:609-661)
+  trajectory_grad     reverse accumulation of the step VJPs over a trajectory
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -647,20 +650,166 @@ def etdab_cn_step_vjp(s, bars):
 STATE = ("psi", "chi", "b") + HISTORY
 
 
-def etd_trajectory_grad(s, nsteps, objective_grad):
-    """Reverse-mode gradient through nsteps steady ETD2AB-CN steps from the
-    oracle Solver s (not changed): forward with every state kept, then the
-    step VJPs in reverse.  objective_grad(final_state) returns the cotangents
-    of the objective with respect to the final state (dict over STATE).
-    Returns the gradient with respect to the state s holds."""
+def trajectory_grad(s, nsteps, objective_grad):
+    """Reverse-mode gradient through nsteps steady steps (AB2-CN or ETD2AB-CN,
+    as s.ph.adams says) from the oracle Solver s (not changed): forward with
+    every state kept, then the step VJPs in reverse.  objective_grad(final)
+    returns the cotangents of the objective with respect to the final state
+    (a dict over AB2_STATE or STATE).  Returns the gradient with respect to
+    the state s holds."""
     import copy
+    adams = s.ph.adams
+    keys = AB2_STATE if adams else STATE
     traj = [copy.deepcopy(s)]
     for _ in range(nsteps):
         nxt = copy.deepcopy(traj[-1])
-        nxt._step_etdab_cn()
+        if adams:
+            nxt._step_ab_cn()
+        else:
+            nxt._step_etdab_cn()
         traj.append(nxt)
-    final = {k: getattr(traj[-1], k) for k in STATE}
-    bars = objective_grad(final)
+    bars = objective_grad({k: getattr(traj[-1], k) for k in keys})
     for i in range(nsteps - 1, -1, -1):
-        bars = etdab_cn_step_vjp(traj[i], bars)
+        bars = ab_cn_step_vjp(traj[i], bars) if adams else etdab_cn_step_vjp(traj[i], bars)
     return bars
+
+
+def etd_trajectory_grad(s, nsteps, objective_grad):
+    """trajectory_grad for an ETD2AB-CN solver."""
+    return trajectory_grad(s, nsteps, objective_grad)
+
+
+# ----------------------------------------------------------------------
+# AB2-CN (mod_march.f90:609-661) pieces.
+
+def ihelm_T(g, A_bar, alp):
+    """Adjoint of IHELM(B, A, ALP) (mod_legops.f90:1204-1354) as the map
+    (B, B%LN) -> (A, A%LN): m >= 1 transposed penta-band solves of
+    (del^2_h - k^2 - alp); m = 0 the transposed (H XM) solve on NN-1 rows and
+    XM^T; the log term A%LN = -B%LN/alp whose del^2 rows move to the rhs."""
+    from .bandmat import band_del2h, band_to_full, band_xm, banbanmul
+    y = _field(A_bar.E, FFF, A_bar.LN)
+    g.chopdo(y)
+    Bb = g.alloc(FFF)
+    K = y.E.shape[2]
+    for mm in range(1, y.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        band0 = band_del2h(nn, g.M[mm], g.ELL, g.LOGNORM[:, mm])
+        band0[:, 2] -= alp
+        for kk in range(K):
+            band = band0.copy()
+            band[:, 2] -= g.AK[mm, kk] ** 2
+            Bb.E[:nn, mm, kk] = _solve_T_column(band, 2, nn, y.E[:nn, mm, kk])
+    nn = int(g.NRCHOPS[0])
+    np_, nm = nn + 1, nn - 1
+    xm = band_xm(np_, g.M[0], g.LOGNORM[:, 0])
+    xmf = band_to_full(xm[:nn], 1, nn)
+    h0 = band_del2h(np_, g.M[0], g.ELL, g.LOGNORM[:, 0])
+    h0[:, 2] -= alp
+    for kk in range(K):
+        h = h0.copy()
+        h[:, 2] -= g.AK[0, kk] ** 2
+        ops, _ = banbanmul(h, 2, xm, 1)
+        w_bar = xmf.T @ y.E[:nn, 0, kk]
+        Bb.E[:nm, 0, kk] = _solve_T_column(ops, 3, nm, w_bar[:nm])
+        Bb.E[nm:nn, 0, kk] = 0.0
+    g.chopdo(Bb)
+    n0 = g.NORM0
+    c = np.array([4.0 / 3 / g.ELL2 / n0[0], -2.0 / n0[1] / g.ELL2, 2.0 / 3 / n0[2] / g.ELL2])
+    # rhs(0..2, 0, 0) = B - A%LN c = B + (B%LN / alp) c;  A%LN = -B%LN / alp
+    Bb.LN = float(-y.LN / alp + np.dot(c, Bb.E[0:3, 0, 0].real) / alp)
+    return Bb
+
+
+def visc2_T(g, out_bar, nu, dt):
+    """Adjoint of VISC2(A, AO, NU, DT) (mod_march.f90:1579-1636):
+    WK = -CHOPDO(DEL2(AO) at CHOPSET(2)) - alp A, WK%LN = -alp A%LN,
+    result IHELM(WK, alp), alp = 2/(NU DT).  Returns (A_bar, AO_bar)."""
+    alp = 2 / nu / dt
+    wk = ihelm_T(g, out_bar, alp)
+    a_bar = _field(-alp * wk.E, FFF, -alp * wk.LN)
+    t = _field(-wk.E, FFF)
+    g.chopdo(t)
+    g.chopset(2)
+    ao_bar = del2_T(g, t)
+    g.chopset(-2)
+    return a_bar, ao_bar
+
+
+def boussi_force_vjp(g, ph, PSI, CHI, B, PSIN_bar, CHIN_bar, BN_bar):
+    """Vector-Jacobian product of CALC_BOUSSI_FORCE (mod_boussinesq.f90:317-410,
+    oracle calc_boussi_force): returns (PSI_bar, CHI_bar, B_bar)."""
+    from .legops import grad, pc2vel, pc2vor, vprodsub
+    from .transforms import tofp
+    g.chopset(3)
+    G = grad(g, B)
+    V = pc2vel(g, PSI, CHI)
+    Om = pc2vor(g, PSI, CHI)
+    U = [tofp(g, F.copy()) for F in V]
+    Wv = [tofp(g, F.copy()) for F in Om]
+    Gp = [tofp(g, F.copy()) for F in G]
+    g.chopset(-3)
+    w_bar = idel2ln_T(g, CHIN_bar)
+    nb = project_ppp_ln0_T(g, _field(PSIN_bar.E, FFF), w_bar)
+    bn = toff_T(g, BN_bar).E
+    o2, n2 = 2 * ph.omega, ph.bv0 ** 2
+    # ROR = N_r + 2 Omega RUP, ROP = N_t - 2 Omega RUR, OZ = N_z - W, BN = -VDOTP + N^2 UZ
+    u_lin = [-o2 * nb[1].E, o2 * nb[0].E, n2 * bn]
+    W_bar = _field(-nb[2].E, PPP)
+    g.chopset(3)
+    u1, wb = vprodsub_T(g, [F.E for F in U], [F.E for F in Wv], [F.E for F in nb])
+    u2, gb = vdotpsub_T(g, [F.E for F in U], [F.E for F in Gp], -bn)
+    ub = [tofp_T(g, _field(u1[q] + u2[q] + u_lin[q], PPP)) for q in range(3)]
+    wbf = [tofp_T(g, _field(wb[q], PPP)) for q in range(3)]
+    gbf = [tofp_T(g, _field(gb[q], PPP)) for q in range(3)]
+    p1, c1 = pc2vel_T(g, *ub)
+    p2, c2 = pc2vor_T(g, *wbf)
+    b1 = grad_T(g, *gbf)
+    g.chopset(-3)
+    b2 = tofp_T(g, W_bar)
+    g.chopdo(b2)
+    return _add(p1, p2), _add(c1, c2), _add(b1, b2)
+
+
+AB2_STATE = ("psi", "chi", "b", "n_psi", "n_chi", "n_b")
+
+
+def ab_cn_step_vjp(s, bars):
+    """Vector-Jacobian product of one steady STEP_BOUSSI_AB_CN (mod_march.f90:
+    609-661) with VISC%SW = 1 as the map of (psi, chi, b, n_psi, n_chi, n_b)
+    to the next state; s (an oracle Solver) is not changed."""
+    from .boussinesq import calc_boussi_force
+    g, ph, dt = s.g, s.ph, s.ph.dt
+    if ph.visc_sw != 1:
+        raise ValueError("ab_cn_step_vjp: VISC%SW = 1 only")
+    PSI, CHI, B = s.psi, s.chi, s.b
+    out = {}
+    pairs = {}
+    for k, nu in (("psi", ph.nu), ("chi", ph.nu), ("b", ph.kappa)):
+        yb = _field(bars[k].E, FFF, bars[k].LN if k != "b" else 0.0)
+        if nu != 0.0:
+            a_bar, ao_bar = visc2_T(g, yb, nu, dt)
+        else:
+            a_bar, ao_bar = yb, _field(np.zeros_like(yb.E), FFF)
+        if k == "b":
+            a_bar.LN = 0.0
+            ao_bar.LN = 0.0
+        pairs[k] = (a_bar, ao_bar)
+    force_bar = []
+    for k, nk in (("psi", "n_psi"), ("chi", "n_chi"), ("b", "n_b")):
+        a_bar, _ = pairs[k]
+        h = _field(bars[nk].E, FFF, bars[nk].LN if k != "b" else 0.0)
+        g.chopdo(h)
+        fb = _field(1.5 * dt * a_bar.E + h.E, FFF, 1.5 * dt * a_bar.LN + h.LN)
+        force_bar.append(fb)
+        out[nk] = _field(-0.5 * dt * a_bar.E, FFF, -0.5 * dt * a_bar.LN)
+    fp, fc, fbb = boussi_force_vjp(g, ph, PSI, CHI, B, *force_bar)
+    for k, f in (("psi", fp), ("chi", fc), ("b", fbb)):
+        a_bar, ao_bar = pairs[k]
+        ao = _field(ao_bar.E, FFF, ao_bar.LN)
+        g.chopdo(ao)
+        out[k] = _add(a_bar, ao, f)
+    out["b"].LN = 0.0
+    return out

@@ -374,3 +374,125 @@ def test_trajectory_gradient_matches_finite_differences():
         an = sum(_dot(grad[k].E, D[k].E) + (grad[k].LN * D[k].LN if k in ("psi", "chi") else 0.0)
                  for k in AD.STATE)
         assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)
+
+
+def test_ab2_step_vjp_matches_finite_differences():
+    """One steady AB2-CN step (CALC_BOUSSI_FORCE with the linear terms, the
+    AB2 update, VISC2 with IHELM for psi, chi and b) as a map of
+    (psi, chi, b, n_psi, n_chi, n_b): its VJP against central differences."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=True)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    s.step()
+    keys = AD.AB2_STATE
+    lnk = ("psi", "chi", "n_psi", "n_chi")
+    rng = np.random.default_rng(31)
+
+    def rnd(ln):
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        F.LN = F.LN if ln else 0.0
+        return F
+
+    Y = {k: rnd(k in lnk) for k in keys}
+    x0 = {k: getattr(s, k).copy() for k in keys}
+
+    def J(state):
+        s2 = copy.deepcopy(s)
+        for k in keys:
+            setattr(s2, k, state[k].copy())
+        s2._step_ab_cn()
+        return sum(_dot(Y[k].E, getattr(s2, k).E) + (Y[k].LN * getattr(s2, k).LN if k in lnk else 0.0)
+                   for k in keys)
+
+    bars = AD.ab_cn_step_vjp(s, Y)
+    for _ in range(2):
+        D = {k: rnd(k in lnk) for k in keys}
+        for k in keys:
+            D[k].E *= np.abs(x0[k].E).max() + 1e-30
+        h = 1e-6
+
+        def shifted(sg):
+            out = {}
+            for k in keys:
+                F = x0[k].copy()
+                F.E = F.E + sg * h * D[k].E
+                F.LN = F.LN + sg * h * D[k].LN
+                out[k] = F
+            return out
+
+        fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+        an = sum(_dot(bars[k].E, D[k].E) + (bars[k].LN * D[k].LN if k in lnk else 0.0) for k in keys)
+        assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)
+
+
+def test_ab2_trajectory_gradient_matches_finite_differences():
+    """The objective of the ETD test after three AB2-CN steps (the stepper of
+    the gradient configuration), reverse accumulation against central
+    differences."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF, Field
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=True)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    n = 3
+    keys = AD.AB2_STATE
+
+    def objective(st):
+        return 0.5 * (_dot(st["b"].E, st["b"].E) + _dot(st["psi"].E, st["psi"].E) + st["psi"].LN ** 2)
+
+    def objective_grad(st):
+        bars = {k: Field(np.zeros(g.shape(FFF), dtype=np.complex128), FFF, 0.0) for k in keys}
+        bars["b"] = Field(st["b"].E.copy(), FFF, 0.0)
+        bars["psi"] = Field(st["psi"].E.copy(), FFF, st["psi"].LN)
+        return bars
+
+    grad = AD.trajectory_grad(s, n, objective_grad)
+
+    def J(state):
+        s2 = copy.deepcopy(s)
+        for k in keys:
+            setattr(s2, k, state[k].copy())
+        for _ in range(n):
+            s2._step_ab_cn()
+        return objective({k: getattr(s2, k) for k in keys})
+
+    x0 = {k: getattr(s, k).copy() for k in keys}
+    rng = np.random.default_rng(12)
+    D = {}
+    for k in keys:
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        F.E *= np.abs(x0[k].E).max() + 1e-30
+        F.LN = F.LN * abs(x0[k].LN) if k in ("psi", "chi", "n_psi", "n_chi") else 0.0
+        D[k] = F
+    h = 1e-6
+
+    def shifted(sg):
+        out = {}
+        for k in keys:
+            F = x0[k].copy()
+            F.E = F.E + sg * h * D[k].E
+            F.LN = F.LN + sg * h * D[k].LN
+            out[k] = F
+        return out
+
+    fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+    an = sum(_dot(grad[k].E, D[k].E) + grad[k].LN * D[k].LN for k in keys)
+    assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)

@@ -33,6 +33,8 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   boussi_force_vjp    CALC_BOUSSI_FORCE (mod_boussinesq.f90:317-410)
   ab_cn_step_vjp      one steady STEP_BOUSSI_AB_CN (mod_march.f90:609-661)
   trajectory_grad     reverse accumulation of the step VJPs over a trajectory
+  energy_objective(_grad)  J = KE of the fluctuations + 1/2 int b^2 dV
+                      (mod_boussinesq.f90:112-206 quadratures) and its gradient
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -813,3 +815,72 @@ def ab_cn_step_vjp(s, bars):
         out[k] = _add(a_bar, ao, f)
     out["b"].LN = 0.0
     return out
+
+
+# ----------------------------------------------------------------------
+# The gradient configuration's objective: J = KE(psi - psi_bar, chi - chi_bar)
+# + 1/2 int b^2 dV, psi_bar, chi_bar the (m, k) = (0, 0) parts (log term
+# included), KE in the quadrature form of CALC_BOUSSI_ENERGY
+# (mod_boussinesq.f90:176-206: PRODCT_MK of RTRAN'd DELSQH / DEL2 at CHOPSET(3))
+# and int b^2 dV = 2 x the summed CALC_BOUSSI_PE (mod_boussinesq.f90:112-136)
+# times N^2.
+
+def _pff_weights(g, inv_om2=False):
+    """Per-entry weights of the PFF quadratures, 4 pi ZLEN ELL2 w_r (/(1-x_r)^2),
+    m = 0 halved: prodct_mk_allk / l2norm_mk_allk summed over (m, k)."""
+    nr = g.NR
+    w = g.W[:nr] / ((1 - g.X[:nr]) ** 2 if inv_om2 else 1.0)
+    f = np.ones(g.NTCHOPDIM)
+    f[0] = 0.5
+    out = np.zeros(g.shape(PFF))
+    out[:nr] = 4.0 * np.pi * g.ZLEN * g.ELL2 * w[:, None, None] * f[None, :, None]
+    return out
+
+
+def _fluct(F):
+    out = F.copy()
+    out.E[:, 0, 0] = 0.0
+    out.LN = 0.0
+    return out
+
+
+def energy_objective(g, psi, chi, b):
+    """J = KE(psi - psi_bar, chi - chi_bar) + 1/2 int b^2 dV (see above)."""
+    from .diagnostics import boussi_energy
+    ke, pe, _ = boussi_energy(g, _fluct(psi), _fluct(chi), _field(b.E, FFF), 1.0)
+    return float(ke.sum() + pe.sum())
+
+
+def energy_objective_grad(g, psi, chi, b):
+    """Gradient of energy_objective with respect to (psi, chi, b) (FFF, with
+    LN): the quadratic forms' symmetric parts through RTRAN(+1)^T, DELSQH^T
+    and DEL2^T at CHOPSET(3)."""
+    from .legops import del2, delsqh
+    from .transforms import rtran
+    Wt = _pff_weights(g)
+    Wb = _pff_weights(g, inv_om2=True)
+    p, c = _fluct(psi), _fluct(chi)
+    g.chopset(3)
+    try:
+        def R(F):
+            X = _field(F.E, FFF)
+            rtran(g, X, 1)
+            return X
+
+        # KE = 1/2 [ -<R p, R Dh p>_W + <R D2 c, R Dh c>_W ]  (LN parts are zero)
+        Rp, RDp = R(p), R(delsqh(g, p))
+        gp = _add(rtran_T(g, _field(-0.5 * Wt * RDp.E, PFF), 1),
+                  delsqh_T(g, rtran_T(g, _field(-0.5 * Wt * Rp.E, PFF), 1)))
+        RD2c, RDc = R(del2(g, c)), R(delsqh(g, c))
+        gc = _add(del2_T(g, rtran_T(g, _field(0.5 * Wt * RDc.E, PFF), 1)),
+                  delsqh_T(g, rtran_T(g, _field(0.5 * Wt * RD2c.E, PFF), 1)))
+        # 1/2 int b^2 = 1/2 <R b, R b>_{W/(1-x)^2}
+        Rb = R(_field(b.E, FFF))
+        gb = rtran_T(g, _field(Wb * Rb.E, PFF), 1)
+    finally:
+        g.chopset(-3)
+    for G in (gp, gc):
+        G.E[:, 0, 0] = 0.0
+        G.LN = 0.0
+    gb.LN = 0.0
+    return gp, gc, gb

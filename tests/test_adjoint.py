@@ -496,3 +496,97 @@ def test_ab2_trajectory_gradient_matches_finite_differences():
     fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
     an = sum(_dot(grad[k].E, D[k].E) + grad[k].LN * D[k].LN for k in keys)
     assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)
+
+
+def test_energy_objective_gradient():
+    """The gradient configuration's objective (fluctuation kinetic energy plus
+    1/2 int b^2) and its gradient against central differences."""
+    from oracle import adjoint as AD
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(24, 12, 8))
+    rng = np.random.default_rng(41)
+
+    def rnd():
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        return F
+
+    x = [rnd(), rnd(), rnd()]
+    x[2].LN = 0.0
+    grads = AD.energy_objective_grad(g, *x)
+    for _ in range(2):
+        d = [rnd(), rnd(), rnd()]
+        d[2].LN = 0.0
+        h = 1e-6
+
+        def J(sg):
+            xs = []
+            for a, b in zip(x, d):
+                F = a.copy()
+                F.E = a.E + sg * h * b.E
+                F.LN = a.LN + sg * h * b.LN
+                xs.append(F)
+            return AD.energy_objective(g, *xs)
+
+        fd = (J(1) - J(-1)) / (2 * h)
+        an = sum(_dot(G.E, b.E) + G.LN * b.LN for G, b in zip(grads, d))
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+
+
+def test_energy_objective_trajectory_gradient():
+    """J = fluctuation KE + 1/2 int b^2 after three AB2-CN steps: reverse
+    accumulation against central differences."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF, Field
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=True)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s.initialize()
+    keys = AD.AB2_STATE
+    n = 3
+
+    def objective_grad(st):
+        gp, gc, gb = AD.energy_objective_grad(g, st["psi"], st["chi"], st["b"])
+        bars = {k: Field(np.zeros(g.shape(FFF), dtype=np.complex128), FFF, 0.0) for k in keys}
+        bars["psi"], bars["chi"], bars["b"] = gp, gc, gb
+        return bars
+
+    grad = AD.trajectory_grad(s, n, objective_grad)
+
+    def J(state):
+        s2 = copy.deepcopy(s)
+        for k in keys:
+            setattr(s2, k, state[k].copy())
+        for _ in range(n):
+            s2._step_ab_cn()
+        return AD.energy_objective(g, s2.psi, s2.chi, s2.b)
+
+    x0 = {k: getattr(s, k).copy() for k in keys}
+    rng = np.random.default_rng(77)
+    D = {}
+    for k in keys:
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        F.E *= np.abs(x0[k].E).max() + 1e-30
+        F.LN = F.LN * abs(x0[k].LN) if k in ("psi", "chi", "n_psi", "n_chi") else 0.0
+        D[k] = F
+    h = 1e-6
+
+    def shifted(sg):
+        out = {}
+        for k in keys:
+            F = x0[k].copy()
+            F.E = F.E + sg * h * D[k].E
+            F.LN = F.LN + sg * h * D[k].LN
+            out[k] = F
+        return out
+
+    fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+    an = sum(_dot(grad[k].E, D[k].E) + grad[k].LN * D[k].LN for k in keys)
+    assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)

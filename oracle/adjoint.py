@@ -35,6 +35,10 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
   trajectory_grad     reverse accumulation of the step VJPs over a trajectory
   energy_objective(_grad)  J = KE of the fluctuations + 1/2 int b^2 dV
                       (mod_boussinesq.f90:112-206 quadratures) and its gradient
+  visc1_T, rich_fe_be_vjp  VISC1 (mod_march.f90:1529-1576), RICH_BOUSSI_FE_BE
+                      (535-606)
+  idelsqh_T, initial_state_T  IDELSQH (mod_legops.f90:136-241) and the seeded
+                      initial state's dependence on its perturbation coefficients
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -884,3 +888,97 @@ def energy_objective_grad(g, psi, chi, b):
         G.LN = 0.0
     gb.LN = 0.0
     return gp, gc, gb
+
+
+def visc1_T(g, out_bar, nu, dt):
+    """Adjoint of VISC1(A, NU, DT) (mod_march.f90:1529-1576) = IHELM(-alp A, alp),
+    alp = 1/(NU DT)."""
+    alp = 1 / (nu * dt)
+    wk = ihelm_T(g, out_bar, alp)
+    return _field(-alp * wk.E, FFF, -alp * wk.LN)
+
+
+def _visc_be_T(g, ph, bars, dt):
+    out = []
+    for k, F in zip(("psi", "chi", "b"), bars):
+        nu = ph.kappa if k == "b" else ph.nu
+        if nu == 0.0:
+            out.append(F.copy())
+        else:
+            out.append(visc1_T(g, F, nu, dt))
+    out[2].LN = 0.0
+    return out
+
+
+def rich_fe_be_vjp(s0, bars):
+    """Vector-Jacobian product of RICH_BOUSSI_FE_BE (mod_march.f90:535-606,
+    the AB2-CN start-up, VISC%SW = 1) as the map (psi, chi, b) -> (psi, chi,
+    b, n_psi, n_chi, n_b); s0 is an oracle Solver holding (psi, chi, b)."""
+    from .boussinesq import calc_boussi_force, calc_boussi_visc_be
+    g, ph, dt = s0.g, s0.ph, s0.ph.dt
+    hdt = 0.5 * dt
+    x0 = [s0.psi.copy(), s0.chi.copy(), s0.b.copy()]
+
+    def axpy(xs, a, fs):
+        out = []
+        for x, f in zip(xs, fs):
+            F = x.copy()
+            F.E = x.E + a * f.E
+            F.LN = x.LN + a * f.LN
+            out.append(F)
+        out[2].LN = x0[2].LN
+        return out
+
+    F0 = calc_boussi_force(g, ph, *[F.copy() for F in x0])
+    x2 = list(calc_boussi_visc_be(g, ph, *axpy(x0, hdt, F0), hdt))
+    out_bar = [_field(bars[k].E, FFF, bars[k].LN if k != "b" else 0.0) for k in ("psi", "chi", "b")]
+    x2pp_bar = [_field(2.0 * F.E, FFF, 2.0 * F.LN) for F in out_bar]
+    x1_bar = [_field(-F.E, FFF, -F.LN) for F in out_bar]
+    y1 = _visc_be_T(g, ph, x1_bar, dt)
+    x2p_bar = _visc_be_T(g, ph, x2pp_bar, hdt)
+    f1_bar = [_field(hdt * F.E, FFF, hdt * F.LN) for F in x2p_bar]
+    fx2 = boussi_force_vjp(g, ph, *x2, *f1_bar)
+    x2_bar = [_add(a, b_) for a, b_ in zip(x2p_bar, fx2)]
+    z = _visc_be_T(g, ph, x2_bar, hdt)
+    f0_bar = []
+    for q, k in enumerate(("n_psi", "n_chi", "n_b")):
+        F = _field(dt * y1[q].E + hdt * z[q].E + bars[k].E, FFF,
+                   dt * y1[q].LN + hdt * z[q].LN + (bars[k].LN if k != "n_b" else 0.0))
+        f0_bar.append(F)
+    fx0 = boussi_force_vjp(g, ph, *x0, *f0_bar)
+    res = {}
+    for q, k in enumerate(("psi", "chi", "b")):
+        res[k] = _add(y1[q], z[q], fx0[q])
+    res["b"].LN = 0.0
+    return res
+
+
+def idelsqh_T(g, A_bar):
+    """Adjoint of IDELSQH(B, A) (mod_legops.f90:136-241): the far-field fix,
+    A = -B ELL2/(n(n+1)) for n >= 1, and A%LN = Re B(1,1,1) NORM(1,1) ELL2."""
+    y = farfield_T(g, A_bar)
+    Bb = g.alloc(FFF)
+    for mm in range(y.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        for i in range(nn):
+            n = int(g.M[mm]) + i
+            if n >= 1:
+                Bb.E[i, mm, :] = -y.E[i, mm, :] * (g.ELL2 / (n * (n + 1)))
+    Bb.E[0, 0, 0] += A_bar.LN * g.NORM0[0] * g.ELL2
+    return Bb
+
+
+def initial_state_T(g, psi_bar, chi_bar, b_bar):
+    """Adjoint of the seeded initial state (oracle layout.initial_state) with
+    respect to the perturbation coefficients (c_psi, c_chi, c_b)."""
+    out = []
+    for F in (psi_bar, chi_bar):
+        q = _field(F.E, FFF, F.LN)
+        g.chopdo(q)
+        p = idelsqh_T(g, q)
+        g.chopdo(p)
+        out.append(-p.E)
+    bb = farfield_T(g, _field(b_bar.E, FFF))
+    g.chopdo(bb)
+    out.append(bb.E)
+    return out

@@ -590,3 +590,57 @@ def test_energy_objective_trajectory_gradient():
     fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
     an = sum(_dot(grad[k].E, D[k].E) + grad[k].LN * D[k].LN for k in keys)
     assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)
+
+
+def test_gradient_wrt_perturbation_coefficients():
+    """The gradient configuration end to end in the oracle: J = fluctuation KE
+    + 1/2 int b^2 after the Richardson start-up and two AB2-CN steps, with
+    respect to the seeded perturbation coefficients (c_psi, c_chi, c_b),
+    against central differences."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF, Field
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=True)
+    g = oracle_grid(cfg)
+    ph = oracle_physics(cfg)
+    cs = [perturbation_coefficients(cfg, i) for i in range(3)]
+    n = 2
+
+    def run(c):
+        P, C, B = layout.initial_state(g, *c)
+        s = BQ.Solver(g, ph, P, C, B)
+        s.initialize()
+        traj = [s]
+        for _ in range(n):
+            s2 = copy.deepcopy(traj[-1])
+            s2._step_ab_cn()
+            traj.append(s2)
+        return P, C, B, traj
+
+    def J(c):
+        return AD.energy_objective(g, *[getattr(run(c)[3][-1], k) for k in ("psi", "chi", "b")])
+
+    P, C, B, traj = run(cs)
+    keys = AD.AB2_STATE
+
+    def objective_grad(st):
+        gp, gc, gb = AD.energy_objective_grad(g, st["psi"], st["chi"], st["b"])
+        bars = {k: Field(np.zeros(g.shape(FFF), dtype=np.complex128), FFF, 0.0) for k in keys}
+        bars["psi"], bars["chi"], bars["b"] = gp, gc, gb
+        return bars
+
+    bars = AD.trajectory_grad(traj[0], n, objective_grad)
+    s0 = BQ.Solver(g, ph, P.copy(), C.copy(), B.copy())
+    x0_bar = AD.rich_fe_be_vjp(s0, bars)
+    c_bar = AD.initial_state_T(g, x0_bar["psi"], x0_bar["chi"], x0_bar["b"])
+    rng = np.random.default_rng(99)
+    for _ in range(2):
+        d = [(rng.standard_normal(c.shape) + 1j * rng.standard_normal(c.shape)) * np.abs(c).max() for c in cs]
+        h = 1e-6
+        fd = (J([c + h * e for c, e in zip(cs, d)]) - J([c - h * e for c, e in zip(cs, d)])) / (2 * h)
+        an = sum(_dot(cb, e) for cb, e in zip(c_bar, d))
+        assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)

@@ -39,6 +39,8 @@ on complex arrays (and LN * LN_bar for the log-term scalar), so that
                       (535-606)
   idelsqh_T, initial_state_T  IDELSQH (mod_legops.f90:136-241) and the seeded
                       initial state's dependence on its perturbation coefficients
+  etdfe_be_vjp, rich_etdfe_be_vjp  STEP_BOUSSI_ETDFE_BE (mod_march.f90:664-753)
+                      and RICH_BOUSSI_ETDFE_BE (756-808)
 
 Every CHOPDO along the way is a 0/1 projection and is its own adjoint.
 
@@ -982,3 +984,110 @@ def initial_state_T(g, psi_bar, chi_bar, b_bar):
     g.chopdo(bb)
     out.append(bb.E)
     return out
+
+
+def etdfe_be_vjp(s, PSI, CHI, B, E, NL, dt, store, bars):
+    """Vector-Jacobian product of STEP_BOUSSI_ETDFE_BE (mod_march.f90:664-753,
+    oracle Solver._etdfe_be, no sponge) from (PSI, CHI, B) to (PSI', CHI', B')
+    and, with store, the seven history fields (r_pi_* = (V - PC2VEL(PSI',
+    CHI'))/2).  E, NL: the ETD matrices for dt; s supplies the filters."""
+    from .boussinesq import calc_boussi_etdfe_sub, calc_boussi_nonlin, _etd_mats
+    from .legops import idel2ln, pc2vel, pc2vor, project
+    g, ph = s.g, s.ph
+    tf = dt / ph.dt
+    hyp = s.hyp
+
+    def filt(F, which):
+        out = _field(F.E, FFF, F.LN)
+        if hyp is not None:
+            hyp._apply(g, out, hyp.hv if which == "v" else hyp.hd, tf)
+        return out
+
+    g.chopset(3)
+    V = pc2vel(g, PSI, CHI)
+    Om = pc2vor(g, PSI, CHI)
+    g.chopset(-3)
+    BN, NR_, NP_, NZ_ = calc_boussi_nonlin(g, B.copy(), *[F.copy() for F in V], *[F.copy() for F in Om])
+    Nf = [filt(F, "v") for F in (NR_, NP_, NZ_)] + [filt(BN, "d")]
+    Vw = [F.copy() for F in V]
+    Bw = B.copy()
+    calc_boussi_etdfe_sub(E, NL, Bw, *Vw, Nf[3], Nf[0], Nf[1], Nf[2], dt)
+    Vf = [filt(F, "v") for F in Vw]
+    # reverse
+    psi1_bar = _field(bars["psi"].E, FFF, bars["psi"].LN)
+    chi1_bar = _field(bars["chi"].E, FFF, bars["chi"].LN)
+    vf_bar = [_field(np.zeros_like(B.E), FFF) for _ in range(3)]
+    if store:
+        g.chopset(3)
+        p_h, c_h = pc2vel_T(g, *[_field(-0.5 * bars[k].E, FFF) for k in ("r_pi_r", "r_pi_p", "pi_z")])
+        g.chopset(-3)
+        psi1_bar = _add(psi1_bar, p_h)
+        chi1_bar = _add(chi1_bar, c_h)
+        vf_bar = [_field(0.5 * bars[k].E, FFF) for k in ("r_pi_r", "r_pi_p", "pi_z")]
+    w_bar = idel2ln_T(g, chi1_bar)
+    pb = project_T(g, psi1_bar, w_bar)
+    c, _ = _vel2pln_vectors(g)
+    pb[1] = vel2pln_T(g, pb[1])
+    pb[1].E[:g.NR, 0, 0] += c * psi1_bar.LN
+    vf_bar = [_add(vf_bar[q], rtran_T(g, pb[q], 1)) for q in range(3)]
+    for F in vf_bar:
+        F.LN = 0.0
+    vw_bar = [filt(F, "v") for F in vf_bar]
+    bw_bar = filt(_field(bars["b"].E, FFF), "d")
+    K = B.E.shape[2]
+    ev_bar = [np.zeros_like(B.E) for _ in range(4)]
+    av_bar = [np.zeros_like(B.E) for _ in range(4)]
+    cvb = [vw_bar[0].E, vw_bar[1].E, vw_bar[2].E, bw_bar.E]
+    for kk in range(K):
+        Er, Nr = _etd_mats(E, NL, dt, kk == 0)
+        cv = np.stack([x[:, :, kk] for x in cvb])
+        e_ = np.einsum("ji,j...->i...", Er, cv)
+        a_ = np.einsum("ji,j...->i...", Nr, cv)
+        for q in range(4):
+            ev_bar[q][:, :, kk] = e_[q]
+            av_bar[q][:, :, kk] = a_[q]
+    nf_bar = [_field(av_bar[q], FFF) for q in range(4)]
+    if store:
+        for q, k in enumerate(("r_n_r", "r_n_p", "n_z", "n_b")):
+            nf_bar[q].E = nf_bar[q].E + bars[k].E
+    n_bar = [filt(nf_bar[q], "v") for q in range(3)] + [filt(nf_bar[3], "d")]
+    nl = boussi_nonlin_vjp(g, B, *V, *Om, n_bar[3], n_bar[0], n_bar[1], n_bar[2])
+    b_bar = _add(_field(ev_bar[3], FFF), nl[0])
+    g.chopset(3)
+    p1, c1 = pc2vel_T(g, *[_add(_field(ev_bar[q], FFF), nl[1 + q]) for q in range(3)])
+    p2, c2 = pc2vor_T(g, *nl[4:7])
+    g.chopset(-3)
+    return _add(p1, p2), _add(c1, c2), b_bar
+
+
+def rich_etdfe_be_vjp(s0, bars):
+    """Vector-Jacobian product of RICH_BOUSSI_ETDFE_BE (mod_march.f90:756-808,
+    the ETD2AB-CN start-up, VISC%SW = 3 so the BE viscous steps are identities)
+    as the map (psi, chi, b) -> (psi, chi, b and the seven history fields)."""
+    from .boussinesq import calc_boussi_etd_op
+    g, ph, dt = s0.g, s0.ph, s0.ph.dt
+    if ph.visc_sw == 1:
+        raise ValueError("rich_etdfe_be_vjp: VISC%SW = 1 not handled")
+    hdt = 0.5 * dt
+    he, hnl = calc_boussi_etd_op(ph.bv0, ph.omega, hdt)
+    x0 = [s0.psi.copy(), s0.chi.copy(), s0.b.copy()]
+    y0 = [g.copy0(F) for F in x0]
+    y2 = list(s0._etdfe_be(*[F.copy() for F in y0], he, hnl, hdt, False))
+    out_bar = {k: bars[k] for k in ("psi", "chi", "b")}
+    z_bars = {k: _field(-bars[k].E, FFF, -bars[k].LN if k != "b" else 0.0) for k in ("psi", "chi", "b")}
+    for k in HISTORY:
+        z_bars[k] = bars[k]
+    fe, fnl = calc_boussi_etd_op(ph.bv0, ph.omega, dt)
+    zp, zc, zb = etdfe_be_vjp(s0, *x0, fe, fnl, dt, True, z_bars)
+    y3_bar = {k: _field(2.0 * out_bar[k].E, FFF, 2.0 * out_bar[k].LN if k != "b" else 0.0)
+              for k in ("psi", "chi", "b")}
+    a = etdfe_be_vjp(s0, *y2, he, hnl, hdt, False, y3_bar)
+    y1_bar = dict(zip(("psi", "chi", "b"), a))
+    y0_bar = etdfe_be_vjp(s0, *y0, he, hnl, hdt, False, y1_bar)
+    res = {}
+    for q, (k, zq) in enumerate(zip(("psi", "chi", "b"), (zp, zc, zb))):
+        y = _field(y0_bar[q].E, FFF, y0_bar[q].LN)
+        g.chopdo(y)
+        res[k] = _add(zq, y)
+    res["b"].LN = 0.0
+    return res

@@ -644,3 +644,61 @@ def test_gradient_wrt_perturbation_coefficients():
         fd = (J([c + h * e for c, e in zip(cs, d)]) - J([c - h * e for c, e in zip(cs, d)])) / (2 * h)
         an = sum(_dot(cb, e) for cb, e in zip(c_bar, d))
         assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)
+
+
+def test_etd_startup_vjp_matches_finite_differences():
+    """The ETD2AB-CN Richardson start-up (two half ETDFE steps against one full
+    step, with the history it stores) as a map of (psi, chi, b): its VJP
+    against central differences."""
+    import copy
+    from oracle import adjoint as AD
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle.grid import FFF
+    from conftest import oracle_physics
+    from mlegs_b200.inputs import perturbation_coefficients
+    cfg = small_cfg(24, 12, 8, adams=False, nup=0.3, kappap=0.3)
+    g = oracle_grid(cfg)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s0 = BQ.Solver(g, oracle_physics(cfg), P, C, B)
+    s0.etd_e, s0.etd_nl = BQ.calc_boussi_etd_op(cfg.bv0, cfg.omega, cfg.dt)   # as INITIALIZE sets them
+    keys = AD.STATE
+    ins = ("psi", "chi", "b")
+    rng = np.random.default_rng(55)
+
+    def rnd(ln):
+        F = _rand(g, FFF, int(rng.integers(1 << 30)))
+        g.chopdo(F)
+        F.LN = F.LN if ln else 0.0
+        return F
+
+    Y = {k: rnd(k in ("psi", "chi")) for k in keys}
+
+    def J(state):
+        s2 = copy.deepcopy(s0)
+        for k in ins:
+            setattr(s2, k, state[k].copy())
+        s2._rich_etdfe_be()
+        return sum(_dot(Y[k].E, getattr(s2, k).E) + (Y[k].LN * getattr(s2, k).LN if k in ("psi", "chi") else 0.0)
+                   for k in keys)
+
+    bars = AD.rich_etdfe_be_vjp(s0, Y)
+    x0 = {k: getattr(s0, k).copy() for k in ins}
+    for _ in range(2):
+        D = {k: rnd(k in ("psi", "chi")) for k in ins}
+        for k in ins:
+            D[k].E *= np.abs(x0[k].E).max()
+        h = 1e-6
+
+        def shifted(sg):
+            out = {}
+            for k in ins:
+                F = x0[k].copy()
+                F.E = F.E + sg * h * D[k].E
+                F.LN = F.LN + sg * h * D[k].LN
+                out[k] = F
+            return out
+
+        fd = (J(shifted(1)) - J(shifted(-1))) / (2 * h)
+        an = sum(_dot(bars[k].E, D[k].E) + bars[k].LN * D[k].LN for k in ins)
+        assert abs(fd - an) <= 1e-6 * max(1e-12, abs(an)), (fd, an)

@@ -389,10 +389,10 @@ __global__ void __launch_bounds__(256) theta4_kernel(DevGrid g, PhysArgs A, cons
 
 // ------------------------------------------------------------------------
 // Fused physical stage with in-place line slots (9 slots of N per warp):
-//   round 1: RUR RUP UZ [B]  -> slots 0 1 2 3
-//   round 2: ROR ROP OZ RBR  -> slots 4 5 6 7, then per sample
+//   phase 1: RUR RUP UZ [B]  -> slots 0 1 2 3
+//   phase 2: ROR ROP OZ RBR  -> slots 4 5 6 7, then per sample
 //            slot 4 <- N_r, 5 <- N_theta, 6 <- N_z (all terms), 7 <- a1 c1
-//   round 3: RBP BZ          -> slots 3 8, then slot 7 <- N_b
+//   phase 3: RBP BZ          -> slots 3 8, then slot 7 <- N_b
 //   forward: slots 4 5 6 7   -> OUT 0 1 2 3
 // Each group's transposes run inside its own line slot (fft4::swz), so a warp
 // needs 9 N complex of shared memory instead of 11 N plus padded tiles.
@@ -508,7 +508,7 @@ __device__ __forceinline__ double2* pick_out(const PhysArgs& A, int i) {
     return p;
 }
 
-// After round 2 (slots: 0-2 velocity, 3 B, 4-6 vorticity, 7 RBR): slots 4-6 <-
+// After phase 2 (slots: 0-2 velocity, 3 B, 4-6 vorticity, 7 RBR): slots 4-6 <-
 // N_r, N_theta, N_z of VPRODSUB (+ the linear terms), slot 7 <- a1 c1.
 template <int N>
 __device__ __forceinline__ void theta_products_r2(double2* L, int lane, double ir2, double o2, int linear) {
@@ -534,7 +534,7 @@ __device__ __forceinline__ void theta_products_r2(double2* L, int lane, double i
     }
 }
 
-// After round 3 (slot 3 RBP, slot 8 BZ): slot 7 <- N_b of VDOTPSUB (+ N^2 u_z).
+// After phase 3 (slot 3 RBP, slot 8 BZ): slot 7 <- N_b of VDOTPSUB (+ N^2 u_z).
 template <int N>
 __device__ __forceinline__ void theta_products_r3(double2* L, int lane, double ir2, double n2, int linear) {
     for (int j = lane; j < N; j += 32) {
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
         // Rows arrive by cp.async one round ahead: the three (four) round-1
         // rows of the next line while this line's forward transforms run, the
         // round-2 rows (and, without the linear terms, the round-3 rows into
-        // the then unused slots 3 and 8) while round 1 computes.
+        // the then unused slots 3 and 8) while phase 1 computes.
         const int mlim = md < g.NTCHOP ? md : g.NTCHOP;
         auto issue_r1 = [&](int ln) {
             const size_t o = (size_t)ln * md;
@@ -599,10 +599,10 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
                              : "memory");
             const double rr = g.r[line / g.NX];
             const double ir2 = 1.0 / (rr * rr);
-            row_async<N2>(pick_in(A, 3 + gid) + off, mlim, L + (size_t)(4 + gid) * N, t);  // round 2
+            row_async<N2>(pick_in(A, 3 + gid) + off, mlim, L + (size_t)(4 + gid) * N, t);  // phase 2
             async_commit();
             if (!A.linear) issue_r3(line);
-            // round 1: fields 0-2 (and B with the linear terms) in slots 0-3
+            // phase 1: fields 0-2 (and B with the linear terms) in slots 0-3
             if (A.linear) async_wait<1>();
             else async_wait<2>();
             __syncwarp();
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
             else
                 idle_group_syncs();
             __syncwarp();
-            // round 2: fields 3-6 in slots 4-7
+            // phase 2: fields 3-6 in slots 4-7
             if (A.linear) async_wait<0>();
             else async_wait<1>();
             __syncwarp();
@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
             __syncwarp();
             theta_products_r2<N>(L, lane, ir2, o2, A.linear);
             __syncwarp();
-            // round 3: RBP -> slot 3, BZ -> slot 8
+            // phase 3: RBP -> slot 3, BZ -> slot 8
             if (A.linear) issue_r3(line);
             async_wait<0>();
             __syncwarp();
@@ -650,9 +650,9 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
         }
         const double rr = g.r[line / g.NX];
         const double ir2 = 1.0 / (rr * rr);
-        // round 1 and 2 (G = 4: one field per group; G = 2: two passes; G = 8: half the groups idle)
-        // round 1: field q (q < 3) or B (q = 3, linear terms only) -> slot q;
-        // round 2: field 3 + q -> slot 4 + q
+        // phase 1 and 2 (G = 4: one field per group; G = 2: two passes; G = 8: half the groups idle)
+        // phase 1: field q (q < 3) or B (q = 3, linear terms only) -> slot q;
+        // phase 2: field 3 + q -> slot 4 + q
         for (int rd = 0; rd < 2; ++rd) {
             for (int f0 = 0; f0 < 4; f0 += G) {
                 const int q = f0 + gid;
@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
         // round-2 products
         theta_products_r2<N>(L, lane, ir2, o2, A.linear);
         __syncwarp();
-        // round 3
+        // phase 3
         for (int f0 = 0; f0 < 4; f0 += G) {
             const int q = f0 + gid;
             if (q < 2)  // RBP -> slot 3, BZ -> slot 8

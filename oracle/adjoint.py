@@ -980,7 +980,11 @@ def initial_state_T(g, psi_bar, chi_bar, b_bar):
         p = idelsqh_T(g, q)
         g.chopdo(p)
         out.append(-p.E)
-    bb = farfield_T(g, _field(b_bar.E, FFF))
+    # The state is zero outside the chop, so its cotangent there is dropped
+    # before the far-field transpose, which would mix it into kept entries.
+    bq = _field(b_bar.E, FFF)
+    g.chopdo(bq)
+    bb = farfield_T(g, bq)
     g.chopdo(bb)
     out.append(bb.E)
     return out

@@ -33,6 +33,7 @@ import math
 from dataclasses import dataclass
 
 import torch
+from torch.autograd.function import once_differentiable
 
 __all__ = ["LoopStats", "CheckpointedLoop", "run_loop"]
 
@@ -95,9 +96,13 @@ class CheckpointedLoop(torch.autograd.Function):
         return tuple(t.clone() for t in cur)
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, *grads):
         stepper, nsteps, every, stats = ctx.stepper, ctx.nsteps, ctx.every, ctx.stats
         checkpoints = ctx.checkpoints
+        if checkpoints is None:
+            raise RuntimeError("run_loop supports a single backward pass: its checkpoints were "
+                               "released by the previous one")
         n = len(grads)
         bars = tuple(grads)
         if nsteps > 0 and any(g is None for g in bars):

@@ -16,9 +16,23 @@ path after --error-steps steps from the same state, against the 1e-9 bound.
 Every step touches several GB (100 MB physical fields), far above the 126 MB
 L2, so no explicit L2 flush is needed between steps.
 
+The error of both GPU paths against the FP64 oracle itself is measured too:
+an oracle process (spawned before the first GPU call, so it runs on the host
+cores while the GPU is timed) runs the Richardson start-up and --oracle-steps
+- 1 steady steps from the same state; "precision_comparison" reports the
+FP64 and the mixed GPU paths' field errors against it, and the mixed path's
+error against the FP64 GPU path after --error-steps steps.
+
+"transform_roundtrip" is the transform-only configuration: FFF -> PPP -> FFF
+(TOFP, TOFF) at 256^3 with 2/3 chops, a batch of 8 fields, per precision
+form (FP64 and split-BF16 S = 4, 5, 6): device time per round trip and the
+relative error of PPP and of the returned FFF against the FP64 oracle for the
+chi, psi and b coefficient sets (mlegs_b200.inputs.roundtrip_coefficients).
+
 --impl reference times the reference's path as restated on the CPU (the
 numpy/scipy FP64 oracle under oracle/, all host cores): the reference itself
-is Fortran 90 + MPI + FFTW + MKL and cannot be built in this image.
+is Fortran 90 + MPI + FFTW + MKL and cannot be built in this image, so that
+arm is a numpy restatement of the reference, not the Fortran solver.
 """
 
 import argparse
@@ -49,6 +63,9 @@ def parse():
     ap.add_argument("--slices", type=int, default=6, help="split-BF16 slices per operand (3..6)")
     ap.add_argument("--no-compare", action="store_true", help="skip the other path and the error check")
     ap.add_argument("--error-steps", type=int, default=100)
+    ap.add_argument("--oracle-steps", type=int, default=10,
+                    help="steps (start-up included) of the oracle trajectory the GPU paths are checked against")
+    ap.add_argument("--no-roundtrip", action="store_true", help="skip the 256^3 transform round-trip leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     return ap.parse_args()
@@ -189,6 +206,101 @@ def oracle_steps(cfg, nsteps, warm=0):
     return nsteps / dt
 
 
+def oracle_trajectory(name, nsteps, threads):
+    """Oracle (E, LN) of psi, chi, b after the Richardson start-up and nsteps - 1
+    steady steps from the benchmark's initial state; runs in a child process
+    on `threads` host threads.  Returns (states, seconds)."""
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = str(threads)
+    from mlegs_b200.inputs import CONFIGS, perturbation_coefficients
+    from oracle import boussinesq as BQ
+    from oracle import layout
+    from oracle import transforms
+    from oracle.grid import Grid
+    transforms.WORKERS = threads
+    cfg = CONFIGS[name]
+    t0 = time.perf_counter()
+    g = Grid(cfg.nr, cfg.nth, cfg.nx, cfg.nrchop, cfg.ntchop, cfg.nxchop, cfg.ell, cfg.zlen)
+    ph = BQ.Physics(dt=cfg.dt, omega=cfg.omega, bv0=cfg.bv0, kappa=cfg.kappa, kappap=cfg.kappap,
+                    adams=cfg.adams, visc_sw=cfg.visc_sw, nu=cfg.nu, nup=cfg.nup, p=cfg.p)
+    P, C, B = layout.initial_state(g, *[perturbation_coefficients(cfg, i) for i in range(3)])
+    s = BQ.Solver(g, ph, P, C, B)
+    s.initialize()
+    for _ in range(nsteps - 1):
+        s.step()
+    return [(F.E, F.LN) for F in (s.psi, s.chi, s.b)], time.perf_counter() - t0
+
+
+def start_oracle_trajectory(name, nsteps):
+    """Start oracle_trajectory in a spawned process (before any GPU call)."""
+    import multiprocessing as mp
+    threads = max(1, (os.cpu_count() or 2) // 2)
+    pool = mp.get_context("spawn").Pool(1)
+    return pool, pool.apply_async(oracle_trajectory, (name, nsteps, threads))
+
+
+def field_errors(got, ref):
+    """max|d| / max|ref| per field and |d LN| / max(1, |LN|) per log term."""
+    import numpy as np
+    errs = {}
+    for name, (E, ln), (R, rl) in zip(("psi", "chi", "b"), got, ref):
+        errs[name] = float(np.abs(E - R).max() / np.abs(R).max())
+        errs[name + "_ln"] = float(abs(ln - rl) / max(1.0, abs(rl)))
+    return errs
+
+
+def roundtrip_leg(local, reps=10, batch=8):
+    """The transform-only configuration: FFF -> PPP -> FFF at 256^3 per precision form."""
+    import numpy as np
+
+    import mlegs_b200 as M
+    from mlegs_b200.inputs import CONFIGS, roundtrip_coefficients
+    from oracle import transforms as T
+    from oracle.grid import FFF, Grid
+    cfg = CONFIGS["roundtrip_256"]
+    g = Grid(cfg.nr, cfg.nth, cfg.nx, cfg.nrchop, cfg.ntchop, cfg.nxchop, cfg.ell, cfg.zlen)
+    names = ("chi", "psi", "b")
+    coefs = [roundtrip_coefficients(cfg, i) for i in range(3)]
+    refs = []
+    for c in coefs:
+        A = g.alloc(FFF)
+        A.E = c.copy()
+        T.tofp(g, A)
+        ppp = A.E.copy()
+        T.toff(g, A)
+        refs.append((ppp, A.E.copy()))
+    out = {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx], "chops": [cfg.nrchop, cfg.ntchop, cfg.nxchop],
+           "batch": batch, "reference": "FP64 oracle (numpy/scipy restatement of TOFP/TOFF)", "forms": {}}
+    for form, prec, S in (("fp64", M.PREC_FP64, 0), ("split4", M.PREC_SPLIT, 4), ("split5", M.PREC_SPLIT, 5),
+                          ("split6", M.PREC_SPLIT, 6)):
+        try:
+            ctx = M.Context(cfg, precision=prec, split_slices=S, device=local)
+        except M.MlegsError as e:
+            out["forms"][form] = {"unsupported": str(e)}
+            continue
+        try:
+            ms, by = ctx.kernel_time("roundtrip", reps=reps)
+            e_ppp, e_fff, e_id = {}, {}, {}
+            f = ctx.field(M.FFF)
+            for name, c, (ppp, fff) in zip(names, coefs, refs):
+                f.upload(c, 0.0, M.FFF)
+                ctx.TOFP(f)
+                E, _ = f.download()
+                e_ppp[name] = float(np.abs(E - ppp).max() / np.abs(ppp).max())
+                ctx.TOFF(f)
+                E, _ = f.download()
+                e_fff[name] = float(np.abs(E - fff).max() / np.abs(fff).max())
+                e_id[name] = float(np.abs(E - c).max() / np.abs(c).max())
+            out["forms"][form] = {"ms_per_roundtrip": ms, "batch_ms": batch * ms,
+                                  "roundtrips_per_s": 1000.0 / ms, "batches_per_s": 1000.0 / (batch * ms),
+                                  "algorithmic_bytes_per_roundtrip": by, "achieved_gbs": by / (ms * 1e-3) / 1e9,
+                                  "rel_err_ppp_vs_oracle": e_ppp, "rel_err_fff_vs_oracle": e_fff,
+                                  "rel_err_fff_vs_input": e_id}
+        finally:
+            ctx.close()
+    return out
+
+
 def run_reference(args, cfg, ws, rank):
     if rank != 0:
         return
@@ -201,6 +313,8 @@ def run_reference(args, cfg, ws, rank):
             "config": {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx],
                        "chops": [cfg.nrchop, cfg.ntchop, cfg.nxchop], "scheme": "ETD2AB-CN" if not cfg.adams else "AB2-CN",
                        "parallelism": "cpu threads"},
+            "reference_kind": "numpy restatement of the reference (Fortran 90/MPI/FFTW solver unavailable: "
+                              "not buildable in this image)",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": "%d steady steps after %d warm-up, FP64 numpy/scipy restatement of the "
                                        "reference path (reference Fortran not buildable here)" % (args.steps, args.warmup)},
@@ -240,6 +354,9 @@ def run_ours(args, cfg, ws, rank, local):
     import mlegs_b200 as M
     split = args.precision == "split"
     prec = M.PREC_SPLIT if split else M.PREC_FP64
+    orc = None
+    if not args.no_compare and rank == 0 and ws == 1:
+        orc = start_oracle_trajectory(cfg.name, args.oracle_steps)  # before the first GPU call
     torch.cuda.set_device(local)
     ctx = M.Context(cfg, precision=prec, split_slices=args.slices if split else 0, device=local)
     psi, chi, b = M.initial_state(ctx)
@@ -326,15 +443,34 @@ def run_ours(args, cfg, ws, rank, local):
         other_value = ws * args.steps / (ms2 / 1000.0)
         ref = _state_after(M, cfg, M.PREC_FP64, 0, args.error_steps, local)
         mix = _state_after(M, cfg, M.PREC_SPLIT, args.slices, args.error_steps, local)
-        errs = {}
-        for name, (E, ln), (R, rl) in zip(("psi", "chi", "b"), mix, ref):
-            errs[name] = float(np.abs(E - R).max() / np.abs(R).max())
-            errs[name + "_ln"] = float(abs(ln - rl) / max(1.0, abs(rl)))
+        errs = field_errors(mix, ref)
         mixed_v, fp64_v = (other_value, value) if other_split else (value, other_value)
         compare = {"fp64_steps_per_s": fp64_v, "mixed_steps_per_s": mixed_v, "split_slices": args.slices,
                    "mixed_over_fp64": mixed_v / fp64_v, "error_steps": args.error_steps,
                    "mixed_rel_error_vs_fp64": errs, "error_bound": 1e-9,
                    "mixed_within_bound": max(errs.values()) <= 1e-9}
+        if orc is not None:
+            pool, job = orc
+            orc_states, orc_s = job.get()
+            pool.close()
+            pool.join()
+            n_o = args.oracle_steps
+            fp_o = _state_after(M, cfg, M.PREC_FP64, 0, n_o, local)
+            mx_o = _state_after(M, cfg, M.PREC_SPLIT, args.slices, n_o, local)
+            e_fp, e_mx = field_errors(fp_o, orc_states), field_errors(mx_o, orc_states)
+            compare.update({"oracle_steps": n_o, "oracle_seconds": orc_s,
+                            "fp64_rel_error_vs_oracle": e_fp, "mixed_rel_error_vs_oracle": e_mx,
+                            "comparand": "FP64 oracle (numpy restatement of the reference path) after %d steps "
+                                         "(start-up included); the %d-step figures compare the mixed GPU path with "
+                                         "the FP64 GPU path" % (n_o, args.error_steps)})
+            orc = None
+
+    if orc is not None:  # comparison skipped: do not leave the oracle process behind
+        orc[0].terminate()
+        orc[0].join()
+    rtrip = None
+    if rank == 0 and ws == 1 and not args.no_roundtrip:
+        rtrip = roundtrip_leg(local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -357,7 +493,8 @@ def run_ours(args, cfg, ws, rank, local):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * nbytes,
                         "d2h_bytes_per_step": 3 * nbytes},
                 "gpu_launches": int(launches), "precision_comparison": compare,
-                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "roofline": roof, "kernels": kernels, "transform_roundtrip": rtrip, "cpu_baseline": cpu,
+                "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
 
 

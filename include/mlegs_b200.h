@@ -21,7 +21,8 @@
  * reference's ERR_FLAGS codes (mod_scalar3.f90:88-106) or an MLEGS_ERR_*
  * code below; nothing aborts the process.  Calls on one context are
  * stream-ordered on that context's CUDA stream and must not be issued
- * concurrently from several host threads; distinct contexts are independent.
+ * concurrently from several host threads; distinct contexts are independent
+ * (except for mlegs_idel2ln_static, whose calls share one array per device).
  */
 #ifndef MLEGS_B200_H
 #define MLEGS_B200_H
@@ -50,6 +51,7 @@ extern "C" {
 #define MLEGS_ERR_NOMEM        102
 #define MLEGS_ERR_NONFINITE    103
 #define MLEGS_ERR_STATE        104
+#define MLEGS_ERR_TIMEOUT      105   /* a bounded device-side wait ran out */
 
 /* Space tags, mod_scalar3.f90:82-85. */
 #define MLEGS_PPP 0
@@ -88,7 +90,16 @@ typedef struct mlegs_field mlegs_field;
 int mlegs_create(const mlegs_params* p, mlegs_ctx** out);
 int mlegs_destroy(mlegs_ctx* ctx);
 const char* mlegs_last_error(const mlegs_ctx* ctx);
+/* Waits for the context's stream; returns MLEGS_ERR_TIMEOUT (once) when a
+ * bounded wait inside a tensor-core kernel ran out since the last sync (the
+ * results of that launch are invalid; the context stays usable). */
 int mlegs_sync(mlegs_ctx* ctx);
+/* Limit of the pipeline waits inside the tensor-core kernels, in SM cycles
+ * (0 restores the default, about one second).  No counterpart in the
+ * reference.  A short limit makes a wait run out: the kernel then drains what
+ * it has in flight, frees its tensor memory and returns, and the next
+ * mlegs_sync reports MLEGS_ERR_TIMEOUT; used to test that error path. */
+int mlegs_set_wait_limit(mlegs_ctx* ctx, int64_t cycles);
 /* Sizes (NDIMR, NDIMTH, NX, NRCHOPDIM, NTCHOPDIM, NXCHOPDIM, NRH, NR, NTH). */
 int mlegs_dims(const mlegs_ctx* ctx, int32_t out[9]);
 
@@ -136,14 +147,26 @@ int mlegs_idel2ln(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad)
  * allocator holds the memory they may use, or the implicit device-wide
  * synchronisation of cudaMalloc is unaffordable in their time loop).  The
  * elimination scratch is a fixed 64 MiB __device__ array inside this library,
- * held by every GPU that loads it until the process exits; grids needing more
+ * held on a device from the first call there (from library load when CUDA's
+ * lazy module loading is off) until the process exits; grids needing more
  * (NRCHOPDIM*4*NTCHOPDIM*NXCHOPDIM doubles > 8,388,608) get MLEGS_ERR_ARG.
  * The first call on a device looks the array up (cudaGetSymbolAddress), so
- * make it before any stream capture.  All calls on a device share the array:
+ * make it before any stream capture.  That address is cached for the life of
+ * the process: a host that resets the device (cudaDeviceReset) must not call
+ * this entry point afterwards.  All calls on a device share the array:
  * calls whose kernels overlap on the GPU race and must be ordered by the
  * caller.  Results equal mlegs_idel2ln's. */
 int mlegs_idel2ln_static(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int pad);
 int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad); /* IHELM 1204 */
+/* IHELMP(P, B, A, ALP, NUIN) (1409-1592): A = (DEL^P + nu DEL^2 - alp)^-1 B for
+ * even p in 4..14 and alp /= 0 (the log term moved to the right-hand side,
+ * A%LN = -B%LN/alp, the far-field fix, CHOPDO). */
+int mlegs_ihelmp(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int p, double alp, double nu, int pad);
+/* HYPERV(A, NU, NUP, P, DT, WK) (mod_march.f90:1639-1686): one implicit
+ * hyperviscosity step of A in place, IHELMP(P, alp A, A, -alp, bet) with
+ * alp = (-1)^(P/2) / (dt nup), bet = -(-1)^(P/2) nu / nup.  The steppers apply
+ * it to PSI, CHI (and B when KAPPAP /= 0) when VISC%SW = 2 (AB2-CN only). */
+int mlegs_hyperv(mlegs_ctx* ctx, mlegs_field* a, double nu, double nup, int p, double dt);
 int mlegs_grad(mlegs_ctx* ctx, const mlegs_field* a, mlegs_field* rgr, mlegs_field* rgp,
                mlegs_field* gz, int pad);                                            /* GRAD   1727 */
 int mlegs_pc2vel(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
@@ -160,6 +183,21 @@ int mlegs_project(mlegs_ctx* ctx, mlegs_field* rur, mlegs_field* rup, mlegs_fiel
 int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi,
                        const mlegs_field* b, mlegs_field* psin, mlegs_field* chin,
                        mlegs_field* bn);
+
+/* CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ), mod_boussinesq.f90:235-314:
+ * GRAD(B) at CHOPSET(1), nine TOFP, VPRODSUB / VDOTPSUB, PROJECT (LN = 0),
+ * IDEL2, PC2VEL at CHOPSET(3), TOFF(BN).  b, rur..oz in FFF.  On return ror,
+ * rop, oz hold the velocity form of the projected u x omega (FFF), bn the
+ * FFF -(u.grad)b; rur, rup, uz are consumed (the reference deallocates them):
+ * they are left holding the physical velocity in PFP.  All fields distinct. */
+int mlegs_boussi_nonlin(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* rur, mlegs_field* rup, mlegs_field* uz,
+                        mlegs_field* bn, mlegs_field* ror, mlegs_field* rop, mlegs_field* oz);
+
+/* TFM%PF (LEGINIT, mod_fft.f90:297): the orthonormal associated Legendre
+ * table the device built, in the reference layout PF(NRH, NRCHOPDIM+1,
+ * NTCHOPDIM) (column-major), NRH*(NRCHOPDIM+1)*NTCHOPDIM doubles.
+ * Synchronises the context's stream. */
+int mlegs_legendre_table(mlegs_ctx* ctx, double* pf);
 
 /* Snapshots in the reference's files (mod_fft.f90:2224-2642), written and
  * read by one process: global = 1 is MSAVEX / MLOADX (one Fortran unformatted
@@ -269,6 +307,7 @@ int mlegs_check_finite(mlegs_ctx* ctx);
 #define MLEGS_K_PROJECT    13   /* PROJECT's five EOMUL/OEMUL products, 3 PFF -> 2 FFF */
 #define MLEGS_K_PROJECT_FFF 14  /* PROJECT of FFF velocity fields via composite matrices, 3 FFF -> 2 FFF */
 #define MLEGS_K_PHYS_NONLIN 15  /* MLEGS_K_PHYS as CALC_BOUSSI_NONLIN runs it: 9 inputs, no linear terms */
+#define MLEGS_K_ROUNDTRIP  16   /* TOFP then TOFF of one field, FFF -> PPP -> FFF (context's precision) */
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
 /* Number of this library's kernel launches issued since the counter was reset. */

@@ -215,6 +215,16 @@ class Context:
         self._ck(self.lib.mlegs_ihelm(self.c, b.h, a.h, float(alp), pad))
         return a
 
+    def IHELMP(self, P, b, a, alp, NU=0.0, pad=0):
+        """IHELMP(P, B, A, ALP, NUIN) (mod_legops.f90:1409-1592)."""
+        self._ck(self.lib.mlegs_ihelmp(self.c, b.h, a.h, int(P), float(alp), float(NU), pad))
+        return a
+
+    def HYPERV(self, a, NU, NUP, P, DT):
+        """HYPERV(A, NU, NUP, P, DT, WK) (mod_march.f90:1639-1686), A in place."""
+        self._ck(self.lib.mlegs_hyperv(self.c, a.h, float(NU), float(NUP), int(P), float(DT)))
+        return a
+
     def GRAD(self, a, rr, rp, gz, pad=0):
         self._ck(self.lib.mlegs_grad(self.c, a.h, rr.h, rp.h, gz.h, pad))
 
@@ -236,6 +246,18 @@ class Context:
 
     def CALC_BOUSSI_FORCE(self, psi, chi, b, psin, chin, bn):
         self._ck(self.lib.mlegs_boussi_force(self.c, psi.h, chi.h, b.h, psin.h, chin.h, bn.h))
+
+    def CALC_BOUSSI_NONLIN(self, b, rur, rup, uz, bn, ror, rop, oz):
+        """CALC_BOUSSI_NONLIN(B, RUR, RUP, UZ, BN, ROR, ROP, OZ) (mod_boussinesq.f90:235-314):
+        ROR, ROP, OZ become the velocity form of the projected u x omega, BN the
+        FFF -(u.grad)b; RUR, RUP, UZ are consumed (left in PFP)."""
+        self._ck(self.lib.mlegs_boussi_nonlin(self.c, b.h, rur.h, rup.h, uz.h, bn.h, ror.h, rop.h, oz.h))
+
+    def legendre_table(self):
+        """TFM%PF (mod_fft.f90:297) as built on the device: (NRH, NRCHOPDIM+1, NTCHOPDIM)."""
+        out = np.empty((self.NRH, self.NRCHOPDIM + 1, self.NTCHOPDIM), dtype=np.float64, order="F")
+        self._ck(self.lib.mlegs_legendre_table(self.c, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
 
     # ------------------------------------------------------------ diagnostics
     def _mk_array(self):
@@ -322,7 +344,7 @@ class Context:
                "horfft_f": 5, "pointwise": 6, "solve": 7, "phys": 8,
                "horfft_wb": 9, "horfft_wf": 10, "split_b2p": 11,
                "split_p2b": 12, "project": 13,
-               "project_fff": 14, "phys_nonlin": 15}
+               "project_fff": 14, "phys_nonlin": 15, "roundtrip": 16}
 
     def kernel_time(self, name, reps=20):
         """Mean device ms per launch of one internal kernel (CUDA events on the

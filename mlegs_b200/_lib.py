@@ -1,7 +1,7 @@
 """ctypes binding of include/mlegs_b200.h (the library's C ABI).
 
 This is the binding a Python host of the reference path would add; the
-Fortran host binds the same symbols through ISO_C_BINDING (INTEGRATION.md).
+Fortran host binds the same symbols through ISO_C_BINDING.
 The library is loaded from the package directory only: there is no CPU
 fallback, and a missing or unloadable library raises immediately.
 """
@@ -47,6 +47,7 @@ SIGNATURES = {
     "mlegs_destroy": (c_int, [c_void_p]),
     "mlegs_last_error": (c_char_p, [c_void_p]),
     "mlegs_sync": (c_int, [c_void_p]),
+    "mlegs_set_wait_limit": (c_int, [c_void_p, c_int64]),
     "mlegs_dims": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "mlegs_field_alloc": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p)]),
     "mlegs_field_free": (c_int, [c_void_p, c_void_p]),
@@ -73,11 +74,15 @@ SIGNATURES = {
     "mlegs_idel2ln": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_idel2ln_static": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_ihelm": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int]),
+    "mlegs_ihelmp": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, c_int]),
+    "mlegs_hyperv": (c_int, [c_void_p, c_void_p, c_double, c_double, c_int, c_double]),
     "mlegs_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_pc2vel": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_pc2vor": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "mlegs_project": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double]),
     "mlegs_boussi_force": (c_int, [c_void_p] + [c_void_p] * 6),
+    "mlegs_boussi_nonlin": (c_int, [c_void_p] + [c_void_p] * 8),
+    "mlegs_legendre_table": (c_int, [c_void_p, c_void_p]),
     "mlegs_boussi_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_boussi_pe": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mlegs_diagnost": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

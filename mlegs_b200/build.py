@@ -39,16 +39,27 @@ def build(force=False, verbose=False):
     """Compile every CUDA source and link the shared library; returns its path."""
     if not force and not _stale():
         return OUT
-    objs = []
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
+    jobs = []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
             continue
         obj = os.path.join(build_dir, src.replace(".cu", ".o"))
         cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append((src, obj, cmd))
+
+    def compile_one(job):
+        src, obj, cmd = job
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per source, several at a time (each is single-threaded)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, jobs))
+    objs = []
+    for (src, r), (_, obj, _) in zip(results, jobs):
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s" % (src, r.stderr))
         if verbose:

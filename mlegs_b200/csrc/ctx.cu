@@ -6,522 +6,9 @@
 // Nothing here computes on the CPU except the FP64 set-up tables that the
 // reference also builds once (LOGNORM, band-operator coefficients, ETD 4x4
 // matrices, hyperviscosity masks).
-#include <cmath>
-#include <complex>
-#include <cstdio>
-#include <cstring>
-#include <functional>
-#include <algorithm>
-#include <initializer_list>
-#include <memory>
-#include <stdexcept>
-#include <string>
-#include <vector>
+#include "ctx_internal.h"
 
-#include "mlegs_internal.h"
-
-using namespace mlegs;
-
-namespace {
-
-struct CudaError : std::runtime_error {
-    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
-};
-struct ApiError : std::runtime_error {
-    int code;
-    ApiError(int c, const std::string& s) : std::runtime_error(s), code(c) {}
-};
-
-#define CK(call)                                                                         \
-    do {                                                                                 \
-        cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
-            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));         \
-    } while (0)
-
-// Every device allocation of a context is recorded here and released in one
-// place, whatever field or scratch slot currently points at it.
-thread_local std::vector<void*>* g_allocs = nullptr;
-
-template <class T>
-T* dalloc(size_t n) {
-    void* p = nullptr;
-    if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-    if (e != cudaSuccess) throw ApiError(MLEGS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    if (g_allocs) g_allocs->push_back(p);
-    return (T*)p;
-}
-
-}  // namespace
-
-struct mlegs_field {
-    Field f;
-    mlegs_ctx* owner;
-};
-
-struct mlegs_ctx {
-    mlegs_params p{};
-    Dims d{};
-    DevGrid g{};
-    cudaStream_t s = nullptr;
-    cudaStream_t s2 = nullptr;         // second stream of the RTRAN(+1) -> VERFFT(+1) pipeline
-    cudaEvent_t evs[64] = {};          // fork/join events, used in rotation
-    int ev_next = 0;
-    double2* pbuf[3] = {};             // PFF images in flight between the two stages
-    int dev = 0;
-    std::string err;
-    int64_t launches = 0;
-    int64_t graph_launches = 0;   // kernels in one captured step
-    std::vector<void*> allocs;
-
-    // device tables
-    double *x = nullptr, *w = nullptr, *r = nullptr, *lnx = nullptr, *pf = nullptr, *ak = nullptr;
-    double *norm0 = nullptr, *explog0 = nullptr, *at1 = nullptr, *tb_xxdx = nullptr, *tb_xm = nullptr,
-           *tb_del2h = nullptr;
-    double *V = nullptr, *D = nullptr, *T = nullptr;
-    double *hv[3] = {nullptr, nullptr, nullptr}, *hd[3] = {nullptr, nullptr, nullptr};
-    // HYP3SET masks (VISC%MASK_R/T/X) and the adaptive state of VISC
-    // (mod_march.f90:70-86): NUP_R/T/X, KAPPAP_R/T/X, the controllers' history.
-    std::vector<double> h3_mr, h3_mt, h3_mx, h3_ak;
-    double nup3[3] = {0, 0, 0}, kap3[3] = {0, 0, 0};
-    Hyp3State adj;
-    double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
-    double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
-    double* diag = nullptr;                                         // 4 x [m][k] quadratures (energy)
-    double *sp_damp = nullptr, *sp_damp_h = nullptr;                // sponge factors for DT and DT/2 (RMV%SW = 2)
-    double *etdE = nullptr, *etdN = nullptr, *hetdE = nullptr, *hetdN = nullptr;
-    FFTPlan fft;
-    std::vector<double> h_x, h_w, h_lognorm;
-
-    // memory
-    double* lnslots = nullptr;
-    int nslots = 0, used_slots = 0;
-    double2* scratch = nullptr;
-    double* solve_scr = nullptr;
-    // split-BF16 tensor-core GEMMs (MLEGS_PREC_SPLIT)
-    int split_S = 0;                 // slices per operand; 0 = FP64 GEMMs
-    uint8_t* split_img = nullptr;    // PF slice images for RTRAN(+1)
-    int* split_eA = nullptr;         // PF row scale exponents
-    int* split_err = nullptr;        // raised by a timed-out wait in a tensor-core kernel
-    uint8_t* fimg[4] = {};           // weight slice images: 0 PF (RTRAN -1), 1 V, 2 D, 3 T (PROJECT)
-    int* feA[4] = {};
-    // out (+)= s Wt . fold(in): FP64 kernel, or the split tensor-core kernel when enabled
-    void fold(int w, const double* Wt, int wt_rows, const double2* in, double2* out, int mode, int scale,
-              int accumulate, int pad, cudaStream_t st = nullptr) {
-        if (!st) st = s;
-        if (split_S)
-            k_split_fold(g, split_S, fimg[w], feA[w], wt_rows, in, out, mode & 1, scale, accumulate, pad,
-                         (mode & 2) ? 1 : 0, split_err, st);
-        else
-            k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, st);
-    }
-    double2* staging = nullptr;
-    int* dflag = nullptr;
-    std::vector<std::unique_ptr<mlegs_field>> owned;  // every field, incl. user ones
-    std::vector<Field*> pool;                         // free temporaries (stack)
-    std::vector<Field*> temps;                        // all temporaries
-    Field* hist[7] = {};
-
-    // solver state
-    Field *psi = nullptr, *chi = nullptr, *b = nullptr;
-    bool solver_ready = false;
-    double t = 0.0;
-    int n = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-
-    // ------------------------------------------------------------------
-    mlegs_field* new_field_h(int space, bool persistent) {
-        auto mf = std::make_unique<mlegs_field>();
-        mf->owner = this;
-        Field& f = mf->f;
-        f.data = dalloc<double2>(d.cap());
-        f.home = f.data;
-        if (used_slots >= nslots) throw ApiError(MLEGS_ERR_NOMEM, "out of LN slots");
-        f.slot = used_slots++;
-        f.ln = lnslots + f.slot;
-        f.space = space;
-        f.persistent = persistent;
-        CK(cudaMemsetAsync(f.data, 0, d.cap() * sizeof(double2), s));
-        mlegs_field* out = mf.get();
-        owned.push_back(std::move(mf));
-        return out;
-    }
-    Field* new_field(int space, bool persistent) { return &new_field_h(space, persistent)->f; }
-    Field* tmp(int space = MLEGS_FFF) {
-        if (pool.empty()) throw ApiError(MLEGS_ERR_NOMEM, "temporary field pool exhausted");
-        Field* f = pool.back();
-        pool.pop_back();
-        f->space = space;
-        return f;
-    }
-    void rel(Field* f) { pool.push_back(f); }
-
-    void set_error(const std::string& e) { err = e; }
-
-    // ------------------------------------------------------------------ set-up
-    void init(const mlegs_params& prm);
-    void destroy();
-
-    // ------------------------------------------------------------------ basic
-    size_t fff() const { return d.fff(); }
-    void zero_fff(Field* f) { k_fill(f->data, fff(), s); }
-    void ln_zero(Field* f) { CK(cudaMemsetAsync(f->ln, 0, sizeof(double), s)); }
-    void chopdo(Field* f, int pad) {
-        if (f->space == MLEGS_FFF) k_chopdo_fff(g, f->data, pad, s);
-        // PFF/PFP/PPP: the device layouts do not store the padded rows/columns.
-    }
-    void require(const Field* f, int space, const char* who) {
-        if (f->space != space)
-            throw ApiError(MLEGS_ERR_TRANSFORM, std::string(who) + ": input not in the expected space");
-    }
-    // COPY0 (mod_fft.f90:705-769): dst = src, CHOPDO for FFF, LN copied.
-    void copy0(Field* dst, const Field* src, int pad) {
-        if (dst == src) return;
-        k_copy(dst->data, src->data, d.elems(src->space), s);
-        dst->space = src->space;
-        CK(cudaMemcpyAsync(dst->ln, src->ln, sizeof(double), cudaMemcpyDeviceToDevice, s));
-        chopdo(dst, pad);
-    }
-    void swap_scratch(Field* f) {
-        if (f->persistent) throw ApiError(MLEGS_ERR_STATE, "in-place transform of a persistent field");
-        std::swap(f->data, scratch);
-    }
-    void swap_scratch_any(Field* f) { std::swap(f->data, scratch); }
-
-    // ------------------------------------------------------------------ transforms
-    // RTRAN(A, IS), mod_fft.f90:1150-1340.  Both directions zero A%LN.
-    void rtran(Field* f, int is, int pad) {
-        if (is == -1) {
-            require(f, MLEGS_PFF, "RTRAN");
-            fold(0, pf, d.NRCHOPDIM + 1, f->data, scratch, 0 | 2, 0, 0, pad);
-            swap_scratch_any(f);
-            f->space = MLEGS_FFF;
-        } else {
-            require(f, MLEGS_FFF, "RTRAN");
-            if (split_S)
-                k_split_b2p(g, split_S, split_img, split_eA, f->data, scratch, f->ln, pad, split_err, s);
-            else
-                k_rtran_b2p(g, f->data, scratch, f->ln, pad, s);
-            swap_scratch_any(f);
-            f->space = MLEGS_PFF;
-        }
-        ln_zero(f);
-    }
-    // VERFFT(A, IS), mod_fft.f90:928-1113 (LN preserved).
-    void verfft(Field* f, int is) {
-        if (is == -1) {
-            require(f, MLEGS_PFP, "VERFFT");
-            if (!k_verfft4(g, fft, f->data, scratch, -1, s)) k_verfft_f(g, fft, f->data, scratch, s);
-            swap_scratch_any(f);
-            f->space = MLEGS_PFF;
-        } else {
-            require(f, MLEGS_PFF, "VERFFT");
-            if (!k_verfft4(g, fft, f->data, scratch, +1, s)) k_verfft_b(g, fft, f->data, scratch, s);
-            swap_scratch_any(f);
-            f->space = MLEGS_PFP;
-        }
-    }
-    // HORFFT(A, IS), mod_fft.f90:771-926.
-    void horfft(Field* f, int is) {
-        if (is == -1) {
-            require(f, MLEGS_PPP, "HORFFT");
-            k_horfft_warp(g, fft, f->data, scratch, -1, s);
-            swap_scratch_any(f);
-            f->space = MLEGS_PFP;
-        } else {
-            require(f, MLEGS_PFP, "HORFFT");
-            k_horfft_warp(g, fft, f->data, scratch, +1, s);
-            swap_scratch_any(f);
-            f->space = MLEGS_PPP;
-        }
-    }
-    void plnfft(Field* f, int is) {
-        if (is == -1) {
-            horfft(f, -1);
-            verfft(f, -1);
-        } else {
-            verfft(f, 1);
-            horfft(f, 1);
-        }
-    }
-    void toff(Field* f, int pad) {
-        if (f->space == MLEGS_PPP) horfft(f, -1);
-        if (f->space == MLEGS_PFP) verfft(f, -1);
-        if (f->space == MLEGS_PFF) rtran(f, -1, pad);
-    }
-    void tofp(Field* f, int pad) {
-        if (f->space == MLEGS_FFF) rtran(f, 1, pad);
-        if (f->space == MLEGS_PFF) verfft(f, 1);
-        if (f->space == MLEGS_PFP) horfft(f, 1);
-    }
-
-    // TOFP of FFF fields up to PFP (RTRAN(+1) then VERFFT(+1), the reference's
-    // order per field) as a two-stream pipeline: the RTRAN(+1) GEMM of field
-    // i + 1 on s runs beside the VERFFT(+1) of field i on s2, through three
-    // rotating PFF buffers.  Each field ends in its own buffer, in PFP, LN 0.
-    cudaEvent_t next_event() {
-        cudaEvent_t e = evs[ev_next];
-        ev_next = (ev_next + 1) % 64;
-        return e;
-    }
-    void tofp_pipe(Field* const* fs, const int* pads, int n, const cudaEvent_t* ready = nullptr) {
-        for (int i = 0; i < n; ++i) require(fs[i], MLEGS_FFF, "RTRAN");
-        cudaEvent_t e0 = next_event();
-        CK(cudaEventRecord(e0, s));
-        CK(cudaStreamWaitEvent(s2, e0, 0));
-        cudaEvent_t done[3] = {nullptr, nullptr, nullptr};  // last VERFFT reading pbuf[j]
-        for (int i = 0; i < n; ++i) {
-            Field* f = fs[i];
-            double2* buf = pbuf[i % 3];
-            if (done[i % 3]) CK(cudaStreamWaitEvent(s, done[i % 3], 0));
-            if (ready && ready[i]) CK(cudaStreamWaitEvent(s, ready[i], 0));  // field made on s2
-            if (split_S)
-                k_split_b2p(g, split_S, split_img, split_eA, f->data, buf, f->ln, pads[i], split_err, s);
-            else
-                k_rtran_b2p(g, f->data, buf, f->ln, pads[i], s);
-            cudaEvent_t eb = next_event();
-            CK(cudaEventRecord(eb, s));
-            CK(cudaStreamWaitEvent(s2, eb, 0));
-            if (!k_verfft4(g, fft, buf, f->data, +1, s2)) k_verfft_b(g, fft, buf, f->data, s2);
-            CK(cudaMemsetAsync(f->ln, 0, sizeof(double), s2));  // RTRAN zeroes LN (off the GEMM stream)
-            cudaEvent_t ev = next_event();
-            CK(cudaEventRecord(ev, s2));
-            done[i % 3] = ev;
-            f->space = MLEGS_PFP;
-        }
-        cudaEvent_t ej = next_event();
-        CK(cudaEventRecord(ej, s2));
-        CK(cudaStreamWaitEvent(s, ej, 0));
-    }
-
-    // ------------------------------------------------------------------ operators
-    void delsqh(const Field* a, Field* b, int pad) {  // mod_legops.f90:76-133
-        require(a, MLEGS_FFF, "DELSQH");
-        k_delsqh(g, a->data, a->ln, b->data, pad, s);
-        b->space = MLEGS_FFF;
-        ln_zero(b);
-    }
-    void idelsqh(const Field* bb, Field* a, int pad) {  // mod_legops.f90:136-241
-        require(bb, MLEGS_FFF, "IDELSQH");
-        // A%LN = B(1,1,1) NORM(1,1) ELL2
-        k_idelsqh(g, bb->data, a->data, pad, s);
-        a->space = MLEGS_FFF;
-        ln_from_coef(a->ln, bb->data, d.ELL2);
-        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
-    }
-    void ln_from_coef(double* ln, const double2* data, double scale);
-    void mulxm(const Field* a, Field* b, int pad) {  // 371-428
-        require(a, MLEGS_FFF, "MULXM");
-        k_band3(g, a->data, b->data, 1, pad, s);
-        b->space = MLEGS_FFF;
-        ln_zero(b);
-    }
-    void xxdx(const Field* a, Field* b, int pad) {  // 680-748
-        require(a, MLEGS_FFF, "XXDX");
-        k_band3(g, a->data, b->data, 0, pad, s);
-        k_logterm_rows(g, b->data, a->ln, 0, 1.0, s);
-        b->space = MLEGS_FFF;
-        ln_zero(b);
-    }
-    void del2(const Field* a, Field* b, int pad) {  // 751-820
-        require(a, MLEGS_FFF, "DEL2");
-        k_del2(g, a->data, b->data, pad, s);
-        k_logterm_rows(g, b->data, a->ln, 1, 1.0, s);
-        b->space = MLEGS_FFF;
-        ln_zero(b);
-    }
-    // IDEL2 (823-1010): has_ln = 0 -> LN absent.
-    // LU factors per (kind, pad, alp), formed on first use outside graph capture
-    struct SolveFactors {
-        int kind, pad;
-        double alp;
-        double *F5, *F7;
-    };
-    std::vector<SolveFactors> sfac;
-    const SolveFactors* factors(int kind, int pad, double alp) {
-        for (const SolveFactors& f : sfac)
-            if (f.kind == kind && f.pad == pad && f.alp == alp) return &f;
-        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-        CK(cudaStreamIsCapturing(s, &cs));
-        if (cs != cudaStreamCaptureStatusNone || sfac.size() >= 8 || pad < 0 || d.NRCHOP + pad > d.NRCHOPDIM)
-            return nullptr;
-        size_t n5, n7;
-        solve_factor_sizes(g, &n5, &n7);
-        SolveFactors f{kind, pad, alp, dalloc<double>(n5), dalloc<double>(n7)};
-        k_solve_factor(g, kind, alp, pad, f.F5, f.F7, s);
-        sfac.push_back(f);
-        return &sfac.back();
-    }
-    void idel2(const Field* bb, Field* a, int has_ln, double ln, int pad) {
-        require(bb, MLEGS_FFF, "IDEL2");
-        if (const SolveFactors* f = factors(1, pad, 0.0)) {
-            k_solve_factored(g, f->F5, f->F7, bb->data, a->data, a->ln, 1, has_ln, ln, pad, 1, s);
-            a->space = MLEGS_FFF;
-            return;
-        }
-        copy0(a, bb, pad);
-        ln_zero(a);
-        k_solve_del2(g, a->data, a->ln, 1, 0.0, has_ln, ln, nullptr, solve_scr, pad, s);
-        chopdo(a, pad);
-        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
-    }
-    void idel2ln(const Field* bb, Field* a, int pad) {  // 1013-1176
-        require(bb, MLEGS_FFF, "IDEL2LN");
-        if (const SolveFactors* f = factors(0, pad, 0.0)) {
-            k_solve_factored(g, f->F5, f->F7, bb->data, a->data, a->ln, 0, 0, 0.0, pad, 1, s);
-            a->space = MLEGS_FFF;
-            return;
-        }
-        copy0(a, bb, pad);
-        ln_zero(a);
-        k_solve_del2(g, a->data, a->ln, 0, 0.0, 0, 0.0, nullptr, solve_scr, pad, s);
-        chopdo(a, pad);
-        k_farfield_fix(g, a->data, d.NRCHOP + pad, s);
-    }
-    void ihelm(const Field* bb, Field* a, double alp, int pad) {  // 1204-1354
-        require(bb, MLEGS_FFF, "IHELM");
-        if (alp == 0.0) throw ApiError(MLEGS_ERR_LEGOPERATOR, "IHELM: ALP CAN'T BE ZERO");
-        copy0(a, bb, pad);
-        k_ln_copy(a->ln, bb->ln, -1.0 / alp, s);      // A%LN = -B%LN/ALP
-        k_logterm_rows(g, a->data, a->ln, 2, 1.0, s);  // rhs -= LN * DEL2(log)
-        if (const SolveFactors* f = factors(2, pad, alp))
-            k_solve_factored(g, f->F5, f->F7, a->data, a->data, nullptr, 2, 0, 0.0, pad, 0, s);
-        else
-            k_solve_del2(g, a->data, nullptr, 2, alp, 0, 0.0, nullptr, solve_scr, pad, s);
-        chopdo(a, pad);
-    }
-    // The fused derivative kernels read row neighbours of their inputs while
-    // writing the outputs, so an output may not share a buffer with an input.
-    static void distinct(std::initializer_list<const Field*> in, std::initializer_list<const Field*> out,
-                         const char* who) {
-        for (const Field* o : out)
-            for (const Field* i : in)
-                if (o->data == i->data)
-                    throw ApiError(MLEGS_ERR_ARG, std::string(who) + ": outputs must be distinct from the inputs");
-    }
-    void grad(const Field* a, Field* rr, Field* rp, Field* gz, int pad, cudaStream_t st = nullptr) {  // 1727-1786
-        require(a, MLEGS_FFF, "GRAD");
-        distinct({a}, {rr, rp, gz}, "GRAD");
-        if (!st) st = s;
-        k_grad_fused(g, a->data, a->ln, rr->data, rp->data, gz->data, pad, st);
-        rr->space = rp->space = gz->space = MLEGS_FFF;
-        for (Field* f : {rr, rp, gz}) CK(cudaMemsetAsync(f->ln, 0, sizeof(double), st));
-    }
-    void pc2vel(const Field* psi_, const Field* chi_, Field* rur, Field* rup, Field* uz, int pad) {  // 1789-1853
-        require(psi_, MLEGS_FFF, "PC2VEL");
-        require(chi_, MLEGS_FFF, "PC2VEL");
-        distinct({psi_, chi_}, {rur, rup, uz}, "PC2VEL");
-        double* zl[3] = {rur->ln, rup->ln, uz->ln};  // set to 0 by the kernel
-        k_pc2vel_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, rur->data, rup->data, uz->data, pad, s, 0, zl);
-        rur->space = rup->space = uz->space = MLEGS_FFF;
-    }
-    void pc2vor(const Field* psi_, const Field* chi_, Field* ror, Field* rop, Field* oz, int pad,
-                cudaStream_t st = nullptr) {  // 1856-1919
-        require(psi_, MLEGS_FFF, "PC2VOR");
-        require(chi_, MLEGS_FFF, "PC2VOR");
-        distinct({psi_, chi_}, {ror, rop, oz}, "PC2VOR");
-        if (!st) st = s;
-        k_pc2vor_fused(g, psi_->data, psi_->ln, chi_->data, chi_->ln, ror->data, rop->data, oz->data, pad, st);
-        ror->space = rop->space = oz->space = MLEGS_FFF;
-        for (Field* f : {ror, rop, oz}) CK(cudaMemsetAsync(f->ln, 0, sizeof(double), st));
-    }
-    // PROJECT (mod_legops.f90:2397-2545).  ln_mode: 0 none, 1 value, 2 PSI%LN by reference.
-    void project(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_, int ln_mode, double ln) {
-        if (!(rur->space == rup->space && rup->space == uz->space))
-            throw ApiError(MLEGS_ERR_TRANSFORM, "PROJECT: RUR, RUP, UZ MUST BE IN THE SAME SPACE.");
-        if (rur->space == MLEGS_PPP) {
-            plnfft(rur, -1);
-            plnfft(rup, -1);
-            plnfft(uz, -1);
-        } else if (rur->space == MLEGS_PFP) {  // PPP already taken through HORFFT(-1)
-            verfft(rur, -1);
-            verfft(rup, -1);
-            verfft(uz, -1);
-        } else if (rur->space == MLEGS_FFF) {
-            rtran(rur, 1, 0);
-            rtran(rup, 1, 0);
-            rtran(uz, 1, 0);
-        } else if (rur->space != MLEGS_PFF) {
-            throw ApiError(MLEGS_ERR_TRANSFORM, "PROJECT: bad input space");
-        }
-        psi_->space = chi_->space = MLEGS_FFF;
-        if (ln_mode == 1) launch_vel2pln(g, rup->data, psi_->ln, 1, ln, v2p_pff, s, chi_->ln);
-        else if (ln_mode == 2) launch_vel2pln(g, rup->data, psi_->ln, 0, 0.0, v2p_pff, s, chi_->ln);
-        else {
-            ln_zero(psi_);
-            ln_zero(chi_);
-        }
-        if (!split_S && dmma_supported(g)) {
-            k_project_dmma(g, V, D, T, rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
-            k_farfield_fix(g, psi_->data, d.NRCHOP, s);
-            return;
-        }
-        const int wr = d.NRCHOPDIM;
-        // PSI = -(i m) EO(V, RUR) - OE(D, RUP)
-        fold(1, V, wr, rur->data, psi_->data, 0, 2, 0, 0);
-        fold(2, D, wr, rup->data, psi_->data, 1, 1, 1, 0);
-        // CHI = (i k) OE(D, RUR) + m k EO(V, RUP) - EO(T, UZ)
-        fold(2, D, wr, rur->data, chi_->data, 1, 3, 0, 0);
-        fold(1, V, wr, rup->data, chi_->data, 0, 4, 1, 0);
-        fold(3, T, wr, uz->data, chi_->data, 0, 1, 1, 0);
-        k_farfield_fix(g, psi_->data, d.NRCHOP, s);
-    }
-
-    // PROJECT(RUR, RUP, UZ, PSI, CHI) with PSI%LN by reference (ln_mode 2) for
-    // FFF inputs whose LN terms are zero: one composite FFF -> FFF product per m
-    // in FP64 contexts (RUP's (0, 0) column is changed in place by VEL2PLN).
-    void project_fff_ln2(Field* rur, Field* rup, Field* uz, Field* psi_, Field* chi_) {
-        if (!compV || rur->space != MLEGS_FFF || rup->space != MLEGS_FFF || uz->space != MLEGS_FFF) {
-            project(rur, rup, uz, psi_, chi_, 2, 0.0);
-            return;
-        }
-        psi_->space = chi_->space = MLEGS_FFF;
-        k_project_fff_dmma(g, compV, compD, compT, rur->data, rup->data, uz->data, psi_->data, chi_->data, psi_->ln,
-                           v2p_fff, s, chi_->ln);
-        k_farfield_fix(g, psi_->data, d.NRCHOP, s);
-    }
-
-    // ------------------------------------------------------------------ physics
-    void force(const Field* PSI, const Field* CHI, const Field* B, Field* PSIN, Field* CHIN, Field* BN);
-    void energy(const Field* PSI, const Field* CHI, const Field* B, double* ke, double* pe, double* dke);
-    void diagnost(const Field* PSI, const Field* CHI, double out[11]);
-    void boussi_pe(const Field* B, double* pe);
-    void enemon(const Field* PSI, const Field* CHI, int pad, double* em, double* ek);
-    void hyp3set(const double nu[3], double** tables);
-    void qvortex(const mlegs_vortex* v, int n, const int32_t* seeds, Field* PSI, Field* CHI);
-    void hyp3adj(const Field* PSI, const Field* CHI, const Field* B);
-    void halfk(const double* all, double sign, double* out, bool accumulate) const;
-    void nonlin(const Field* B, Field* RUR, Field* RUP, Field* UZ, Field* ROR, Field* ROP, Field* OZ,
-                Field* BN, cudaEvent_t vor_ready = nullptr, Field* PSIN = nullptr, Field* CHIN = nullptr);
-    void visc1(Field* A, double nu, double dt);
-    void visc2(Field* A, const Field* AO, double nu, double dt);
-    void visc_be(Field* P, Field* C, Field* B, double dt);
-    void visc_cn(Field* P, Field* C, Field* B, const Field* PO, const Field* CO, const Field* BO);
-    void hyperv3(Field* P, Field* C, Field* B, double tf);
-    void etd_hyperv(Field* R, Field* Pp, Field* Z, Field* B, double tf);
-    void sponge(Field* UZ, Field* B, double dt);
-    void rich_fe_be();
-    void step_ab_cn();
-    void etdfe_be(Field* P, Field* C, Field* B, const double* E, const double* NL, double dt, bool store);
-    void rich_etdfe_be();
-    void step_etdab_cn();
-    void step_once() { p.adams ? step_ab_cn() : step_etdab_cn(); }
-
-    // snapshot of the temporaries' buffers so every step reuses the same pointers
-    std::vector<double2*> snap;
-    double2* snap_scratch = nullptr;
-    void mark() {
-        snap.clear();
-        for (Field* f : temps) snap.push_back(f->data);
-        snap_scratch = scratch;
-    }
-    void restore() {
-        for (size_t i = 0; i < temps.size(); ++i) temps[i]->data = snap[i];
-        scratch = snap_scratch;
-    }
-};
+thread_local std::vector<void*>* mlegs_host::g_allocs = nullptr;
 
 // ====================================================================== set-up
 namespace {
@@ -547,6 +34,70 @@ std::vector<double> leg_log_norm(int ndim, int ntchopdim) {
 }
 
 }  // namespace
+
+// Band x band product in BANBANMUL's order (mod_bandmat.f90:1288-1345): C(r, k)
+// accumulates A(r, i) B(r + i - ac, k - i) over i ascending; rows and columns
+// outside [0, nn) are skipped.  Widths aw, bw; centres ac, bc (0-based).
+static std::vector<double> banbanmul(const std::vector<double>& A, int aw, int ac, const std::vector<double>& B,
+                                     int bw, int bc, int nn) {
+    const int cw = aw + bw - 1;
+    std::vector<double> C((size_t)nn * cw, 0.0);
+    for (int i = 0; i < aw; ++i) {
+        const int as = i - ac;
+        for (int j = 0; j < bw; ++j) {
+            const int k = i + j, bs = j - bc;
+            for (int r = 0; r < nn; ++r) {
+                const int rb = r + as;  // row of B = column of A
+                if (rb < 0 || rb >= nn || rb + bs < 0 || rb + bs >= nn) continue;
+                C[(size_t)r * cw + k] += A[(size_t)r * aw + i] * B[(size_t)rb * bw + j];
+            }
+        }
+    }
+    return C;
+}
+
+const double* mlegs_ctx::helmp_tables(int P) {
+    for (const auto& t : helmp_tab)
+        if (t.first == P) return t.second;
+    no_capture("IHELMP");
+    const int HP = P / 2, rows = helmp_rows();
+    // DEL2H rows i < rows + P - 2 (BAND_LOGLEG_RAT_DEL2H with S = 0, mod_lin_legendre.f90:1986-2092):
+    // the powers' rows below `rows` are then those of the untruncated operator
+    const int nd = std::min(rows + P - 2, d.NLN - 2);
+    const size_t per_m = (size_t)rows * HP * (2 * HP + 1);
+    std::vector<double> h((size_t)d.NTCHOPDIM * per_m, 0.0);
+    for (int m = 0; m < d.NTCHOPDIM; ++m) {
+        const double* ln = &h_lognorm[(size_t)m * d.NLN];
+        const double am = m, e2 = d.ELL2;
+        auto ex = [&](int a, int b2) { return std::exp(ln[a] - ln[b2]); };
+        std::vector<double> D((size_t)nd * 5, 0.0);
+        for (int nn = 0; nn < nd; ++nn) {
+            const double N = am + nn;
+            double* db = &D[(size_t)nn * 5];
+            if (nn >= 2)
+                db[0] = -(N - am - 1.0) * (N - am) * (N - 2) * (N - 1) / (2 * N - 3.) / (2 * N - 1.0) / e2 *
+                        ex(nn - 2, nn);
+            if (nn >= 1) db[1] = 2.0 * N * (N - am) * (N - 1) / (2 * N - 1.0) / e2 * ex(nn - 1, nn);
+            db[2] = (-2.0 * N * (N + 1.0) * (3.0 * N * N + 3 * N - am * am - 2)) / (2 * N - 1.0) / (2 * N + 3.0) / e2;
+            db[3] = 2.0 * (N + 1) * (N + am + 1.0) * (N + 2) / (2 * N + 3.0) / e2 * ex(nn + 1, nn);
+            db[4] = -(N + am + 1.0) * (N + am + 2.0) * (N + 3) * (N + 2) / (2 * N + 3.0) / (2 * N + 5.0) / e2 *
+                    ex(nn + 2, nn);
+        }
+        std::vector<double> Dq = D;
+        for (int q = 1; q <= HP; ++q) {
+            const int w = 4 * q + 1;
+            if (q > 1) Dq = banbanmul(Dq, 4 * q - 3, 2 * q - 2, D, 5, 2, nd);  // D^q = D^(q-1) D
+            double* out = &h[(size_t)m * per_m + (size_t)rows * q * (2 * q - 1)];
+            for (int r = 0; r < rows && r < nd; ++r)
+                for (int e = 0; e < w; ++e) out[(size_t)r * w + e] = Dq[(size_t)r * w + e];
+        }
+    }
+    double* dp = dalloc<double>(h.size());
+    CK(cudaMemcpyAsync(dp, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    helmp_tab.emplace_back(P, dp);
+    return dp;
+}
 
 void mlegs_ctx::init(const mlegs_params& prm) {
     p = prm;
@@ -751,6 +302,15 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     fft.tw_t = twid(d.NTH, 2.0);
     fft.tw_h = twid(d.NTH, 1.0);
 
+    // --- VISC%SW = 2: HYPERV / IHELMP (AB2-CN only; SOLVER_T%INITIALIZE aborts for ETD,
+    //     mod_march.f90:189-201)
+    if (p.visc_sw == 2) {
+        if (!p.adams)
+            throw ApiError(MLEGS_ERR_SOLVER, "SOLVER: ETD scheme MUST use velocity-based hyperviscosity.");
+        if (p.visc_p < 4 || p.visc_p > 14 || p.visc_p % 2)
+            throw ApiError(MLEGS_ERR_ARG, "HYPERV: VISC%P must be even, 4..14, for VISC%SW = 2");
+        if (p.nup == 0.0) throw ApiError(MLEGS_ERR_SOLVER, "HYPERV: NUP CAN'T BE ZERO");
+    }
     // --- hyperviscosity (HYP3SET, mod_march.f90:3320-3408)
     if (p.visc_sw == 3) {
         auto mask = [](const std::vector<double>& kv, size_t size, double ratio, double steep) {
@@ -874,6 +434,10 @@ void mlegs_ctx::init(const mlegs_params& prm) {
         pool.push_back(f);
     }
     for (int q = 0; q < 7; ++q) hist[q] = new_field(MLEGS_FFF, true);
+    if (p.visc_sw == 2) {  // IHELMP tables and scratch before any step graph is captured
+        helmp_tables(p.visc_p);
+        helmp_scratch(p.visc_p);
+    }
     CK(cudaStreamSynchronize(s));
 }
 
@@ -1428,7 +992,13 @@ void mlegs_ctx::visc_cn(Field* P, Field* C, Field* B, const Field* PO, const Fie
     if (p.kappa != 0.0) visc2(B, BO, p.kappa, p.dt);
 }
 void mlegs_ctx::hyperv3(Field* P, Field* C, Field* B, double tf) {  // CALC_BOUSSI_HYPERV 1305-1349
-    if (p.visc_sw == 2) throw ApiError(MLEGS_ERR_SOLVER, "VISC%SW = 2 is not on the configured path");
+    if (p.visc_sw == 2) {  // HYPERV per field, B only when KAPPAP /= 0 (1327-1335)
+        const double dt = tf * p.dt;
+        hyperv2(P, p.nu, p.nup, p.visc_p, dt);
+        hyperv2(C, p.nu, p.nup, p.visc_p, dt);
+        if (p.kappap != 0.0) hyperv2(B, p.kappa, p.kappap, p.visc_p, dt);
+        return;
+    }
     if (p.visc_sw != 3) return;
     k_hyperv(g, P->data, hv[0], hv[1], hv[2], tf, 0, s);
     k_hyperv(g, C->data, hv[0], hv[1], hv[2], tf, 0, s);
@@ -1698,47 +1268,6 @@ void mlegs_ctx::step_etdab_cn() {
 }
 
 // ====================================================================== C ABI
-namespace {
-template <class F>
-int guard(mlegs_ctx* ctx, F&& fn) {
-    if (!ctx) return MLEGS_ERR_ARG;
-    int64_t* prev = g_launch_counter;
-    std::vector<void*>* prev_allocs = g_allocs;
-    g_launch_counter = &ctx->launches;
-    g_allocs = &ctx->allocs;
-    int rc = MLEGS_OK;
-    try {
-        cudaSetDevice(ctx->dev);
-        fn();
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e));
-    } catch (const ApiError& e) {
-        ctx->set_error(e.what());
-        rc = e.code;
-    } catch (const CudaError& e) {
-        ctx->set_error(e.what());
-        rc = MLEGS_ERR_CUDA;
-    } catch (const std::exception& e) {
-        ctx->set_error(e.what());
-        rc = MLEGS_ERR_STATE;
-    }
-    g_launch_counter = prev;
-    g_allocs = prev_allocs;
-    return rc;
-}
-Field* F(mlegs_field* f) {
-    if (!f) throw ApiError(MLEGS_ERR_ARG, "null field");
-    return &f->f;
-}
-const Field* F(const mlegs_field* f) {
-    if (!f) throw ApiError(MLEGS_ERR_ARG, "null field");
-    return &f->f;
-}
-void check_pad(const mlegs_ctx* c, int pad) {
-    if (c->d.NRCHOP + pad > c->d.NRCHOPDIM || c->d.NRCHOP + pad < 0)
-        throw ApiError(MLEGS_ERR_SCALAR3, "CHOPSET: NRCHOP TOO LARGE");
-}
-}  // namespace
 
 extern "C" {
 
@@ -1784,12 +1313,21 @@ int mlegs_destroy(mlegs_ctx* ctx) {
 
 const char* mlegs_last_error(const mlegs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int mlegs_set_wait_limit(mlegs_ctx* ctx, int64_t cycles) {
+    if (!ctx || cycles < 0) return MLEGS_ERR_ARG;
+    ctx->split_wait = (uint64_t)cycles;
+    return MLEGS_OK;
+}
+
 int mlegs_sync(mlegs_ctx* ctx) {
     return guard(ctx, [&] {
         CK(cudaStreamSynchronize(ctx->s));
         int e = 0;
         CK(cudaMemcpy(&e, ctx->split_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (e) throw CudaError("tensor-core GEMM: a bounded wait timed out (results invalid)");
+        if (e) {  // reported once; the context stays usable
+            CK(cudaMemset(ctx->split_err, 0, sizeof(int)));
+            throw ApiError(MLEGS_ERR_TIMEOUT, "tensor-core GEMM: a bounded wait timed out (results invalid)");
+        }
     });
 }
 
@@ -2121,6 +1659,21 @@ int mlegs_idel2ln_static(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, i
         k_farfield_fix(ctx->g, fa->data, ctx->d.NRCHOP + pad, ctx->s);
     });
 }
+int mlegs_ihelmp(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, int p, double alp, double nu, int pad) {
+    return guard(ctx, [&] {
+        check_pad(ctx, pad);
+        ctx->ihelmp(F(b), F(a), p, alp, nu, pad);
+    });
+}
+int mlegs_hyperv(mlegs_ctx* ctx, mlegs_field* a, double nu, double nup, int p, double dt) {
+    return guard(ctx, [&] {
+        if (p < 4 || p > 14 || p % 2) throw ApiError(MLEGS_ERR_ARG, "HYPERV: P must be even, 4..14");
+        if (dt == 0.0) throw ApiError(MLEGS_ERR_ARG, "HYPERV: DT must not be zero");
+        ctx->mark();
+        ctx->hyperv2(F(a), nu, nup, p, dt);
+        ctx->restore();
+    });
+}
 int mlegs_ihelm(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* a, double alp, int pad) {
     return guard(ctx, [&] { check_pad(ctx, pad); ctx->ihelm(F(b), F(a), alp, pad); });
 }
@@ -2146,7 +1699,21 @@ int mlegs_project(mlegs_ctx* ctx, mlegs_field* rur, mlegs_field* rup, mlegs_fiel
         ctx->copy0(ta, a, 0);
         ctx->copy0(tb, b2, 0);
         ctx->copy0(tc, c, 0);
-        ctx->project(ta, tb, tc, F(psi), F(chi), ln_mode, ln);
+        // FFF velocity with PSI%LN by reference and zero input log terms: the
+        // steppers' form, one composite FFF -> FFF product per m
+        bool composite = false;
+        if (ln_mode == 2 && a->space == MLEGS_FFF && b2->space == MLEGS_FFF && c->space == MLEGS_FFF) {
+            double lns[3];
+            CK(cudaMemcpyAsync(&lns[0], a->ln, sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaMemcpyAsync(&lns[1], b2->ln, sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaMemcpyAsync(&lns[2], c->ln, sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            composite = lns[0] == 0.0 && lns[1] == 0.0 && lns[2] == 0.0;
+        }
+        if (composite)
+            ctx->project_fff_ln2(ta, tb, tc, F(psi), F(chi));
+        else
+            ctx->project(ta, tb, tc, F(psi), F(chi), ln_mode, ln);
         ctx->copy0(a, ta, 0);
         ctx->copy0(b2, tb, 0);
         ctx->copy0(c, tc, 0);
@@ -2161,6 +1728,33 @@ int mlegs_boussi_force(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field
         ctx->mark();
         ctx->force(F(psi), F(chi), F(b), F(psin), F(chin), F(bn));
         ctx->restore();
+    });
+}
+int mlegs_boussi_nonlin(mlegs_ctx* ctx, const mlegs_field* b, mlegs_field* rur, mlegs_field* rup, mlegs_field* uz,
+                        mlegs_field* bn, mlegs_field* ror, mlegs_field* rop, mlegs_field* oz) {
+    return guard(ctx, [&] {
+        const Field* B = F(b);
+        Field *a[7] = {F(rur), F(rup), F(uz), F(ror), F(rop), F(oz), F(bn)};
+        if (B->space != MLEGS_FFF)
+            throw ApiError(MLEGS_ERR_LEGOPERATOR, "CALC_BOUSSI_NONLIN: B SHOULD BE IN FFF SPACE!");
+        for (int i = 0; i < 6; ++i) ctx->require(a[i], MLEGS_FFF, "CALC_BOUSSI_NONLIN");
+        for (int i = 0; i < 7; ++i) {
+            if (a[i]->data == B->data) throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_NONLIN: fields must be distinct");
+            for (int j = 0; j < i; ++j)
+                if (a[i]->data == a[j]->data)
+                    throw ApiError(MLEGS_ERR_ARG, "CALC_BOUSSI_NONLIN: fields must be distinct");
+        }
+        ctx->mark();
+        ctx->nonlin(B, a[0], a[1], a[2], a[3], a[4], a[5], a[6]);
+        ctx->restore();
+    });
+}
+int mlegs_legendre_table(mlegs_ctx* ctx, double* pf) {
+    return guard(ctx, [&] {
+        if (!pf) throw ApiError(MLEGS_ERR_ARG, "null table");
+        const size_t n = (size_t)ctx->d.NTCHOPDIM * (ctx->d.NRCHOPDIM + 1) * ctx->d.NRH;
+        CK(cudaStreamSynchronize(ctx->s));
+        CK(cudaMemcpy(pf, ctx->pf, n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }
 
@@ -2368,7 +1962,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 15) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 16) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -2429,17 +2023,24 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     double2* out[4] = {a->data, b->data, c->data, e->data};
                     k_theta_fused(g, ctx->fft, in, out, 0.0, 0.0, 0, s);
                 } break;
+                case 16:  // TOFP then TOFF of one FFF field (RTRAN, VERFFT, HORFFT and back)
+                    ctx->mark();
+                    a->space = MLEGS_FFF;
+                    ctx->tofp(a, 0);
+                    ctx->toff(a, 0);
+                    ctx->restore();
+                    break;
                 case 9: k_horfft_warp(g, ctx->fft, a->data, b->data, +1, s); break;
                 case 11:
                     if (!ctx->split_S) throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
                     k_split_b2p(g, ctx->split_S, ctx->split_img, ctx->split_eA, a->data, b->data, nullptr, 0,
-                                ctx->split_err, s);
+                                ctx->split_err, ctx->split_wait, s);
                     break;
                 case 10: k_horfft_warp(g, ctx->fft, a->data, b->data, -1, s); break;
                 case 12:
                     if (!ctx->split_S) throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
                     k_split_fold(g, ctx->split_S, ctx->fimg[0], ctx->feA[0], d.NRCHOPDIM + 1, a->data, b->data, 0,
-                                 0, 0, 0, 1, ctx->split_err, s);
+                                 0, 0, 0, 1, ctx->split_err, ctx->split_wait, s);
                     break;
                 case 14:  // PROJECT of FFF inputs f9[0..2] -> b, c through the composites
                     if (!ctx->compV) throw ApiError(MLEGS_ERR_STATE, "needs an FP64 context on the tensor path");
@@ -2473,6 +2074,8 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 15: bytes = B16 * 13.0 * (double)d.pfp(); break;  // 9 read, 4 written
             case 13: bytes = B16 * (3.0 * (double)d.pff() + 2.0 * (double)d.fff()); break;
             case 14: bytes = B16 * 5.0 * (double)d.fff(); break;
+            // each stage reads its input and writes its output, both ways
+            case 16: bytes = 2.0 * B16 * ((double)d.fff() + 2.0 * (double)d.pff() + 2.0 * (double)d.pfp() + (double)d.ppp()); break;
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
         }
         for (int q = 0; q < 3; ++q) launch();  // warm-up

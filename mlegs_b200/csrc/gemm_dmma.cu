@@ -52,13 +52,12 @@ constexpr int NST_B2P = 2;   // ring stages of b2p_dmma_kernel
 constexpr int NST_FOLD = 2;  // ring stages of legfold_dmma_kernel
 constexpr int NST_PFFF = 2;  // ring stages of projfff_dmma_kernel
 
+// One (m, 32-column) tile of RTRAN(+1): the body of b2p_dmma_kernel, also run
+// per work item by the grouped ensemble kernel (ensemble.cu).
 template <int NW, int MTW>
-__global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const double* __restrict__ A,
-                                                           double* __restrict__ out, const double* ln, int pad,
-                                                           int SA) {
-    extern __shared__ double smd[];
+__device__ __forceinline__ void b2p_tile(const DevGrid& g, const double* __restrict__ A, double* __restrict__ out,
+                                         const double* ln, int pad, int SA, int m, int c0, double* smd) {
     const size_t stg = (size_t)KCB * (SA + SBS);
-    const int m = blockIdx.y, c0 = blockIdx.x * CT;
     const int ncol = 2 * g.NXCHOPDIM;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
     const int RT = (g.NRH + 7) / 8;
@@ -172,6 +171,14 @@ __global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const doub
     }
 }
 
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32) b2p_dmma_kernel(DevGrid g, const double* __restrict__ A,
+                                                           double* __restrict__ out, const double* ln, int pad,
+                                                           int SA) {
+    extern __shared__ double smd[];
+    b2p_tile<NW, MTW>(g, A, out, ln, pad, SA, blockIdx.y, blockIdx.x * CT, smd);
+}
+
 // Fold GEMMs: RTRAN(-1) and PROJECT's five EOMUL/OEMUL products.  One CTA
 // computes the output rows n = 2r + pr of one parity, one m and 32 columns,
 // over a K extent of nseg segments of NRH rows each:
@@ -212,10 +219,11 @@ __device__ __forceinline__ T pick5(const T (&a)[5], int i) {
     return v;
 }
 
+// One (m, output parity, 32-column) tile of the fold GEMMs: the body of
+// legfold_dmma_kernel, also run per work item by the grouped ensemble kernel.
 template <int NW, int MTW>
-__global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, FoldArgs fa, int RTmax) {
-    extern __shared__ double smd[];
-    const int m = blockIdx.z, pr = blockIdx.y, c0 = blockIdx.x * CT;
+__device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& fa, int RTmax, int m, int pr, int c0,
+                                             double* smd) {
     const int ncol = 2 * g.NXCHOPDIM;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, q = lane & 3;
     int nn = g.NRCHOP + fa.pad - m;
@@ -339,6 +347,12 @@ __global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, Fol
         if (gc == fa.split * nch - 1 || gc == total - 1) epilogue(acc, gc < fa.split * nch ? fa.out0 : fa.out1);
         __syncthreads();  // the stage is refilled by the next iteration's prefetch
     }
+}
+
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32, 4) legfold_dmma_kernel(DevGrid g, FoldArgs fa, int RTmax) {
+    extern __shared__ double smd[];
+    legfold_tile<NW, MTW>(g, fa, RTmax, blockIdx.z, blockIdx.y, blockIdx.x * CT, smd);
 }
 
 // PROJECT of velocity fields given as FFF coefficients, as one FFF -> FFF

@@ -229,9 +229,10 @@ void k_mk_combine(const DevGrid& g, int op, const double2* x, const double2* y, 
     count_launch();
 }
 
-// a(n=0, m=0, k) -= sum_{n < nr_sum} AT1(n) a(n, 0, k) / AT1(0)   (CALCAT1 fix)
+// a(n=0, m=0, k) -= sum_{n < nr_sum} AT1(n) a(n, 0, k) / AT1(0)   (CALCAT1 fix);
+// by_pf: divided by TFM%PF(1,1,1) instead, as IHELMP writes it (mod_legops.f90:1586).
 // One warp per k: lanes stride over n, shuffle reduction.
-__global__ void farfield_kernel(DevGrid g, double2* a, int nr_sum) {
+__global__ void farfield_kernel(DevGrid g, double2* a, int nr_sum, int by_pf) {
     int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (k >= g.NXCHOPDIM) return;
@@ -246,12 +247,13 @@ __global__ void farfield_kernel(DevGrid g, double2* a, int nr_sum) {
         sy += __shfl_xor_sync(0xffffffffu, sy, o);
     }
     if (lane == 0) {
-        a[k].x -= sx / g.at1[0];
-        a[k].y -= sy / g.at1[0];
+        const double den = by_pf ? g.pf[0] : g.at1[0];
+        a[k].x -= sx / den;
+        a[k].y -= sy / den;
     }
 }
-void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s) {
-    farfield_kernel<<<nblk(g.NXCHOPDIM, 8), 256, 0, s>>>(g, a, nr_sum);
+void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s, int by_pf) {
+    farfield_kernel<<<nblk(g.NXCHOPDIM, 8), 256, 0, s>>>(g, a, nr_sum, by_pf);
     count_launch();
 }
 

@@ -93,10 +93,13 @@ size_t split_image_bytes(const DevGrid& g, int S, int mode, int wt_rows);
 void k_split_prepare(const DevGrid& g, int S, int mode, const double* W, int wt_rows, uint8_t* img, int* eA,
                      cudaStream_t s);
 void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, const double2* a, double2* b,
-                 const double* ln, int pad, int* err, cudaStream_t s);
-// Same contract as k_fold_gemm (mode bit 0 = EO/OE, use_w separate).
+                 const double* ln, int pad, int* err, uint64_t wait_cycles, cudaStream_t s);
+// Same contract as k_fold_gemm (mode bit 0 = EO/OE, use_w separate).  wait_cycles:
+// limit of the kernel's pipeline waits in SM cycles (0: the default, about a second);
+// a wait that runs out sets *err and the kernel returns early.
 void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
-                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s);
+                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err,
+                  uint64_t wait_cycles, cudaStream_t s);
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
 // FP64 tensor-path (mma.sync m8n8k4.f64) forms used by k_rtran_b2p / k_fold_gemm when supported.
 bool dmma_supported(const DevGrid& g);
@@ -159,7 +162,12 @@ void k_pc2vel_fused(const DevGrid& g, const double2* psi, const double* psi_ln, 
                     double* const* zero_ln = nullptr);
 void k_pc2vor_fused(const DevGrid& g, const double2* psi, const double* psi_ln, const double2* chi, const double* chi_ln,
                     double2* ror, double2* rop, double2* oz, int pad, cudaStream_t s);
-void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s);
+void k_farfield_fix(const DevGrid& g, double2* a, int nr_sum, cudaStream_t s, int by_pf = 0);
+// IHELMP (solve.cu): dq = DEL2H power tables [m][q][rows][4q+1], scratch of
+// ihelmp_scratch_doubles(g, P) doubles; a is solved in place, ln = A%LN.
+size_t ihelmp_scratch_doubles(const DevGrid& g, int P);
+void k_ihelmp(const DevGrid& g, int P, const double* dq, int rows, double2* a, const double* ln, double alp,
+              double nu, double* scratch, int pad, cudaStream_t s);
 // VEL2PLN through its coefficient vectors (k_vel2pln_coef, once per context):
 // on the PFF line of RUP (Lpff, NR entries), or on RUP's FFF (0, 0) column
 // (Lfff, NRCHOP entries; mode 0, applied to that column).

@@ -228,8 +228,11 @@ __global__ void solve_kernel(DevGrid g, double2* A, double* ln_out, int kind, do
 //   F7 [row][7][k]       f3, f2, f1, U(r, r .. r+3) for the 7-band m = 0 systems
 //                        of kinds 1 and 2.
 // The multipliers and pivots are the ones solve_kernel forms, and the
-// substitutions apply them in the same order, so both paths give the same
-// bits.
+// substitutions apply them in the same order.  The two kernels are compiled
+// separately (solve_kernel's elimination is unrolled in register windows), so
+// the compiler contracts different products into FMAs: the results agree to a
+// few units in the last place (about 2e-16 relative to the field, 1e-15 at
+// most, measured on B200), not bit for bit.
 __global__ void factor_kernel(DevGrid g, int kind, double alp, int pad, double* F5, double* F7) {
     const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -489,6 +492,145 @@ void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double
                   const double* b_ln, double* scratch, int pad, cudaStream_t s) {
     int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
     solve_kernel<<<(nsys + 63) / 64, 64, 0, s>>>(g, a, ln_out, kind, alp, has_ln, ln_in, b_ln, scratch, pad);
+    count_launch();
+}
+
+// ---------------------------------------------------------------------------
+// IHELMP (mod_legops.f90:1409-1592), the implicit hyperviscosity solve of
+// HYPERV (VISC%SW = 2, mod_march.f90:1639-1686): per (m, k) the system
+//   H = (DEL2H - k^2)^(P/2) + NU (DEL2H - k^2) - ALP
+// of half-bandwidth P on the leading NN = NRCHOP + pad - m rows.  H's rows are
+// formed from the powers D^q of the DEL2H band (table dq, built on the host
+// with BANBANMUL's summation order), combined binomially as the reference
+// writes them out for each P (D^(P/2) - C(P/2,1) k^2 D^(P/2-1) + ... ), then
+// eliminated without pivoting, one thread per (m, k), the U rows in scratch
+// [row][P+1][system], the right-hand side in place.  The (m, k) = (0, 0)
+// thread first moves the log term's contribution to the right-hand side:
+// rows -= AL + NU AL2, AL2 the DEL2 image of LN (-log(1-x)) and AL = D^(P/2-1) AL2.
+// dq layout: [m][q = 1..HP][row < rows][4q + 1], q's block at rows * q(2q - 1).
+template <int HP>
+__global__ void ihelmp_kernel(DevGrid g, const double* dq, int rows, double2* A, const double* ln, double alp,
+                              double nu, double* scratch, int pad) {
+    constexpr int P = 2 * HP, W = 2 * P + 1;
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nsys) return;
+    const int k = t % g.NXCHOPDIM;
+    const int m = t / g.NXCHOPDIM;
+    int nn = g.NRCHOP + pad - m;
+    if (nn > rows) nn = rows;
+    if (nn <= 0) return;
+    const double K2 = g.ak[k] * g.ak[k];
+    const size_t mstride = (size_t)rows * HP * (2 * HP + 1);  // sum_q (4q + 1) rows
+    const double* dm = dq + (size_t)m * mstride;
+    auto dq_row = [&](int q, int r) { return dm + (size_t)rows * q * (2 * q - 1) + (size_t)r * (4 * q + 1); };
+    double2* col = A + (size_t)m * g.NRCHOPDIM * g.NXCHOPDIM + k;
+    const size_t st = g.NXCHOPDIM;
+    if (m == 0 && k == 0) {
+        // log term (1444-1466): A%LN was set to -B%LN/ALP by the caller
+        const int nr = g.NRCHOP + pad;
+        const double L = *ln;
+        double al2[P + 3], al[P + 3], y[P + 3];
+        for (int i = 0; i < P + 3; ++i) al2[i] = 0.0;
+        al2[0] = L * (4.0 / 3 / g.ELL2) / g.norm0[0];
+        al2[1] = L * (-2 / g.norm0[1] / g.ELL2);
+        al2[2] = L * (+2.0 / 3 / g.norm0[2] / g.ELL2);
+        for (int i = 0; i < P + 3; ++i) al[i] = al2[i];
+        const double* d2 = g.del2h;  // m = 0 rows, [row][5]
+        for (int rep = 1; rep < HP; ++rep) {  // BANMUL(DEL2H, 3, AL), band index ascending
+            for (int r = 0; r < P + 3; ++r) {
+                double v = 0.0;
+                for (int e = 0; e < 5; ++e) {
+                    const int c = r + e - 2;
+                    if (r < nr && c >= 0 && c < nr && c < P + 3) v += d2[(size_t)r * 5 + e] * al[c];
+                }
+                y[r] = v;
+            }
+            for (int r = 0; r < P + 3; ++r) al[r] = y[r];
+        }
+        for (int r = 0; r < P + 3 && r < nr; ++r) {
+            double2 v = col[(size_t)r * st];
+            v.x -= al[r] + nu * al2[r];
+            col[(size_t)r * st] = v;
+        }
+    }
+    // forward elimination, left-looking per row (the pivot rows come from scratch)
+    for (int r = 0; r < nn; ++r) {
+        double w[W];
+        const double* top = dq_row(HP, r);
+#pragma unroll
+        for (int e = 0; e < W; ++e) w[e] = top[e];
+        double c = 1.0;
+#pragma unroll
+        for (int j = 1; j <= HP; ++j) {
+            c *= -K2;
+            // binomial coefficient C(HP, j)
+            double bin = 1.0;
+            for (int q = 1; q <= j; ++q) bin = bin * (HP - q + 1) / q;
+            const int q = HP - j;
+            if (q == 0) {
+                w[P] += c;
+            } else {
+                const double* dr = dq_row(q, r);
+                const double f = bin * c;
+                for (int e = 0; e <= 4 * q; ++e) w[P - 2 * q + e] += f * dr[e];
+            }
+        }
+        {
+            const double* d1 = dq_row(1, r);
+            for (int e = 0; e < 5; ++e) w[P - 2 + e] += nu * (e == 2 ? d1[e] - K2 : d1[e]);
+        }
+        w[P] -= alp;
+        double2 rhs = col[(size_t)r * st];
+        for (int d = P; d >= 1; --d) {
+            if (r - d < 0) continue;
+            const double* u = scratch + (size_t)(r - d) * (P + 1) * nsys + t;
+            const double f = w[P - d] / u[0];
+            w[P - d] = 0.0;
+            for (int j = 1; j <= P; ++j) {
+                const int qq = P - d + j;
+                if (qq < W) w[qq] -= f * u[(size_t)j * nsys];
+            }
+            const double2 pr = col[(size_t)(r - d) * st];
+            rhs.x -= f * pr.x;
+            rhs.y -= f * pr.y;
+        }
+        double* ur = scratch + (size_t)r * (P + 1) * nsys + t;
+        for (int j = 0; j <= P; ++j) ur[(size_t)j * nsys] = w[P + j];
+        col[(size_t)r * st] = rhs;
+    }
+    // back substitution
+    for (int r = nn - 1; r >= 0; --r) {
+        const double* ur = scratch + (size_t)r * (P + 1) * nsys + t;
+        double2 v = col[(size_t)r * st];
+        for (int j = 1; j <= P && r + j < nn; ++j) {
+            const double u = ur[(size_t)j * nsys];
+            const double2 x = col[(size_t)(r + j) * st];
+            v.x -= u * x.x;
+            v.y -= u * x.y;
+        }
+        v.x /= ur[0];
+        v.y /= ur[0];
+        col[(size_t)r * st] = v;
+    }
+}
+
+size_t ihelmp_scratch_doubles(const DevGrid& g, int P) {
+    return (size_t)g.NRCHOPDIM * (P + 1) * g.NTCHOPDIM * g.NXCHOPDIM;
+}
+
+void k_ihelmp(const DevGrid& g, int P, const double* dq, int rows, double2* a, const double* ln, double alp,
+              double nu, double* scratch, int pad, cudaStream_t s) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int bs = 128, nb = (nsys + bs - 1) / bs;
+    switch (P) {
+        case 4: ihelmp_kernel<2><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+        case 6: ihelmp_kernel<3><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+        case 8: ihelmp_kernel<4><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+        case 10: ihelmp_kernel<5><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+        case 12: ihelmp_kernel<6><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+        default: ihelmp_kernel<7><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
+    }
     count_launch();
 }
 

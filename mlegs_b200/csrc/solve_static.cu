@@ -7,14 +7,19 @@
 // cudaMalloc's implicit device-wide synchronisation.  The banded solve keeps
 // its U rows in global scratch (NRCHOPDIM * 4 * NTCHOPDIM * NXCHOPDIM
 // doubles); here that scratch is a file-scope __device__ array, so the entry
-// point allocates nothing.  The array costs kStaticSolveBytes on every GPU
-// that loads this library, held until the process exits.
+// point allocates nothing.  The array costs kStaticSolveBytes on a device
+// from the first call there (CUDA's lazy module loading, the default, loads
+// this file's module at the symbol lookup; with eager loading it is held from
+// library load) until the process exits.
 //
 // Set-up: the first call on a device, with that device current, asks the
 // runtime for the array's device address (cudaGetSymbolAddress) and caches it
 // per device; that first call should therefore come before any stream
-// capture.  `g_static_solve_scr` below is a host-side stand-in for the
-// symbol; only the cached address is ever handed to a kernel.
+// capture.  The cache assumes the device's primary context lives until the
+// process exits: after a cudaDeviceReset the module reloads elsewhere and the
+// cached address would be stale, so hosts that reset a device must not call
+// the entry point again.  `g_static_solve_scr` below is a host-side stand-in
+// for the symbol; only the cached address is ever handed to a kernel.
 //
 // Sharing: every call on a device uses the same array, which keeps the last
 // call's contents.  No entry has to start at zero: each (m, k) system writes

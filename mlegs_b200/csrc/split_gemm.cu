@@ -221,13 +221,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
 }
 
-// Bounded wait that gives up at once when another role has aborted.
-__device__ bool wait_ab(uint64_t* bar, uint32_t parity, volatile int* abort_f) {
+// Bounded wait of the pipeline roles (limit in SM cycles) that gives up at
+// once when another role has aborted.  The drain waits after an abort use
+// mbar_wait with the full WAIT_NS, so a short role limit (set by the host to
+// exercise the error path) still lets every copy and MMA in flight land.
+__device__ bool wait_ab(uint64_t* bar, uint32_t parity, volatile int* abort_f, uint64_t limit) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = gtimer();
     while (!mbar_try(bar, parity)) {
         if (*abort_f) return false;
-        if (gtimer() - t0 > WAIT_NS) {
+        if (gtimer() - t0 > limit) {
             *abort_f = 1;
             return false;
         }
@@ -334,6 +337,7 @@ struct SplitArgs {
     double* out;
     const double* ln;  // MODE 0: A%LN of the input (may be null)
     int* err;
+    unsigned long long wlim;  // role wait limit in SM cycles
     int pad, RG, NCH, trows;
     int mode, scale, accumulate, use_w;  // MODE 1
 };
@@ -342,7 +346,10 @@ struct SplitArgs {
 // stage the item's FP64 field columns in shared memory (one bulk copy per
 // row, double-buffered one item ahead), take the column maxima there, and
 // split 16-row chunks into the ring.
-template <int S, int MODE, int NS>
+// STREAM: the weight chunks come with each ring stage by one bulk copy (MODE 0
+// always; MODE 1 when one (m, parity)'s chunks do not fit in shared memory
+// beside the staged field tile, e.g. NR = 256) instead of staying resident.
+template <int S, int MODE, int NS, bool STREAM>
 __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArgs P) {
     constexpr int NL = S;  // one accumulator per level qa + qb
     constexpr uint32_t TCOLS = 512;
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
     const uint32_t TB = (uint32_t)P.trows * TROWB;  // one staged field tile
     uint8_t* tile_s = sm;                           // [2][trows][32] doubles
     uint8_t* stA = sm + 2 * TB;
-    const uint32_t A_bytes = (MODE == 0) ? NS * SA : (uint32_t)P.NCH * CB + (uint32_t)(16 - P.RG) * 256;
+    const uint32_t A_bytes = STREAM ? NS * SA : (uint32_t)P.NCH * CB + (uint32_t)(16 - P.RG) * 256;
     uint8_t* stB = stA + A_bytes;
     int* ebs = (int*)(stB + NS * SB);               // [2][32] column exponents
     double* cmax = (double*)(ebs + 2 * NT2);        // [4][32]
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
     if (warp == 0) tmem_alloc(tslot, TCOLS);
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
-            mbar_init(&full[s], MODE == 0 ? NPROD + 1 : NPROD);
+            mbar_init(&full[s], STREAM ? NPROD + 1 : NPROD);
             mbar_init(&empty[s], 1);
         }
         for (int q = 0; q < 2; ++q) {
@@ -461,11 +468,11 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
             int m, pr, tile, nn, n0, n1;
             item_info(item, m, pr, tile, nn, n0, n1);
             if (item + istep < ie) issue_tile(item + istep, k + 1);
-            if (MODE == 1 && m * 2 + pr != cur_mp) {
+            if (MODE == 1 && !STREAM && m * 2 + pr != cur_mp) {
                 // bring the weight chunks of the new (m, parity) once the MMAs on the old ones are done
                 if (warp == 4) {
                     if (lane == 0 && !ab) {
-                        if (a_loads > 0) wait_ab(a_free, (a_loads - 1) & 1, abort_f);
+                        if (a_loads > 0) wait_ab(a_free, (a_loads - 1) & 1, abort_f, P.wlim);
                         mbar_expect_tx(a_full, (uint32_t)P.NCH * CB);
                         const uint8_t* src = P.img + (size_t)((m * 2 + pr) * P.NCH) * CB;
                         for (int c = 0; c < P.NCH; ++c) bulk_g2s(stA + c * CB, src + (size_t)c * CB, CB, a_full);
@@ -476,8 +483,8 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
                 ++a_loads;
             }
             const double* T = (const double*)(tile_s + (k & 1) * TB);
-            if (!ab) wait_ab(&tile_full[k & 1], (k >> 1) & 1, abort_f);
-            if (k >= 2 && !*abort_f) wait_ab(&eb_free[k & 1], ((k >> 1) - 1) & 1, abort_f);
+            if (!ab) wait_ab(&tile_full[k & 1], (k >> 1) & 1, abort_f, P.wlim);
+            if (k >= 2 && !*abort_f) wait_ab(&eb_free[k & 1], ((k >> 1) - 1) & 1, abort_f, P.wlim);
             const int col = tile * NT2 + j;
             const bool cok = col < ncol;
             const int fp = pr ^ P.mode;
@@ -541,8 +548,8 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
                     }
                 }
                 const uint32_t s = gch % NS, rnd = gch / NS;
-                if (rnd > 0 && !*abort_f) wait_ab(&empty[s], (rnd - 1) & 1, abort_f);
-                if (MODE == 0 && pt == 0 && !*abort_f) {
+                if (rnd > 0 && !*abort_f) wait_ab(&empty[s], (rnd - 1) & 1, abort_f, P.wlim);
+                if (STREAM && pt == 0 && !*abort_f) {
                     mbar_expect_tx(&full[s], CB);
                     bulk_g2s(stA + s * SA, P.img + (size_t)((m * 2 + p) * P.NCH + c) * CB, CB, &full[s]);
                     ++issued;
@@ -562,7 +569,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
         if (pt == 0 && *abort_f) {
             const uint32_t first = issued > (uint32_t)NS ? issued - NS : 0;
             for (uint32_t q = first; q < issued; ++q) mbar_wait(&full[q % NS], (q / NS) & 1);
-            if (MODE == 1 && a_loads > 0) mbar_wait(a_full, (a_loads - 1) & 1);
+            if (MODE == 1 && !STREAM && a_loads > 0) mbar_wait(a_full, (a_loads - 1) & 1);
         }
     } else if (warp == 8) {
         // ------------------------------------------------------------ MMA issuer
@@ -573,21 +580,21 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
             for (int item = ib; item < ie && !*abort_f; item += istep) {
                 int m, pr, tile, nn, n0, n1;
                 item_info(item, m, pr, tile, nn, n0, n1);
-                if (MODE == 1 && m * 2 + pr != cur_mp) {
+                if (MODE == 1 && !STREAM && m * 2 + pr != cur_mp) {
                     if (a_uses > 0) mma_commit(a_free);
-                    if (!wait_ab(a_full, a_uses & 1, abort_f)) break;
+                    if (!wait_ab(a_full, a_uses & 1, abort_f, P.wlim)) break;
                     cur_mp = m * 2 + pr;
                     ++a_uses;
                 }
                 const int buf = tt % NBUF;
-                if (tt >= (uint32_t)NBUF && !wait_ab(&tempty[buf], ((tt / NBUF) - 1) & 1, abort_f)) break;
+                if (tt >= (uint32_t)NBUF && !wait_ab(&tempty[buf], ((tt / NBUF) - 1) & 1, abort_f, P.wlim)) break;
                 tc_after();
                 bool ok = true;
                 for (int ci = 0; ci < n0 + n1; ++ci) {
                     const int p = (MODE == 0) ? (ci < n0 ? 0 : 1) : 0;
                     const int c = (MODE == 0 && ci >= n0) ? ci - n0 : ci;
                     const uint32_t s = gch % NS, rnd = gch / NS;
-                    if (!wait_ab(&full[s], rnd & 1, abort_f)) {
+                    if (!wait_ab(&full[s], rnd & 1, abort_f, P.wlim)) {
                         ok = false;
                         break;
                     }
@@ -596,7 +603,7 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
                     // of levels qa..S-1 land in consecutive accumulators.
 #pragma unroll
                     for (int qa = 0; qa < S; ++qa) {
-                        const uint32_t abase = (MODE == 0) ? a0 + s * SA : a0 + c * CB;
+                        const uint32_t abase = STREAM ? a0 + s * SA : a0 + c * CB;
                         const uint64_t ad = sdesc(abase + qa * P.RG * 256, 128, 256);
                         const uint64_t bd = sdesc(b0 + s * SB, 128, 256);
                         const uint32_t idesc = idesc_bf16(128, (S - qa) * NT2);
@@ -624,8 +631,8 @@ __global__ void __launch_bounds__(NTH2, 1) split_gemm_kernel(DevGrid g, SplitArg
             int m, pr, tile, nn, n0, n1;
             item_info(item, m, pr, tile, nn, n0, n1);
             const int buf = tt % NBUF;
-            const bool w1 = wait_ab(&tfull[buf], (tt / NBUF) & 1, abort_f);
-            const bool w2 = wait_ab(&eb_ready[tt & 1], (tt >> 1) & 1, abort_f);
+            const bool w1 = wait_ab(&tfull[buf], (tt / NBUF) & 1, abort_f, P.wlim);
+            const bool w2 = wait_ab(&eb_ready[tt & 1], (tt >> 1) & 1, abort_f, P.wlim);
             if (!__all_sync(0xffffffffu, w1 && w2)) break;
             tc_after();
             const int c0 = tile * NT2;
@@ -775,18 +782,23 @@ void split_geometry(const DevGrid& g, int mode, int wt_rows, int* RG, int* NCH) 
 
 static int tile_rows(const DevGrid& g, int mode) { return mode == 0 ? g.NRCHOPDIM : g.NR; }
 
-size_t split_smem(int S, int RG, int NCH, int trows, int ns, int mode) {
+size_t split_smem(int S, int RG, int NCH, int trows, int ns, bool stream) {
     const size_t sa = (size_t)(S * RG + 16 - RG) * 256, sb = (size_t)S * BSLICE;
-    const size_t a = (mode == 0) ? ns * sa : (size_t)NCH * S * RG * 256 + (size_t)(16 - RG) * 256;
+    const size_t a = stream ? ns * sa : (size_t)NCH * S * RG * 256 + (size_t)(16 - RG) * 256;
     return 2 * (size_t)trows * NT2 * 8 + a + ns * sb + 2 * NT2 * 4 + 4 * NT2 * 8 + 128 * 8 + 8 * (2 * ns + 13) + 16 + 64;
 }
 
-// ring depth per mode: 4 stages where they fit, else 3, else 2
-static int split_stages(const DevGrid& g, int S, int mode, int wt_rows) {
+// Ring depth and weight placement per mode: resident weight chunks (MODE 1)
+// with 4, 3 or 2 stages where they fit, else streamed weights with 4, 3 or 2.
+static int split_stages(const DevGrid& g, int S, int mode, int wt_rows, bool* stream) {
     int RG, NCH;
     split_geometry(g, mode, wt_rows, &RG, &NCH);
-    for (int ns = 4; ns >= 2; --ns)
-        if (split_smem(S, RG, NCH, tile_rows(g, mode), ns, mode) <= 227 * 1024) return ns;
+    for (int st = (mode == 0) ? 1 : 0; st < 2; ++st)
+        for (int ns = 4; ns >= 2; --ns)
+            if (split_smem(S, RG, NCH, tile_rows(g, mode), ns, st != 0) <= 227 * 1024) {
+                *stream = st != 0;
+                return ns;
+            }
     return 0;
 }
 
@@ -801,7 +813,8 @@ bool split_supported(const DevGrid& g, int S, int wt_rows) {
     for (int mode = 0; mode < 2; ++mode) {
         int RG, NCH;
         split_geometry(g, mode, wt_rows, &RG, &NCH);
-        if (RG > 16 || split_stages(g, S, mode, wt_rows) == 0) return false;
+        bool st;
+        if (RG > 16 || split_stages(g, S, mode, wt_rows, &st) == 0) return false;
     }
     return true;
 }
@@ -827,34 +840,45 @@ void k_split_prepare(const DevGrid& g, int S, int mode, const double* W, int wt_
     }
 }
 
-template <int S, int MODE, int NS>
+template <int S, int MODE, int NS, bool STREAM>
 static void launch_ns(const DevGrid& g, const SplitArgs& A, size_t smem, int grid, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(split_gemm_kernel<S, MODE, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(split_gemm_kernel<S, MODE, NS, STREAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              227 * 1024);
         attr = true;
     }
-    split_gemm_kernel<S, MODE, NS><<<grid, NTH2, smem, s>>>(g, A);
+    split_gemm_kernel<S, MODE, NS, STREAM><<<grid, NTH2, smem, s>>>(g, A);
 }
 
 template <int S, int MODE>
 static void launch_split(const DevGrid& g, const SplitArgs& P, int wt_rows, cudaStream_t s) {
     int RG, NCH;
     split_geometry(g, MODE, wt_rows, &RG, &NCH);
-    const int ns = split_stages(g, S, MODE, wt_rows);
+    bool stream = true;
+    const int ns = split_stages(g, S, MODE, wt_rows, &stream);
     SplitArgs A = P;
     A.RG = RG;
     A.NCH = NCH;
     A.trows = tile_rows(g, MODE);
     // at least 120 KB: one CTA per SM, so no CTA waits in tcgen05.alloc for another's columns
-    const size_t smem = std::max(split_smem(S, RG, NCH, A.trows, ns, MODE), (size_t)120 * 1024);
+    const size_t smem = std::max(split_smem(S, RG, NCH, A.trows, ns, stream), (size_t)120 * 1024);
     const int ncol = 2 * g.NXCHOPDIM;
     const int nitems = (MODE == 0 ? 1 : 2) * g.NTCHOPDIM * ((ncol + NT2 - 1) / NT2);
     const int grid = std::min(nitems, sm_count_split());
-    if (ns >= 4) launch_ns<S, MODE, 4>(g, A, smem, grid, s);
-    else if (ns == 3) launch_ns<S, MODE, 3>(g, A, smem, grid, s);
-    else launch_ns<S, MODE, 2>(g, A, smem, grid, s);
+    if constexpr (MODE == 0) {
+        if (ns >= 4) launch_ns<S, MODE, 4, true>(g, A, smem, grid, s);
+        else if (ns == 3) launch_ns<S, MODE, 3, true>(g, A, smem, grid, s);
+        else launch_ns<S, MODE, 2, true>(g, A, smem, grid, s);
+    } else if (stream) {
+        if (ns >= 4) launch_ns<S, MODE, 4, true>(g, A, smem, grid, s);
+        else if (ns == 3) launch_ns<S, MODE, 3, true>(g, A, smem, grid, s);
+        else launch_ns<S, MODE, 2, true>(g, A, smem, grid, s);
+    } else {
+        if (ns >= 4) launch_ns<S, MODE, 4, false>(g, A, smem, grid, s);
+        else if (ns == 3) launch_ns<S, MODE, 3, false>(g, A, smem, grid, s);
+        else launch_ns<S, MODE, 2, false>(g, A, smem, grid, s);
+    }
     count_launch();
 }
 
@@ -869,8 +893,9 @@ static void launch_any(const DevGrid& g, int S, const SplitArgs& P, int wt_rows,
 }
 
 void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, const double2* a, double2* b,
-                 const double* ln, int pad, int* err, cudaStream_t s) {
+                 const double* ln, int pad, int* err, uint64_t wait_cycles, cudaStream_t s) {
     SplitArgs P{};
+    P.wlim = wait_cycles ? wait_cycles : WAIT_NS;
     P.img = img;
     P.eA = eA;
     P.in = (const double*)a;
@@ -882,8 +907,10 @@ void k_split_b2p(const DevGrid& g, int S, const uint8_t* img, const int* eA, con
 }
 
 void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, int wt_rows, const double2* in,
-                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err, cudaStream_t s) {
+                  double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err,
+                  uint64_t wait_cycles, cudaStream_t s) {
     SplitArgs P{};
+    P.wlim = wait_cycles ? wait_cycles : WAIT_NS;
     P.img = img;
     P.eA = eA;
     P.in = (const double*)in;

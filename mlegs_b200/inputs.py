@@ -73,8 +73,8 @@ CONFIGS = {
         omega=1.0, bv0=2.0, visc_sw=3, nu=1.0 / 5000, kappa=0.0, nup=1e-10, kappap=1e-10, p=2,
         amp=1e-2, mmax=8, kmax=16, decay=10.0,
         notes=["VISC%SW=3: Re=5000 has no effect (CALC_BOUSSI_VISC_CN returns, mod_march.f90:1251)"]),
-    # Transform round trips at 256^3 (batch of fields).
-    "roundtrip_256": Config("roundtrip_256", 256, 256, 256, 170, 170, 85),
+    # Transform round trips at 256^3 (batch of 8 fields; chi, psi, b coefficients).
+    "roundtrip_256": Config("roundtrip_256", 256, 256, 256, 170, 170, 85, decay=10.0),
 }
 
 
@@ -126,4 +126,27 @@ def buoyancy_perturbation(cfg):
         e[max(cfg.nrchop - m, 0):, m, :] = 0.0
     at1 = np.sqrt((2 * np.arange(cfg.nrchop) + 1) / 2.0)
     e[0, 0, :] -= (at1 @ e[:cfg.nrchop, 0, :]) / at1[0]
+    return e
+
+
+def roundtrip_coefficients(cfg, fid):
+    """Spectral coefficients of the transform round-trip workload: E[n, m, k]
+    with amplitude exp(-(n + |m| + |k|) / decay) and Gaussian real and
+    imaginary parts (numpy Philox, seed + fid; fid 0 chi, 1 psi, 2 b, further
+    ids for the rest of a batch), chopped at NRCHOPS(m) = NRCHOP - m, Hermitian
+    in k at m = 0 (coef(-k) = conj coef(k), real at k = 0)."""
+    import numpy as np
+
+    shape = fff_shape(cfg)
+    rng = np.random.Generator(np.random.Philox(cfg.seed + 100 + fid))
+    e = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    n = np.arange(shape[0])[:, None, None]
+    m = np.arange(shape[1])[None, :, None]
+    kk = np.arange(shape[2])
+    kv = np.where(kk + 1 > cfg.nxchop, -(shape[2] - kk), kk)
+    e = e * np.exp(-(n + m + np.abs(kv)[None, None, :]) / cfg.decay)
+    neg = np.r_[0, np.arange(shape[2] - 1, 0, -1)]
+    e[:, 0, :] = 0.5 * (e[:, 0, :] + np.conj(e[:, 0, neg]))
+    for mm in range(shape[1]):
+        e[max(cfg.nrchop - mm, 0):, mm, :] = 0.0
     return e

@@ -339,7 +339,15 @@ class Solver:
         if self.ph.visc_sw == 3:
             self.hyp.hyperv3(self.g, PSI, CHI, B, dt / self.ph.dt)
         elif self.ph.visc_sw == 2:
-            raise NotImplementedError("VISC%SW = 2 is not on the configured path")
+            # HYPERV per field, B only when KAPPAP /= 0 (1327-1335); in place
+            from .legops import hyperv
+            ph, g = self.ph, self.g
+            fields = [(PSI, ph.nu, ph.nup), (CHI, ph.nu, ph.nup)]
+            if ph.kappap != 0.0:
+                fields.append((B, ph.kappa, ph.kappap))
+            for F, nu, nup in fields:
+                R = hyperv(g, F, nu, nup, ph.p, dt)
+                F.E, F.LN = R.E, R.LN
 
     def _etd_hyperv(self, RUR, RUP, UZ, B, dt):
         if self.ph.visc_sw == 3:

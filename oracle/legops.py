@@ -4,6 +4,7 @@ Restates mod_legops.f90:
   76-133    DELSQH        136-241  IDELSQH (initial condition only)
   371-428   MULXM         680-748  XXDX           751-820  DEL2
   823-1010  IDEL2         1013-1176 IDEL2LN       1204-1354 IHELM
+  1409-1592 IHELMP (VISC%SW = 2, with HYPERV of mod_march.f90:1639-1686)
   1727-1786 GRAD          1789-1853 PC2VEL        1856-1919 PC2VOR
   1972-2133 VPRODSUB      2136-2232 VDOTPSUB      2277-2339 VEL2PLN
   2397-2545 PROJECT       2548-2648 EOMUL / OEMUL
@@ -210,6 +211,90 @@ def ihelm(g, B, alp):
     _solve_m_nonzero(g, A, alp, 1)
     g.chopdo(A)
     return A
+
+
+def ihelmp(g, B, p, alp, nu=0.0):
+    """IHELMP(P, B, A, ALP, NUIN), mod_legops.f90:1409-1592:
+    A = (DEL^P + NU DEL^2 - ALP)^-1 B, P even in 4..14.
+
+    The log term: A.LN = -B.LN / ALP and its contribution AL + NU AL2 moves
+    to the (m, k) = (0, 0) right-hand side, AL2 the DEL2 image of LN(-log(1-x))
+    on the first three rows and AL = DEL2H^(P/2-1) AL2 (BANMUL, 1444-1466).
+    Per m the band of (DEL2H - k^2)^(P/2) is expanded binomially from the
+    powers DEL2H^q (BANBANMUL at size NN + P) exactly as the reference writes
+    each P out (1476-1573), plus NU (DEL2H - k^2) - ALP, and solved by the
+    unpivoted band LU on the leading NN = NRCHOPS(m) rows; then the far-field
+    fix A(1,1,:) -= CALCAT1(A) / PF(1,1,1) and CHOPDO.
+    """
+    _require(B, FFF, "IHELMP")
+    if alp == 0.0:
+        raise ValueError("IHELMP: ALP CANNOT BE ZERO.")
+    if p < 4 or p > 14 or p % 2:
+        raise ValueError("P OUT OF RANGE. P=%d" % p)
+    hp = p // 2
+    A = g.copy0(B)
+    A.LN = -B.LN / alp
+    nrc = int(g.NRCHOP)
+    n0 = g.NORM0
+    al2 = np.zeros(nrc)
+    al2[0] = A.LN * (4.0 / 3 / g.ELL2) / n0[0]
+    al2[1] = A.LN * (-2 / n0[1] / g.ELL2)
+    al2[2] = A.LN * (+2.0 / 3 / n0[2] / g.ELL2)
+    al = al2.copy()
+    d2 = band_del2h(nrc, g.M[0], g.ELL, g.LOGNORM[:, 0])
+    for _ in range(4, p + 1, 2):
+        al = banmul(d2, 2, al)
+    A.E[:nrc, 0, 0] = A.E[:nrc, 0, 0] - al - nu * al2
+    K = A.E.shape[2]
+    for mm in range(A.E.shape[1]):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        np_ = nn + p
+        d1 = band_del2h(np_, g.M[mm], g.ELL, g.LOGNORM[:, mm])
+        dq = {1: d1}
+        for q in range(2, hp + 1):
+            dq[q], _ = banbanmul(dq[q - 1], 2 * q - 2, d1, 2)
+        bands = np.zeros((K, nn, 2 * p + 1))
+        for kk in range(K):
+            k2 = g.AK[mm, kk] ** 2
+            h = np.zeros((np_, 2 * p + 1))
+            h[:, :] = dq[hp]
+            c = 1.0
+            for j in range(1, hp + 1):
+                c = c * (-k2)
+                binom = 1.0
+                for q in range(1, j + 1):
+                    binom = binom * (hp - q + 1) / q
+                q = hp - j
+                if q == 0:
+                    h[:, p] += c
+                else:
+                    h[:, p - 2 * q:p + 2 * q + 1] += (binom * c) * dq[q]
+            dv = d1.copy()
+            dv[:, 2] -= k2
+            h[:nn, p - 2:p + 3] += nu * dv[:nn, :]
+            h[:nn, p] -= alp
+            bands[kk] = h[:nn]
+        A.E[:nn, mm, :] = band_lu_solve(bands, p, A.E[:nn, mm, :].T).T
+    A.E[0, 0, :] = A.E[0, 0, :] - g.calcat1(A) / g.PF[0, 0, 0]
+    g.chopdo(A)
+    return A
+
+
+def hyperv(g, A, nu, nup, p, dt):
+    """HYPERV(A, NU, NUP, P, DT, WK), mod_march.f90:1639-1686: returns the new A,
+    IHELMP(P, ALP A, A, -ALP, BET), ALP = (-1)^(P/2) / (DT NUP), BET = -(-1)^(P/2) NU / NUP."""
+    if nup == 0.0:
+        raise ValueError("HYPERV: NUP CAN'T BE ZERO")
+    _require(A, FFF, "HYPERV")
+    ph = p // 2
+    alp = 1 / dt / nup * (-1) ** ph
+    bet = -(-1) ** ph * nu / nup
+    WK = A.copy()
+    WK.E = alp * A.E
+    WK.LN = alp * A.LN
+    return ihelmp(g, WK, p, -alp, bet)
 
 
 def grad(g, A):

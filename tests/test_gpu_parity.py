@@ -452,3 +452,59 @@ def test_graph_replay_matches_eager(lib_built, adams):
         ctx.close()
     for (E0, l0), (E1, l1) in zip(*res):
         assert np.array_equal(E0, E1) and l0 == l1
+
+
+@pytest.mark.parametrize("P", [4, 6, 8])
+def test_ihelmp_and_hyperv(env, P):
+    """IHELMP (mod_legops.f90:1409-1592) and HYPERV (mod_march.f90:1639-1686)
+    against the oracle, with the ALP = 1/(DT NUP) scale of a hyperviscosity
+    step (the system is then diagonally dominant; both sides eliminate
+    without pivoting)."""
+    from oracle import legops as L
+    M, ctx, g, cfg = env
+    A = random_fff(g, 60 + P, decay=5.0)
+    A.LN = -0.35
+    f = up(ctx, A)
+    out = ctx.field(M.FFF)
+    alp, nu = 3e7, 0.4
+    ctx.IHELMP(P, f, out, alp, nu)
+    R = L.ihelmp(g, A, P, alp, nu)
+    E, ln = out.download()
+    assert rel(E, R.E) < 1e-11
+    assert abs(ln - R.LN) <= 1e-14 * max(1.0, abs(R.LN))
+    h = up(ctx, A)
+    ctx.HYPERV(h, 1e-3, 1e-5, P, 1e-3)
+    R = L.hyperv(g, A, 1e-3, 1e-5, P, 1e-3)
+    E, ln = h.download()
+    assert rel(E, R.E) < 1e-11
+    assert abs(ln - R.LN) <= 1e-13 * max(1.0, abs(R.LN))
+    with pytest.raises(M.MlegsError) as ei:
+        ctx.IHELMP(5, f, out, alp)
+    assert ei.value.code == 101
+    with pytest.raises(M.MlegsError) as ei:
+        ctx.IHELMP(P, f, out, 0.0)
+    assert ei.value.code == 3
+
+
+@pytest.mark.parametrize("prec", ["fp64", "split6"])
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_ab2_steps_with_hyperv_sw2(lib_built, prec, graph):
+    """VISC%SW = 2 on the AB2-CN path: CALC_BOUSSI_HYPERV -> HYPERV -> IHELMP
+    for PSI, CHI and B (KAPPAP /= 0) in the Richardson start-up (three calls)
+    and every AB2-CN step (mod_march.f90:565, 583, 593, 658), P = 4."""
+    import mlegs_b200 as M
+    cfg = small_cfg(32, 16, 16, adams=True, visc_sw=2, p=4, nu=1e-3, nup=1e-5, kappa=1e-3, kappap=2e-5)
+    kw = {} if prec == "fp64" else dict(precision=M.PREC_SPLIT, split_slices=6)
+    out, ref = _run_pair(cfg, 5, graph=graph, **kw)
+    for (E, ln), R in zip(out, ref):
+        assert rel(E, R.E) < 1e-10
+        assert abs(ln - R.LN) < 1e-10 * max(1.0, abs(R.LN))
+
+
+def test_hyperv_sw2_rejected_for_etd(lib_built):
+    """SOLVER_T%INITIALIZE aborts VISC%SW = 2 with the ETD scheme (ERR_FLAGS%SOLVER)."""
+    import mlegs_b200 as M
+    cfg = small_cfg(32, 16, 16, adams=False, visc_sw=2, p=4, nup=1e-5)
+    with pytest.raises(M.MlegsError) as ei:
+        M.Context(cfg)
+    assert ei.value.code == 5

@@ -363,3 +363,81 @@ def test_sponge_profile_and_k0_kat():
     s._etd_sponge(U, B, ph.dt)
     assert np.abs(B.E[:, :, 0] - damp.mean() * ref).max() < 1e-12 * np.abs(ref).max()
     assert np.abs(U.E).max() == 0.0
+
+
+@pytest.mark.parametrize("P,nu,alp,fwd", [(4, 0.0, 3.0, 2e-9), (4, 0.7, -2.5, 5e-10), (6, 0.3, 5.0, 2e-7),
+                                           (8, 0.0, -7.0, 5e-5), (8, 1e-3, 2e4, 1e-6)])
+def test_ihelmp_known_answer(P, nu, alp, fwd):
+    """IHELMP (mod_legops.f90:1409-1592) recovers a field from its image under
+    (DEL^P + NU DEL^2 - ALP), the image formed independently with dense
+    matrices: (D - k^2)^(P/2) + NU (D - k^2) - ALP for D the DEL2H band
+    (mod_lin_legendre.f90:1986-2092) as a dense matrix, per (m, k), applied to
+    coefficients supported on rows < NRCHOPS(m) - P (so the truncated band
+    system reproduces them exactly), with the log term LN (-log(1-x)) whose
+    DEL2 image is AL2 and whose DEL^P image is DEL2H^(P/2-1) AL2, and with
+    CALCAT1 = 0 at m = 0 (the far-field fix then leaves row 0 alone).
+
+    The unpivoted band LU is backward stable here: the residual of every
+    (m, k) system is below 1e-14 of |H| |A|.  The forward error follows the
+    conditioning of DEL^P - ALP (DEL2H's entries reach n^2 / ELL^2, so
+    DEL^P's reach n^(2P)): bounded per case, from 2e-9 at P = 4 to 5e-5 at
+    P = 8 with |ALP| of order one (1e-6 with ALP = 2e4, still far below
+    DEL^8's largest entries)."""
+    from oracle import legops as L
+    from oracle.bandmat import band_del2h, band_to_full
+    from oracle.grid import FFF
+    g = oracle_grid(small_cfg(48, 16, 16))
+    rng = np.random.default_rng(P)
+    A0 = g.alloc(FFF)
+    for mm in range(g.NTCHOPDIM):
+        nn = int(g.NRCHOPS[mm])
+        if nn - P > 0:
+            sh = (nn - P, g.NXCHOPDIM)
+            A0.E[: nn - P, mm, :] = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    A0.E[0, 0, :] -= g.calcat1(A0) / g.AT1[0]
+    A0.LN = 0.3
+    B = g.alloc(FFF)
+    B.LN = -alp * A0.LN
+    hp = P // 2
+    H = {}
+    for mm in range(g.NTCHOPDIM):
+        nn = int(g.NRCHOPS[mm])
+        if nn < 1:
+            continue
+        big = nn + 2 * P
+        D = band_to_full(band_del2h(big, g.M[mm], g.ELL, g.LOGNORM[:, mm]), 2, big)
+        for kk in range(g.NXCHOPDIM):
+            k2 = g.AK[mm, kk] ** 2
+            Dk = D - k2 * np.eye(big)
+            H[mm, kk] = np.linalg.matrix_power(Dk, hp) + nu * Dk - alp * np.eye(big)
+            x = np.zeros(big, dtype=complex)
+            x[:nn] = A0.E[:nn, mm, kk]
+            B.E[:nn, mm, kk] = (H[mm, kk] @ x)[:nn]
+    n0 = g.NORM0
+    al2 = np.zeros(g.NRCHOP)
+    al2[:3] = A0.LN * np.array([(4.0 / 3 / g.ELL2) / n0[0], -2 / n0[1] / g.ELL2, (2.0 / 3) / n0[2] / g.ELL2])
+    D0 = band_to_full(band_del2h(g.NRCHOP, g.M[0], g.ELL, g.LOGNORM[:, 0]), 2, g.NRCHOP)
+    logpart = np.linalg.matrix_power(D0, hp - 1) @ al2 + nu * al2
+    B.E[: g.NRCHOP, 0, 0] += logpart
+    A = L.ihelmp(g, B, P, alp, nu)
+    assert abs(A.LN - A0.LN) < 1e-14
+    worst = 0.0
+    for (mm, kk), Hm in H.items():
+        nn = int(g.NRCHOPS[mm])
+        rhs = B.E[:nn, mm, kk].copy()
+        if mm == 0 and kk == 0:
+            rhs -= logpart[:nn]
+        a = A.E[:nn, mm, kk]
+        Ht = Hm[:nn, :nn]
+        res = np.abs(Ht @ a - rhs).max() / (np.abs(Ht).sum(axis=1).max() * np.abs(a).max())
+        worst = max(worst, res)
+    assert worst < 1e-14, worst
+    assert rel(A.E, A0.E) < fwd
+    # HYPERV is IHELMP(P, ALP A, A, -ALP, BET) with ALP = (-1)^(P/2)/(DT NUP)
+    dt, nup = 1e-3, 0.05
+    Hv = L.hyperv(g, A0.copy(), 1e-3, nup, P, dt)
+    a = (-1) ** hp / dt / nup
+    W = A0.copy()
+    W.E, W.LN = a * A0.E, a * A0.LN
+    R = L.ihelmp(g, W, P, -a, -(-1) ** hp * 1e-3 / nup)
+    assert np.array_equal(Hv.E, R.E) and Hv.LN == R.LN

@@ -8,6 +8,8 @@ parity tests; and an oversized grid must be rejected before any GPU work.
 This file is collected last and also passes when run alone.
 """
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -15,8 +17,21 @@ from conftest import oracle_grid, random_fff, rel, small_cfg
 
 pytestmark = pytest.mark.gpu
 
-SOLVE_TOL = 1e-10
+# The static path eliminates on the fly (solve_kernel); IDEL2LN substitutes
+# with stored factors (solve_factored_kernel).  Same multipliers and order, but
+# the compiler contracts different products into FMAs, so the two agree to a
+# few ulps (2e-16 relative measured), not bit for bit.
+SOLVE_TOL = 1e-13
 MLEGS_ERR_ARG = 101
+
+
+def _free_device_bytes():
+    """cudaMemGetInfo's free bytes on device 0 (the device the tests use)."""
+    rt = ctypes.CDLL("libcudart.so")
+    free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    assert rt.cudaSetDevice(0) == 0
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
 
 
 def _solve_both(M, ctx, g, seed, pad):
@@ -47,6 +62,30 @@ def test_static_scratch_matches_idel2ln(lib_built, dims):
             assert np.isfinite(E_new).all()
             assert rel(E_new, E_ref) < SOLVE_TOL
             assert abs(ln_new - ln_ref) <= SOLVE_TOL * max(1.0, abs(ln_ref))
+    finally:
+        ctx.close()
+
+
+def test_static_scratch_allocates_nothing(lib_built):
+    """After a first call (which looks the array up), further calls leave the
+    device's free memory unchanged: no cudaMalloc behind the entry point."""
+    import mlegs_b200 as M
+    cfg = small_cfg(64, 32, 32)
+    g = oracle_grid(cfg)
+    ctx = M.Context(cfg)
+    try:
+        B = random_fff(g, 13)
+        b = ctx.field(M.FFF)
+        b.upload(B.E, 0.0, M.FFF)
+        a = ctx.field(M.FFF)
+        for pad in (0, 3):
+            assert ctx.lib.mlegs_idel2ln_static(ctx.c, b.h, a.h, pad) == 0
+        ctx.sync()
+        before = _free_device_bytes()
+        for pad in (0, 3, 0):
+            assert ctx.lib.mlegs_idel2ln_static(ctx.c, b.h, a.h, pad) == 0
+        ctx.sync()
+        assert _free_device_bytes() == before
     finally:
         ctx.close()
 

@@ -23,6 +23,12 @@ cores while the GPU is timed) runs the Richardson start-up and --oracle-steps
 FP64 and the mixed GPU paths' field errors against it, and the mixed path's
 error against the FP64 GPU path after --error-steps steps.
 
+"ensemble" is the batched-run configuration: 64 AB2-CN runs of different
+grids (NR 48..192, NTH 32..128, NX 32..256, Re 500..5000, N 0.5..4) stepped
+50 times together with grouped launches (graph-replayed, after the
+autotuner's pass), beside the same 64 runs one after another on their own
+contexts, with each instance's field error against that FP64 run.
+
 "transform_roundtrip" is the transform-only configuration: FFF -> PPP -> FFF
 (TOFP, TOFF) at 256^3 with 2/3 chops, a batch of 8 fields, per precision
 form (FP64 and split-BF16 S = 4, 5, 6): device time per round trip and the
@@ -66,6 +72,7 @@ def parse():
     ap.add_argument("--oracle-steps", type=int, default=10,
                     help="steps (start-up included) of the oracle trajectory the GPU paths are checked against")
     ap.add_argument("--no-roundtrip", action="store_true", help="skip the 256^3 transform round-trip leg")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     return ap.parse_args()
@@ -301,6 +308,66 @@ def roundtrip_leg(local, reps=10, batch=8):
     return out
 
 
+def ensemble_leg(local, n=64, steps=50, warm=3):
+    """The batched-run configuration: n AB2-CN instances of different grids
+    (mlegs_b200.inputs.ensemble_configs) stepped together with grouped
+    launches, graph-replayed; aggregate steps/s against the same instances
+    run one after another on their own contexts (graph-replayed too), and
+    each instance's field error against that standalone FP64 run."""
+    import numpy as np
+    import torch
+
+    import mlegs_b200 as M
+    from mlegs_b200.inputs import ensemble_configs
+    cfgs = ensemble_configs(n)
+    ens = M.Ensemble(cfgs, device=local)
+    states = []
+    for ctx, c in zip(ens.contexts, cfgs):
+        fs = M.initial_state(ctx, c)
+        ctx.initialize(*fs)
+        states.append(fs)
+    ens.step(warm, graph=True)  # eager step, autotuning, capture, replays
+    ens.sync()
+    st = torch.cuda.ExternalStream(ens.stream(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ens.launches()
+    e0.record(st)
+    ens.step(steps, graph=True)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = ens.launches() - l0
+    rows, ctas = ens.tuning()
+    got = [[f.download() for f in fs] for fs in states]
+    ens.close()
+    # the same instances on their own contexts, one after another
+    solo_ms, errs = 0.0, []
+    for c, g_out in zip(cfgs, got):
+        ctx = M.Context(c, device=local)
+        fs = M.initial_state(ctx, c)
+        ctx.initialize(*fs)
+        ctx.step(warm, graph=True)
+        ctx.sync()
+        s = torch.cuda.ExternalStream(ctx.stream(), device=local)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        ctx.step(steps, graph=True)
+        b.record(s)
+        b.synchronize()
+        solo_ms += a.elapsed_time(b)
+        ref = [f.download() for f in fs]
+        errs.append(max(float(np.abs(E - R).max() / np.abs(R).max()) for (E, _), (R, _) in zip(g_out, ref)))
+        ctx.close()
+    grids = sorted({(c.nr, c.nth, c.nx) for c in cfgs})
+    return {"workload": "ensemble_%d_ab2" % n, "instances": n, "steps": steps, "distinct_grids": len(grids),
+            "ms": ms, "aggregate_steps_per_s": n * steps / (ms * 1e-3), "gpu_launches": int(launches),
+            "standalone_sequential_ms": solo_ms, "standalone_aggregate_steps_per_s": n * steps / (solo_ms * 1e-3),
+            "speedup_vs_standalone": solo_ms / ms, "max_rel_error_vs_standalone_fp64": max(errs),
+            "tuning": {"classes": [{"transform": "rtran+1" if r[0] == 0 else "fold", "NRH": r[1], "NRCHOP": r[2],
+                                    "tile_columns": r[3]} for r in rows],
+                       "ctas_per_sm": {"rtran+1": ctas[0], "fold": ctas[1]}}}
+
+
 def run_reference(args, cfg, ws, rank):
     if rank != 0:
         return
@@ -471,6 +538,9 @@ def run_ours(args, cfg, ws, rank, local):
     rtrip = None
     if rank == 0 and ws == 1 and not args.no_roundtrip:
         rtrip = roundtrip_leg(local)
+    ensl = None
+    if rank == 0 and ws == 1 and not args.no_ensemble:
+        ensl = ensemble_leg(local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -493,7 +563,8 @@ def run_ours(args, cfg, ws, rank, local):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * nbytes,
                         "d2h_bytes_per_step": 3 * nbytes},
                 "gpu_launches": int(launches), "precision_comparison": compare,
-                "roofline": roof, "kernels": kernels, "transform_roundtrip": rtrip, "cpu_baseline": cpu,
+                "roofline": roof, "kernels": kernels, "transform_roundtrip": rtrip, "ensemble": ensl,
+                "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
 

@@ -286,6 +286,40 @@ int mlegs_time(const mlegs_ctx* ctx, double* t, int32_t* n);
  * returns MLEGS_ERR_NONFINITE if any state coefficient is NaN/Inf. */
 int mlegs_check_finite(mlegs_ctx* ctx);
 
+/* Ensembles: n independent AB2-CN runs of different grids (the batched-run
+ * configuration) on one device, advanced in lock-step.  No counterpart in the
+ * reference, which runs one instance per MPI job.  Each instance is a context
+ * as mlegs_create makes it (fields, uploads, mlegs_solver_init and downloads
+ * go through mlegs_ensemble_context(e, i); the ensemble owns and destroys
+ * them).  mlegs_ensemble_step advances every instance by nsteps AB2-CN steps
+ * (STEP_BOUSSI_AB_CN, mod_march.f90:609-661): per step, the Legendre GEMMs of
+ * all instances (10 RTRAN(+1); PROJECT's five products and one RTRAN(-1)) and
+ * their banded solves (IDEL2LN; IHELM) run as four grouped launches, the GEMMs
+ * persistent with a global work counter, everything else per instance on its
+ * own stream.  graph = 1 runs the first step eagerly, autotunes the grouped
+ * GEMMs (mlegs_ensemble_tune) and captures one step as a CUDA graph over all
+ * streams for the rest.  Requirements: every instance FP64, BOUSSINESQ ABSW =
+ * 1, mlegs_solver_init done, NRH <= 96 and NRCHOPDIM <= 190. */
+typedef struct mlegs_ensemble mlegs_ensemble;
+int mlegs_ensemble_create(const mlegs_params* p, int n, mlegs_ensemble** out);
+int mlegs_ensemble_destroy(mlegs_ensemble* e);
+const char* mlegs_ensemble_last_error(const mlegs_ensemble* e);
+int mlegs_ensemble_size(const mlegs_ensemble* e);
+mlegs_ctx* mlegs_ensemble_context(mlegs_ensemble* e, int i);
+int mlegs_ensemble_step(mlegs_ensemble* e, int nsteps, int graph);
+/* Autotuner: per class of GEMM problems (transform, NRH, NRCHOP) the column
+ * tile (16 or 32 columns) with the shortest grouped launch (best of 3), then
+ * persistent CTAs per SM (2, 3, 4) per transform; cached for the process.
+ * Needs one step first.  mlegs_ensemble_tuning writes up to cap rows
+ * (transform 0 RTRAN(+1) / 1 fold, NRH, NRCHOP, tile columns) and returns the
+ * row count; mlegs_ensemble_ctas writes the two CTA-per-SM choices. */
+int mlegs_ensemble_tune(mlegs_ensemble* e);
+int mlegs_ensemble_tuning(const mlegs_ensemble* e, int32_t* out, int cap);
+int mlegs_ensemble_ctas(const mlegs_ensemble* e, int32_t* out);
+int mlegs_ensemble_sync(mlegs_ensemble* e);
+int64_t mlegs_ensemble_launch_count(const mlegs_ensemble* e);
+void* mlegs_ensemble_stream(mlegs_ensemble* e);
+
 /* Kernel timing for profiling and roofline reports: launches one internal
  * kernel `reps` times on scratch fields of this context, bracketed by CUDA
  * events on the context's stream, and returns the mean device time per launch

@@ -69,37 +69,58 @@ class Field:
         return (np.ascontiguousarray(E) if out is None else E), ln.value
 
 
+def params_of(cfg, precision=PREC_FP64, split_slices=0, device=0):
+    """mlegs_params of a configuration."""
+    p = _lib.Params()
+    p.nr, p.nth, p.nx = cfg.nr, cfg.nth, cfg.nx
+    p.nrchop, p.ntchop, p.nxchop = cfg.nrchop, cfg.ntchop, cfg.nxchop
+    p.ell, p.zlen, p.dt = cfg.ell, cfg.zlen, cfg.dt
+    p.adams = 1 if cfg.adams else 0
+    p.omega, p.bv0, p.kappa, p.kappap = cfg.omega, cfg.bv0, cfg.kappa, cfg.kappap
+    p.visc_sw, p.visc_p = cfg.visc_sw, cfg.p
+    p.nu, p.nup = cfg.nu, cfg.nup
+    p.precision, p.split_slices, p.device = precision, split_slices, device
+    p.rmv_sw = int(getattr(cfg, "rmv_sw", 0))
+    return p
+
+
 class Context:
     """One grid + solver on one GPU (LEGINIT, mod_fft.f90:180-367)."""
 
     def __init__(self, cfg, precision=PREC_FP64, split_slices=0, device=0):
         self.lib = _lib.load()
         self.cfg = cfg
-        p = _lib.Params()
-        p.nr, p.nth, p.nx = cfg.nr, cfg.nth, cfg.nx
-        p.nrchop, p.ntchop, p.nxchop = cfg.nrchop, cfg.ntchop, cfg.nxchop
-        p.ell, p.zlen, p.dt = cfg.ell, cfg.zlen, cfg.dt
-        p.adams = 1 if cfg.adams else 0
-        p.omega, p.bv0, p.kappa, p.kappap = cfg.omega, cfg.bv0, cfg.kappa, cfg.kappap
-        p.visc_sw, p.visc_p = cfg.visc_sw, cfg.p
-        p.nu, p.nup = cfg.nu, cfg.nup
-        p.precision, p.split_slices, p.device = precision, split_slices, device
-        p.rmv_sw = int(getattr(cfg, "rmv_sw", 0))
+        self._owned = True
+        p = params_of(cfg, precision, split_slices, device)
         h = ctypes.c_void_p()
         rc = self.lib.mlegs_create(ctypes.byref(p), ctypes.byref(h))
         if rc != 0:
             raise MlegsError(rc, "mlegs_create failed")
+        self._attach(h)
+
+    @classmethod
+    def _wrap(cls, handle, cfg):
+        """A context owned by someone else (an ensemble instance): not destroyed here."""
+        self = cls.__new__(cls)
+        self.lib = _lib.load()
+        self.cfg = cfg
+        self._owned = False
+        self._attach(ctypes.c_void_p(handle))
+        return self
+
+    def _attach(self, h):
         self.c = h
         d = (ctypes.c_int32 * 9)()
         self.lib.mlegs_dims(self.c, d)
         (self.NDIMR, self.NDIMTH, self.NX, self.NRCHOPDIM, self.NTCHOPDIM, self.NXCHOPDIM,
          self.NRH, self.NR, self.NTH) = list(d)
-        self.NTCHOP, self.NXCHOP = int(cfg.ntchop), int(cfg.nxchop)
+        self.NTCHOP, self.NXCHOP = int(self.cfg.ntchop), int(self.cfg.nxchop)
 
     # ------------------------------------------------------------------
     def close(self):
         if getattr(self, "c", None):
-            self.lib.mlegs_destroy(self.c)
+            if getattr(self, "_owned", True):
+                self.lib.mlegs_destroy(self.c)
             self.c = None
 
     def __del__(self):
@@ -355,6 +376,68 @@ class Context:
         return ms.value, by.value
 
 
+class Ensemble:
+    """Independent AB2-CN runs of different grids advanced in lock-step on one
+    GPU with grouped launches (mlegs_ensemble_*, include/mlegs_b200.h); no
+    counterpart in the reference.  ``contexts[i]`` is instance i's Context
+    (fields, uploads, ``initialize``), owned by the ensemble."""
+
+    def __init__(self, cfgs, device=0):
+        self.lib = _lib.load()
+        self.cfgs = list(cfgs)
+        arr = (_lib.Params * len(self.cfgs))(*[params_of(c, device=device) for c in self.cfgs])
+        h = ctypes.c_void_p()
+        rc = self.lib.mlegs_ensemble_create(arr, len(self.cfgs), ctypes.byref(h))
+        if rc != 0:
+            raise MlegsError(rc, "mlegs_ensemble_create failed")
+        self.e = h
+        self.contexts = [Context._wrap(self.lib.mlegs_ensemble_context(self.e, i), c)
+                         for i, c in enumerate(self.cfgs)]
+
+    def _ck(self, rc):
+        if rc != 0:
+            msg = self.lib.mlegs_ensemble_last_error(self.e)
+            raise MlegsError(rc, msg.decode() if msg else "")
+
+    def step(self, n=1, graph=True):
+        self._ck(self.lib.mlegs_ensemble_step(self.e, int(n), 1 if graph else 0))
+
+    def tune(self):
+        self._ck(self.lib.mlegs_ensemble_tune(self.e))
+
+    def tuning(self):
+        """(rows, ctas): rows of (transform 0 RTRAN(+1) / 1 fold, NRH, NRCHOP,
+        tile columns) chosen by the autotuner; CTAs per SM per transform."""
+        buf = (ctypes.c_int32 * 512)()
+        n = self.lib.mlegs_ensemble_tuning(self.e, buf, 128)
+        rows = [tuple(buf[4 * i:4 * i + 4]) for i in range(max(n, 0))]
+        c = (ctypes.c_int32 * 2)()
+        self._ck(self.lib.mlegs_ensemble_ctas(self.e, c))
+        return rows, (c[0], c[1])
+
+    def sync(self):
+        self._ck(self.lib.mlegs_ensemble_sync(self.e))
+
+    def stream(self):
+        return self.lib.mlegs_ensemble_stream(self.e)
+
+    def launches(self):
+        return self.lib.mlegs_ensemble_launch_count(self.e)
+
+    def close(self):
+        if getattr(self, "e", None):
+            for c in self.contexts:
+                c.c = None
+            self.lib.mlegs_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _spectrum_call(name, espec, ratio):
     e = np.ascontiguousarray(espec, dtype=np.float64)
     out = ctypes.c_double(0.0)
@@ -452,6 +535,6 @@ def initial_state(ctx, cfg=None):
     return psi, chi, b
 
 
-__all__ = ["Context", "Field", "MlegsError", "qvortex", "QVORTEX", "initial_state", "CONFIGS", "Config",
+__all__ = ["Context", "Ensemble", "params_of", "Field", "MlegsError", "qvortex", "QVORTEX", "initial_state", "CONFIGS", "Config",
            "SPECURV", "SPESLOP", "PDAJUST", "HYP3_CONTROLLER",
            "PPP", "FFF", "PFP", "PFF", "PREC_FP64", "PREC_SPLIT"]

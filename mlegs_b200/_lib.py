@@ -102,6 +102,18 @@ SIGNATURES = {
     "mlegs_time": (c_int, [c_void_p, dptr, ctypes.POINTER(ctypes.c_int32)]),
     "mlegs_check_finite": (c_int, [c_void_p]),
     "mlegs_kernel_time": (c_int, [c_void_p, c_int, c_int, dptr, dptr]),
+    "mlegs_ensemble_create": (c_int, [ctypes.POINTER(Params), c_int, ctypes.POINTER(c_void_p)]),
+    "mlegs_ensemble_destroy": (c_int, [c_void_p]),
+    "mlegs_ensemble_last_error": (c_char_p, [c_void_p]),
+    "mlegs_ensemble_size": (c_int, [c_void_p]),
+    "mlegs_ensemble_context": (c_void_p, [c_void_p, c_int]),
+    "mlegs_ensemble_step": (c_int, [c_void_p, c_int, c_int]),
+    "mlegs_ensemble_tune": (c_int, [c_void_p]),
+    "mlegs_ensemble_tuning": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int32), c_int]),
+    "mlegs_ensemble_ctas": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    "mlegs_ensemble_sync": (c_int, [c_void_p]),
+    "mlegs_ensemble_launch_count": (c_int64, [c_void_p]),
+    "mlegs_ensemble_stream": (c_void_p, [c_void_p]),
     "mlegs_launch_count": (c_int64, [c_void_p]),
     "mlegs_reset_launch_count": (None, [c_void_p]),
     "mlegs_stream": (c_void_p, [c_void_p]),

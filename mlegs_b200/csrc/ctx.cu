@@ -64,7 +64,7 @@ const double* mlegs_ctx::helmp_tables(int P) {
     // DEL2H rows i < rows + P - 2 (BAND_LOGLEG_RAT_DEL2H with S = 0, mod_lin_legendre.f90:1986-2092):
     // the powers' rows below `rows` are then those of the untruncated operator
     const int nd = std::min(rows + P - 2, d.NLN - 2);
-    const size_t per_m = (size_t)rows * HP * (2 * HP + 1);
+    const size_t per_m = (size_t)rows * HP * (2 * HP + 3);  // rows * sum_{q <= HP} (4q + 1)
     std::vector<double> h((size_t)d.NTCHOPDIM * per_m, 0.0);
     for (int m = 0; m < d.NTCHOPDIM; ++m) {
         const double* ln = &h_lognorm[(size_t)m * d.NLN];
@@ -87,7 +87,7 @@ const double* mlegs_ctx::helmp_tables(int P) {
         for (int q = 1; q <= HP; ++q) {
             const int w = 4 * q + 1;
             if (q > 1) Dq = banbanmul(Dq, 4 * q - 3, 2 * q - 2, D, 5, 2, nd);  // D^q = D^(q-1) D
-            double* out = &h[(size_t)m * per_m + (size_t)rows * q * (2 * q - 1)];
+            double* out = &h[(size_t)m * per_m + (size_t)rows * (q - 1) * (2 * q + 1)];
             for (int r = 0; r < rows && r < nd; ++r)
                 for (int e = 0; e < w; ++e) out[(size_t)r * w + e] = Dq[(size_t)r * w + e];
         }

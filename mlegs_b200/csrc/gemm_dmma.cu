@@ -52,9 +52,9 @@ constexpr int NST_B2P = 2;   // ring stages of b2p_dmma_kernel
 constexpr int NST_FOLD = 2;  // ring stages of legfold_dmma_kernel
 constexpr int NST_PFFF = 2;  // ring stages of projfff_dmma_kernel
 
-// One (m, 32-column) tile of RTRAN(+1): the body of b2p_dmma_kernel, also run
-// per work item by the grouped ensemble kernel (ensemble.cu).
-template <int NW, int MTW>
+// One (m, 8 NJ-column) tile of RTRAN(+1): the body of b2p_dmma_kernel (NJ = 4),
+// also run per work item by the grouped ensemble kernel (ensemble.cu).
+template <int NW, int MTW, int NJ = 4>
 __device__ __forceinline__ void b2p_tile(const DevGrid& g, const double* __restrict__ A, double* __restrict__ out,
                                          const double* ln, int pad, int SA, int m, int c0, double* smd) {
     const size_t stg = (size_t)KCB * (SA + SBS);
@@ -92,40 +92,40 @@ __device__ __forceinline__ void b2p_tile(const DevGrid& g, const double* __restr
                 ++tt;
             }
         }
-        for (int e = tid; e < KCB * (CT / 2); e += NW * 32) {
-            const int tt = e / (CT / 2), ch = e - tt * (CT / 2);
+        for (int e = tid; e < KCB * (4 * NJ); e += NW * 32) {
+            const int tt = e / (4 * NJ), ch = e - tt * (4 * NJ);
             const int t = t0 + tt, c = c0 + 2 * ch;
             const bool ok = t < kp && c < ncol;
             cp16(Bs + (size_t)tt * SBS + 2 * ch, ok ? a + (size_t)(2 * t + p) * ncol + c : a, ok);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    auto mma_chunk = [&](double (&acc)[MTW][4][2], const double* As, const double* Bs, int ksteps) {
+    auto mma_chunk = [&](double (&acc)[MTW][NJ][2], const double* As, const double* Bs, int ksteps) {
 #pragma unroll
         for (int s4 = 0; s4 < KCB / 4; ++s4) {
             if (s4 < ksteps) {
                 const int k = 4 * s4 + q;
-                double bf[4];
+                double bf[NJ];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) bf[j] = Bs[(size_t)k * SBS + j * 8 + gq];
+                for (int j = 0; j < NJ; ++j) bf[j] = Bs[(size_t)k * SBS + j * 8 + gq];
 #pragma unroll
                 for (int i = 0; i < MTW; ++i) {
                     const int mt = warp + NW * i;
                     if (mt < RT) {
                         const double af = As[(size_t)k * SA + mt * 8 + gq];
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) dmma(acc[i][j], af, bf[j]);
+                        for (int j = 0; j < NJ; ++j) dmma(acc[i][j], af, bf[j]);
                     }
                 }
             }
         }
     };
 
-    double acc0[MTW][4][2], acc1[MTW][4][2];
+    double acc0[MTW][NJ][2], acc1[MTW][NJ][2];
 #pragma unroll
     for (int i = 0; i < MTW; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc0[i][j][0] = acc0[i][j][1] = acc1[i][j][0] = acc1[i][j][1] = 0.0;
+        for (int j = 0; j < NJ; ++j) acc0[i][j][0] = acc0[i][j][1] = acc1[i][j][0] = acc1[i][j][1] = 0.0;
     // ring: NST_B2P - 1 chunks in flight ahead of the one computed; every
     // iteration commits one group (empty past the end), so the wait count is fixed
 #pragma unroll
@@ -156,7 +156,7 @@ __device__ __forceinline__ void b2p_tile(const DevGrid& g, const double* __restr
         if (row >= g.NRH) continue;
         const int rh = g.NR - 1 - row;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < NJ; ++j) {
             const int c = c0 + j * 8 + 2 * q;
             if (c >= ncol) continue;
             double2 lo = make_double2(acc0[i][j][0] + acc1[i][j][0], acc0[i][j][1] + acc1[i][j][1]);
@@ -199,16 +199,6 @@ constexpr int KC2 = 16;       // K rows per chunk
 constexpr int SA2 = KC2 + 4;  // weight row stride (doubles), = 4 mod 16
 constexpr int SX2 = CT + 8;   // input / folded row stride (doubles), = 8 mod 16
 
-struct FoldArgs {
-    const double* w[5];  // weights per segment, [m][wt_rows][NRH]
-    const double* x[5];  // inputs per segment, PFF [m][NR][2 NXCHOPDIM]
-    int mode[5];         // 0: EO fold, 1: OE fold
-    int scale[5];        // 0 none, 1 -v, 2 -i m v, 3 i k v, 4 m k v
-    int nseg, split;     // segments [0, split) -> out0, [split, nseg) -> out1
-    double* out0;
-    double* out1;
-    int wt_rows, pad, use_w, accumulate;
-};
 
 template <class T>
 __device__ __forceinline__ T pick5(const T (&a)[5], int i) {
@@ -219,9 +209,10 @@ __device__ __forceinline__ T pick5(const T (&a)[5], int i) {
     return v;
 }
 
-// One (m, output parity, 32-column) tile of the fold GEMMs: the body of
-// legfold_dmma_kernel, also run per work item by the grouped ensemble kernel.
-template <int NW, int MTW>
+// One (m, output parity, 8 NJ-column) tile of the fold GEMMs: the body of
+// legfold_dmma_kernel (NJ = 4), also run per work item by the grouped ensemble
+// kernel.
+template <int NW, int MTW, int NJ = 4>
 __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& fa, int RTmax, int m, int pr, int c0,
                                              double* smd) {
     const int ncol = 2 * g.NXCHOPDIM;
@@ -239,8 +230,9 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
     double* ws = Bs + KC2 * SX2;         // [nch * KC2] fold weights (w_i, or 1), 0 past NRH
     const size_t wofs = (size_t)m * fa.wt_rows * g.NRH, xofs = (size_t)m * g.NR * ncol;
     for (int i = tid; i < nch * KC2; i += NW * 32) ws[i] = (i < g.NRH) ? (fa.use_w ? g.w[i] : 1.0) : 0.0;
-    // fold pass: thread -> column pair p2 (fixed), rows j = tid / 16 + (NW * 2) t
-    const int p2 = tid & 15;
+    // fold pass: thread -> column pair p2 (fixed), rows j = tid / (4 NJ) + (NW * 32 / (4 NJ)) t
+    constexpr int NP2 = 4 * NJ;
+    const int p2 = tid % NP2;
     const int cp = c0 + 2 * p2;
     const double akv = (cp < ncol) ? g.ak[cp >> 1] : 0.0;
 
@@ -256,8 +248,8 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
             const bool ok = n < nw && i < g.NRH;
             cp16(As + (size_t)r * SA2 + 2 * c2, ok ? w + (size_t)n * g.NRH + i : w, ok);
         }
-        for (int e = tid; e < 2 * KC2 * (CT / 2); e += NW * 32) {
-            const int rr = e / (CT / 2), c2 = e - rr * (CT / 2);
+        for (int e = tid; e < 2 * KC2 * (4 * NJ); e += NW * 32) {
+            const int rr = e / (4 * NJ), c2 = e - rr * (4 * NJ);
             const int j = rr % KC2, i = i0 + j;
             const int src_row = rr < KC2 ? i : g.NR - 1 - i;
             const int c = c0 + 2 * c2;
@@ -266,7 +258,7 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    auto epilogue = [&](double (&acc)[MTW][4][2], double* out) {
+    auto epilogue = [&](double (&acc)[MTW][NJ][2], double* out) {
         double* o = out + (size_t)m * g.NRCHOPDIM * ncol;
 #pragma unroll
         for (int t = 0; t < MTW; ++t) {
@@ -274,7 +266,7 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
             const int n = 2 * r + pr;
             if (r >= rows || n >= g.NRCHOPDIM) continue;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < NJ; ++j) {
                 const int c = c0 + j * 8 + 2 * q;
                 double2 v = make_double2(acc[t][j][0], acc[t][j][1]);
                 acc[t][j][0] = acc[t][j][1] = 0.0;
@@ -292,11 +284,11 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
         }
     };
 
-    double acc[MTW][4][2];
+    double acc[MTW][NJ][2];
 #pragma unroll
     for (int t = 0; t < MTW; ++t)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
+        for (int j = 0; j < NJ; ++j) acc[t][j][0] = acc[t][j][1] = 0.0;
 #pragma unroll
     for (int c = 0; c < NST_FOLD - 1; ++c) {
         if (c < total) stage(c);
@@ -312,7 +304,7 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
         const double* Xs = As + stA;
         const double sgn = (pr ^ pick5(fa.mode, sg)) ? -1.0 : 1.0;
         const int sc = pick5(fa.scale, sg);
-        for (int j = tid >> 4; j < KC2; j += NW * 2) {
+        for (int j = tid / NP2; j < KC2; j += (NW * 32) / NP2) {
             const double2 top = *(const double2*)(Xs + (size_t)j * SX2 + 2 * p2);
             const double2 bot = *(const double2*)(Xs + (size_t)(KC2 + j) * SX2 + 2 * p2);
             const double wv = ws[ch * KC2 + j];
@@ -331,16 +323,16 @@ __device__ __forceinline__ void legfold_tile(const DevGrid& g, const FoldArgs& f
 #pragma unroll
         for (int kk = 0; kk < KC2; kk += 4) {
             const int j = kk + q;
-            double bf[4];
+            double bf[NJ];
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) bf[jj] = Bs[(size_t)j * SX2 + jj * 8 + gq];
+            for (int jj = 0; jj < NJ; ++jj) bf[jj] = Bs[(size_t)j * SX2 + jj * 8 + gq];
 #pragma unroll
             for (int t = 0; t < MTW; ++t) {
                 const int mt = warp + NW * t;
                 if (mt < RTv) {
                     const double af = As[(size_t)(mt * 8 + gq) * SA2 + j];
 #pragma unroll
-                    for (int jj = 0; jj < 4; ++jj) dmma(acc[t][jj], af, bf[jj]);
+                    for (int jj = 0; jj < NJ; ++jj) dmma(acc[t][jj], af, bf[jj]);
                 }
             }
         }
@@ -692,6 +684,118 @@ void k_project_fff_dmma(const DevGrid& g, const double* CV, const double* CD, co
         case 3: projfff_launch<4, 3>(g, pa, s); break;
         default: projfff_launch<4, 4>(g, pa, s); break;
     }
+}
+
+
+// ---------------------------------------------------------------------------
+// Grouped persistent Legendre GEMMs for ensembles of instances of different
+// grids (ensemble.cu).  One launch covers every RTRAN(+1) (or every fold
+// product) of every instance: the work items are (problem, m[, parity],
+// column tile) tiles numbered consecutively problem by problem; persistent
+// CTAs take the next tile from a global counter (atomicAdd, no waiting on
+// other CTAs) and run the same tile bodies as the single-grid kernels, with
+// the problem's own grid and a per-problem column-tile width (8 * nj columns,
+// nj = 2 or 4, chosen per class by the ensemble's autotuner).
+namespace {
+
+__device__ __forceinline__ int find_problem(const int* __restrict__ first, int np, int tile) {
+    int lo = 0, hi = np - 1;  // largest i with first[i] <= tile
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32) grouped_b2p_kernel(const GroupB2P* __restrict__ pr,
+                                                              const int* __restrict__ first, int np, int total,
+                                                              int* next) {
+    extern __shared__ double smd[];
+    __shared__ int tile_s;
+    for (;;) {
+        if (threadIdx.x == 0) tile_s = atomicAdd(next, 1);
+        __syncthreads();
+        const int tile = tile_s;
+        __syncthreads();
+        if (tile >= total) break;
+        const GroupB2P P = pr[find_problem(first, np, tile)];
+        const int local = tile - P.first;
+        const int m = local / P.ntx, cx = local - m * P.ntx;
+        if (P.nj == 2) b2p_tile<NW, MTW, 2>(P.g, P.in, P.out, P.ln, P.pad, P.SA, m, cx * 16, smd);
+        else b2p_tile<NW, MTW, 4>(P.g, P.in, P.out, P.ln, P.pad, P.SA, m, cx * 32, smd);
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+template <int NW, int MTW>
+__global__ void __launch_bounds__(NW * 32) grouped_fold_kernel(const GroupFold* __restrict__ pr,
+                                                               const int* __restrict__ first, int np, int total,
+                                                               int* next) {
+    extern __shared__ double smd[];
+    __shared__ int tile_s;
+    for (;;) {
+        if (threadIdx.x == 0) tile_s = atomicAdd(next, 1);
+        __syncthreads();
+        const int tile = tile_s;
+        __syncthreads();
+        if (tile >= total) break;
+        const GroupFold P = pr[find_problem(first, np, tile)];
+        const int local = tile - P.first;
+        const int mp = local / P.ntx, cx = local - mp * P.ntx;
+        const int m = mp >> 1, par = mp & 1;
+        if (P.nj == 2) legfold_tile<NW, MTW, 2>(P.g, P.fa, P.RTmax, m, par, cx * 16, smd);
+        else legfold_tile<NW, MTW, 4>(P.g, P.fa, P.RTmax, m, par, cx * 32, smd);
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int group_b2p_prepare(GroupB2P& p) {
+    p.SA = pad16_8(((p.g.NRH + 7) / 8) * 8);
+    const int ct = 8 * p.nj;
+    p.ntx = (2 * p.g.NXCHOPDIM + ct - 1) / ct;
+    return p.ntx * p.g.NTCHOPDIM;
+}
+size_t group_b2p_smem(const GroupB2P& p) { return NST_B2P * (size_t)KCB * (p.SA + SBS) * sizeof(double); }
+
+int group_fold_prepare(GroupFold& p) {
+    p.RTmax = ((p.g.NRCHOPDIM + 1) / 2 + 7) / 8;
+    const int ct = 8 * p.nj;
+    p.ntx = (2 * p.g.NXCHOPDIM + ct - 1) / ct;
+    return p.ntx * 2 * p.g.NTCHOPDIM;
+}
+size_t group_fold_smem(const GroupFold& p) {
+    const int nch = (p.g.NRH + KC2 - 1) / KC2;
+    return (NST_FOLD * ((size_t)p.RTmax * 8 * SA2 + (size_t)2 * KC2 * SX2) + (size_t)KC2 * SX2 + (size_t)nch * KC2) *
+           sizeof(double);
+}
+bool group_supported(const DevGrid& g) { return dmma_supported(g) && (g.NRH + 7) / 8 <= 12 && ((g.NRCHOPDIM + 1) / 2 + 7) / 8 <= 12; }
+
+void k_grouped_b2p(const GroupB2P* d, const int* first, int np, int total, size_t smem, int ctas, int* next,
+                   cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(grouped_b2p_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    cudaMemsetAsync(next, 0, sizeof(int), s);
+    grouped_b2p_kernel<4, 3><<<ctas, 128, smem, s>>>(d, first, np, total, next);
+    count_launch();
+}
+
+void k_grouped_fold(const GroupFold* d, const int* first, int np, int total, size_t smem, int ctas, int* next,
+                    cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(grouped_fold_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    cudaMemsetAsync(next, 0, sizeof(int), s);
+    grouped_fold_kernel<4, 3><<<ctas, 128, smem, s>>>(d, first, np, total, next);
+    count_launch();
 }
 
 }  // namespace mlegs

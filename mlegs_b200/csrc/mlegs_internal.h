@@ -101,6 +101,59 @@ void k_split_fold(const DevGrid& g, int S, const uint8_t* img, const int* eA, in
                   double2* out, int mode, int scale, int accumulate, int pad, int use_w, int* err,
                   uint64_t wait_cycles, cudaStream_t s);
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
+// Fold GEMM arguments (gemm_dmma.cu): RTRAN(-1) and PROJECT's five EOMUL/OEMUL
+// products as K-concatenated segments.
+struct FoldArgs {
+    const double* w[5];  // weights per segment, [m][wt_rows][NRH]
+    const double* x[5];  // inputs per segment, PFF [m][NR][2 NXCHOPDIM]
+    int mode[5];         // 0: EO fold, 1: OE fold
+    int scale[5];        // 0 none, 1 -v, 2 -i m v, 3 i k v, 4 m k v
+    int nseg, split;     // segments [0, split) -> out0, [split, nseg) -> out1
+    double* out0;
+    double* out1;
+    int wt_rows, pad, use_w, accumulate;
+};
+// Grouped persistent GEMMs over the instances of an ensemble (gemm_dmma.cu):
+// one problem per (instance, transform); `first` = its first tile number;
+// nj = 2 or 4 (column tiles of 8 nj columns).  *_prepare fills SA/RTmax and
+// ntx and returns the problem's tile count; *_smem its shared memory.
+struct GroupB2P {
+    DevGrid g;
+    const double* in;
+    double* out;
+    const double* ln;
+    int pad, SA, nj, ntx, first;
+};
+struct GroupFold {
+    DevGrid g;
+    FoldArgs fa;
+    int RTmax, nj, ntx, first;
+};
+bool group_supported(const DevGrid& g);
+int group_b2p_prepare(GroupB2P& p);
+size_t group_b2p_smem(const GroupB2P& p);
+int group_fold_prepare(GroupFold& p);
+size_t group_fold_smem(const GroupFold& p);
+void k_grouped_b2p(const GroupB2P* d, const int* first, int np, int total, size_t smem, int ctas, int* next,
+                   cudaStream_t s);
+void k_grouped_fold(const GroupFold* d, const int* first, int np, int total, size_t smem, int ctas, int* next,
+                    cudaStream_t s);
+// Grouped banded substitutions (solve.cu): one problem per (instance, solve);
+// 64 systems (128 threads: real and imaginary parts) per block, `first` =
+// the problem's first block.
+struct GroupSolve {
+    DevGrid g;
+    const double* F5;
+    const double* F7;
+    const double2* src;
+    double2* dst;
+    double* ln_out;
+    int kind, has_ln;
+    double ln_in;
+    int pad, farfield, first;
+};
+int group_solve_blocks(const GroupSolve& p);
+void k_grouped_solve(const GroupSolve* d, const int* first, int np, int total_blocks, cudaStream_t s);
 // FP64 tensor-path (mma.sync m8n8k4.f64) forms used by k_rtran_b2p / k_fold_gemm when supported.
 bool dmma_supported(const DevGrid& g);
 void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);

@@ -292,12 +292,13 @@ __global__ void factor_kernel(DevGrid g, int kind, double alp, int pad, double* 
 // from src, writes the solution to dst (rows >= the system size are zeroed),
 // then the per-kind tails of solve_kernel; farfield = 1 also applies the
 // CALCAT1 row-0 correction over n < NRCHOP + pad to the m = 0 columns.
-__global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const double* __restrict__ F5,
-                                                             const double* __restrict__ F7, const double2* src,
-                                                             double2* dst, double* ln_out, int kind, int has_ln,
-                                                             double ln_in, int pad, int farfield) {
+// One (system, real or imaginary part) u of the factored substitutions: the
+// body of solve_factored_kernel, also run by the grouped ensemble kernel.
+__device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const double* __restrict__ F5,
+                                                   const double* __restrict__ F7, const double2* src, double2* dst,
+                                                   double* ln_out, int kind, int has_ln, double ln_in, int pad,
+                                                   int farfield, int u) {
     const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int t = u >> 1, comp = u & 1;
     if (t >= nsys) return;
     const int k = t % g.NXCHOPDIM;
@@ -480,6 +481,14 @@ void k_solve_factor(const DevGrid& g, int kind, double alp, int pad, double* F5,
     count_launch();
 }
 
+__global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const double* __restrict__ F5,
+                                                             const double* __restrict__ F7, const double2* src,
+                                                             double2* dst, double* ln_out, int kind, int has_ln,
+                                                             double ln_in, int pad, int farfield) {
+    solve_factored_sys(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield,
+                       blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 void k_solve_factored(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
                       double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s) {
     const int n = 2 * g.NTCHOPDIM * g.NXCHOPDIM;
@@ -507,7 +516,8 @@ void k_solve_del2(const DevGrid& g, double2* a, double* ln_out, int kind, double
 // [row][P+1][system], the right-hand side in place.  The (m, k) = (0, 0)
 // thread first moves the log term's contribution to the right-hand side:
 // rows -= AL + NU AL2, AL2 the DEL2 image of LN (-log(1-x)) and AL = D^(P/2-1) AL2.
-// dq layout: [m][q = 1..HP][row < rows][4q + 1], q's block at rows * q(2q - 1).
+// dq layout: [m][q = 1..HP][row < rows][4q + 1], q's block at rows (q - 1)(2q + 1)
+// within the m block of rows HP (2 HP + 3) doubles.
 template <int HP>
 __global__ void ihelmp_kernel(DevGrid g, const double* dq, int rows, double2* A, const double* ln, double alp,
                               double nu, double* scratch, int pad) {
@@ -521,9 +531,10 @@ __global__ void ihelmp_kernel(DevGrid g, const double* dq, int rows, double2* A,
     if (nn > rows) nn = rows;
     if (nn <= 0) return;
     const double K2 = g.ak[k] * g.ak[k];
-    const size_t mstride = (size_t)rows * HP * (2 * HP + 1);  // sum_q (4q + 1) rows
+    const size_t mstride = (size_t)rows * HP * (2 * HP + 3);  // rows * sum_{q <= HP} (4q + 1)
     const double* dm = dq + (size_t)m * mstride;
-    auto dq_row = [&](int q, int r) { return dm + (size_t)rows * q * (2 * q - 1) + (size_t)r * (4 * q + 1); };
+    // q's block starts after rows * sum_{q' < q} (4q' + 1) = rows (q - 1)(2q + 1)
+    auto dq_row = [&](int q, int r) { return dm + (size_t)rows * (q - 1) * (2 * q + 1) + (size_t)r * (4 * q + 1); };
     double2* col = A + (size_t)m * g.NRCHOPDIM * g.NXCHOPDIM + k;
     const size_t st = g.NXCHOPDIM;
     if (m == 0 && k == 0) {
@@ -631,6 +642,30 @@ void k_ihelmp(const DevGrid& g, int P, const double* dq, int rows, double2* a, c
         case 12: ihelmp_kernel<6><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
         default: ihelmp_kernel<7><<<nb, bs, 0, s>>>(g, dq, rows, a, ln, alp, nu, scratch, pad); break;
     }
+    count_launch();
+}
+
+// Grouped factored substitutions over the instances of an ensemble: each
+// block belongs to one problem (found by binary search over `first`), 64
+// systems per block.
+__global__ void __launch_bounds__(128) grouped_solve_kernel(const GroupSolve* __restrict__ pr,
+                                                            const int* __restrict__ first, int np) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const GroupSolve P = pr[lo];
+    solve_factored_sys(P.g, P.F5, P.F7, P.src, P.dst, P.ln_out, P.kind, P.has_ln, P.ln_in, P.pad, P.farfield,
+                       (b - P.first) * 128 + threadIdx.x);
+}
+
+int group_solve_blocks(const GroupSolve& p) { return (2 * p.g.NTCHOPDIM * p.g.NXCHOPDIM + 127) / 128; }
+
+void k_grouped_solve(const GroupSolve* d, const int* first, int np, int total_blocks, cudaStream_t s) {
+    grouped_solve_kernel<<<total_blocks, 128, 0, s>>>(d, first, np);
     count_launch();
 }
 

@@ -150,3 +150,33 @@ def roundtrip_coefficients(cfg, fid):
     for mm in range(shape[1]):
         e[max(cfg.nrchop - mm, 0):, mm, :] = 0.0
     return e
+
+
+ENSEMBLE_NR = (48, 64, 96, 128, 192)
+ENSEMBLE_NTH = (32, 64, 128)
+ENSEMBLE_NX = (32, 64, 128, 256)
+
+
+def ensemble_configs(n=64, seed=2024, nrs=ENSEMBLE_NR, nths=ENSEMBLE_NTH, nxs=ENSEMBLE_NX):
+    """The batched-run configuration: n independent AB2-CN runs with (NR, NTH,
+    NX) drawn uniformly from nrs x nths x nxs, Re uniform in [500, 5000] (NU =
+    KAPPA = 1/Re), N uniform in [0.5, 4], dt = 1e-3, the AB2-CN IVP physics
+    otherwise (Omega = 1, VISC%SW = 1) and its initial condition (q-vortex plus
+    a perturbation of amplitude 1e-3 in |m|, |k| <= 4 decaying as exp(-n/8)),
+    seeded per instance; chops by the 2/3 rule (chops())."""
+    import numpy as np
+
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for i in range(n):
+        nr = int(rng.choice(nrs))
+        nth = int(rng.choice(nths))
+        nx = int(rng.choice(nxs))
+        re = float(rng.uniform(500.0, 5000.0))
+        bv0 = float(rng.uniform(0.5, 4.0))
+        nrc, ntc, nxc = chops(nr, nth, nx)
+        out.append(Config("ens%02d_%dx%dx%d" % (i, nr, nth, nx), nr, nth, nx, nrc, ntc, nxc, dt=1e-3, nsteps=50,
+                          adams=True, omega=1.0, bv0=bv0, visc_sw=1, nu=1.0 / re, kappa=1.0 / re, amp=1e-3,
+                          mmax=4, kmax=4, decay=8.0, seed=1234 + 7 * i,
+                          notes=["Re = %.1f, N = %.3f" % (re, bv0)]))
+    return out

@@ -383,28 +383,44 @@ void mlegs_ensemble::prepare() {
     prepared = true;
 }
 
+// Launch errors are attributed to the stage that raised them (outside capture).
+static void stage_check(bool capturing, const char* stage) {
+    if (capturing) return;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError(std::string("ensemble ") + stage + ": " + cudaGetErrorString(e));
+}
+
 void mlegs_ensemble::step() {
     gb2p.h.clear();
     gfold.h.clear();
     gs1.h.clear();
     gs2.h.clear();
     for (EnsInst& I : st) phase0(*this, I);
+    stage_check(capturing, "phase 0");
     join_to_group();
     launch_b2p();
+    stage_check(capturing, "grouped RTRAN(+1)");
     group_to_all();
     for (EnsInst& I : st) phase1(*this, I);
+    stage_check(capturing, "phase 1");
     join_to_group();
     launch_fold();
+    stage_check(capturing, "grouped folds");
     group_to_all();
     for (EnsInst& I : st) phase2(*this, I);
+    stage_check(capturing, "phase 2");
     join_to_group();
     launch_solve(gs1);
+    stage_check(capturing, "grouped IDEL2LN");
     group_to_all();
     for (EnsInst& I : st) phase3(*this, I);
+    stage_check(capturing, "phase 3");
     join_to_group();
     launch_solve(gs2);
+    stage_check(capturing, "grouped IHELM");
     group_to_all();
     for (EnsInst& I : st) phase4(*this, I);
+    stage_check(capturing, "phase 4");
     join_to_group();
 }
 

@@ -753,6 +753,9 @@ __global__ void __launch_bounds__(NW * 32) grouped_fold_kernel(const GroupFold* 
 
 }  // namespace
 
+// the grouped kernels also hold a static work-item slot in shared memory
+constexpr int kGroupedSmemMax = 227 * 1024 - 128;
+
 int group_b2p_prepare(GroupB2P& p) {
     p.SA = pad16_8(((p.g.NRH + 7) / 8) * 8);
     const int ct = 8 * p.nj;
@@ -778,7 +781,7 @@ void k_grouped_b2p(const GroupB2P* d, const int* first, int np, int total, size_
                    cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(grouped_b2p_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(grouped_b2p_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupedSmemMax);
         attr = true;
     }
     cudaMemsetAsync(next, 0, sizeof(int), s);
@@ -790,7 +793,7 @@ void k_grouped_fold(const GroupFold* d, const int* first, int np, int total, siz
                     cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(grouped_fold_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(grouped_fold_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupedSmemMax);
         attr = true;
     }
     cudaMemsetAsync(next, 0, sizeof(int), s);

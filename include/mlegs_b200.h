@@ -320,6 +320,74 @@ int mlegs_ensemble_sync(mlegs_ensemble* e);
 int64_t mlegs_ensemble_launch_count(const mlegs_ensemble* e);
 void* mlegs_ensemble_stream(mlegs_ensemble* e);
 
+/* ---- Adjoint (vector-Jacobian products) of the AB2-CN path.  No counterpart in
+ * the reference (it has no adjoint); these replace nothing and bind only from
+ * the Python gradient path.  Transposes are for the real inner product
+ * <a, b> = sum(Re a Re b + Im a Im b) over the stored entries, plus LN_a LN_b
+ * where a field's log term enters the map.  FP64 contexts only; the step maps
+ * and VJPs need AB2-CN with VISC%SW = 1.  Synchronise with mlegs_sync before
+ * the host reads results. */
+
+/* One transpose (op: MLEGS_T_* below) at CHOPSET(pad): y[] the cotangents of
+ * the operator's outputs, x[] receives those of its inputs.  p1: ALP for
+ * MLEGS_T_IHELM, NU for MLEGS_T_VISC2 (DT from the context). */
+#define MLEGS_T_RTRAN_P      0   /* RTRAN(+1)^T:  y PFF -> x FFF (with LN)            */
+#define MLEGS_T_RTRAN_M      1   /* RTRAN(-1)^T:  y FFF -> x PFF                      */
+#define MLEGS_T_VERFFT_P     2   /* VERFFT(+1)^T: y PFP -> x PFF                      */
+#define MLEGS_T_VERFFT_M     3   /* VERFFT(-1)^T: y PFF -> x PFP                      */
+#define MLEGS_T_HORFFT_P     4   /* HORFFT(+1)^T: y PPP -> x PFP                      */
+#define MLEGS_T_HORFFT_M     5   /* HORFFT(-1)^T: y PFP -> x PPP                      */
+#define MLEGS_T_TOFP         6   /* TOFP^T:  y PPP -> x FFF (with LN)                 */
+#define MLEGS_T_TOFF         7   /* TOFF^T:  y FFF -> x PPP                           */
+#define MLEGS_T_XXDX         8   /* XXDX^T   (with LN)                                */
+#define MLEGS_T_MULXM        9   /* MULXM^T                                           */
+#define MLEGS_T_DELSQH      10   /* DELSQH^T (with LN)                                */
+#define MLEGS_T_DEL2        11   /* DEL2^T   (with LN)                                */
+#define MLEGS_T_GRAD        12   /* GRAD^T:   y[3] -> x[0]                            */
+#define MLEGS_T_PC2VEL      13   /* PC2VEL^T: y[3] -> x[0] psi, x[1] chi              */
+#define MLEGS_T_PC2VOR      14   /* PC2VOR^T: y[3] -> x[0] psi, x[1] chi              */
+#define MLEGS_T_IDEL2LN     15   /* IDEL2LN^T at CHOPSET(0): y (with LN) -> x         */
+#define MLEGS_T_IHELM       16   /* IHELM^T at CHOPSET(0): y (with LN) -> x (with LN) */
+#define MLEGS_T_PROJECT_PPP 17   /* PROJECT(.., PSI, W, 0.0) of PPP inputs: y[0] PSI, y[1] W -> x[3] PPP */
+#define MLEGS_T_VISC2       18   /* VISC2^T: y -> x[0] A, x[1] AO                     */
+#define MLEGS_T_IDELSQH     19   /* IDELSQH^T (y with LN)                             */
+#define MLEGS_T_FARFIELD    20   /* the far-field fix (CALCAT1) transposed            */
+int mlegs_transpose(mlegs_ctx* ctx, int op, const mlegs_field* const* y, mlegs_field* const* x, int pad, double p1);
+
+/* VJP of CALC_BOUSSI_FORCE (mod_boussinesq.f90:317-410) at (psi, chi, b):
+ * output cotangents (psin_bar, chin_bar with LN, bn_bar) -> input cotangents. */
+int mlegs_boussi_force_vjp(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
+                           const mlegs_field* psin_bar, const mlegs_field* chin_bar, const mlegs_field* bn_bar,
+                           mlegs_field* psi_bar, mlegs_field* chi_bar, mlegs_field* b_bar);
+
+/* One steady STEP_BOUSSI_AB_CN (mod_march.f90:609-661) as a map of the state
+ * (psi, chi, b, n_psi, n_chi, n_b) = in[6] -> out[6], and its VJP at state[3]
+ * (psi, chi, b before the step): bar[6] -> out[6].  The map leaves the
+ * context's own solver state, history and time unchanged. */
+int mlegs_ab2_step_map(mlegs_ctx* ctx, const mlegs_field* const* in, mlegs_field* const* out);
+int mlegs_ab2_step_vjp(mlegs_ctx* ctx, const mlegs_field* const* state, const mlegs_field* const* bar,
+                       mlegs_field* const* out);
+/* RICH_BOUSSI_FE_BE (535-606) as the map (psi, chi, b) = in[3] -> out[6]
+ * (state and history), and its VJP at state[3]: bar[6] -> out[3]. */
+int mlegs_ab2_startup_map(mlegs_ctx* ctx, const mlegs_field* const* in, mlegs_field* const* out);
+int mlegs_ab2_startup_vjp(mlegs_ctx* ctx, const mlegs_field* const* state, const mlegs_field* const* bar,
+                          mlegs_field* const* out);
+/* Transpose of the seeded initial state psi = vortex + IDELSQH(-c_psi), chi
+ * likewise, b = c_b with the CALCAT1 far-field fix: state_bar[3] -> coef_bar[3]. */
+int mlegs_initial_state_T(mlegs_ctx* ctx, const mlegs_field* const* state_bar, mlegs_field* const* coef_bar);
+/* J = fluctuation kinetic energy (CALC_BOUSSI_ENERGY's quadrature,
+ * mod_boussinesq.f90:176-206, without the (m, k) = (0, 0) part) + 1/2 int b^2 dV
+ * (CALC_BOUSSI_PE's quadrature, 112-136) and its gradient (gpsi, gchi, gb).
+ * Synchronises the context's stream. */
+int mlegs_energy_objective(mlegs_ctx* ctx, const mlegs_field* psi, const mlegs_field* chi, const mlegs_field* b,
+                           double* J, mlegs_field* gpsi, mlegs_field* gchi, mlegs_field* gb);
+/* Device-to-device copy between a field and a caller's device buffer in the
+ * device layout of `space` (FFF [m][n][k], PFF [m][r][k], PFP [r][z][m], PPP
+ * [r][z][j], complex doubles): to_field 1 copies dev -> f (and LN from ln_dev,
+ * or LN 0 when ln_dev is null), 0 copies f -> dev (LN to ln_dev when given).
+ * Ordered on the context's stream. */
+int mlegs_field_device_copy(mlegs_ctx* ctx, mlegs_field* f, int to_field, int space, void* dev, double* ln_dev);
+
 /* Kernel timing for profiling and roofline reports: launches one internal
  * kernel `reps` times on scratch fields of this context, bracketed by CUDA
  * events on the context's stream, and returns the mean device time per launch

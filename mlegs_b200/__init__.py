@@ -91,6 +91,7 @@ class Context:
         self.lib = _lib.load()
         self.cfg = cfg
         self._owned = True
+        self.device = int(device)
         p = params_of(cfg, precision, split_slices, device)
         h = ctypes.c_void_p()
         rc = self.lib.mlegs_create(ctypes.byref(p), ctypes.byref(h))
@@ -279,6 +280,71 @@ class Context:
         out = np.empty((self.NRH, self.NRCHOPDIM + 1, self.NTCHOPDIM), dtype=np.float64, order="F")
         self._ck(self.lib.mlegs_legendre_table(self.c, out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+    # ------------------------------------------------------------ adjoint
+    # Transposes and VJPs of the AB2-CN path (include/mlegs_b200.h, MLEGS_T_*);
+    # cotangents are fields like any other, LN included where the map uses it.
+    T_OPS = {"RTRAN+1": 0, "RTRAN-1": 1, "VERFFT+1": 2, "VERFFT-1": 3, "HORFFT+1": 4, "HORFFT-1": 5,
+             "TOFP": 6, "TOFF": 7, "XXDX": 8, "MULXM": 9, "DELSQH": 10, "DEL2": 11, "GRAD": 12,
+             "PC2VEL": 13, "PC2VOR": 14, "IDEL2LN": 15, "IHELM": 16, "PROJECT_PPP": 17, "VISC2": 18,
+             "IDELSQH": 19, "FARFIELD": 20}
+
+    @staticmethod
+    def _handles(fields):
+        arr = (ctypes.c_void_p * len(fields))(*[f.h for f in fields])
+        return arr, ctypes.cast(arr, ctypes.c_void_p)
+
+    def TRANSPOSE(self, op, ys, xs, pad=0, p1=0.0):
+        """Transpose of one operator (name in T_OPS) at CHOPSET(pad): ys, the
+        cotangents of its outputs -> xs, those of its inputs."""
+        ya, yp = self._handles(list(ys))
+        xa, xp = self._handles(list(xs))
+        self._ck(self.lib.mlegs_transpose(self.c, self.T_OPS[op], yp, xp, int(pad), float(p1)))
+
+    def CALC_BOUSSI_FORCE_VJP(self, psi, chi, b, psin_bar, chin_bar, bn_bar, psi_bar, chi_bar, b_bar):
+        self._ck(self.lib.mlegs_boussi_force_vjp(self.c, psi.h, chi.h, b.h, psin_bar.h, chin_bar.h, bn_bar.h,
+                                                 psi_bar.h, chi_bar.h, b_bar.h))
+
+    def AB2_STEP_MAP(self, ins, outs):
+        """One steady STEP_BOUSSI_AB_CN of (psi, chi, b, n_psi, n_chi, n_b)."""
+        ia, ip = self._handles(list(ins))
+        oa, op = self._handles(list(outs))
+        self._ck(self.lib.mlegs_ab2_step_map(self.c, ip, op))
+
+    def AB2_STEP_VJP(self, state, bars, outs):
+        sa, sp = self._handles(list(state))
+        ba, bp = self._handles(list(bars))
+        oa, op = self._handles(list(outs))
+        self._ck(self.lib.mlegs_ab2_step_vjp(self.c, sp, bp, op))
+
+    def AB2_STARTUP_MAP(self, ins, outs):
+        """RICH_BOUSSI_FE_BE of (psi, chi, b) -> (psi, chi, b, n_psi, n_chi, n_b)."""
+        ia, ip = self._handles(list(ins))
+        oa, op = self._handles(list(outs))
+        self._ck(self.lib.mlegs_ab2_startup_map(self.c, ip, op))
+
+    def AB2_STARTUP_VJP(self, state, bars, outs):
+        sa, sp = self._handles(list(state))
+        ba, bp = self._handles(list(bars))
+        oa, op = self._handles(list(outs))
+        self._ck(self.lib.mlegs_ab2_startup_vjp(self.c, sp, bp, op))
+
+    def INITIAL_STATE_T(self, state_bar, coef_bar):
+        sa, sp = self._handles(list(state_bar))
+        ca, cp = self._handles(list(coef_bar))
+        self._ck(self.lib.mlegs_initial_state_T(self.c, sp, cp))
+
+    def ENERGY_OBJECTIVE(self, psi, chi, b, gpsi, gchi, gb):
+        """J = fluctuation KE + 1/2 int b^2 dV; its gradient into (gpsi, gchi, gb)."""
+        J = ctypes.c_double()
+        self._ck(self.lib.mlegs_energy_objective(self.c, psi.h, chi.h, b.h, ctypes.byref(J), gpsi.h, gchi.h, gb.h))
+        return J.value
+
+    def DEVICE_COPY(self, f, to_field, space, ptr, ln_ptr=None):
+        """Device-to-device copy between field f and a device buffer (device layout)."""
+        self._ck(self.lib.mlegs_field_device_copy(self.c, f.h, 1 if to_field else 0, int(space),
+                                                  ctypes.c_void_p(int(ptr)),
+                                                  None if ln_ptr is None else ctypes.c_void_p(int(ln_ptr))))
 
     # ------------------------------------------------------------ diagnostics
     def _mk_array(self):

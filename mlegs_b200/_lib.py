@@ -114,6 +114,15 @@ SIGNATURES = {
     "mlegs_ensemble_sync": (c_int, [c_void_p]),
     "mlegs_ensemble_launch_count": (c_int64, [c_void_p]),
     "mlegs_ensemble_stream": (c_void_p, [c_void_p]),
+    "mlegs_transpose": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int, c_double]),
+    "mlegs_boussi_force_vjp": (c_int, [c_void_p] + [c_void_p] * 9),
+    "mlegs_ab2_step_map": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mlegs_ab2_step_vjp": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_ab2_startup_map": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mlegs_ab2_startup_vjp": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mlegs_initial_state_T": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mlegs_energy_objective": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, dptr, c_void_p, c_void_p, c_void_p]),
+    "mlegs_field_device_copy": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "mlegs_launch_count": (c_int64, [c_void_p]),
     "mlegs_reset_launch_count": (None, [c_void_p]),
     "mlegs_stream": (c_void_p, [c_void_p]),

@@ -395,7 +395,7 @@ void mlegs_ctx::init(const mlegs_params& prm) {
     }
 
     // --- memory: LN slots, scratch buffers, temporaries, history
-    nslots = 256;
+    nslots = 512;
     lnslots = dalloc<double>(nslots);
     CK(cudaMemsetAsync(lnslots, 0, nslots * sizeof(double), s));
     scratch = dalloc<double2>(d.cap());

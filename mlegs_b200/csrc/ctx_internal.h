@@ -8,6 +8,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <algorithm>
 #include <initializer_list>
@@ -123,6 +124,16 @@ struct mlegs_ctx {
     std::vector<Field*> pool;                         // free temporaries (stack)
     std::vector<Field*> temps;                        // all temporaries
     Field* hist[7] = {};
+
+    // adjoint (adjoint.cu), formed on first use: the grid with transposed band
+    // tables, PROJECT's weights in PF's row stride, a reduction slot, NORM(1:3, m = 0)
+    // on the host and the scratch state of the step and start-up maps
+    bool adj_ready = false;
+    DevGrid gT{};
+    double* adj_w[3] = {};
+    double* adj_dot = nullptr;
+    double adj_n0[3] = {};
+    Field* adj_state[6] = {};
 
     // solver state
     Field *psi = nullptr, *chi = nullptr, *b = nullptr;
@@ -340,13 +351,13 @@ struct mlegs_ctx {
         double alp;
         double *F5, *F7;
     };
-    std::vector<SolveFactors> sfac;
+    std::deque<SolveFactors> sfac;  // a deque: entries stay put as the cache grows
     const SolveFactors* factors(int kind, int pad, double alp) {
         for (const SolveFactors& f : sfac)
             if (f.kind == kind && f.pad == pad && f.alp == alp) return &f;
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         CK(cudaStreamIsCapturing(s, &cs));
-        if (cs != cudaStreamCaptureStatusNone || sfac.size() >= 8 || pad < 0 || d.NRCHOP + pad > d.NRCHOPDIM)
+        if (cs != cudaStreamCaptureStatusNone || sfac.size() >= 16 || pad < 0 || d.NRCHOP + pad > d.NRCHOPDIM)
             return nullptr;
         size_t n5, n7;
         solve_factor_sizes(g, &n5, &n7);

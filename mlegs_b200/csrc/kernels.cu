@@ -198,6 +198,8 @@ void k_logterm_rows(const DevGrid& g, double2* b, const double* ln, int which, d
 // m/k combinations of PC2VEL, PC2VOR and GRAD (rows n < NN, zero beyond):
 //  op 0: i m x + i k y    op 1: -y - m k x    op 2: -i m x + i k y
 //  op 3:  y - k m x       op 4: i m x         op 5: i k x          op 6: -x
+//  and the conjugate factors of their transposes:
+//  op 7: -i m x           op 8: -i k x        op 9: m k x          op 10: -m k x
 __global__ void mk_kernel(DevGrid g, int op, const double2* x, const double2* y, double2* out, int pad) {
     size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
@@ -217,6 +219,10 @@ __global__ void mk_kernel(DevGrid g, int op, const double2* x, const double2* y,
             case 3: v = make_double2(yv.x - (kv * mv) * xv.x, yv.y - (kv * mv) * xv.y); break;
             case 4: v = cmuli(xv, mv); break;
             case 5: v = cmuli(xv, kv); break;
+            case 7: v = cmuli(xv, -mv); break;
+            case 8: v = cmuli(xv, -kv); break;
+            case 9: v = cscale(xv, mv * kv); break;
+            case 10: v = cscale(xv, -(mv * kv)); break;
             default: v = make_double2(-xv.x, -xv.y); break;
         }
     }

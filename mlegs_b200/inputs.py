@@ -75,6 +75,14 @@ CONFIGS = {
         notes=["VISC%SW=3: Re=5000 has no effect (CALC_BOUSSI_VISC_CN returns, mod_march.f90:1251)"]),
     # Transform round trips at 256^3 (batch of 8 fields; chi, psi, b coefficients).
     "roundtrip_256": Config("roundtrip_256", 256, 256, 256, 170, 170, 85, decay=10.0),
+    # Gradient of the final fluctuation KE + buoyancy variance after the
+    # start-up and 200 AB2-CN steps w.r.t. the perturbation coefficients
+    # (checkpoints every 20 steps).
+    "grad_96x64x64": Config(
+        "grad_96x64x64", 96, 64, 64, 64, 42, 21, dt=1e-3, nsteps=200, adams=True,
+        omega=1.0, bv0=1.0, visc_sw=1, nu=1.0 / 2000, kappa=1.0 / 2000, amp=1e-4, mmax=4, kmax=4, decay=8.0,
+        notes=["Re = 2000: NU = 1/2000; KAPPA unspecified: Pr = 1 (KAPPA = NU)",
+               "checkpoint every 20 steps with recomputation"]),
 }
 
 

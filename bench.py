@@ -35,6 +35,13 @@ form (FP64 and split-BF16 S = 4, 5, 6): device time per round trip and the
 relative error of PPP and of the returned FFF against the FP64 oracle for the
 chi, psi and b coefficient sets (mlegs_b200.inputs.roundtrip_coefficients).
 
+"gradient" is the gradient configuration: J = fluctuation KE + 1/2 int b^2
+after the AB2-CN start-up and 200 steps at 96x64x64, differentiated with
+respect to the perturbation coefficients through torch.autograd on the
+device (step maps and VJPs of the library, checkpoints every 20 steps):
+seconds per gradient beside the graph-replayed forward alone, and central
+differences on two random directions.
+
 --impl reference times the reference's path as restated on the CPU (the
 numpy/scipy FP64 oracle under oracle/, all host cores): the reference itself
 is Fortran 90 + MPI + FFTW + MKL and cannot be built in this image, so that
@@ -73,6 +80,7 @@ def parse():
                     help="steps (start-up included) of the oracle trajectory the GPU paths are checked against")
     ap.add_argument("--no-roundtrip", action="store_true", help="skip the 256^3 transform round-trip leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the adjoint gradient leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     return ap.parse_args()
@@ -368,6 +376,63 @@ def ensemble_leg(local, n=64, steps=50, warm=3):
                        "ctas_per_sm": {"rtran+1": ctas[0], "fold": ctas[1]}}}
 
 
+def gradient_leg(local, fd_directions=2):
+    """The gradient configuration (grad_96x64x64): J = fluctuation KE + 1/2
+    int b^2 after the AB2-CN start-up and 200 steps, differentiated with
+    respect to the perturbation coefficients through torch.autograd (device
+    step maps and VJPs, checkpoints every 20 steps).  Wall-clock seconds per
+    gradient (host-driven: each step and VJP call synchronises) beside the
+    forward alone on the context's graph-replayed solver, and central
+    differences on a few random directions."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import mlegs_b200 as M
+    from mlegs_b200.adjoint import DeviceAB2, gradient, objective_of, ref_to_dev
+    from mlegs_b200.checkpoint import LoopStats
+    from mlegs_b200.inputs import CONFIGS, perturbation_coefficients
+    cfg = CONFIGS["grad_96x64x64"]
+    ctx = M.Context(cfg, device=local)
+    try:
+        solver = DeviceAB2(ctx)
+        cs = [ref_to_dev(perturbation_coefficients(cfg, i)) for i in range(3)]
+        gradient(solver, cs, nsteps=4, every=2)  # set-up: factors, transposed tables, temporaries
+        objective_of(solver, cs, cfg.nsteps)
+        torch.cuda.synchronize(local)
+        stats = LoopStats()
+        l0 = ctx.launches()
+        t0 = time.perf_counter()
+        J, grads = gradient(solver, cs, nsteps=cfg.nsteps, every=20, stats=stats)
+        torch.cuda.synchronize(local)
+        t_grad = time.perf_counter() - t0
+        launches = ctx.launches() - l0
+        t0 = time.perf_counter()
+        J_fwd = objective_of(solver, cs, cfg.nsteps)
+        torch.cuda.synchronize(local)
+        t_fwd = time.perf_counter() - t0
+        rng = np.random.default_rng(7)
+        scale = max(float(c.abs().max()) for c in cs)
+        h, errs = 1e-5, []
+        for _ in range(fd_directions):
+            d = [torch.from_numpy((rng.standard_normal(c.shape) + 1j * rng.standard_normal(c.shape)) * scale)
+                 for c in cs]
+            fd = (objective_of(solver, [c + h * e for c, e in zip(cs, d)], cfg.nsteps)
+                  - objective_of(solver, [c - h * e for c, e in zip(cs, d)], cfg.nsteps)) / (2 * h)
+            an = sum(float((g.cpu() * e.conj()).real.sum()) for g, e in zip(grads, d))
+            errs.append(abs(fd - an) / abs(an))
+    finally:
+        ctx.close()
+    return {"workload": cfg.name, "grid": [cfg.nr, cfg.nth, cfg.nx], "steps": cfg.nsteps, "checkpoint_every": 20,
+            "J": J, "J_forward_only": J_fwd, "seconds_per_gradient": t_grad,
+            "seconds_forward_only_graph": t_fwd, "gradient_over_forward": t_grad / t_fwd,
+            "checkpoints": stats.checkpoints, "recomputed_steps": stats.recomputed_steps,
+            "vjp_steps": stats.vjp_steps, "peak_states": stats.peak_states, "gpu_launches": int(launches),
+            "fd_directions": fd_directions, "fd_max_rel_error": max(errs),
+            "timing": "wall clock around the host-driven gradient (every step map and VJP synchronises)"}
+
+
 def run_reference(args, cfg, ws, rank):
     if rank != 0:
         return
@@ -541,6 +606,9 @@ def run_ours(args, cfg, ws, rank, local):
     ensl = None
     if rank == 0 and ws == 1 and not args.no_ensemble:
         ensl = ensemble_leg(local)
+    gradl = None
+    if rank == 0 and ws == 1 and not args.no_gradient:
+        gradl = gradient_leg(local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -564,6 +632,7 @@ def run_ours(args, cfg, ws, rank, local):
                         "d2h_bytes_per_step": 3 * nbytes},
                 "gpu_launches": int(launches), "precision_comparison": compare,
                 "roofline": roof, "kernels": kernels, "transform_roundtrip": rtrip, "ensemble": ensl,
+                "gradient": gradl,
                 "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmlegs_b200.so")
-SOURCES = ["tables.cu", "kernels.cu", "fft.cu", "gemm.cu", "gemm_dmma.cu", "solve.cu", "phys.cu", "ctx.cu", "solve_static.cu", "split_gemm.cu", "hyperadj.cu", "ensemble.cu", "adjoint.cu"]
+SOURCES = ["tables.cu", "kernels.cu", "fft.cu", "gemm.cu", "gemm_dmma.cu", "solve.cu", "phys.cu", "ctx.cu", "solve_static.cu", "split_gemm.cu", "hyperadj.cu", "ensemble.cu", "adjoint.cu", "gemm_bulk.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -283,6 +283,16 @@ void mlegs_ctx::init(const mlegs_params& prm) {
         k_proj_comp(g, D, 1, compD, s);
         k_proj_comp(g, T, 0, compT, s);
     }
+    if (p.precision == MLEGS_PREC_FP64 && fold_bulk_supported(g, d.NRCHOPDIM + 1)) {
+        fc_pf = dalloc<double>(fold_table_doubles(g, d.NRCHOPDIM + 1));
+        k_fold_table(g, pf, d.NRCHOPDIM + 1, 1, fc_pf, s);
+        double** fcs[3] = {&fc_V, &fc_D, &fc_T};
+        const double* W[3] = {V, D, T};
+        for (int q = 0; q < 3; ++q) {
+            *fcs[q] = dalloc<double>(fold_table_doubles(g, d.NRCHOPDIM));
+            k_fold_table(g, W[q], d.NRCHOPDIM, 0, *fcs[q], s);
+        }
+    }
 
     // --- FFT twiddles (host long double, rounded once)
     auto lg2 = [](int v) { int l = 0; while ((1 << l) < v) ++l; return l; };
@@ -1328,6 +1338,8 @@ int mlegs_sync(mlegs_ctx* ctx) {
             CK(cudaMemset(ctx->split_err, 0, sizeof(int)));
             throw ApiError(MLEGS_ERR_TIMEOUT, "tensor-core GEMM: a bounded wait timed out (results invalid)");
         }
+        if (bulk_gemm_error(true) > 0)
+            throw ApiError(MLEGS_ERR_TIMEOUT, "RTRAN(+1) GEMM: a bounded pipeline wait timed out (results invalid)");
     });
 }
 
@@ -1992,7 +2004,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
         auto launch = [&]() {
             switch (kernel) {
                 case 0: k_rtran_b2p(g, a->data, b->data, nullptr, 0, s); break;
-                case 1: k_fold_gemm(g, ctx->pf, d.NRCHOPDIM + 1, a->data, b->data, 2, 0, 0, 0, s); break;
+                case 1: ctx->fold(0, ctx->pf, d.NRCHOPDIM + 1, a->data, b->data, 0 | 2, 0, 0, 0, s); break;
                 case 2:
                     if (!k_verfft4(g, ctx->fft, a->data, b->data, +1, s)) k_verfft_b(g, ctx->fft, a->data, b->data, s);
                     break;
@@ -2049,7 +2061,9 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     break;
                 case 13: {  // PROJECT's fold products: f9[0..2] (PFF) -> b, c (FFF)
                     const int wr = d.NRCHOPDIM;
-                    if (!ctx->split_S && dmma_supported(g)) {
+                    if (!ctx->split_S && ctx->fc_V) {
+                        ctx->project_bulk(f9[0]->data, f9[1]->data, f9[2]->data, b->data, c->data, s);
+                    } else if (!ctx->split_S && dmma_supported(g)) {
                         k_project_dmma(g, ctx->V, ctx->D, ctx->T, f9[0]->data, f9[1]->data, f9[2]->data, b->data,
                                        c->data, s);
                     } else {

@@ -88,6 +88,9 @@ struct mlegs_ctx {
     double nup3[3] = {0, 0, 0}, kap3[3] = {0, 0, 0};
     Hyp3State adj;
     double *compV = nullptr, *compD = nullptr, *compT = nullptr;  // PROJECT composites (FP64 contexts)
+    // chunked weight tables of the bulk fold GEMMs (FP64 contexts): PF times w_i
+    // (RTRAN(-1)) and V, D, T (PROJECT of PFF inputs)
+    double *fc_pf = nullptr, *fc_V = nullptr, *fc_D = nullptr, *fc_T = nullptr;
     double *v2p_pff = nullptr, *v2p_fff = nullptr;                 // VEL2PLN coefficient vectors
     double* diag = nullptr;                                         // 4 x [m][k] quadratures (energy)
     double *sp_damp = nullptr, *sp_damp_h = nullptr;                // sponge factors for DT and DT/2 (RMV%SW = 2)
@@ -112,11 +115,20 @@ struct mlegs_ctx {
     void fold(int w, const double* Wt, int wt_rows, const double2* in, double2* out, int mode, int scale,
               int accumulate, int pad, cudaStream_t st = nullptr) {
         if (!st) st = s;
-        if (split_S)
+        if (split_S) {
             k_split_fold(g, split_S, fimg[w], feA[w], wt_rows, in, out, mode & 1, scale, accumulate, pad,
                          (mode & 2) ? 1 : 0, split_err, split_wait, st);
-        else
-            k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, st);
+            return;
+        }
+        // RTRAN(-1) (PF with the Gauss weights) on the bulk-copy pipeline when its table exists
+        if (w == 0 && (mode & 2) && Wt == pf && fc_pf) {
+            const double* wc[1] = {fc_pf};
+            const double2* x[1] = {in};
+            const int md[1] = {mode & 1}, sc[1] = {scale};
+            k_fold_bulk(g, wc, x, md, sc, 1, 1, out, nullptr, wt_rows, pad, accumulate, st);
+            return;
+        }
+        k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, st);
     }
     double2* staging = nullptr;
     int* dflag = nullptr;
@@ -514,6 +526,11 @@ struct mlegs_ctx {
             ln_zero(psi_);
             ln_zero(chi_);
         }
+        if (!split_S && fc_V) {
+            project_bulk(rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
+            k_farfield_fix(g, psi_->data, d.NRCHOP, s);
+            return;
+        }
         if (!split_S && dmma_supported(g)) {
             k_project_dmma(g, V, D, T, rur->data, rup->data, uz->data, psi_->data, chi_->data, s);
             k_farfield_fix(g, psi_->data, d.NRCHOP, s);
@@ -530,6 +547,16 @@ struct mlegs_ctx {
         k_farfield_fix(g, psi_->data, d.NRCHOP, s);
     }
 
+    // PROJECT's five fold products of PFF inputs (mod_legops.f90:2497-2535) on
+    // the bulk-copy pipeline: PSI = -(i m) EO(V, RUR) - OE(D, RUP),
+    // CHI = (i k) OE(D, RUR) + m k EO(V, RUP) - EO(T, UZ).
+    void project_bulk(const double2* rur, const double2* rup, const double2* uz, double2* psi_, double2* chi_,
+                      cudaStream_t st) {
+        const double* wc[5] = {fc_V, fc_D, fc_D, fc_V, fc_T};
+        const double2* x[5] = {rur, rup, rur, rup, uz};
+        const int md[5] = {0, 1, 1, 0, 0}, sc[5] = {2, 1, 3, 4, 1};
+        k_fold_bulk(g, wc, x, md, sc, 5, 2, psi_, chi_, d.NRCHOPDIM, 0, 0, st);
+    }
     // PROJECT(RUR, RUP, UZ, PSI, CHI) with PSI%LN by reference (ln_mode 2) for
     // FFF inputs whose LN terms are zero: one composite FFF -> FFF product per m
     // in FP64 contexts (RUP's (0, 0) column is changed in place by VEL2PLN).

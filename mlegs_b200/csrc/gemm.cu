@@ -102,6 +102,10 @@ __global__ void __launch_bounds__(128) rtran_b2p_kernel(DevGrid g, const double*
 }
 
 void k_rtran_b2p(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
+    if (b2p_bulk_supported(g)) {
+        k_rtran_b2p_bulk(g, a, b, ln, pad, s);
+        return;
+    }
     if (dmma_supported(g)) {
         k_rtran_b2p_dmma(g, a, b, ln, pad, s);
         return;

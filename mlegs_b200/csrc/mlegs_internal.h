@@ -154,6 +154,23 @@ struct GroupSolve {
 };
 int group_solve_blocks(const GroupSolve& p);
 void k_grouped_solve(const GroupSolve* d, const int* first, int np, int total_blocks, cudaStream_t s);
+// RTRAN(+1) with bulk-copy staging and a warp-specialised mbarrier pipeline
+// (gemm_bulk.cu), the form k_rtran_b2p takes when supported; a timed-out
+// wait raises the module's error word, read (and cleared) by bulk_gemm_error.
+bool b2p_bulk_supported(const DevGrid& g);
+void k_rtran_b2p_bulk(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
+int bulk_gemm_error(bool reset);
+// Fold GEMMs (RTRAN(-1), PROJECT's products) on the same pipeline: weight
+// tables re-laid per (m, parity, 16-row chunk) by k_fold_table (times w_i when
+// use_w), then k_fold_bulk over nseg segments (mode / scale as in FoldArgs;
+// segments [0, split) -> out0, the rest -> out1).
+int fold_table_rows(const DevGrid& g, int wt_rows);
+size_t fold_table_doubles(const DevGrid& g, int wt_rows);
+void k_fold_table(const DevGrid& g, const double* W, int wt_rows, int use_w, double* Wc, cudaStream_t s);
+bool fold_bulk_supported(const DevGrid& g, int wt_rows);
+void k_fold_bulk(const DevGrid& g, const double* const* wc, const double2* const* x, const int* mode,
+                 const int* scale, int nseg, int split, double2* out0, double2* out1, int wt_rows, int pad,
+                 int accumulate, cudaStream_t s);
 // FP64 tensor-path (mma.sync m8n8k4.f64) forms used by k_rtran_b2p / k_fold_gemm when supported.
 bool dmma_supported(const DevGrid& g);
 void k_rtran_b2p_dmma(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);

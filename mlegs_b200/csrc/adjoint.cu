@@ -1040,6 +1040,65 @@ void on_scratch_state(mlegs_ctx* ctx, Fn&& fn) {
     put_back();
 }
 
+// Runs fn through the context's graph cache G for the field set `key`: the
+// first call with a key runs eagerly (tables, factors and temporaries are set up
+// there), the second is captured into a CUDA graph and launched, later calls
+// with the same key replay it.  fn must issue the same work for the same key.
+template <class Fn>
+void run_cached(mlegs_ctx* ctx, mlegs_ctx::AdjGraph& G, const std::vector<const void*>& key, Fn&& fn) {
+    if (G.exec && G.key == key) {
+        CK(cudaGraphLaunch(G.exec, ctx->s));
+        ctx->launches += G.launches;
+        return;
+    }
+    if (!G.warm || G.key != key) {
+        if (G.exec) {
+            cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
+        }
+        G.key = key;
+        G.warm = true;
+        ctx->mark();
+        fn();
+        ctx->restore();
+        return;
+    }
+    ctx->mark();
+    const int64_t before = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+        fn();
+    } catch (...) {
+        cudaStreamEndCapture(ctx->s, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        ctx->restore();
+        G.warm = false;
+        throw;
+    }
+    CK(cudaStreamEndCapture(ctx->s, &graph));
+    G.launches = ctx->launches - before;
+    ctx->launches = before;
+    ctx->restore();
+    const cudaError_t e = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        G.exec = nullptr;
+        throw CudaError(std::string("adjoint graph: ") + cudaGetErrorString(e));
+    }
+    CK(cudaGraphLaunch(G.exec, ctx->s));
+    ctx->launches += G.launches;
+}
+
+std::vector<const void*> field_key(std::initializer_list<const Field*> fs) {
+    std::vector<const void*> k;
+    for (const Field* f : fs) {
+        k.push_back(f);
+        k.push_back(f->data);
+    }
+    return k;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1116,14 +1175,18 @@ int mlegs_ab2_step_map(mlegs_ctx* ctx, const mlegs_field* const* in, mlegs_field
         if (!in || !out) throw ApiError(MLEGS_ERR_ARG, "mlegs_ab2_step_map: null field array");
         require_ab2_sw1(ctx);
         for (int q = 0; q < 6; ++q) require_fff({F(in[q])}, "mlegs_ab2_step_map");
+        const std::vector<const void*> key = field_key({F(in[0]), F(in[1]), F(in[2]), F(in[3]), F(in[4]), F(in[5]),
+                                                         F(out[0]), F(out[1]), F(out[2]), F(out[3]), F(out[4]),
+                                                         F(out[5])});
         on_scratch_state(ctx, [&] {
-            for (int q = 0; q < 3; ++q) ctx->copy0(ctx->adj_state[q], F(in[q]), 0);
-            for (int q = 0; q < 3; ++q) ctx->copy0(ctx->hist[q], F(in[3 + q]), 0);
-            ctx->mark();
-            ctx->step_ab_cn();
-            ctx->restore();
-            for (int q = 0; q < 3; ++q) ctx->copy0(F(out[q]), ctx->adj_state[q], 0);
-            for (int q = 0; q < 3; ++q) ctx->copy0(F(out[3 + q]), ctx->hist[q], 0);
+            run_cached(ctx, ctx->adj_g[0], key, [&] {
+                for (int q = 0; q < 3; ++q) ctx->copy0(ctx->adj_state[q], F(in[q]), 0);
+                for (int q = 0; q < 3; ++q) ctx->copy0(ctx->hist[q], F(in[3 + q]), 0);
+                ctx->step_ab_cn();
+                for (int q = 0; q < 3; ++q) ctx->copy0(F(out[q]), ctx->adj_state[q], 0);
+                for (int q = 0; q < 3; ++q) ctx->copy0(F(out[3 + q]), ctx->hist[q], 0);
+            });
+            for (int q = 0; q < 6; ++q) F(out[q])->space = MLEGS_FFF;
         });
     });
 }
@@ -1160,9 +1223,10 @@ int mlegs_ab2_step_vjp(mlegs_ctx* ctx, const mlegs_field* const* state, const ml
         require_fff({st[0], st[1], st[2], b6[0], b6[1], b6[2], b6[3], b6[4], b6[5]}, "mlegs_ab2_step_vjp");
         Adj A(ctx);
         A.prepare();
-        ctx->mark();
-        A.ab2_step_vjp(st, b6, o6);
-        ctx->restore();
+        const std::vector<const void*> key = field_key({st[0], st[1], st[2], b6[0], b6[1], b6[2], b6[3], b6[4],
+                                                         b6[5], o6[0], o6[1], o6[2], o6[3], o6[4], o6[5]});
+        run_cached(ctx, ctx->adj_g[1], key, [&] { A.ab2_step_vjp(st, b6, o6); });
+        for (int q = 0; q < 6; ++q) o6[q]->space = MLEGS_FFF;
     });
 }
 

@@ -453,6 +453,8 @@ void mlegs_ctx::init(const mlegs_params& prm) {
 
 void mlegs_ctx::destroy() {
     if (gexec) cudaGraphExecDestroy(gexec);
+    for (AdjGraph& a : adj_g)
+        if (a.exec) cudaGraphExecDestroy(a.exec);
     if (graph) cudaGraphDestroy(graph);
     for (void* q : allocs) cudaFree(q);
     allocs.clear();

@@ -146,6 +146,16 @@ struct mlegs_ctx {
     double* adj_dot = nullptr;
     double adj_n0[3] = {};
     Field* adj_state[6] = {};
+    // CUDA graphs of the step map (0) and the step VJP (1), keyed by their fields:
+    // the first call with a key runs eagerly (set-up), the second captures, later
+    // ones replay
+    struct AdjGraph {
+        std::vector<const void*> key;
+        cudaGraphExec_t exec = nullptr;
+        bool warm = false;
+        int64_t launches = 0;
+    };
+    AdjGraph adj_g[2];
 
     // solver state
     Field *psi = nullptr, *chi = nullptr, *b = nullptr;

@@ -347,9 +347,7 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
 #pragma unroll
             for (int q = 0; q < RBF; ++q) {
                 if (r0 + q >= size) break;
-                double y = rb[q];
-                y -= fa[q] * y2;
-                y -= fb[q] * y1;
+                const double y = __fma_rn(-fb[q], y1, __fma_rn(-fa[q], y2, rb[q]));
                 col[(size_t)(r0 + q) * st] = y;
                 y2 = y1;
                 y1 = y;
@@ -367,14 +365,22 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
                 u1[q] = ok ? F5[((size_t)r * 5 + 3) * nsys + t] : 0.0;
                 u2[q] = ok ? F5[((size_t)r * 5 + 4) * nsys + t] : 0.0;
             }
+            // the diagonal's reciprocal and the scaled row are formed off the
+            // recurrence, which then costs one dependent FMA per row (a divide
+            // on the recurrence made the substitution latency-bound)
+#pragma unroll
+            for (int q = 0; q < RBF; ++q) {
+                const int r = r1 - q;
+                const double ri = 1.0 / u0[q];
+                vb[q] = __dmul_rn(vb[q], ri);
+                u1[q] = (r + 1 < size) ? __dmul_rn(u1[q], ri) : 0.0;
+                u2[q] = (r + 2 < size) ? __dmul_rn(u2[q], ri) : 0.0;
+            }
 #pragma unroll
             for (int q = 0; q < RBF; ++q) {
                 const int r = r1 - q;
                 if (r < 0) break;
-                double v = vb[q];
-                if (r + 1 < size) v -= u1[q] * x1;
-                if (r + 2 < size) v -= u2[q] * x2;
-                v /= u0[q];
+                const double v = __fma_rn(-u1[q], x1, __fma_rn(-u2[q], x2, vb[q]));
                 col[(size_t)r * st] = v;
                 x2 = x1;
                 x1 = v;
@@ -382,11 +388,12 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
         }
     } else {
         const size_t NK = g.NXCHOPDIM;
+        constexpr int RBW = 8;  // the 7-band rows hold more factors per row
         double y1 = 0.0, y2 = 0.0, y3 = 0.0;
-        for (int r0 = 0; r0 < size; r0 += RBF) {
-            double rb[RBF], f3[RBF], f2[RBF], f1[RBF];
+        for (int r0 = 0; r0 < size; r0 += RBW) {
+            double rb[RBW], f3[RBW], f2[RBW], f1[RBW];
 #pragma unroll
-            for (int q = 0; q < RBF; ++q) {
+            for (int q = 0; q < RBW; ++q) {
                 const int r = r0 + q;
                 const bool ok = r < size;
                 const double* f = F7 + (size_t)r * 7 * NK + k;
@@ -396,12 +403,9 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
                 f1[q] = ok ? f[2 * NK] : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < RBF; ++q) {
+            for (int q = 0; q < RBW; ++q) {
                 if (r0 + q >= size) break;
-                double y = rb[q];
-                y -= f3[q] * y3;
-                y -= f2[q] * y2;
-                y -= f1[q] * y1;
+                const double y = __fma_rn(-f1[q], y1, __fma_rn(-f2[q], y2, __fma_rn(-f3[q], y3, rb[q])));
                 col[(size_t)(r0 + q) * st] = y;
                 y3 = y2;
                 y2 = y1;
@@ -409,10 +413,10 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
             }
         }
         double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-        for (int r1 = size - 1; r1 >= 0; r1 -= RBF) {
-            double vb[RBF], u0[RBF], u1[RBF], u2[RBF], u3[RBF];
+        for (int r1 = size - 1; r1 >= 0; r1 -= RBW) {
+            double vb[RBW], u0[RBW], u1[RBW], u2[RBW], u3[RBW];
 #pragma unroll
-            for (int q = 0; q < RBF; ++q) {
+            for (int q = 0; q < RBW; ++q) {
                 const int r = r1 - q;
                 const bool ok = r >= 0;
                 const double* f = F7 + (size_t)(ok ? r : 0) * 7 * NK + k;
@@ -423,14 +427,19 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
                 u3[q] = ok ? f[6 * NK] : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < RBF; ++q) {
+            for (int q = 0; q < RBW; ++q) {
+                const int r = r1 - q;
+                const double ri = 1.0 / u0[q];
+                vb[q] = __dmul_rn(vb[q], ri);
+                u1[q] = (r + 1 < size) ? __dmul_rn(u1[q], ri) : 0.0;
+                u2[q] = (r + 2 < size) ? __dmul_rn(u2[q], ri) : 0.0;
+                u3[q] = (r + 3 < size) ? __dmul_rn(u3[q], ri) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < RBW; ++q) {
                 const int r = r1 - q;
                 if (r < 0) break;
-                double v = vb[q];
-                if (r + 1 < size) v -= u1[q] * x1;
-                if (r + 2 < size) v -= u2[q] * x2;
-                if (r + 3 < size) v -= u3[q] * x3;
-                v /= u0[q];
+                const double v = __fma_rn(-u1[q], x1, __fma_rn(-u2[q], x2, __fma_rn(-u3[q], x3, vb[q])));
                 col[(size_t)r * st] = v;
                 x3 = x2;
                 x2 = x1;

@@ -381,7 +381,7 @@ def gradient_leg(local, fd_directions=2):
     int b^2 after the AB2-CN start-up and 200 steps, differentiated with
     respect to the perturbation coefficients through torch.autograd (device
     step maps and VJPs, checkpoints every 20 steps).  Wall-clock seconds per
-    gradient (host-driven: each step and VJP call synchronises) beside the
+    gradient (host-driven calls, stream-ordered: the host waits only for J) beside the
     forward alone on the context's graph-replayed solver, and central
     differences on a few random directions."""
     import time
@@ -430,7 +430,7 @@ def gradient_leg(local, fd_directions=2):
             "checkpoints": stats.checkpoints, "recomputed_steps": stats.recomputed_steps,
             "vjp_steps": stats.vjp_steps, "peak_states": stats.peak_states, "gpu_launches": int(launches),
             "fd_directions": fd_directions, "fd_max_rel_error": max(errs),
-            "timing": "wall clock around the host-driven gradient (every step map and VJP synchronises)"}
+            "timing": "wall clock around the gradient (host-driven calls, stream-ordered by events; one host wait for J)"}
 
 
 def run_reference(args, cfg, ws, rank):

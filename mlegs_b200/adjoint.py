@@ -58,29 +58,52 @@ class DeviceAB2:
         self._vortex = None
 
     # ------------------------------------------------------------ transfers
-    def _load(self, fields, tensors, ln):
-        """tensors (and ln[q], or LN 0 when ln is None) -> fields, on the context's
-        stream, after torch's stream has finished producing them."""
+    # Tensors reach the context's fields and come back by device copies on the
+    # context's stream, ordered against torch's current stream by events (no
+    # host synchronisation): the context's stream waits for torch's work up to
+    # the call (the outputs are allocated before that point), and torch's
+    # stream waits for the results before the call returns.  Every tensor the
+    # context's stream touched is referenced until then, so the caching
+    # allocator can hand its memory out again only to torch-stream work that
+    # is ordered after those copies.
+    def _ext(self):
+        if getattr(self, "_ext_stream", None) is None:
+            self._ext_stream = torch.cuda.ExternalStream(self.ctx.stream(), device=self.device)
+        return self._ext_stream
+
+    def _prep(self, tensors, ln):
         ts = [t.detach().to(self.device, torch.complex128).contiguous() for t in tensors]
         for t in ts:
             if tuple(t.shape) != self.shape:
                 raise ValueError("state tensor of shape %s, expected %s" % (tuple(t.shape), self.shape))
         lt = None if ln is None else ln.detach().to(self.device, torch.float64).contiguous()
-        torch.cuda.current_stream(self.device).synchronize()
-        for q, (f, t) in enumerate(zip(fields, ts)):
-            lp = None if lt is None else lt.data_ptr() + 8 * q
-            self.ctx.DEVICE_COPY(f, True, FFF, t.data_ptr(), lp)
-        return ts + ([] if lt is None else [lt])
+        return ts, lt
 
-    def _store(self, fields, keep=None):
-        """fields -> new tensors and their LN (float64, one per field); synchronises."""
-        outs = [torch.empty(self.shape, dtype=torch.complex128, device=self.device) for _ in fields]
-        ln = torch.empty(len(fields), dtype=torch.float64, device=self.device)
-        for q, f in enumerate(fields):
-            self.ctx.DEVICE_COPY(f, False, FFF, outs[q].data_ptr(), ln.data_ptr() + 8 * q)
-        self.ctx.sync()
-        del keep
-        return outs, ln
+    def _run(self, loads, outs_fields, call):
+        """loads: [(fields, tensors, ln or None)]; call() runs on the context's
+        stream; returns (tensors, ln) read from outs_fields."""
+        ext = self._ext()
+        cur = torch.cuda.current_stream(self.device)
+        prepped = [(fs, *self._prep(ts, ln)) for fs, ts, ln in loads]
+        outs = [torch.empty(self.shape, dtype=torch.complex128, device=self.device) for _ in outs_fields]
+        lno = torch.empty(len(outs_fields), dtype=torch.float64, device=self.device)
+        ev_in = torch.cuda.Event()
+        ev_in.record(cur)
+        ext.wait_event(ev_in)
+        used = [lno] + outs
+        for fields, ts, lt in prepped:
+            for q, (f, t) in enumerate(zip(fields, ts)):
+                lp = None if lt is None else lt.data_ptr() + 8 * q
+                self.ctx.DEVICE_COPY(f, True, FFF, t.data_ptr(), lp)
+            used += ts + ([] if lt is None else [lt])
+        call()
+        for q, f in enumerate(outs_fields):
+            self.ctx.DEVICE_COPY(f, False, FFF, outs[q].data_ptr(), lno.data_ptr() + 8 * q)
+        ev_out = torch.cuda.Event()
+        ev_out.record(ext)
+        cur.wait_event(ev_out)
+        del used
+        return outs, lno
 
     def _zeros_like_state(self, n):
         return ([torch.zeros(self.shape, dtype=torch.complex128, device=self.device) for _ in range(n)],
@@ -90,37 +113,31 @@ class DeviceAB2:
     def step(self, state):
         """One steady AB2-CN step of the 7-tuple state."""
         *fs, ln = state
-        keep = self._load(self.f_in, fs, ln)
-        self.ctx.AB2_STEP_MAP(self.f_in, self.f_out)
-        outs, lno = self._store(self.f_out, keep)
+        outs, lno = self._run([(self.f_in, fs, ln)], self.f_out,
+                              lambda: self.ctx.AB2_STEP_MAP(self.f_in, self.f_out))
         return tuple(outs) + (lno,)
 
     def step_vjp(self, state, bars):
         """Cotangents of `state` given those of step(state)."""
         *fs, ln = state
         *bs, bln = bars
-        keep = self._load(self.f_st, fs[:3], ln[:3])
-        keep += self._load(self.f_bar, bs, bln)
-        self.ctx.AB2_STEP_VJP(self.f_st, self.f_bar, self.f_out)
-        outs, lno = self._store(self.f_out, keep)
+        outs, lno = self._run([(self.f_st, fs[:3], ln[:3]), (self.f_bar, bs, bln)], self.f_out,
+                              lambda: self.ctx.AB2_STEP_VJP(self.f_st, self.f_bar, self.f_out))
         return tuple(outs) + (lno,)
 
     # ------------------------------------------------------------ the other maps
     def startup(self, x0):
         """RICH_BOUSSI_FE_BE of (psi, chi, b, ln[3]) -> the 7-tuple state."""
         *fs, ln = x0
-        keep = self._load(self.f_st, fs, ln)
-        self.ctx.AB2_STARTUP_MAP(self.f_st, self.f_out)
-        outs, lno = self._store(self.f_out, keep)
+        outs, lno = self._run([(self.f_st, fs, ln)], self.f_out,
+                              lambda: self.ctx.AB2_STARTUP_MAP(self.f_st, self.f_out))
         return tuple(outs) + (lno,)
 
     def startup_vjp(self, x0, bars):
         *fs, ln = x0
         *bs, bln = bars
-        keep = self._load(self.f_st, fs, ln)
-        keep += self._load(self.f_bar, bs, bln)
-        self.ctx.AB2_STARTUP_VJP(self.f_st, self.f_bar, self.f_out[:3])
-        outs, lno = self._store(self.f_out[:3], keep)
+        outs, lno = self._run([(self.f_st, fs, ln), (self.f_bar, bs, bln)], self.f_out[:3],
+                              lambda: self.ctx.AB2_STARTUP_VJP(self.f_st, self.f_bar, self.f_out[:3]))
         return tuple(outs) + (lno,)
 
     def vortex(self):
@@ -135,18 +152,19 @@ class DeviceAB2:
         ctx = self.ctx
         c_psi, c_chi, c_b = coefs
         neg = [(-c_psi), (-c_chi)]
-        keep = self._load(self.f_in[3:5], neg, None)
-        keep += self._load(self.f_in[5:6], [c_b], None)
-        for q, vf in enumerate(self.vortex()):
-            tmp, out, F = self.f_in[3 + q], self.f_bar[q], self.f_out[q]
-            ctx.CHOPDO(tmp)
-            ctx.IDELSQH(tmp, out)
-            ctx.COPY(F, vf)
-            ctx.AXPBY(F, 1.0, out, 0.0, None, 1.0)
-            ctx.CHOPDO(F)
-        ctx.COPY(self.f_out[2], self.f_in[5])
-        ctx.CHOPDO(self.f_out[2])
-        outs, ln = self._store(self.f_out[:3], keep)
+        vortex = self.vortex()
+
+        def build():
+            for q, vf in enumerate(vortex):
+                tmp, out, F = self.f_in[3 + q], self.f_bar[q], self.f_out[q]
+                ctx.CHOPDO(tmp)
+                ctx.IDELSQH(tmp, out)
+                ctx.COPY(F, vf)
+                ctx.AXPBY(F, 1.0, out, 0.0, None, 1.0)
+                ctx.CHOPDO(F)
+            ctx.COPY(self.f_out[2], self.f_in[5])
+            ctx.CHOPDO(self.f_out[2])
+        outs, ln = self._run([(self.f_in[3:5], neg, None), (self.f_in[5:6], [c_b], None)], self.f_out[:3], build)
         # the CALCAT1 far-field value of b (m = 0, every k) removed, as the
         # reference's far-field fix writes it (mod_legops.f90:2540)
         n = int(ctx.cfg.nrchop)
@@ -158,18 +176,19 @@ class DeviceAB2:
 
     def initial_state_T(self, bars):
         *bs, bln = bars
-        keep = self._load(self.f_st, bs, bln)
-        self.ctx.INITIAL_STATE_T(self.f_st, self.f_out[:3])
-        outs, _ = self._store(self.f_out[:3], keep)
+        outs, _ = self._run([(self.f_st, bs, bln)], self.f_out[:3],
+                            lambda: self.ctx.INITIAL_STATE_T(self.f_st, self.f_out[:3]))
         return tuple(outs)
 
     def objective(self, psi, chi, b):
         """J and (gpsi, gchi, gb)."""
-        keep = self._load(self.f_st, [psi, chi, b], None)
-        J = self.ctx.ENERGY_OBJECTIVE(self.f_st[0], self.f_st[1], self.f_st[2],
-                                      self.f_out[0], self.f_out[1], self.f_out[2])
-        outs, _ = self._store(self.f_out[:3], keep)
-        return J, outs
+        res = {}
+
+        def call():
+            res["J"] = self.ctx.ENERGY_OBJECTIVE(self.f_st[0], self.f_st[1], self.f_st[2],
+                                                 self.f_out[0], self.f_out[1], self.f_out[2])
+        outs, _ = self._run([(self.f_st, [psi, chi, b], None)], self.f_out[:3], call)
+        return res["J"], outs
 
 
 class InitialState(torch.autograd.Function):
@@ -236,6 +255,7 @@ def gradient(solver, coefs, nsteps=200, every=20, stats=None):
     final = run_loop(solver, st, nsteps, every=every, stats=stats)
     J = Objective.apply(solver, final[0], final[1], final[2])
     J.backward()
+    solver.ctx.sync()  # the library's deferred error checks (no call above waits for the device)
     return float(J.item()), [c.grad for c in cs]
 
 
@@ -246,11 +266,13 @@ def objective_of(solver, coefs, nsteps, graph=True):
     ctx = solver.ctx
     if not hasattr(solver, "f_run"):
         solver.f_run = [ctx.field(FFF) for _ in range(3)]
-    with torch.no_grad():
-        psi, chi, b, ln = solver.initial_state(tuple(c.to(solver.device, torch.complex128) for c in coefs))
-        keep = solver._load(solver.f_run, [psi, chi, b], ln)
+    res = {}
+
+    def call():
         ctx.initialize(*solver.f_run)
         ctx.step(nsteps, graph=graph)
-        J = ctx.ENERGY_OBJECTIVE(*solver.f_run, *solver.f_out[:3])
-        del keep
-    return J
+        res["J"] = ctx.ENERGY_OBJECTIVE(*solver.f_run, *solver.f_out[:3])
+    with torch.no_grad():
+        psi, chi, b, ln = solver.initial_state(tuple(c.to(solver.device, torch.complex128) for c in coefs))
+        solver._run([(solver.f_run, [psi, chi, b], ln)], [], call)
+    return res["J"]

@@ -294,6 +294,8 @@ __global__ void factor_kernel(DevGrid g, int kind, double alp, int pad, double* 
 // CALCAT1 row-0 correction over n < NRCHOP + pad to the m = 0 columns.
 // One (system, real or imaginary part) u of the factored substitutions: the
 // body of solve_factored_kernel, also run by the grouped ensemble kernel.
+// WB: rows per load block of the 7-band systems (16 where registers allow)
+template <int WB>
 __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const double* __restrict__ F5,
                                                    const double* __restrict__ F7, const double2* src, double2* dst,
                                                    double* ln_out, int kind, int has_ln, double ln_in, int pad,
@@ -388,7 +390,7 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
         }
     } else {
         const size_t NK = g.NXCHOPDIM;
-        constexpr int RBW = 8;  // the 7-band rows hold more factors per row
+        constexpr int RBW = WB;
         double y1 = 0.0, y2 = 0.0, y3 = 0.0;
         for (int r0 = 0; r0 < size; r0 += RBW) {
             double rb[RBW], f3[RBW], f2[RBW], f1[RBW];
@@ -493,16 +495,25 @@ void k_solve_factor(const DevGrid& g, int kind, double alp, int pad, double* F5,
 __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const double* __restrict__ F5,
                                                              const double* __restrict__ F7, const double2* src,
                                                              double2* dst, double* ln_out, int kind, int has_ln,
-                                                             double ln_in, int pad, int farfield) {
-    solve_factored_sys(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield,
-                       blockIdx.x * blockDim.x + threadIdx.x);
+                                                             double ln_in, int pad, int farfield, int wpad) {
+    // kinds 1 and 2: the 7-band m = 0 systems (u < 2 NXCHOPDIM) take whole
+    // warps, the 5-band ones start after wpad idle threads, so that no warp
+    // runs both substitutions one after the other
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nw = 2 * g.NXCHOPDIM;
+    if (wpad) {
+        if (u >= nw && u < nw + wpad) return;
+        if (u >= nw) u -= wpad;
+    }
+    solve_factored_sys<16>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield, u);
 }
 
 void k_solve_factored(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
                       double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s) {
-    const int n = 2 * g.NTCHOPDIM * g.NXCHOPDIM;
+    const int wpad = kind == 0 ? 0 : (32 - (2 * g.NXCHOPDIM) % 32) % 32;
+    const int n = 2 * g.NTCHOPDIM * g.NXCHOPDIM + wpad;
     solve_factored_kernel<<<(n + 127) / 128, 128, 0, s>>>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad,
-                                                          farfield);
+                                                          farfield, wpad);
     count_launch();
 }
 
@@ -667,7 +678,7 @@ __global__ void __launch_bounds__(128) grouped_solve_kernel(const GroupSolve* __
         else hi = mid - 1;
     }
     const GroupSolve P = pr[lo];
-    solve_factored_sys(P.g, P.F5, P.F7, P.src, P.dst, P.ln_out, P.kind, P.has_ln, P.ln_in, P.pad, P.farfield,
+    solve_factored_sys<8>(P.g, P.F5, P.F7, P.src, P.dst, P.ln_out, P.kind, P.has_ln, P.ln_in, P.pad, P.farfield,
                        (b - P.first) * 128 + threadIdx.x);
 }
 

@@ -457,27 +457,29 @@ __device__ __forceinline__ void solve_factored_sys(const DevGrid& g, const doubl
         for (int r = 0; r < nn; ++r) {
             const double cur = col[(size_t)r * st];
             const double nxt = (r + 1 < nn) ? col[(size_t)(r + 1) * st] : 0.0;
+            // explicit roundings here and below: every kernel that runs this
+            // body (single and grouped) gives the same bits
             double v = cur;
-            if (r >= 1) v += xm[(size_t)r * 2] * prev;
-            if (r + 1 < nn) v += xm[(size_t)r * 2 + 1] * nxt;
+            if (r >= 1) v = __fma_rn(xm[(size_t)r * 2], prev, v);
+            if (r + 1 < nn) v = __fma_rn(xm[(size_t)r * 2 + 1], nxt, v);
             col[(size_t)r * st] = v;
             prev = cur;
         }
     }
     if (m == 0 && k == 0 && size > 0) {
         if (kind == 0) {
-            if (!comp) *ln_out = col[0] * g.norm0[0];
+            if (!comp) *ln_out = __dmul_rn(col[0], g.norm0[0]);
             col[0] = 0.0;
         } else if (kind == 1 && !comp && ln_out) {
-            *ln_out = has_ln ? col[0] * g.norm0[0] : 0.0;
+            *ln_out = has_ln ? __dmul_rn(col[0], g.norm0[0]) : 0.0;
         }
     }
     if (farfield && m == 0) {
         // a(n=0, m=0, k) -= sum_{n < NRCHOP+pad} AT1(n) a(n, 0, k) / AT1(0)
         const int nr_sum = g.NRCHOP + pad;
         double sum = 0.0;
-        for (int r = 0; r < nr_sum && r < g.NRCHOPDIM; ++r) sum += g.at1[r] * col[(size_t)r * st];
-        col[0] -= sum / g.at1[0];
+        for (int r = 0; r < nr_sum && r < g.NRCHOPDIM; ++r) sum = __fma_rn(g.at1[r], col[(size_t)r * st], sum);
+        col[0] = __dsub_rn(col[0], __ddiv_rn(sum, g.at1[0]));
     }
 }
 
@@ -678,11 +680,18 @@ __global__ void __launch_bounds__(128) grouped_solve_kernel(const GroupSolve* __
         else hi = mid - 1;
     }
     const GroupSolve P = pr[lo];
-    solve_factored_sys<8>(P.g, P.F5, P.F7, P.src, P.dst, P.ln_out, P.kind, P.has_ln, P.ln_in, P.pad, P.farfield,
-                       (b - P.first) * 128 + threadIdx.x);
+    // the 7-band m = 0 systems in whole warps, as in solve_factored_kernel
+    int u = (b - P.first) * 128 + threadIdx.x;
+    const int nw = 2 * P.g.NXCHOPDIM, wpad = P.kind == 0 ? 0 : (32 - nw % 32) % 32;
+    if (u >= nw && u < nw + wpad) return;
+    if (u >= nw) u -= wpad;
+    solve_factored_sys<8>(P.g, P.F5, P.F7, P.src, P.dst, P.ln_out, P.kind, P.has_ln, P.ln_in, P.pad, P.farfield, u);
 }
 
-int group_solve_blocks(const GroupSolve& p) { return (2 * p.g.NTCHOPDIM * p.g.NXCHOPDIM + 127) / 128; }
+int group_solve_blocks(const GroupSolve& p) {
+    const int nw = 2 * p.g.NXCHOPDIM, wpad = p.kind == 0 ? 0 : (32 - nw % 32) % 32;
+    return (2 * p.g.NTCHOPDIM * p.g.NXCHOPDIM + wpad + 127) / 128;
+}
 
 void k_grouped_solve(const GroupSolve* d, const int* first, int np, int total_blocks, cudaStream_t s) {
     grouped_solve_kernel<<<total_blocks, 128, 0, s>>>(d, first, np);

@@ -694,12 +694,16 @@ __global__ void __launch_bounds__(384, 1) theta5_kernel(DevGrid g, PhysArgs A, c
     }
 }
 
-// Single-field HORFFT with the four-step blocks, G lines per warp.  dir +1: PFP -> PPP, -1: PPP -> PFP.
+// Single-field HORFFT on the in-slot transforms of theta5_kernel: each lane
+// group owns two line slots and, while it transforms the row in one, the next
+// row of its line sequence arrives in the other by cp.async.
+//   dir +1: PFP -> PPP (samples written from their slot positions),
+//   dir -1: PPP -> PFP (the row copied straight to its slot positions).
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) horfft4_kernel(DevGrid g, const double2* src, double2* dst,
-                                                      const double2* tw_g, const double2* twh_g, int dir) {
+__global__ void __launch_bounds__(256) horfft5_kernel(DevGrid g, const double2* __restrict__ src,
+                                                      double2* __restrict__ dst, const double2* tw_g,
+                                                      const double2* twh_g, int dir) {
     constexpr int N = N1 * N2, G = 32 / N2;
-    constexpr int TILE = N1 * (N2 + 1);
     extern __shared__ double2 sm[];
     double2* tw = sm;
     double2* twh = tw + (N + 1);
@@ -710,26 +714,50 @@ __global__ void __launch_bounds__(256) horfft4_kernel(DevGrid g, const double2* 
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int gid = lane / N2, t = lane % N2;
-    double2* P = twh + (N + 1) + (size_t)warp * G * (N + TILE) + gid * (N + TILE);
-    double2* S = P + N;
-    const int md = g.NTCHOPDIM;
+    double2* L0 = twh + (N + 1) + (size_t)(warp * G + gid) * 2 * N;
+    const int md = g.NTCHOPDIM, mlim = md < g.NTCHOP ? md : g.NTCHOP;
     const int nlines = g.NR * g.NX;
     const int stride = gridDim.x * nw * G;
-    for (int l0 = (blockIdx.x * nw + warp) * G; l0 < nlines; l0 += stride) {
-        const int line = l0 + gid;
-        const bool ok = line < nlines;
-        if (dir > 0) {
-            grp_inverse<N1, N2>(ok ? src + (size_t)line * md : nullptr, ok, md, g.NTCHOP, tw, twh, S, P, t);
-            __syncwarp();
-            if (ok)
-                for (int j = t; j < N; j += N2) dst[(size_t)line * N + j] = P[j];
-        } else {
-            for (int j = t; j < N; j += N2) P[j] = ok ? src[(size_t)line * N + j] : make_double2(0.0, 0.0);
-            __syncwarp();
-            grp_forward<N1, N2>(P, ok, ok ? dst + (size_t)line * md : nullptr, md, g.NTCHOP, tw, twh, S, t);
+    // the warp's groups step through their lines together (the transforms
+    // synchronise the warp); a group past the last line works on zeros
+    auto fetch = [&](int line, double2* L) {
+        if (line < nlines) {
+            if (dir > 0) {
+                row_async<N2>(src + (size_t)line * md, mlim, L, t);
+            } else {
+                const double2* row = src + (size_t)line * N;
+                for (int j = t; j < N; j += N2)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(L + phys_pos<N1, N2>(j))),
+                                 "l"(row + j)
+                                 : "memory");
+            }
         }
+        async_commit();
+    };
+    const int first = (blockIdx.x * nw + warp) * G + gid;
+    fetch(first, L0);
+    int slot = 0;
+    for (int base = (blockIdx.x * nw + warp) * G; base < nlines; base += stride, slot ^= 1) {
+        const int line = base + gid;
+        const bool ok = line < nlines;
+        double2* L = L0 + slot * N;
+        fetch(line + stride, L0 + (slot ^ 1) * N);
+        async_wait<1>();
         __syncwarp();
+        if (dir > 0) {
+            grp_inverse5<N1, N2>(nullptr, ok, md, g.NTCHOP, tw, twh, L, t, true);
+            __syncwarp();
+            if (ok) {
+                double2* out = dst + (size_t)line * N;
+                for (int j = t; j < N; j += N2) out[j] = L[phys_pos<N1, N2>(j)];
+            }
+        } else {
+            grp_forward5<N1, N2>(L, ok, ok ? dst + (size_t)line * md : nullptr, md, g.NTCHOP, tw, twh, t);
+        }
+        __syncwarp();  // the slot is refilled two lines on
     }
+    async_wait<0>();
 }
 
 static int pp_of(int nth) {
@@ -918,28 +946,6 @@ static bool launch_theta5(const DevGrid& g, const FFTPlan& p, const PhysArgs& A,
     return true;
 }
 
-template <int N1, int N2>
-static void launch_horfft4(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
-                           cudaStream_t s) {
-    constexpr int N = N1 * N2, G = 32 / N2, TILE = N1 * (N2 + 1);
-    const size_t per_warp = (size_t)G * (N + TILE) * sizeof(double2);
-    const size_t fixed = 2 * (size_t)(N + 1) * sizeof(double2);
-    int warps = (int)((110 * 1024 - fixed) / per_warp);
-    if (warps > 8) warps = 8;
-    if (warps < 1) warps = 1;
-    size_t sm = fixed + warps * per_warp;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(horfft4_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
-    }
-    int nlines = g.NR * g.NX;
-    int per_cta = warps * G;
-    int blocks = std::min((nlines + per_cta - 1) / per_cta, sm_count() * 4);
-    horfft4_kernel<N1, N2><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, dir);
-    count_launch();
-}
-
 void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[10], double2* const out[4],
                    double omega, double bv0, int linear, cudaStream_t s) {
     PhysArgs A;
@@ -971,14 +977,37 @@ void k_theta_fused(const DevGrid& g, const FFTPlan& p, const double2* const in[1
     count_launch();
 }
 
+template <int N1, int N2>
+static void launch_horfft5(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir,
+                           cudaStream_t s) {
+    constexpr int N = N1 * N2, G = 32 / N2;
+    const size_t per_warp = (size_t)G * 2 * N * sizeof(double2);
+    const size_t fixed = 2 * (size_t)(N + 1) * sizeof(double2);
+    // two CTAs per SM
+    int warps = (int)((227 * 1024 / 2 - 1024 - fixed) / per_warp);
+    if (warps > 8) warps = 8;
+    if (warps < 1) warps = 1;
+    const size_t sm = fixed + warps * per_warp;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(horfft5_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    const int nlines = g.NR * g.NX;
+    const int per_cta = warps * G;
+    const int blocks = std::min((nlines + per_cta - 1) / per_cta, sm_count() * 2);
+    horfft5_kernel<N1, N2><<<blocks, warps * 32, sm, s>>>(g, src, dst, p.tw_t, p.tw_h, dir);
+    count_launch();
+}
+
 void k_horfft_warp(const DevGrid& g, const FFTPlan& p, const double2* src, double2* dst, int dir, cudaStream_t s) {
     switch (g.NTH) {
-        case 16: launch_horfft4<4, 4>(g, p, src, dst, dir, s); return;
-        case 32: launch_horfft4<8, 4>(g, p, src, dst, dir, s); return;
-        case 64: launch_horfft4<8, 8>(g, p, src, dst, dir, s); return;
-        case 128: launch_horfft4<16, 8>(g, p, src, dst, dir, s); return;
-        case 256: launch_horfft4<16, 16>(g, p, src, dst, dir, s); return;
-        case 512: launch_horfft4<32, 16>(g, p, src, dst, dir, s); return;
+        case 16: launch_horfft5<4, 4>(g, p, src, dst, dir, s); return;
+        case 32: launch_horfft5<8, 4>(g, p, src, dst, dir, s); return;
+        case 64: launch_horfft5<8, 8>(g, p, src, dst, dir, s); return;
+        case 128: launch_horfft5<16, 8>(g, p, src, dst, dir, s); return;
+        case 256: launch_horfft5<16, 16>(g, p, src, dst, dir, s); return;
+        case 512: launch_horfft5<32, 16>(g, p, src, dst, dir, s); return;
         default: break;
     }
     const int warps = 8;

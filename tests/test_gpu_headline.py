@@ -1,7 +1,7 @@
 """GPU parity at the headline grid and at every FFT instantiation, through the C ABI.
 
 The step kernels are compiled per size: the theta transforms and products
-(`theta5_kernel<N1, N2>`), HORFFT (`horfft4_kernel<N1, N2>`) and VERFFT
+(`theta5_kernel<N1, N2>`), HORFFT (`horfft5_kernel<N1, N2>`) and VERFFT
 (`verfft4_kernel<N1, N2>`) are templates dispatched on NTH and NX.  These tests
 run each dispatched form against the FP64 oracle:
 
@@ -114,7 +114,7 @@ def test_rtran_headline(head, prec, pad):
 
 
 def test_verfft_horfft_headline(head):
-    """VERFFT(+-1) at NX = 256 (verfft4<16,16>) and HORFFT(+-1) at NTH = 128 (horfft4<16,8>)."""
+    """VERFFT(+-1) at NX = 256 (verfft4<16,16>) and HORFFT(+-1) at NTH = 128 (horfft5<16,8>)."""
     from oracle import transforms as T
     from oracle.grid import PFF, PFP
     M, ctxs, g, cfg = head
@@ -293,7 +293,7 @@ def test_etd_steps_headline(head, head_state, head_oracle_steps, prec):
 
 
 # ---------------------------------------------------------------- other sizes
-# (NR, NTH, NX) -> theta5 / horfft4 <N1, N2> at NTH, verfft4 <N1, N2> at NX
+# (NR, NTH, NX) -> theta5 / horfft5 <N1, N2> at NTH, verfft4 <N1, N2> at NX
 GRIDS = [(32, 64, 128), (32, 256, 64), (16, 512, 512)]
 
 

@@ -122,17 +122,23 @@ __global__ void vel2pln_T_kernel(const DevGrid g, double2* y, const double* c) {
 // Transpose of the far-field fix a(0, 0, k) -= sum_{n < nr} AT1(n) a(n, 0, k) / AT1(0)
 // (CALCAT1, mod_scalar3.f90:286-310), in place on an FFF field: rows 1 .. nr-1
 // of m = 0 -= AT1(n)/AT1(0) row 0, then row 0 = 0.
-__global__ void farfield_T_kernel(const DevGrid g, double2* y, int nr) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.NXCHOPDIM) return;
+// CALCAT1's row-0 fix transposed: y(n, 0, k) -= AT1(n)/AT1(0) y(0, 0, k) for
+// 1 <= n < nr, then y(0, 0, k) = 0.  A block is 32 k by 8 row groups; every
+// thread reads y(0, 0, k) before the barrier, row 0 is zeroed after it.
+__global__ void __launch_bounds__(256) farfield_T_kernel(const DevGrid g, double2* y, int nr) {
+    const int kl = threadIdx.x & 31, ny = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + kl;
+    const bool ok = k < g.NXCHOPDIM;
     const size_t st = g.NXCHOPDIM;
-    const double2 y0 = y[k];
-    for (int n = 1; n < nr && n < g.NRCHOPDIM; ++n) {
+    const double2 y0 = ok ? y[k] : make_double2(0.0, 0.0);
+    __syncthreads();
+    if (!ok) return;
+    for (int n = 1 + ny; n < nr && n < g.NRCHOPDIM; n += 8) {
         const double f = g.at1[n] / g.at1[0];
         const double2 v = y[(size_t)n * st + k];
         y[(size_t)n * st + k] = make_double2(v.x - f * y0.x, v.y - f * y0.y);
     }
-    y[k] = make_double2(0.0, 0.0);
+    if (ny == 0) y[k] = make_double2(0.0, 0.0);
 }
 
 // Transposed banded solves with the stored unpivoted factors A = L U of the
@@ -145,11 +151,22 @@ __global__ void farfield_T_kernel(const DevGrid g, double2* y, int nr) {
 //   kind 2  IHELM: m >= 1 5-band; m = 0 the forward solves (H XM) v = rhs on
 //           NN - 1 rows and returns XM v (NN rows), so the transpose forms
 //           w = XM^T y, solves (H XM)^T on NN - 1 rows and zeroes row NN - 1.
+// The substitutions run in load blocks of TB (TW for the 7-band systems)
+// rows: a block's right-hand sides and factors are loaded together, the
+// diagonal's reciprocal and the scaled off-diagonals are formed off the
+// recurrence, which then costs one dependent FMA per row.  wpad idle threads
+// after the 7-band m = 0 systems of kind 2 keep them in warps of their own.
 __global__ void __launch_bounds__(128) solve_T_kernel(const DevGrid g, const double* __restrict__ F5,
                                                       const double* __restrict__ F7, double2* yfield, int kind,
-                                                      int pad) {
+                                                      int pad, int wpad) {
+    constexpr int TB = 16, TW = 8;
     const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nw = 2 * g.NXCHOPDIM;
+    if (wpad) {
+        if (u >= nw && u < nw + wpad) return;
+        if (u >= nw) u -= wpad;
+    }
     const int t = u >> 1, comp = u & 1;
     if (t >= nsys) return;
     const int k = t % g.NXCHOPDIM, m = t / g.NXCHOPDIM;
@@ -158,24 +175,53 @@ __global__ void __launch_bounds__(128) solve_T_kernel(const DevGrid g, const dou
     const size_t st = 2 * (size_t)g.NXCHOPDIM;
     if (!(m == 0 && kind == 2)) {
         const int size = nn;
+        // U^T z = y: z(r) = (y(r) - U(r-1, r) z(r-1) - U(r-2, r) z(r-2)) / U(r, r)
         double z1 = 0.0, z2 = 0.0;
-        for (int r = 0; r < size; ++r) {
-            double v = col[(size_t)r * st];
-            if (r >= 1) v -= F5[((size_t)(r - 1) * 5 + 3) * nsys + t] * z1;
-            if (r >= 2) v -= F5[((size_t)(r - 2) * 5 + 4) * nsys + t] * z2;
-            v /= F5[((size_t)r * 5 + 2) * nsys + t];
-            col[(size_t)r * st] = v;
-            z2 = z1;
-            z1 = v;
+        for (int r0 = 0; r0 < size; r0 += TB) {
+            double yv[TB], a1[TB], a2[TB];
+#pragma unroll
+            for (int q = 0; q < TB; ++q) {
+                const int r = r0 + q;
+                const bool ok = r < size;
+                yv[q] = ok ? col[(size_t)r * st] : 0.0;
+                const double d = ok ? F5[((size_t)r * 5 + 2) * nsys + t] : 1.0;
+                a1[q] = (ok && r >= 1) ? F5[((size_t)(r - 1) * 5 + 3) * nsys + t] : 0.0;
+                a2[q] = (ok && r >= 2) ? F5[((size_t)(r - 2) * 5 + 4) * nsys + t] : 0.0;
+                const double ri = 1.0 / d;
+                yv[q] = __dmul_rn(yv[q], ri);
+                a1[q] = __dmul_rn(a1[q], ri);
+                a2[q] = __dmul_rn(a2[q], ri);
+            }
+#pragma unroll
+            for (int q = 0; q < TB; ++q) {
+                if (r0 + q >= size) break;
+                const double v = __fma_rn(-a1[q], z1, __fma_rn(-a2[q], z2, yv[q]));
+                col[(size_t)(r0 + q) * st] = v;
+                z2 = z1;
+                z1 = v;
+            }
         }
+        // L^T x = z: x(r) = z(r) - L(r+1, r) x(r+1) - L(r+2, r) x(r+2)
         double x1 = 0.0, x2 = 0.0;
-        for (int r = size - 1; r >= 0; --r) {
-            double v = col[(size_t)r * st];
-            if (r + 1 < size) v -= F5[((size_t)(r + 1) * 5 + 1) * nsys + t] * x1;
-            if (r + 2 < size) v -= F5[((size_t)(r + 2) * 5 + 0) * nsys + t] * x2;
-            col[(size_t)r * st] = v;
-            x2 = x1;
-            x1 = v;
+        for (int r1 = size - 1; r1 >= 0; r1 -= TB) {
+            double zv[TB], e1[TB], e2[TB];
+#pragma unroll
+            for (int q = 0; q < TB; ++q) {
+                const int r = r1 - q;
+                const bool ok = r >= 0;
+                zv[q] = ok ? col[(size_t)r * st] : 0.0;
+                e1[q] = (ok && r + 1 < size) ? F5[((size_t)(r + 1) * 5 + 1) * nsys + t] : 0.0;
+                e2[q] = (ok && r + 2 < size) ? F5[((size_t)(r + 2) * 5 + 0) * nsys + t] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < TB; ++q) {
+                const int r = r1 - q;
+                if (r < 0) break;
+                const double v = __fma_rn(-e1[q], x1, __fma_rn(-e2[q], x2, zv[q]));
+                col[(size_t)r * st] = v;
+                x2 = x1;
+                x1 = v;
+            }
         }
         return;
     }
@@ -185,40 +231,75 @@ __global__ void __launch_bounds__(128) solve_T_kernel(const DevGrid g, const dou
     const double* xm = g.xm;
     {
         double prev = 0.0;
-        for (int r = 0; r < nn; ++r) {
-            const double yr = col[(size_t)r * st];
-            double v = yr;
-            if (r + 1 < nn) v += xm[(size_t)(r + 1) * 2 + 0] * col[(size_t)(r + 1) * st];
-            if (r >= 1) v += xm[(size_t)(r - 1) * 2 + 1] * prev;
-            col[(size_t)r * st] = v;
-            prev = yr;
+        for (int r0 = 0; r0 < nn; r0 += TW) {
+            double yv[TW + 1];
+#pragma unroll
+            for (int q = 0; q <= TW; ++q) yv[q] = (r0 + q < nn) ? col[(size_t)(r0 + q) * st] : 0.0;
+#pragma unroll
+            for (int q = 0; q < TW; ++q) {
+                const int r = r0 + q;
+                if (r >= nn) break;
+                double v = yv[q];
+                if (r + 1 < nn) v = __fma_rn(xm[(size_t)(r + 1) * 2 + 0], yv[q + 1], v);
+                if (r >= 1) v = __fma_rn(xm[(size_t)(r - 1) * 2 + 1], prev, v);
+                col[(size_t)r * st] = v;
+                prev = yv[q];
+            }
         }
     }
     const int size = nn - 1;
     const size_t NK = g.NXCHOPDIM;
     auto f7 = [&](int r, int j) { return F7[((size_t)r * 7 + j) * NK + k]; };
     double z1 = 0.0, z2 = 0.0, z3 = 0.0;
-    for (int r = 0; r < size; ++r) {
-        double v = col[(size_t)r * st];
-        if (r >= 1) v -= f7(r - 1, 4) * z1;
-        if (r >= 2) v -= f7(r - 2, 5) * z2;
-        if (r >= 3) v -= f7(r - 3, 6) * z3;
-        v /= f7(r, 3);
-        col[(size_t)r * st] = v;
-        z3 = z2;
-        z2 = z1;
-        z1 = v;
+    for (int r0 = 0; r0 < size; r0 += TW) {
+        double yv[TW], a1[TW], a2[TW], a3[TW];
+#pragma unroll
+        for (int q = 0; q < TW; ++q) {
+            const int r = r0 + q;
+            const bool ok = r < size;
+            yv[q] = ok ? col[(size_t)r * st] : 0.0;
+            const double d = ok ? f7(r, 3) : 1.0;
+            a1[q] = (ok && r >= 1) ? f7(r - 1, 4) : 0.0;
+            a2[q] = (ok && r >= 2) ? f7(r - 2, 5) : 0.0;
+            a3[q] = (ok && r >= 3) ? f7(r - 3, 6) : 0.0;
+            const double ri = 1.0 / d;
+            yv[q] = __dmul_rn(yv[q], ri);
+            a1[q] = __dmul_rn(a1[q], ri);
+            a2[q] = __dmul_rn(a2[q], ri);
+            a3[q] = __dmul_rn(a3[q], ri);
+        }
+#pragma unroll
+        for (int q = 0; q < TW; ++q) {
+            if (r0 + q >= size) break;
+            const double v = __fma_rn(-a1[q], z1, __fma_rn(-a2[q], z2, __fma_rn(-a3[q], z3, yv[q])));
+            col[(size_t)(r0 + q) * st] = v;
+            z3 = z2;
+            z2 = z1;
+            z1 = v;
+        }
     }
     double x1 = 0.0, x2 = 0.0, x3 = 0.0;
-    for (int r = size - 1; r >= 0; --r) {
-        double v = col[(size_t)r * st];
-        if (r + 1 < size) v -= f7(r + 1, 2) * x1;
-        if (r + 2 < size) v -= f7(r + 2, 1) * x2;
-        if (r + 3 < size) v -= f7(r + 3, 0) * x3;
-        col[(size_t)r * st] = v;
-        x3 = x2;
-        x2 = x1;
-        x1 = v;
+    for (int r1 = size - 1; r1 >= 0; r1 -= TW) {
+        double zv[TW], c1[TW], c2[TW], c3[TW];
+#pragma unroll
+        for (int q = 0; q < TW; ++q) {
+            const int r = r1 - q;
+            const bool ok = r >= 0;
+            zv[q] = ok ? col[(size_t)r * st] : 0.0;
+            c1[q] = (ok && r + 1 < size) ? f7(r + 1, 2) : 0.0;
+            c2[q] = (ok && r + 2 < size) ? f7(r + 2, 1) : 0.0;
+            c3[q] = (ok && r + 3 < size) ? f7(r + 3, 0) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < TW; ++q) {
+            const int r = r1 - q;
+            if (r < 0) break;
+            const double v = __fma_rn(-c1[q], x1, __fma_rn(-c2[q], x2, __fma_rn(-c3[q], x3, zv[q])));
+            col[(size_t)r * st] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
     }
     col[(size_t)size * st] = 0.0;
 }
@@ -592,7 +673,7 @@ struct Adj {
 
     // ------------------------------------------------------------- solves
     void farfield_T(Field* y, int nr) {
-        farfield_T_kernel<<<nb(c->d.NXCHOPDIM, 64), 64, 0, s()>>>(g(), y->data, nr);
+        farfield_T_kernel<<<nb(c->d.NXCHOPDIM, 32), 256, 0, s()>>>(g(), y->data, nr);
         count_launch();
     }
     const mlegs_ctx::SolveFactors* factors(int kind, double alp) {
@@ -601,8 +682,9 @@ struct Adj {
         return f;
     }
     void solve_T(const mlegs_ctx::SolveFactors* f, Field* y, int kind) {
-        const int n = 2 * c->d.NTCHOPDIM * c->d.NXCHOPDIM;
-        solve_T_kernel<<<nb(n, 128), 128, 0, s()>>>(g(), f->F5, f->F7, y->data, kind, 0);
+        const int nw = 2 * c->d.NXCHOPDIM, wpad = kind == 2 ? (32 - nw % 32) % 32 : 0;
+        const int n = 2 * c->d.NTCHOPDIM * c->d.NXCHOPDIM + wpad;
+        solve_T_kernel<<<nb(n, 128), 128, 0, s()>>>(g(), f->F5, f->F7, y->data, kind, 0, wpad);
         count_launch();
     }
     // IDEL2LN(B, A) (mod_legops.f90:1013-1176) as B -> (A, A%LN): A_bar -> B_bar (LN 0)

@@ -505,9 +505,9 @@ struct Adj {
         c->ln_zero(f);
     }
     void copy(Field* dst, const Field* src) {
-        k_copy(dst->data, src->data, c->d.elems(src->space), s());
+        if (dst == src) return;
+        k_copy_ln(dst->data, src->data, c->d.elems(src->space), dst->ln, src->ln, s());
         dst->space = src->space;
-        CK(cudaMemcpyAsync(dst->ln, src->ln, sizeof(double), cudaMemcpyDeviceToDevice, s()));
     }
     void add(Field* y, const Field* x, double a = 1.0) {  // y += a x, E and LN
         k_axpby(y->data, a, x->data, 0.0, nullptr, 1.0, c->d.elems(y->space), s());

@@ -213,10 +213,12 @@ struct mlegs_ctx {
     // COPY0 (mod_fft.f90:705-769): dst = src, CHOPDO for FFF, LN copied.
     void copy0(Field* dst, const Field* src, int pad) {
         if (dst == src) return;
-        k_copy(dst->data, src->data, d.elems(src->space), s);
         dst->space = src->space;
-        CK(cudaMemcpyAsync(dst->ln, src->ln, sizeof(double), cudaMemcpyDeviceToDevice, s));
-        chopdo(dst, pad);
+        if (src->space == MLEGS_FFF) {  // copy, LN and CHOPDO in one pass
+            k_copy_chop_fff(g, dst->data, src->data, dst->ln, src->ln, pad, s);
+            return;
+        }
+        k_copy_ln(dst->data, src->data, d.elems(src->space), dst->ln, src->ln, s);
     }
     void swap_scratch(Field* f) {
         if (f->persistent) throw ApiError(MLEGS_ERR_STATE, "in-place transform of a persistent field");

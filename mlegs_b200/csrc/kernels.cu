@@ -45,6 +45,17 @@ void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s) {
     count_launch();
 }
 
+// dst = src over n entries and the field's LN slot (thread 0), in one launch.
+__global__ void copy_ln_kernel(double2* d, const double2* a, size_t n, double* dln, const double* aln) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t == 0) *dln = *aln;
+    if (t < n) d[t] = a[t];
+}
+void k_copy_ln(double2* dst, const double2* src, size_t n, double* dln, const double* sln, cudaStream_t s) {
+    copy_ln_kernel<<<nblk(n > 0 ? n : 1, 256), 256, 0, s>>>(dst, src, n, dln, sln);
+    count_launch();
+}
+
 // CHOPDO on FFF (mod_scalar3.f90:227-234): rows n >= NRCHOPS(m) -> 0.
 __global__ void chopdo_fff_kernel(DevGrid g, double2* a, int pad) {
     size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -57,6 +68,25 @@ __global__ void chopdo_fff_kernel(DevGrid g, double2* a, int pad) {
 void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s) {
     size_t n = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
     chopdo_fff_kernel<<<nblk(n, 256), 256, 0, s>>>(g, a, pad);
+    count_launch();
+}
+
+// COPY0 of an FFF field in one pass: dst = src with the entries CHOPDO clears
+// (rows n >= NRCHOPS(m) at pad, m >= NTCHOP) written as zero, LN copied.
+__global__ void copy_chop_fff_kernel(DevGrid g, double2* d, const double2* a, double* dln, const double* aln,
+                                     int pad) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t total = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    if (t == 0) *dln = *aln;
+    if (t >= total) return;
+    const int n = (int)((t / g.NXCHOPDIM) % g.NRCHOPDIM);
+    const int m = (int)(t / ((size_t)g.NXCHOPDIM * g.NRCHOPDIM));
+    d[t] = (n >= nrchops(g, m, pad) || m >= g.NTCHOP) ? make_double2(0.0, 0.0) : a[t];
+}
+void k_copy_chop_fff(const DevGrid& g, double2* dst, const double2* src, double* dln, const double* sln, int pad,
+                     cudaStream_t s) {
+    const size_t n = (size_t)g.NTCHOPDIM * g.NRCHOPDIM * g.NXCHOPDIM;
+    copy_chop_fff_kernel<<<nblk(n, 256), 256, 0, s>>>(g, dst, src, dln, sln, pad);
     count_launch();
 }
 

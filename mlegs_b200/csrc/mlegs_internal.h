@@ -84,6 +84,9 @@ void fft_set_attributes();
 void k_fill(double2* p, size_t n, cudaStream_t s);
 void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s);
 void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s);
+void k_copy_ln(double2* dst, const double2* src, size_t n, double* dln, const double* sln, cudaStream_t s);
+void k_copy_chop_fff(const DevGrid& g, double2* dst, const double2* src, double* dln, const double* sln, int pad,
+                     cudaStream_t s);
 
 // Legendre transforms (FP64 and split-BF16 tensor-core forms).
 // Split-BF16 tensor-core forms (split_gemm.cu).  mode 0: RTRAN(+1) images from

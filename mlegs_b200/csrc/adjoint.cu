@@ -510,12 +510,12 @@ struct Adj {
         dst->space = src->space;
     }
     void add(Field* y, const Field* x, double a = 1.0) {  // y += a x, E and LN
-        k_axpby(y->data, a, x->data, 0.0, nullptr, 1.0, c->d.elems(y->space), s());
-        k_ln_axpby(y->ln, a, x->ln, 0.0, nullptr, 1.0, s());
+        k_axpby_ln(y->data, a, x->data, 0.0, nullptr, 1.0, c->d.elems(y->space),
+                   y->ln, a, x->ln, 0.0, nullptr, 1.0, s());
     }
     void scale(Field* y, double a) {
-        k_axpby(y->data, a, y->data, 0.0, nullptr, 0.0, c->d.elems(y->space), s());
-        k_ln_copy(y->ln, y->ln, a, s());
+        k_axpby_ln(y->data, a, y->data, 0.0, nullptr, 0.0, c->d.elems(y->space),
+                   y->ln, a, y->ln, 0.0, nullptr, 0.0, s());
     }
     void chop(Field* f, int pad) { c->chopdo(f, pad); }
     void ln_rows(const Field* y, Field* out, double c0, double c1, double c2, bool acc) {
@@ -938,8 +938,8 @@ struct Adj {
             reserve(16);
             c->force(st[0], st[1], st[2], F0[0], F0[1], F0[2]);
             for (int q = 0; q < 3; ++q) {
-                k_axpby(x2[q]->data, 1.0, st[q]->data, hdt, F0[q]->data, 0.0, N, s());
-                k_ln_axpby(x2[q]->ln, 1.0, st[q]->ln, hdt, F0[q]->ln, 0.0, s());
+                k_axpby_ln(x2[q]->data, 1.0, st[q]->data, hdt, F0[q]->data, 0.0, N,
+                           x2[q]->ln, 1.0, st[q]->ln, hdt, F0[q]->ln, 0.0, s());
                 x2[q]->space = MLEGS_FFF;
             }
             c->ln_zero(x2[2]);

@@ -973,8 +973,7 @@ void mlegs_ctx::visc1(Field* A, double nu, double dt) {
     if (nu == 0.0) throw ApiError(MLEGS_ERR_SOLVER, "VISC1: NU CAN'T BE ZERO");
     double alp = 1 / (nu * dt);
     Field* WK = tmp();
-    k_axpby(WK->data, -alp, A->data, 0.0, nullptr, 0.0, fff(), s);
-    k_ln_copy(WK->ln, A->ln, -alp, s);
+    k_axpby_ln(WK->data, -alp, A->data, 0.0, nullptr, 0.0, fff(), WK->ln, -alp, A->ln, 0.0, nullptr, 0.0, s);
     WK->space = MLEGS_FFF;
     ihelm(WK, A, alp, 0);
     rel(WK);
@@ -986,8 +985,7 @@ void mlegs_ctx::visc2(Field* A, const Field* AO, double nu, double dt) {
     Field* WK = tmp();
     del2(AO, WK, 2);
     chopdo(WK, 0);
-    k_axpby(WK->data, -alp, A->data, 0.0, nullptr, -1.0, fff(), s);
-    k_ln_copy(WK->ln, A->ln, -alp, s);
+    k_axpby_ln(WK->data, -alp, A->data, 0.0, nullptr, -1.0, fff(), WK->ln, -alp, A->ln, 0.0, nullptr, 0.0, s);
     ihelm(WK, A, alp, 0);
     rel(WK);
 }
@@ -1050,38 +1048,29 @@ void mlegs_ctx::rich_fe_be() {
     force(psi, chi, b, NP, NC, NB);
     Field *P2 = tmp(), *C2 = tmp(), *B2 = tmp();
     const size_t N = fff();
-    k_axpby(P2->data, 1.0, psi->data, hdt, NP->data, 0.0, N, s);
-    k_ln_axpby(P2->ln, 1.0, psi->ln, hdt, NP->ln, 0.0, s);
-    k_axpby(C2->data, 1.0, chi->data, hdt, NC->data, 0.0, N, s);
-    k_ln_axpby(C2->ln, 1.0, chi->ln, hdt, NC->ln, 0.0, s);
-    k_axpby(B2->data, 1.0, b->data, hdt, NB->data, 0.0, N, s);
-    k_ln_set(B2->ln, 0.0, s);
+    k_axpby_ln(P2->data, 1.0, psi->data, hdt, NP->data, 0.0, N, P2->ln, 1.0, psi->ln, hdt, NP->ln, 0.0, s);
+    k_axpby_ln(C2->data, 1.0, chi->data, hdt, NC->data, 0.0, N, C2->ln, 1.0, chi->ln, hdt, NC->ln, 0.0, s);
+    k_axpby_ln(B2->data, 1.0, b->data, hdt, NB->data, 0.0, N, B2->ln, 0.0, nullptr, 0.0, nullptr, 0.0, s);
     P2->space = C2->space = B2->space = MLEGS_FFF;
     visc_be(P2, C2, B2, hdt);
     hyperv3(P2, C2, B2, hdt / p.dt);
     Field *PN = tmp(), *CN = tmp(), *BN = tmp();
     force(P2, C2, B2, PN, CN, BN);
-    k_axpby(P2->data, hdt, PN->data, 0.0, nullptr, 1.0, N, s);
-    k_ln_axpby(P2->ln, hdt, PN->ln, 0.0, nullptr, 1.0, s);
-    k_axpby(C2->data, hdt, CN->data, 0.0, nullptr, 1.0, N, s);
-    k_ln_axpby(C2->ln, hdt, CN->ln, 0.0, nullptr, 1.0, s);
+    k_axpby_ln(P2->data, hdt, PN->data, 0.0, nullptr, 1.0, N, P2->ln, hdt, PN->ln, 0.0, nullptr, 1.0, s);
+    k_axpby_ln(C2->data, hdt, CN->data, 0.0, nullptr, 1.0, N, C2->ln, hdt, CN->ln, 0.0, nullptr, 1.0, s);
     k_axpby(B2->data, hdt, BN->data, 0.0, nullptr, 1.0, N, s);
     rel(PN);
     rel(CN);
     rel(BN);
     visc_be(P2, C2, B2, hdt);
     hyperv3(P2, C2, B2, hdt / p.dt);
-    k_axpby(psi->data, dt, NP->data, 0.0, nullptr, 1.0, N, s);
-    k_ln_axpby(psi->ln, dt, NP->ln, 0.0, nullptr, 1.0, s);
-    k_axpby(chi->data, dt, NC->data, 0.0, nullptr, 1.0, N, s);
-    k_ln_axpby(chi->ln, dt, NC->ln, 0.0, nullptr, 1.0, s);
+    k_axpby_ln(psi->data, dt, NP->data, 0.0, nullptr, 1.0, N, psi->ln, dt, NP->ln, 0.0, nullptr, 1.0, s);
+    k_axpby_ln(chi->data, dt, NC->data, 0.0, nullptr, 1.0, N, chi->ln, dt, NC->ln, 0.0, nullptr, 1.0, s);
     k_axpby(b->data, dt, NB->data, 0.0, nullptr, 1.0, N, s);
     visc_be(psi, chi, b, dt);
     hyperv3(psi, chi, b, 1.0);
-    k_axpby(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, s);
-    k_ln_axpby(psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
-    k_axpby(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, s);
-    k_ln_axpby(chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby_ln(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby_ln(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
     k_axpby(b->data, 2.0, B2->data, 0.0, nullptr, -1.0, N, s);
     rel(P2);
     rel(C2);
@@ -1101,10 +1090,10 @@ void mlegs_ctx::step_ab_cn() {
     copy0(C0, chi, 0);
     copy0(B0, b, 0);
     const size_t N = fff();
-    k_axpby(psi->data, 1.5 * dt, PN->data, -0.5 * dt, NP->data, 1.0, N, s);
-    k_ln_axpby(psi->ln, 1.5 * dt, PN->ln, -0.5 * dt, NP->ln, 1.0, s);
-    k_axpby(chi->data, 1.5 * dt, CN->data, -0.5 * dt, NC->data, 1.0, N, s);
-    k_ln_axpby(chi->ln, 1.5 * dt, CN->ln, -0.5 * dt, NC->ln, 1.0, s);
+    k_axpby_ln(psi->data, 1.5 * dt, PN->data, -0.5 * dt, NP->data, 1.0, N,
+               psi->ln, 1.5 * dt, PN->ln, -0.5 * dt, NP->ln, 1.0, s);
+    k_axpby_ln(chi->data, 1.5 * dt, CN->data, -0.5 * dt, NC->data, 1.0, N,
+               chi->ln, 1.5 * dt, CN->ln, -0.5 * dt, NC->ln, 1.0, s);
     k_axpby(b->data, 1.5 * dt, BN->data, -0.5 * dt, NB->data, 1.0, N, s);
     copy0(NP, PN, 0);
     copy0(NC, CN, 0);
@@ -1181,10 +1170,8 @@ void mlegs_ctx::rich_etdfe_be() {
     etdfe_be(psi, chi, b, etdE, etdN, dt, true);
     visc_be(psi, chi, b, dt);
     const size_t N = fff();
-    k_axpby(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, s);
-    k_ln_axpby(psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
-    k_axpby(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, s);
-    k_ln_axpby(chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby_ln(psi->data, 2.0, P2->data, 0.0, nullptr, -1.0, N, psi->ln, 2.0, P2->ln, 0.0, nullptr, -1.0, s);
+    k_axpby_ln(chi->data, 2.0, C2->data, 0.0, nullptr, -1.0, N, chi->ln, 2.0, C2->ln, 0.0, nullptr, -1.0, s);
     k_axpby(b->data, 2.0, B2->data, 0.0, nullptr, -1.0, N, s);
     rel(P2);
     rel(C2);
@@ -1385,8 +1372,8 @@ int mlegs_field_axpby(mlegs_ctx* ctx, mlegs_field* y, double a, const mlegs_fiel
         const Field* f2 = x2 ? F(x2) : nullptr;
         for (const Field* q : {(const Field*)fy, f1, f2})
             if (q && q->space != MLEGS_FFF) throw ApiError(MLEGS_ERR_TRANSFORM, "axpby: FFF fields only");
-        k_axpby(fy->data, a, f1 ? f1->data : nullptr, b, f2 ? f2->data : nullptr, c, ctx->fff(), ctx->s);
-        k_ln_axpby(fy->ln, a, f1 ? f1->ln : nullptr, b, f2 ? f2->ln : nullptr, c, ctx->s);
+        k_axpby_ln(fy->data, a, f1 ? f1->data : nullptr, b, f2 ? f2->data : nullptr, c, ctx->fff(),
+                   fy->ln, a, f1 ? f1->ln : nullptr, b, f2 ? f2->ln : nullptr, c, ctx->s);
     });
 }
 

@@ -471,8 +471,7 @@ struct mlegs_ctx {
         const double alp = 1 / dt / nup * sg;
         const double bet = -sg * nu / nup;
         Field* wk = tmp();
-        k_axpby(wk->data, alp, a->data, 0.0, nullptr, 0.0, fff(), s);
-        k_ln_copy(wk->ln, a->ln, alp, s);
+        k_axpby_ln(wk->data, alp, a->data, 0.0, nullptr, 0.0, fff(), wk->ln, alp, a->ln, 0.0, nullptr, 0.0, s);
         wk->space = MLEGS_FFF;
         ihelmp(wk, a, P, -alp, bet, 0);
         rel(wk);

@@ -495,6 +495,36 @@ void k_axpby(double2* y, double a, const double2* x1, double b, const double2* x
     axpby_kernel<<<nblk(n, 256), 256, 0, s>>>(y, a, x1, b, x2, c, n);
     count_launch();
 }
+// k_axpby and k_ln_axpby in one launch: the field's entries as axpby_kernel,
+// its LN slot (thread 0) as ln_axpby_kernel.
+__global__ void axpby_ln_kernel(double2* y, double a, const double2* x1, double b, const double2* x2, double c,
+                                size_t n, double* yl, double la, const double* l1, double lb, const double* l2,
+                                double lc) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t == 0) {
+        double v = (lc != 0.0) ? lc * (*yl) : 0.0;
+        if (l1) v += la * (*l1);
+        if (l2) v += lb * (*l2);
+        *yl = v;
+    }
+    if (t >= n) return;
+    double2 v = make_double2(0.0, 0.0);
+    if (c != 0.0) v = cscale(y[t], c);
+    if (x1) {
+        v.x += a * x1[t].x;
+        v.y += a * x1[t].y;
+    }
+    if (x2) {
+        v.x += b * x2[t].x;
+        v.y += b * x2[t].y;
+    }
+    y[t] = v;
+}
+void k_axpby_ln(double2* y, double a, const double2* x1, double b, const double2* x2, double c, size_t n, double* yl,
+                double la, const double* l1, double lb, const double* l2, double lc, cudaStream_t s) {
+    axpby_ln_kernel<<<nblk(n > 0 ? n : 1, 256), 256, 0, s>>>(y, a, x1, b, x2, c, n, yl, la, l1, lb, l2, lc);
+    count_launch();
+}
 __global__ void ln_axpby_kernel(double* y, double a, const double* x1, double b, const double* x2, double c) {
     double v = (c != 0.0) ? c * (*y) : 0.0;
     if (x1) v += a * (*x1);

@@ -85,6 +85,8 @@ void k_fill(double2* p, size_t n, cudaStream_t s);
 void k_copy(double2* dst, const double2* src, size_t n, cudaStream_t s);
 void k_chopdo_fff(const DevGrid& g, double2* a, int pad, cudaStream_t s);
 void k_copy_ln(double2* dst, const double2* src, size_t n, double* dln, const double* sln, cudaStream_t s);
+void k_axpby_ln(double2* y, double a, const double2* x1, double b, const double2* x2, double c, size_t n, double* yl,
+                double la, const double* l1, double lb, const double* l2, double lc, cudaStream_t s);
 void k_copy_chop_fff(const DevGrid& g, double2* dst, const double2* src, double* dln, const double* sln, int pad,
                      cudaStream_t s);
 

@@ -301,10 +301,10 @@ void phase3(mlegs_ensemble& E, EnsInst& I) {
     c->copy0(I.B0, c->b, 0);
     const size_t N = c->fff();
     Field **H = c->hist;
-    k_axpby(c->psi->data, 1.5 * dt, I.PN->data, -0.5 * dt, H[0]->data, 1.0, N, c->s);
-    k_ln_axpby(c->psi->ln, 1.5 * dt, I.PN->ln, -0.5 * dt, H[0]->ln, 1.0, c->s);
-    k_axpby(c->chi->data, 1.5 * dt, I.CN->data, -0.5 * dt, H[1]->data, 1.0, N, c->s);
-    k_ln_axpby(c->chi->ln, 1.5 * dt, I.CN->ln, -0.5 * dt, H[1]->ln, 1.0, c->s);
+    k_axpby_ln(c->psi->data, 1.5 * dt, I.PN->data, -0.5 * dt, H[0]->data, 1.0, N,
+               c->psi->ln, 1.5 * dt, I.PN->ln, -0.5 * dt, H[0]->ln, 1.0, c->s);
+    k_axpby_ln(c->chi->data, 1.5 * dt, I.CN->data, -0.5 * dt, H[1]->data, 1.0, N,
+               c->chi->ln, 1.5 * dt, I.CN->ln, -0.5 * dt, H[1]->ln, 1.0, c->s);
     k_axpby(c->b->data, 1.5 * dt, I.BN->data, -0.5 * dt, H[2]->data, 1.0, N, c->s);
     c->copy0(H[0], I.PN, 0);
     c->copy0(H[1], I.CN, 0);
@@ -324,8 +324,8 @@ void phase3(mlegs_ensemble& E, EnsInst& I) {
         Field* WK = c->tmp();
         c->del2(AO[q], WK, 2);
         c->chopdo(WK, 0);
-        k_axpby(WK->data, -alp, A[q]->data, 0.0, nullptr, -1.0, N, c->s);
-        k_ln_copy(WK->ln, A[q]->ln, -alp, c->s);
+        k_axpby_ln(WK->data, -alp, A[q]->data, 0.0, nullptr, -1.0, N,
+                   WK->ln, -alp, A[q]->ln, 0.0, nullptr, 0.0, c->s);
         // IHELM(WK, A, ALP) up to its substitutions (mod_legops.f90:1204-1354)
         c->copy0(A[q], WK, 0);
         k_ln_copy(A[q]->ln, WK->ln, -1.0 / alp, c->s);

@@ -304,6 +304,127 @@ __global__ void __launch_bounds__(128) solve_T_kernel(const DevGrid g, const dou
     col[(size_t)size * st] = 0.0;
 }
 
+// solve_T_kernel for small systems (NRCHOP + pad <= 72 rows): one warp takes 16
+// systems, copies their factor rows and columns into shared memory in one
+// burst of cp.async copies, and runs the same substitutions there; rows from
+// the system size on are left as they are.  Blocks [0, nb0) hold the 7-band
+// m = 0 systems of kind 2.  Shared memory per block: R x 144 doubles.
+__global__ void __launch_bounds__(32) solve_T_small_kernel(const DevGrid g, const double* __restrict__ F5,
+                                                           const double* __restrict__ F7, double2* yfield, int kind,
+                                                           int pad, int t_begin, int nb0) {
+    extern __shared__ __align__(16) double sms[];
+    const int R = g.NRCHOP + pad;
+    double* Fs = sms;                         // [R][7][16]
+    double2* Xs = (double2*)(sms + R * 112);  // [R][16]
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int lane = threadIdx.x, sy = lane >> 1, comp = lane & 1;
+    const bool wide = (int)blockIdx.x < nb0;
+    const int tb = wide ? blockIdx.x * 16 : t_begin + (blockIdx.x - nb0) * 16;
+    const int nsb = min(16, (wide ? t_begin : nsys) - tb);
+    const size_t NK = g.NXCHOPDIM;
+    if (wide) {
+        for (int e = lane; e < R * 112; e += 32) {
+            const int r = e / 112, j = (e / 16) % 7, q = e % 16;
+            if (q < nsb)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(Fs + e)),
+                             "l"(F7 + ((size_t)r * 7 + j) * NK + tb + q)
+                             : "memory");
+        }
+    } else {
+        for (int e = lane; e < R * 80; e += 32) {
+            const int r = e / 80, j = (e / 16) % 5, q = e % 16;
+            if (q < nsb)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(Fs + (r * 7 + j) * 16 + q)),
+                             "l"(F5 + ((size_t)r * 5 + j) * nsys + tb + q)
+                             : "memory");
+        }
+    }
+    for (int e = lane; e < R * 16; e += 32) {
+        const int r = e / 16, q = e % 16;
+        if (q < nsb) {
+            const int tq = tb + q, mq = tq / g.NXCHOPDIM, kq = tq - mq * g.NXCHOPDIM;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(Xs + e)),
+                         "l"(yfield + (size_t)mq * g.NRCHOPDIM * NK + (size_t)r * NK + kq)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+    if (sy >= nsb) return;
+    const int t = tb + sy, k = t % g.NXCHOPDIM, m = t / g.NXCHOPDIM;
+    const int nn = nrc(g, m, pad);
+    double* X = (double*)Xs + sy * 2 + comp;  // row r at X[r * 32]
+    auto F = [&](int r, int j) { return Fs[(r * 7 + j) * 16 + sy]; };
+    int rows_out = 0;
+    if (!wide) {
+        const int size = nn;
+        double z1 = 0.0, z2 = 0.0;
+        for (int r = 0; r < size; ++r) {
+            const double ri = 1.0 / F(r, 2);
+            const double a1 = r >= 1 ? __dmul_rn(F(r - 1, 3), ri) : 0.0;
+            const double a2 = r >= 2 ? __dmul_rn(F(r - 2, 4), ri) : 0.0;
+            const double v = __fma_rn(-a1, z1, __fma_rn(-a2, z2, __dmul_rn(X[r * 32], ri)));
+            X[r * 32] = v;
+            z2 = z1;
+            z1 = v;
+        }
+        double x1 = 0.0, x2 = 0.0;
+        for (int r = size - 1; r >= 0; --r) {
+            const double e1 = r + 1 < size ? F(r + 1, 1) : 0.0;
+            const double e2 = r + 2 < size ? F(r + 2, 0) : 0.0;
+            const double v = __fma_rn(-e1, x1, __fma_rn(-e2, x2, X[r * 32]));
+            X[r * 32] = v;
+            x2 = x1;
+            x1 = v;
+        }
+        rows_out = size;
+    } else if (nn > 0) {
+        // w = XM^T y, then the transposed 7-band solve on NN - 1 rows, row NN - 1 zeroed
+        const double* xm = g.xm;
+        double prev = 0.0;
+        for (int r = 0; r < nn; ++r) {
+            const double yr = X[r * 32];
+            double v = yr;
+            if (r + 1 < nn) v = __fma_rn(xm[(size_t)(r + 1) * 2 + 0], X[(r + 1) * 32], v);
+            if (r >= 1) v = __fma_rn(xm[(size_t)(r - 1) * 2 + 1], prev, v);
+            X[r * 32] = v;
+            prev = yr;
+        }
+        const int size = nn - 1;
+        double z1 = 0.0, z2 = 0.0, z3 = 0.0;
+        for (int r = 0; r < size; ++r) {
+            const double ri = 1.0 / F(r, 3);
+            const double a1 = r >= 1 ? __dmul_rn(F(r - 1, 4), ri) : 0.0;
+            const double a2 = r >= 2 ? __dmul_rn(F(r - 2, 5), ri) : 0.0;
+            const double a3 = r >= 3 ? __dmul_rn(F(r - 3, 6), ri) : 0.0;
+            const double v = __fma_rn(-a1, z1, __fma_rn(-a2, z2, __fma_rn(-a3, z3, __dmul_rn(X[r * 32], ri))));
+            X[r * 32] = v;
+            z3 = z2;
+            z2 = z1;
+            z1 = v;
+        }
+        double x1 = 0.0, x2 = 0.0, x3 = 0.0;
+        for (int r = size - 1; r >= 0; --r) {
+            const double c1 = r + 1 < size ? F(r + 1, 2) : 0.0;
+            const double c2 = r + 2 < size ? F(r + 2, 1) : 0.0;
+            const double c3 = r + 3 < size ? F(r + 3, 0) : 0.0;
+            const double v = __fma_rn(-c1, x1, __fma_rn(-c2, x2, __fma_rn(-c3, x3, X[r * 32])));
+            X[r * 32] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
+        X[size * 32] = 0.0;
+        rows_out = nn;
+    }
+    double* col = (double*)(yfield + (size_t)m * g.NRCHOPDIM * NK + k) + comp;
+    const size_t st = 2 * NK;
+    for (int r = 0; r < rows_out; ++r) col[(size_t)r * st] = X[r * 32];
+}
+
 // Adjoints of VPRODSUB's cross product and VDOTPSUB's dot product
 // (mod_legops.f90:2105-2130, 2207-2225), pointwise on the packed physical
 // samples [r][z][j] (real and imaginary parts are separate samples):
@@ -682,6 +803,19 @@ struct Adj {
         return f;
     }
     void solve_T(const mlegs_ctx::SolveFactors* f, Field* y, int kind) {
+        if (c->d.NRCHOP <= 72) {  // the whole system fits in shared memory
+            const int nsys = c->d.NTCHOPDIM * c->d.NXCHOPDIM, t_begin = kind == 2 ? c->d.NXCHOPDIM : 0;
+            const int nb0 = (t_begin + 15) / 16, nb1 = (nsys - t_begin + 15) / 16;
+            const size_t smem = (size_t)c->d.NRCHOP * 144 * sizeof(double);
+            static size_t attr = 0;
+            if (smem > attr && smem > 48 * 1024) {
+                cudaFuncSetAttribute(solve_T_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                attr = smem;
+            }
+            solve_T_small_kernel<<<nb0 + nb1, 32, smem, s()>>>(g(), f->F5, f->F7, y->data, kind, 0, t_begin, nb0);
+            count_launch();
+            return;
+        }
         const int nw = 2 * c->d.NXCHOPDIM, wpad = kind == 2 ? (32 - nw % 32) % 32 : 0;
         const int n = 2 * c->d.NTCHOPDIM * c->d.NXCHOPDIM + wpad;
         solve_T_kernel<<<nb(n, 128), 128, 0, s()>>>(g(), f->F5, f->F7, y->data, kind, 0, wpad);

@@ -510,8 +510,174 @@ __global__ void __launch_bounds__(128) solve_factored_kernel(DevGrid g, const do
     solve_factored_sys<16>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield, u);
 }
 
+// Small systems (NRCHOP + pad <= SMALL_R rows): one warp takes 16 systems
+// (lane = system x real/imaginary part), copies their factor rows and
+// right-hand sides into shared memory in one burst of cp.async copies, and
+// runs the substitutions and the tails of solve_factored_sys there, with the
+// same operations in the same order.  Blocks [0, nb0) hold the t_begin
+// 7-band m = 0 systems of kinds 1 and 2, the rest the 5-band ones, so no
+// warp mixes the two.  Shared memory per block: R x 144 doubles (factor rows
+// [r][7][16], values [r][16] complex), R = NRCHOP + pad.
+constexpr int SMALL_R = 72;
+
+__device__ __forceinline__ void cpa8(double* d, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(d)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa16(double2* d, const double2* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(d)), "l"(src)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(32) solve_small_kernel(DevGrid g, const double* __restrict__ F5,
+                                                         const double* __restrict__ F7, const double2* src,
+                                                         double2* dst, double* ln_out, int kind, int has_ln,
+                                                         double ln_in, int pad, int farfield, int t_begin, int nb0) {
+    extern __shared__ __align__(16) double sms[];
+    const int R = g.NRCHOP + pad;
+    double* Fs = sms;                         // [R][7][16]
+    double2* Xs = (double2*)(sms + R * 112);  // [R][16]
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int lane = threadIdx.x, sy = lane >> 1, comp = lane & 1;
+    const bool wide_blk = (int)blockIdx.x < nb0;
+    const int tb = wide_blk ? blockIdx.x * 16 : t_begin + (blockIdx.x - nb0) * 16;
+    const int tend = wide_blk ? t_begin : nsys;
+    const int nsb = min(16, tend - tb);
+    const size_t NK = g.NXCHOPDIM;
+    // the burst: factor rows, then the right-hand sides
+    if (wide_blk) {
+        for (int e = lane; e < R * 112; e += 32) {
+            const int r = e / 112, j = (e / 16) % 7, q = e % 16;
+            if (q < nsb) cpa8(Fs + e, F7 + ((size_t)r * 7 + j) * NK + tb + q);
+        }
+    } else {
+        for (int e = lane; e < R * 80; e += 32) {
+            const int r = e / 80, j = (e / 16) % 5, q = e % 16;
+            if (q < nsb) cpa8(Fs + (r * 7 + j) * 16 + q, F5 + ((size_t)r * 5 + j) * nsys + tb + q);
+        }
+    }
+    for (int e = lane; e < R * 16; e += 32) {
+        const int r = e / 16, q = e % 16;
+        if (q < nsb) {
+            const int tq = tb + q, mq = tq / g.NXCHOPDIM, kq = tq - mq * g.NXCHOPDIM;
+            cpa16(Xs + e, src + (size_t)mq * g.NRCHOPDIM * NK + (size_t)r * NK + kq);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+    if (sy >= nsb) return;
+    const int t = tb + sy, k = t % g.NXCHOPDIM, m = t / g.NXCHOPDIM;
+    int nn = g.NRCHOP + pad - m;
+    if (nn < 0) nn = 0;
+    const bool wide = wide_blk;
+    int size = (m == 0 && kind == 2) ? nn - 1 : nn;
+    if (size < 0) size = 0;
+    double* X = (double*)Xs + sy * 2 + comp;  // row r at X[r * 32]
+    auto F = [&](int r, int j) { return Fs[(r * 7 + j) * 16 + sy]; };
+    // IDEL2 (m = 0, k = 0): right-hand side shifted down one row, row 0 <- the LN condition
+    if (kind == 1 && m == 0 && k == 0) {
+        for (int r = size - 1; r >= 1; --r) X[r * 32] = X[(r - 1) * 32];
+        if (size > 0) X[0] = comp ? 0.0 : (has_ln ? ln_in / g.norm0[0] : 0.0);
+    }
+    if (!wide) {
+        double y1 = 0.0, y2 = 0.0;
+        for (int r = 0; r < size; ++r) {
+            const double y = __fma_rn(-F(r, 1), y1, __fma_rn(-F(r, 0), y2, X[r * 32]));
+            X[r * 32] = y;
+            y2 = y1;
+            y1 = y;
+        }
+        double x1 = 0.0, x2 = 0.0;
+        for (int r = size - 1; r >= 0; --r) {
+            const double ri = 1.0 / F(r, 2);
+            const double a1 = (r + 1 < size) ? __dmul_rn(F(r, 3), ri) : 0.0;
+            const double a2 = (r + 2 < size) ? __dmul_rn(F(r, 4), ri) : 0.0;
+            const double v = __fma_rn(-a1, x1, __fma_rn(-a2, x2, __dmul_rn(X[r * 32], ri)));
+            X[r * 32] = v;
+            x2 = x1;
+            x1 = v;
+        }
+    } else {
+        double y1 = 0.0, y2 = 0.0, y3 = 0.0;
+        for (int r = 0; r < size; ++r) {
+            const double y = __fma_rn(-F(r, 2), y1, __fma_rn(-F(r, 1), y2, __fma_rn(-F(r, 0), y3, X[r * 32])));
+            X[r * 32] = y;
+            y3 = y2;
+            y2 = y1;
+            y1 = y;
+        }
+        double x1 = 0.0, x2 = 0.0, x3 = 0.0;
+        for (int r = size - 1; r >= 0; --r) {
+            const double ri = 1.0 / F(r, 3);
+            const double a1 = (r + 1 < size) ? __dmul_rn(F(r, 4), ri) : 0.0;
+            const double a2 = (r + 2 < size) ? __dmul_rn(F(r, 5), ri) : 0.0;
+            const double a3 = (r + 3 < size) ? __dmul_rn(F(r, 6), ri) : 0.0;
+            const double v =
+                __fma_rn(-a1, x1, __fma_rn(-a2, x2, __fma_rn(-a3, x3, __dmul_rn(X[r * 32], ri))));
+            X[r * 32] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
+    }
+    // the tails of solve_factored_sys, on the staged column
+    for (int r = size; r < R; ++r) X[r * 32] = 0.0;
+    if (m == 0 && kind == 2 && nn > 0) {
+        const double* xm = g.xm;
+        double prev = 0.0;
+        for (int r = 0; r < nn; ++r) {
+            const double cur = X[r * 32];
+            const double nxt = (r + 1 < nn) ? X[(r + 1) * 32] : 0.0;
+            double v = cur;
+            if (r >= 1) v = __fma_rn(xm[(size_t)r * 2], prev, v);
+            if (r + 1 < nn) v = __fma_rn(xm[(size_t)r * 2 + 1], nxt, v);
+            X[r * 32] = v;
+            prev = cur;
+        }
+    }
+    if (m == 0 && k == 0 && size > 0) {
+        if (kind == 0) {
+            if (!comp) *ln_out = __dmul_rn(X[0], g.norm0[0]);
+            X[0] = 0.0;
+        } else if (kind == 1 && !comp && ln_out) {
+            *ln_out = has_ln ? __dmul_rn(X[0], g.norm0[0]) : 0.0;
+        }
+    }
+    if (farfield && m == 0) {
+        double sum = 0.0;
+        for (int r = 0; r < R && r < g.NRCHOPDIM; ++r) sum = __fma_rn(g.at1[r], X[r * 32], sum);
+        X[0] = __dsub_rn(X[0], __ddiv_rn(sum, g.at1[0]));
+    }
+    double* col = (double*)(dst + (size_t)m * g.NRCHOPDIM * NK + k) + comp;
+    const size_t st = 2 * NK;
+    for (int r = 0; r < g.NRCHOPDIM; ++r) col[(size_t)r * st] = r < R ? X[r * 32] : 0.0;
+}
+
+bool solve_small_ok(const DevGrid& g, int pad) { return g.NRCHOP + pad <= SMALL_R; }
+
+void k_solve_small(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
+                   double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s) {
+    const int nsys = g.NTCHOPDIM * g.NXCHOPDIM;
+    const int t_begin = kind == 0 ? 0 : g.NXCHOPDIM;
+    const int nb0 = (t_begin + 15) / 16, nb1 = (nsys - t_begin + 15) / 16;
+    const int R = g.NRCHOP + pad;
+    const size_t smem = (size_t)R * 144 * sizeof(double);
+    static size_t attr = 0;
+    if (smem > attr && smem > 48 * 1024) {
+        cudaFuncSetAttribute(solve_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = smem;
+    }
+    solve_small_kernel<<<nb0 + nb1, 32, smem, s>>>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield,
+                                                   t_begin, nb0);
+    count_launch();
+}
+
 void k_solve_factored(const DevGrid& g, const double* F5, const double* F7, const double2* src, double2* dst,
                       double* ln_out, int kind, int has_ln, double ln_in, int pad, int farfield, cudaStream_t s) {
+    if (solve_small_ok(g, pad)) {  // the whole system fits in shared memory
+        k_solve_small(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad, farfield, s);
+        return;
+    }
     const int wpad = kind == 0 ? 0 : (32 - (2 * g.NXCHOPDIM) % 32) % 32;
     const int n = 2 * g.NTCHOPDIM * g.NXCHOPDIM + wpad;
     solve_factored_kernel<<<(n + 127) / 128, 128, 0, s>>>(g, F5, F7, src, dst, ln_out, kind, has_ln, ln_in, pad,

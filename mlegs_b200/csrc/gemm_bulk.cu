@@ -597,9 +597,9 @@ int bulk_sm_count() {
     return n;
 }
 
-template <int MTW>
-void launch_b2p_bulk(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
-    constexpr int NST = 4;
+template <int MTW, int NST>
+void launch_b2p_bulk_n(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, int per_sm,
+                       cudaStream_t s) {
     constexpr int SA = BNW * MTW * 8 + (((BNW * MTW) & 1) ? 0 : 8);
     constexpr size_t smem = (size_t)NST * (BK * SA + BK * BSB) * sizeof(double) + 2 * NST * sizeof(uint64_t);
     static bool attr = false;
@@ -609,10 +609,17 @@ void launch_b2p_bulk(const DevGrid& g, const double2* a, double2* b, const doubl
     }
     const int ncol = 2 * g.NXCHOPDIM;
     const int ntiles = ((ncol + BCT - 1) / BCT) * g.NTCHOPDIM;
-    const int per_sm = MTW <= 3 ? 3 : 2;
     const int grid = std::min(ntiles, bulk_sm_count() * per_sm);
     b2p_bulk_kernel<MTW, NST><<<grid, (BNW + 1) * 32, smem, s>>>(g, (const double*)a, (double*)b, ln, pad);
     count_launch();
+}
+
+// Three stages at three CTAs per SM (55 KB each at MTW = 3) leave room on every
+// SM for a VERFFT(+1) CTA, which runs beside the GEMM on the other stream in
+// TOFP; four stages filled the SM (545 vs 541 steps/s at 192x128x256).
+template <int MTW>
+void launch_b2p_bulk(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s) {
+    launch_b2p_bulk_n<MTW, 3>(g, a, b, ln, pad, MTW <= 3 ? 3 : 2, s);
 }
 
 template <int MT>

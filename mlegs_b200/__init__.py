@@ -431,7 +431,7 @@ class Context:
                "horfft_f": 5, "pointwise": 6, "solve": 7, "phys": 8,
                "horfft_wb": 9, "horfft_wf": 10, "split_b2p": 11,
                "split_p2b": 12, "project": 13,
-               "project_fff": 14, "phys_nonlin": 15, "roundtrip": 16}
+               "project_fff": 14, "phys_nonlin": 15, "roundtrip": 16, "dmma_peak": 17}
 
     def kernel_time(self, name, reps=20):
         """Mean device ms per launch of one internal kernel (CUDA events on the

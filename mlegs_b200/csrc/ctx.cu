@@ -1963,7 +1963,7 @@ int mlegs_check_finite(mlegs_ctx* ctx) {
 }
 
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch) {
-    if (reps < 1 || kernel < 0 || kernel > 16) return MLEGS_ERR_ARG;
+    if (reps < 1 || kernel < 0 || kernel > 17) return MLEGS_ERR_ARG;
     return guard(ctx, [&] {
         const Dims& d = ctx->d;
         const DevGrid& g = ctx->g;
@@ -1971,6 +1971,9 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
         if ((kernel == 11 || kernel == 12) && !ctx->split_S)
             throw ApiError(MLEGS_ERR_STATE, "context was not created with MLEGS_PREC_SPLIT");
         if (kernel == 14 && !ctx->compV) throw ApiError(MLEGS_ERR_STATE, "needs an FP64 context on the tensor path");
+        // k_dmma_peak writes one double per thread: SMs x 4 CTAs x 256 threads
+        if (kernel == 17 && (double)d.cap() * 2.0 < dmma_peak_flops() / (8.0 * 4096 * 8 * 512.0 / 256.0))
+            throw ApiError(MLEGS_ERR_ARG, "field buffers too small for the FP64 ceiling kernel's output");
         // the temporaries go back to the pool however the timing ends
         struct PoolReturn {
             mlegs_ctx* c;
@@ -2024,6 +2027,9 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
                     double2* out[4] = {a->data, b->data, c->data, e->data};
                     k_theta_fused(g, ctx->fft, in, out, 0.0, 0.0, 0, s);
                 } break;
+                case 17:  // the FP64 tensor-path ceiling (FLOPs in place of bytes)
+                    k_dmma_peak((double*)a->data, s);
+                    break;
                 case 16:  // TOFP then TOFF of one FFF field (RTRAN, VERFFT, HORFFT and back)
                     ctx->mark();
                     a->space = MLEGS_FFF;
@@ -2079,6 +2085,7 @@ int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launc
             case 14: bytes = B16 * 5.0 * (double)d.fff(); break;
             // each stage reads its input and writes its output, both ways
             case 16: bytes = 2.0 * B16 * ((double)d.fff() + 2.0 * (double)d.pff() + 2.0 * (double)d.pfp() + (double)d.ppp()); break;
+            case 17: bytes = dmma_peak_flops(); break;  // FLOPs, not bytes
             default: bytes = B16 * ((double)d.pfp() + (double)d.ppp()); break;
         }
         for (int q = 0; q < 3; ++q) launch();  // warm-up

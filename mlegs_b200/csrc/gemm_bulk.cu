@@ -665,7 +665,37 @@ bool field_map(const DevGrid& g, const double* x, CUtensorMap* map) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Register-only ceiling of the FP64 tensor path: every warp issues DPK_ITER
+// rounds of eight independent mma.sync.m8n8k4.f64 on register fragments (no
+// memory traffic but one store per thread at the end), DPK_CTAS CTAs of eight
+// warps per SM.  The GEMMs' tensor-pipe fractions are read against it.
+constexpr int DPK_ITER = 4096, DPK_CTAS = 4;
+__global__ void __launch_bounds__(256) dmma_peak_kernel(double* out, double seed) {
+    double acc[8][2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+    const double a = seed * (1 + (threadIdx.x & 3)), b = seed * (2 + (threadIdx.x >> 5));
+    for (int it = 0; it < DPK_ITER; ++it) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) dmma(acc[j], a, b);
+    }
+    double v = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v += acc[j][0] + acc[j][1];
+    out[blockIdx.x * (size_t)blockDim.x + threadIdx.x] = v;
+}
+
 }  // namespace
+
+// FLOPs of one k_dmma_peak launch: CTAs x warps x rounds x MMAs x (8 x 8 x 4 x 2)
+double dmma_peak_flops() { return (double)bulk_sm_count() * DPK_CTAS * 8 * DPK_ITER * 8 * 512.0; }
+
+// out: at least SMs x DPK_CTAS x 256 doubles
+double k_dmma_peak(double* out, cudaStream_t s) {
+    dmma_peak_kernel<<<bulk_sm_count() * DPK_CTAS, 256, 0, s>>>(out, 1e-3);
+    count_launch();
+    return dmma_peak_flops();
+}
 
 bool b2p_bulk_supported(const DevGrid& g) {
     const int RT = (g.NRH + 7) / 8;

@@ -163,6 +163,9 @@ void k_grouped_solve(const GroupSolve* d, const int* first, int np, int total_bl
 // (gemm_bulk.cu), the form k_rtran_b2p takes when supported; a timed-out
 // wait raises the module's error word, read (and cleared) by bulk_gemm_error.
 bool b2p_bulk_supported(const DevGrid& g);
+// FP64 tensor-path ceiling microbenchmark (register-only MMAs); FLOPs per launch
+double k_dmma_peak(double* out, cudaStream_t s);
+double dmma_peak_flops();
 void k_rtran_b2p_bulk(const DevGrid& g, const double2* a, double2* b, const double* ln, int pad, cudaStream_t s);
 int bulk_gemm_error(bool reset);
 // Fold GEMMs (RTRAN(-1), PROJECT's products) on the same pipeline: weight

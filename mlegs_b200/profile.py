@@ -10,7 +10,8 @@ The launch count before the steps is printed so a profiler can skip it.
 
 With --kernel, runs Context.kernel_time(NAME, reps) instead: 3 warm-up
 launches of that one kernel, then --reps timed ones, on the configuration's
-field sizes (for a single-kernel capture: skip 3, capture 1).
+field sizes (for a single-kernel capture: skip 3, capture 1).  --kernel
+dmma_peak times register-only FP64 MMAs and prints the tensor path's ceiling.
 """
 
 import argparse
@@ -33,7 +34,10 @@ def main():
     ctx = M.Context(cfg, precision=M.PREC_FP64 if a.precision == "fp64" else M.PREC_SPLIT)
     if a.kernel:
         ms, nbytes = ctx.kernel_time(a.kernel, a.reps)
-        print("%s: %.1f us per launch, %.1f GB/s algorithmic" % (a.kernel, ms * 1e3, nbytes / ms / 1e6))
+        if a.kernel == "dmma_peak":  # the figure is FLOPs: the FP64 tensor-path ceiling
+            print("%s: %.1f us per launch, %.2f TFLOP/s" % (a.kernel, ms * 1e3, nbytes / ms / 1e9))
+        else:
+            print("%s: %.1f us per launch, %.1f GB/s algorithmic" % (a.kernel, ms * 1e3, nbytes / ms / 1e6))
         ctx.close()
         return
     psi, chi, b = M.initial_state(ctx)

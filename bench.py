@@ -192,6 +192,14 @@ def traffic_table():
         return {}
 
 
+def legendre_flops(cfg, nxchopdim):
+    """FP64 flops of one RTRAN-equivalent Legendre product with the parity fold
+    (mod_fft.f90:1264-1336): 2 NR (sum over m < NTCHOP of NRCHOPS(m)) NXCHOPDIM,
+    NRCHOPS(m) = NRCHOP - m (474 MFLOP at 192x128x256)."""
+    snn = sum(max(0, cfg.nrchop - m) for m in range(cfg.ntchop))
+    return 2.0 * cfg.nr * snn * nxchopdim
+
+
 def oracle_steps(cfg, nsteps, warm=0):
     """Time steady-state oracle steps (zeroed AB/ETD history: same arithmetic)."""
     import numpy as np
@@ -553,6 +561,15 @@ def run_ours(args, cfg, ws, rank, local):
             kernels[name] = {"ms": ms, "flops": by, "tflops": by / (ms * 1e-3) / 1e12}
         else:
             kernels[name] = {"ms": ms, "bytes": by, "gbs": by / (ms * 1e-3) / 1e9}
+    # the Legendre GEMMs in useful FP64 flops against the FP64 tensor path's ceiling
+    # (register-only m8n8k4 MMAs, timed above); PROJECT is five fold products
+    ceil = kernels.get("dmma_peak", {}).get("tflops")
+    if ceil and not split:
+        fl = legendre_flops(cfg, ctx.NXCHOPDIM)
+        for name, nprod in (("rtran_b2p", 1), ("rtran_p2b", 1), ("project", 5)):
+            if name in kernels:
+                tf = nprod * fl / (kernels[name]["ms"] * 1e-3) / 1e12
+                kernels[name].update(fp64_flops=nprod * fl, tflops=tf, frac_of_fp64_ceiling=tf / ceil)
     dom = DOMINANT
     tr = traffic_table().get(cfg.name, {}).get(dom)
     ach = kernels[dom]["gbs"]

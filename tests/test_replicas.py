@@ -60,5 +60,20 @@ def test_reference_arm_runs_on_rank0_only(capsys):
     assert capsys.readouterr().out == ""
 
 
+def test_legendre_flop_count():
+    """The useful FP64 flops bench.py divides the GEMM times into: 2 NR (sum over
+    m < NTCHOP of NRCHOP - m) NXCHOPDIM, i.e. 474 MFLOP per RTRAN-equivalent at
+    192x128x256 (chops 128, 85, 85: sum 7310, NXCHOPDIM 169)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from mlegs_b200.inputs import CONFIGS
+    cfg = CONFIGS["etd_192x128x256"]
+    assert (cfg.nr, cfg.nrchop, cfg.ntchop, cfg.nxchop) == (192, 128, 85, 85)
+    assert bench.legendre_flops(cfg, 2 * cfg.nxchop - 1) == 2.0 * 192 * 7310 * 169
+    # m past NRCHOP contributes nothing
+    small = type("C", (), {"nr": 8, "nrchop": 3, "ntchop": 6})()
+    assert bench.legendre_flops(small, 5) == 2.0 * 8 * (3 + 2 + 1) * 5
+
+
 if __name__ == "__main__":
     sys.exit(pytest.main([__file__, "-q"]))

@@ -280,6 +280,19 @@ int mlegs_solver_init(mlegs_ctx* ctx, mlegs_field* psi, mlegs_field* chi, mlegs_
 int mlegs_step(mlegs_ctx* ctx, int nsteps);
 /* Capture one steady-state step as a CUDA graph and replay it nsteps times. */
 int mlegs_step_graph(mlegs_ctx* ctx, int nsteps);
+/* nsteps graph-replayed steps with the state streamed through host memory:
+ * per step the same as mlegs_field_upload(psi, chi, b in FFF from host[0..2],
+ * LN ln[0..2]), mlegs_step_graph(ctx, 1) and mlegs_field_download into the
+ * same buffers (host-driven time stepping, TIME_STEPPING mod_march.f90:243-307,
+ * with the state on the host between steps).  host[i] is a FFF array in the
+ * reference layout (NRCHOPDIM x NTCHOPDIM x NXCHOPDIM complex, Fortran order),
+ * page-locked for the copies to overlap; ln is read at the start and holds the
+ * last step's LN values on return.  The copies run on their own streams, each
+ * direction on its own: the upload of field i for the next step waits only for
+ * field i's download, so it overlaps the downloads of the fields after it.
+ * Returns after the last download; nsteps = 0 only sets up the streams and
+ * buffers (3 + 3 FFF staging arrays on the device). */
+int mlegs_run_host(mlegs_ctx* ctx, int nsteps, double* const* host, double* ln);
 /* Simulation time and step counter (TIM%T, TIM%N). */
 int mlegs_time(const mlegs_ctx* ctx, double* t, int32_t* n);
 /* Non-finite check of the state (ANYNAN, mod_scalar3.f90:998-1045):

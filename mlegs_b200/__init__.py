@@ -415,6 +415,22 @@ class Context:
         fn = self.lib.mlegs_step_graph if graph else self.lib.mlegs_step
         self._ck(fn(self.c, int(n)))
 
+    def run_host(self, hosts, lns, n=1):
+        """n graph-replayed steps with the state streamed through host memory
+        (mlegs_run_host): per step psi, chi, b are uploaded from ``hosts`` (FFF,
+        Fortran-ordered complex128, page-locked for overlapped copies) with LN
+        ``lns`` and downloaded back into them.  Returns the last LN values."""
+        if len(hosts) != 3 or len(lns) != 3:
+            raise ValueError("run_host streams the three state fields psi, chi, b")
+        want = self.shape(FFF)
+        for h in hosts:
+            if tuple(h.shape) != want or h.dtype != np.complex128 or not h.flags.f_contiguous:
+                raise ValueError("hosts must be Fortran-ordered complex128 arrays of shape %s" % (want,))
+        ptrs = (ctypes.c_void_p * 3)(*[h.ctypes.data for h in hosts])
+        ln = (ctypes.c_double * 3)(*[float(v) for v in lns])
+        self._ck(self.lib.mlegs_run_host(self.c, int(n), ctypes.cast(ptrs, ctypes.c_void_p), ln))
+        return [ln[0], ln[1], ln[2]]
+
     def time(self):
         t = ctypes.c_double()
         n = ctypes.c_int32()

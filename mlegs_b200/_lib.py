@@ -99,6 +99,7 @@ SIGNATURES = {
     "mlegs_solver_init": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mlegs_step": (c_int, [c_void_p, c_int]),
     "mlegs_step_graph": (c_int, [c_void_p, c_int]),
+    "mlegs_run_host": (c_int, [c_void_p, c_int, c_void_p, dptr]),
     "mlegs_time": (c_int, [c_void_p, dptr, ctypes.POINTER(ctypes.c_int32)]),
     "mlegs_check_finite": (c_int, [c_void_p]),
     "mlegs_kernel_time": (c_int, [c_void_p, c_int, c_int, dptr, dptr]),

@@ -460,6 +460,13 @@ void mlegs_ctx::destroy() {
     allocs.clear();
     for (cudaEvent_t& e : evs)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : io_ev)
+        if (e) cudaEventDestroy(e);
+    if (io_ln) cudaFreeHost(io_ln);
+    io_ln = nullptr;
+    if (s_up) cudaStreamDestroy(s_up);
+    if (s_down) cudaStreamDestroy(s_down);
+    s_up = s_down = nullptr;
     if (s2) cudaStreamDestroy(s2);
     s2 = nullptr;
     if (s) cudaStreamDestroy(s);
@@ -1903,38 +1910,118 @@ int mlegs_step(mlegs_ctx* ctx, int nsteps) {
     });
 }
 
+// nsteps replays of the captured steady step on ctx->s (captured on first use)
+static void graph_steps(mlegs_ctx* ctx, int nsteps) {
+    if (!ctx->gexec) {
+        ctx->mark();
+        double t0 = ctx->t;
+        int n0 = ctx->n;
+        int64_t before = ctx->launches;
+        CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+        try {
+            ctx->step_once();
+        } catch (...) {
+            cudaGraph_t gtmp = nullptr;
+            cudaStreamEndCapture(ctx->s, &gtmp);
+            if (gtmp) cudaGraphDestroy(gtmp);
+            ctx->restore();
+            throw;
+        }
+        CK(cudaStreamEndCapture(ctx->s, &ctx->graph));
+        ctx->graph_launches = ctx->launches - before;
+        ctx->launches = before;
+        ctx->restore();
+        ctx->t = t0;
+        ctx->n = n0;
+        CK(cudaGraphInstantiate(&ctx->gexec, ctx->graph, 0));
+    }
+    for (int q = 0; q < nsteps; ++q) {
+        CK(cudaGraphLaunch(ctx->gexec, ctx->s));
+        ctx->launches += ctx->graph_launches;
+        ctx->t += ctx->p.dt;
+        ctx->n += 1;
+    }
+}
+
 int mlegs_step_graph(mlegs_ctx* ctx, int nsteps) {
     return guard(ctx, [&] {
         if (!ctx->solver_ready) throw ApiError(MLEGS_ERR_STATE, "mlegs_solver_init has not run");
-        if (!ctx->gexec) {
-            ctx->mark();
-            double t0 = ctx->t;
-            int n0 = ctx->n;
-            int64_t before = ctx->launches;
-            CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
-            try {
-                ctx->step_once();
-            } catch (...) {
-                cudaGraph_t gtmp = nullptr;
-                cudaStreamEndCapture(ctx->s, &gtmp);
-                if (gtmp) cudaGraphDestroy(gtmp);
-                ctx->restore();
-                throw;
+        graph_steps(ctx, nsteps);
+    });
+}
+
+// Per step: mlegs_field_upload of the three state fields (FFF) from host[i] /
+// ln[i], one graph replay, mlegs_field_download into the same buffers.  The
+// copies run on s_up / s_down and the layout conversions and the step on
+// ctx->s.  Each field moves in IO_CHUNKS pieces and the next step's upload of
+// a piece waits only for that piece's download, so the uploads run beside the
+// downloads one piece behind them.
+int mlegs_run_host(mlegs_ctx* ctx, int nsteps, double* const* host, double* ln) {
+    if (nsteps < 0 || !host || !ln) return MLEGS_ERR_ARG;
+    for (int i = 0; i < 3; ++i)
+        if (!host[i]) return MLEGS_ERR_ARG;
+    return guard(ctx, [&] {
+        if (!ctx->solver_ready) throw ApiError(MLEGS_ERR_STATE, "mlegs_solver_init has not run");
+        const Dims& d = ctx->d;
+        const size_t bytes = (size_t)d.NRCHOPDIM * d.NTCHOPDIM * d.NXCHOPDIM * sizeof(double2);
+        Field* st[3] = {ctx->psi, ctx->chi, ctx->b};
+        // set up on first use (each piece again if an earlier set-up stopped half way)
+        if (!ctx->s_up) CK(cudaStreamCreateWithFlags(&ctx->s_up, cudaStreamNonBlocking));
+        if (!ctx->s_down) CK(cudaStreamCreateWithFlags(&ctx->s_down, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : ctx->io_ev)
+            if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (int i = 0; i < 3; ++i) {
+            if (!ctx->io_in[i]) ctx->io_in[i] = dalloc<double2>(bytes / sizeof(double2));
+            if (!ctx->io_out[i]) ctx->io_out[i] = dalloc<double2>(bytes / sizeof(double2));
+        }
+        if (!ctx->io_ln) CK(cudaHostAlloc((void**)&ctx->io_ln, 3 * sizeof(double), cudaHostAllocDefault));
+        if (nsteps == 0) return;
+        for (int i = 0; i < 3; ++i) ctx->io_ln[i] = ln[i];
+        // the first uploads overwrite the state's LN slots: after the work already queued on ctx->s
+        cudaEvent_t* ev = ctx->io_ev;
+        constexpr int NC = mlegs_ctx::IO_CHUNKS;
+        size_t cut[NC + 1];  // byte offsets of the pieces, on 16-byte entries
+        const size_t elems = bytes / sizeof(double2);
+        for (int j = 0; j <= NC; ++j) cut[j] = elems * j / NC * sizeof(double2);
+        CK(cudaEventRecord(ev[0], ctx->s));
+        CK(cudaStreamWaitEvent(ctx->s_up, ev[0], 0));
+        try {
+            for (int k = 0; k < nsteps; ++k) {
+                for (int i = 0; i < 3; ++i) {
+                    for (int j = 0; j < NC; ++j) {
+                        if (k > 0) CK(cudaStreamWaitEvent(ctx->s_up, ev[6 + NC * i + j], 0));
+                        CK(cudaMemcpyAsync((char*)ctx->io_in[i] + cut[j], (const char*)host[i] + cut[j],
+                                           cut[j + 1] - cut[j], cudaMemcpyHostToDevice, ctx->s_up));
+                    }
+                    CK(cudaMemcpyAsync(st[i]->ln, ctx->io_ln + i, sizeof(double), cudaMemcpyHostToDevice, ctx->s_up));
+                    CK(cudaEventRecord(ev[i], ctx->s_up));
+                    CK(cudaStreamWaitEvent(ctx->s, ev[i], 0));
+                    k_from_ref(ctx->g, MLEGS_FFF, ctx->io_in[i], st[i]->data, ctx->s);
+                    st[i]->space = MLEGS_FFF;
+                }
+                graph_steps(ctx, 1);
+                for (int i = 0; i < 3; ++i) {
+                    k_to_ref(ctx->g, MLEGS_FFF, st[i]->data, ctx->io_out[i], ctx->s);
+                    CK(cudaEventRecord(ev[3 + i], ctx->s));
+                    CK(cudaStreamWaitEvent(ctx->s_down, ev[3 + i], 0));
+                    for (int j = 0; j < NC; ++j) {
+                        CK(cudaMemcpyAsync((char*)host[i] + cut[j], (const char*)ctx->io_out[i] + cut[j],
+                                           cut[j + 1] - cut[j], cudaMemcpyDeviceToHost, ctx->s_down));
+                        if (j == NC - 1)  // the last piece's event covers the LN too
+                            CK(cudaMemcpyAsync(ctx->io_ln + i, st[i]->ln, sizeof(double), cudaMemcpyDeviceToHost,
+                                               ctx->s_down));
+                        CK(cudaEventRecord(ev[6 + NC * i + j], ctx->s_down));
+                    }
+                }
             }
-            CK(cudaStreamEndCapture(ctx->s, &ctx->graph));
-            ctx->graph_launches = ctx->launches - before;
-            ctx->launches = before;
-            ctx->restore();
-            ctx->t = t0;
-            ctx->n = n0;
-            CK(cudaGraphInstantiate(&ctx->gexec, ctx->graph, 0));
+        } catch (...) {  // no copy to or from the caller's buffers outlives the call
+            cudaStreamSynchronize(ctx->s_up);
+            cudaStreamSynchronize(ctx->s_down);
+            throw;
         }
-        for (int q = 0; q < nsteps; ++q) {
-            CK(cudaGraphLaunch(ctx->gexec, ctx->s));
-            ctx->launches += ctx->graph_launches;
-            ctx->t += ctx->p.dt;
-            ctx->n += 1;
-        }
+        CK(cudaStreamSynchronize(ctx->s_down));
+        CK(cudaStreamSynchronize(ctx->s));
+        for (int i = 0; i < 3; ++i) ln[i] = ctx->io_ln[i];
     });
 }
 

@@ -131,6 +131,16 @@ struct mlegs_ctx {
         k_fold_gemm(g, Wt, wt_rows, in, out, mode, scale, accumulate, pad, st);
     }
     double2* staging = nullptr;
+    // mlegs_run_host, set up on its first call: copy streams each way, staging
+    // per state field and direction, page-locked LN slots, and the events per
+    // field i "uploaded" [i], "converted for download" [3 + i] and, per chunk j
+    // of its download, "downloaded" [6 + IO_CHUNKS i + j]
+    static constexpr int IO_CHUNKS = 4;
+    cudaStream_t s_up = nullptr, s_down = nullptr;
+    double2* io_in[3] = {};
+    double2* io_out[3] = {};
+    double* io_ln = nullptr;
+    cudaEvent_t io_ev[6 + 3 * IO_CHUNKS] = {};
     int* dflag = nullptr;
     std::vector<std::unique_ptr<mlegs_field>> owned;  // every field, incl. user ones
     std::vector<Field*> pool;                         // free temporaries (stack)

@@ -423,6 +423,9 @@ int mlegs_field_device_copy(mlegs_ctx* ctx, mlegs_field* f, int to_field, int sp
 #define MLEGS_K_PROJECT_FFF 14  /* PROJECT of FFF velocity fields via composite matrices, 3 FFF -> 2 FFF */
 #define MLEGS_K_PHYS_NONLIN 15  /* MLEGS_K_PHYS as CALC_BOUSSI_NONLIN runs it: 9 inputs, no linear terms */
 #define MLEGS_K_ROUNDTRIP  16   /* TOFP then TOFF of one field, FFF -> PPP -> FFF (context's precision) */
+#define MLEGS_K_DMMA_PEAK  17   /* the FP64 tensor path's ceiling: register-only m8n8k4 MMAs, 4 CTAs x 8
+                                   warps per SM; bytes_per_launch returns its FLOPs instead (MLEGS_ERR_ARG
+                                   if a field buffer cannot hold one double per thread) */
 int mlegs_kernel_time(mlegs_ctx* ctx, int kernel, int reps, double* ms_per_launch, double* bytes_per_launch);
 
 /* Number of this library's kernel launches issued since the counter was reset. */
